@@ -1,0 +1,272 @@
+"""Python mirror of the libssa C API, backed by the B200 build.
+
+The functions below have the names, arguments and behaviour of the C entry
+points in ``include/libssa.h`` (the reference's ``src/libssa.h``), bound with
+ctypes to ``_lib/libssa.so``.  The database is served by ``_lib/libsdb_b200.so``,
+the plugin implementing ``libssa_extern_db.h``; ``load_db_memory`` feeds it
+sequences straight from Python.
+
+The shared libraries must have been built (``python -m libssa_b200.build``);
+importing this package fails loudly otherwise.  All searching runs on the GPU.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_DIR = os.path.join(HERE, "_lib")
+LIB_PATH = os.path.join(LIB_DIR, "libssa.so")
+PLUGIN_PATH = os.path.join(LIB_DIR, "libsdb_b200.so")
+
+# constants of libssa.h (reference: src/libssa.h:29-72)
+NUCLEOTIDE, AMINOACID, TRANS_QUERY, TRANS_DB, TRANS_BOTH = 0, 1, 2, 3, 4
+FORWARD_STRAND, COMPLEMENTARY_STRAND, BOTH_STRANDS = 1, 2, 3
+BIT_WIDTH_8, BIT_WIDTH_16, BIT_WIDTH_64 = 8, 16, 64
+OUTPUT_SILENT, OUTPUT_ERROR, OUTPUT_WARNING, OUTPUT_INFO = 0, 1, 2, 3
+COMPUTE_SCORE, COMPUTE_ALIGNMENT = 0, 1
+READ_FROM_FILE, READ_FROM_STRING, MATRIX_BUILDIN = 0, 1, 2
+COMPUTE_ON_SSE2, COMPUTE_ON_SSE41, COMPUTE_ON_AVX2 = 0, 1, 2
+SSA_SMITH_WATERMAN, SSA_NEEDLEMAN_WUNSCH = 0, 1
+
+EXPORTED = [
+    "set_output_mode", "set_simd_compute_mode", "set_chunk_size", "set_thread_count", "init_score_matrix",
+    "init_constant_scores", "init_gap_penalties", "init_symbol_translation", "init_db", "init_sequence_fasta",
+    "free_sequence", "sw_align", "nw_align", "free_alignment", "ssa_exit", "ssa_align_batch", "ssa_get_stats",
+    "ssa_query_length", "ssa_db_refresh",
+]
+
+
+class DbSeq(ctypes.Structure):
+    _fields_ = [("seq", ctypes.c_void_p), ("len", ctypes.c_size_t), ("ID", ctypes.c_size_t),
+                ("strand", ctypes.c_int), ("frame", ctypes.c_int)]
+
+
+class QSeq(ctypes.Structure):
+    _fields_ = [("seq", ctypes.c_void_p), ("len", ctypes.c_size_t), ("strand", ctypes.c_int),
+                ("frame", ctypes.c_int)]
+
+
+class Alignment(ctypes.Structure):
+    _fields_ = [("db_seq", DbSeq), ("query", QSeq), ("alignment", ctypes.c_char_p),
+                ("alignment_len", ctypes.c_size_t), ("score", ctypes.c_long), ("align_q_start", ctypes.c_size_t),
+                ("align_q_end", ctypes.c_size_t), ("align_d_start", ctypes.c_size_t),
+                ("align_d_end", ctypes.c_size_t)]
+
+
+class AlignmentList(ctypes.Structure):
+    _fields_ = [("alignments", ctypes.POINTER(ctypes.POINTER(Alignment))), ("len", ctypes.c_size_t)]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("overflow_8_to_16", ctypes.c_uint64), ("overflow_16_to_64", ctypes.c_uint64),
+                ("cells", ctypes.c_uint64), ("gpu_seconds", ctypes.c_double),
+                ("kernel_launches_total", ctypes.c_uint64)]
+
+
+P_LIST = ctypes.POINTER(AlignmentList)
+
+_lib = None
+_plugin = None
+
+
+def libraries_built() -> bool:
+    return os.path.exists(LIB_PATH) and os.path.exists(PLUGIN_PATH)
+
+
+def load():
+    """Loads the plugin and the library (RTLD_GLOBAL so libssa.so resolves
+    the ssa_db_* imports against the plugin)."""
+    global _lib, _plugin
+    if _lib is not None:
+        return _lib
+    if not libraries_built():
+        raise RuntimeError("libssa_b200 is not built: run `python -m libssa_b200.build` (the GPU library has "
+                           "no CPU fallback)")
+    _plugin = ctypes.CDLL(PLUGIN_PATH, mode=ctypes.RTLD_GLOBAL)
+    lib = ctypes.CDLL(LIB_PATH, mode=ctypes.RTLD_GLOBAL)
+    lib.set_output_mode.argtypes = [ctypes.c_int]
+    lib.set_simd_compute_mode.argtypes = [ctypes.c_int]
+    lib.set_chunk_size.argtypes = [ctypes.c_size_t]
+    lib.set_thread_count.argtypes = [ctypes.c_size_t]
+    lib.init_score_matrix.argtypes = [ctypes.c_int, ctypes.c_char_p]
+    lib.init_constant_scores.argtypes = [ctypes.c_int8, ctypes.c_int8]
+    lib.init_gap_penalties.argtypes = [ctypes.c_int8, ctypes.c_int8]
+    lib.init_symbol_translation.argtypes = [ctypes.c_int] * 4
+    lib.init_db.argtypes = [ctypes.c_char_p]
+    lib.init_sequence_fasta.argtypes = [ctypes.c_int, ctypes.c_char_p]
+    lib.init_sequence_fasta.restype = ctypes.c_void_p
+    lib.free_sequence.argtypes = [ctypes.c_void_p]
+    for fn in (lib.sw_align, lib.nw_align):
+        fn.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int, ctypes.c_int]
+        fn.restype = P_LIST
+    lib.free_alignment.argtypes = [P_LIST]
+    lib.ssa_exit.argtypes = []
+    lib.ssa_align_batch.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p), ctypes.c_size_t,
+                                    ctypes.c_size_t, ctypes.c_int, ctypes.c_int, ctypes.POINTER(P_LIST)]
+    lib.ssa_align_batch.restype = ctypes.c_int
+    lib.ssa_get_stats.argtypes = [ctypes.POINTER(Stats)]
+    lib.ssa_db_refresh.argtypes = []
+    lib.ssa_query_length.argtypes = [ctypes.c_void_p]
+    lib.ssa_query_length.restype = ctypes.c_size_t
+    _plugin.ssa_db_b200_load_memory.argtypes = [ctypes.c_size_t, ctypes.c_char_p, ctypes.POINTER(ctypes.c_uint64)]
+    _plugin.ssa_db_b200_load_memory.restype = ctypes.c_int
+    _plugin.ssa_db_get_sequence_count.restype = ctypes.c_size_t
+    _lib = lib
+    return lib
+
+
+# --------------------------------------------------------------------------
+# libssa.h mirror
+# --------------------------------------------------------------------------
+def set_output_mode(mode: int) -> None:
+    load().set_output_mode(mode)
+
+
+def set_simd_compute_mode(mode: int) -> None:
+    load().set_simd_compute_mode(mode)
+
+
+def set_chunk_size(size: int) -> None:
+    load().set_chunk_size(size)
+
+
+def set_thread_count(count: int) -> None:
+    load().set_thread_count(count)
+
+
+def init_score_matrix(mode: int, matrix: str) -> None:
+    load().init_score_matrix(mode, matrix.encode())
+
+
+def init_constant_scores(match: int, mismatch: int) -> None:
+    load().init_constant_scores(match, mismatch)
+
+
+def init_gap_penalties(gap_open: int, gap_extend: int) -> None:
+    load().init_gap_penalties(gap_open, gap_extend)
+
+
+def init_symbol_translation(symtype: int, strands: int, db_gencode: int, q_gencode: int) -> None:
+    load().init_symbol_translation(symtype, strands, db_gencode, q_gencode)
+
+
+def init_db(path: str) -> None:
+    load().init_db(path.encode())
+
+
+def init_sequence_fasta(mode: int, text: str):
+    """Returns an opaque query handle (int) or None when the reference would
+    return NULL."""
+    q = load().init_sequence_fasta(mode, text.encode("latin-1"))
+    return q or None
+
+
+def free_sequence(q) -> None:
+    if q:
+        load().free_sequence(q)
+
+
+@dataclass
+class Hit:
+    id: int
+    score: int
+    cigar: str | None
+    q_start: int
+    q_end: int
+    d_start: int
+    d_end: int
+    dlen: int
+    qlen: int
+    db_seq: bytes = b""
+
+    def key(self):
+        return (self.id, self.score, self.cigar, self.q_start, self.q_end, self.d_start, self.d_end)
+
+
+def _read_list(lp) -> list[Hit]:
+    out = []
+    lst = lp.contents
+    for i in range(lst.len):
+        a = lst.alignments[i].contents
+        cig = a.alignment.decode() if a.alignment is not None else None
+        seq = ctypes.string_at(a.db_seq.seq, a.db_seq.len) if a.db_seq.seq else b""
+        out.append(Hit(int(a.db_seq.ID), int(a.score), cig, int(a.align_q_start), int(a.align_q_end),
+                       int(a.align_d_start), int(a.align_d_end), int(a.db_seq.len), int(a.query.len), seq))
+    return out
+
+
+def sw_align(q, hitcount: int, bit_width: int, align_type: int) -> list[Hit]:
+    lib = load()
+    lp = lib.sw_align(q, hitcount, bit_width, align_type)
+    try:
+        return _read_list(lp)
+    finally:
+        lib.free_alignment(lp)
+
+
+def nw_align(q, hitcount: int, bit_width: int, align_type: int) -> list[Hit]:
+    lib = load()
+    lp = lib.nw_align(q, hitcount, bit_width, align_type)
+    try:
+        return _read_list(lp)
+    finally:
+        lib.free_alignment(lp)
+
+
+def ssa_exit() -> None:
+    load().ssa_exit()
+
+
+# --------------------------------------------------------------------------
+# libssa_b200.h extensions
+# --------------------------------------------------------------------------
+def align_batch(algorithm: int, queries: list, hitcount: int, bit_width: int, align_type: int) -> list[list[Hit]]:
+    """Batched search of several query handles; one hit list per query."""
+    lib = load()
+    n = len(queries)
+    qarr = (ctypes.c_void_p * max(1, n))(*queries)
+    res = (P_LIST * max(1, n))()
+    lib.ssa_align_batch(algorithm, qarr, n, hitcount, bit_width, align_type, res)
+    out = []
+    for i in range(n):
+        out.append(_read_list(res[i]))
+        lib.free_alignment(res[i])
+    return out
+
+
+def stats() -> Stats:
+    s = Stats()
+    load().ssa_get_stats(ctypes.byref(s))
+    return s
+
+
+def query_length(q) -> int:
+    return int(load().ssa_query_length(q))
+
+
+def load_db_memory(seqs: list[bytes] | None = None, flat: np.ndarray | None = None,
+                   offsets: np.ndarray | None = None) -> None:
+    """Installs a database in the plugin from memory (ASCII residues)."""
+    load()
+    if seqs is not None:
+        offsets = np.zeros(len(seqs) + 1, dtype=np.uint64)
+        offsets[1:] = np.cumsum([len(s) for s in seqs])
+        flat_bytes = b"".join(seqs)
+    else:
+        flat_bytes = np.ascontiguousarray(flat, dtype=np.uint8).tobytes()
+    offsets = np.ascontiguousarray(offsets, dtype=np.uint64)
+    rc = _plugin.ssa_db_b200_load_memory(len(offsets) - 1, flat_bytes,
+                                         offsets.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)))
+    if rc != 0:
+        raise MemoryError("database plugin could not store the sequences")
+    # the library re-packs on the next search
+    load().ssa_db_refresh()
+
+
+def db_count() -> int:
+    load()
+    return int(_plugin.ssa_db_get_sequence_count())

@@ -1,0 +1,575 @@
+// api.cpp -- the libssa.h entry points of the B200 build.
+//
+// The public functions keep the reference's names, argument meaning, global
+// state, messages and error behaviour (reference: src/libssa.c:38-271,
+// src/query.c, src/matrices.c, src/util/util.c:36-98).  Configuration errors
+// print to stderr and exit(1) like the reference's fatal(); a bad query file
+// prints an error and returns NULL.  The search itself is delegated to the
+// GPU engine (engine.cu); there is no CPU search path.
+#include "ssa_internal.h"
+#include "libssa_b200.h"
+#include "libssa_extern_db.h"
+
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <strings.h>
+
+namespace ssa {
+
+Config & config() {
+    static Config c;
+    return c;
+}
+
+// ---- messages (reference: src/util/util.c:36-89) -------------------------------
+void fatal( const char * fmt, ... ) {
+    if( fmt ) {
+        va_list ap;
+        va_start( ap, fmt );
+        vfprintf( stderr, fmt, ap );
+        fprintf( stderr, "\n" );
+        va_end( ap );
+    }
+    exit( 1 );
+}
+
+static void emit( int level, const char * prefix, bool newline, const char * fmt, va_list ap ) {
+    if( level > config().output_mode )
+        return;
+    printf( "%s", prefix );
+    vprintf( fmt, ap );
+    if( newline )
+        printf( "\n" );
+}
+
+void print_info( const char * fmt, ... ) {
+    va_list ap;
+    va_start( ap, fmt );
+    emit( OUTPUT_INFO, "libssa INFO: ", false, fmt, ap );
+    va_end( ap );
+}
+
+void print_warning( const char * fmt, ... ) {
+    va_list ap;
+    va_start( ap, fmt );
+    emit( OUTPUT_WARNING, "libssa WARNING: ", true, fmt, ap );
+    va_end( ap );
+}
+
+void print_error( const char * fmt, ... ) {
+    va_list ap;
+    va_start( ap, fmt );
+    emit( OUTPUT_ERROR, "libssa ERROR: ", true, fmt, ap );
+    va_end( ap );
+}
+
+// ---- residue maps (reference: src/util/util_sequence.c:38-88) ------------------
+// Code k of the amino-acid alphabet is AA_SYMBOLS[k] (code 0, the pad, has no
+// symbol); nucleotides use the IUPAC nt16 bit codes with U read as T.
+static const char AA_SYMBOLS[] = "-ABCDEFGHIKLMNPQRSTVWXYZU*OJ";
+static const char NT_SYMBOLS[] = "-ACMGRSVTWYHKDBN";
+
+struct Maps {
+    signed char aa[256];
+    signed char nt[256];
+    Maps() {
+        memset( aa, -1, sizeof(aa) );
+        memset( nt, -1, sizeof(nt) );
+        for( int k = 1; k < 28; k++ ) {
+            unsigned char c = (unsigned char) AA_SYMBOLS[k];
+            aa[c] = (signed char) k;
+            if( c >= 'A' && c <= 'Z' )
+                aa[c - 'A' + 'a'] = (signed char) k;
+        }
+        for( int k = 0; k < 16; k++ ) {
+            unsigned char c = (unsigned char) NT_SYMBOLS[k];
+            nt[c] = (signed char) k;
+            if( c >= 'A' && c <= 'Z' )
+                nt[c - 'A' + 'a'] = (signed char) k;
+        }
+        nt[(unsigned char) 'U'] = nt[(unsigned char) 'T'];
+        nt[(unsigned char) 'u'] = nt[(unsigned char) 'T'];
+    }
+};
+
+static const Maps & maps() {
+    static Maps m;
+    return m;
+}
+
+int map_aa( unsigned char c ) {
+    return maps().aa[c];
+}
+
+int map_nt16( unsigned char c ) {
+    return maps().nt[c];
+}
+
+// ---- matrices (reference: src/matrices.c:335-568) ------------------------------
+struct BuiltinMatrix {
+    const char * name;
+    const char * symbols;
+    int values[25 * 25];
+};
+
+static const BuiltinMatrix BUILTINS[] = {
+#include "builtin_matrices.inc"
+};
+
+static void matrix_clear( int64_t * out ) {
+    for( int k = 0; k < 1024; k++ )
+        out[k] = -1;   // unset cells score -1 (reference: src/matrices.c:344)
+}
+
+bool matrix_builtin( const char * name, int64_t * out ) {
+    for( const BuiltinMatrix & m : BUILTINS ) {
+        if( strcasecmp( name, m.name ) != 0 )
+            continue;
+        matrix_clear( out );
+        const int n = (int) strlen( m.symbols );
+        for( int a = 0; a < n; a++ ) {
+            int ca = map_aa( (unsigned char) m.symbols[a] );
+            for( int b = 0; b < n; b++ ) {
+                int cb = map_aa( (unsigned char) m.symbols[b] );
+                if( ca >= 0 && cb >= 0 )
+                    out[(ca << 5) + cb] = m.values[a * n + b];
+            }
+        }
+        return true;
+    }
+    return false;
+}
+
+// Matrix text: '#' comments and blank lines are skipped, a line starting
+// with blank space lists the column symbols, every other line is a row symbol
+// followed by one score per column symbol (reference: src/matrices.c:388-437).
+void matrix_from_string( const char * text, int64_t * out ) {
+    matrix_clear( out );
+    std::vector<int> order;
+    const char * s = text;
+    while( *s ) {
+        const char * e = strchr( s, '\n' );
+        const size_t n = e ? (size_t) (e - s) : strlen( s );
+        std::string line( s, n );
+        s = e ? e + 1 : s + n;
+        if( line.empty() || line[0] == '#' )
+            continue;
+        if( line[0] == ' ' || line[0] == '\t' ) {
+            for( size_t k = 1; k < line.size(); k++ )
+                if( !strchr( " \t\n\r", line[k] ) )
+                    order.push_back( map_aa( (unsigned char) line[k] ) );
+            continue;
+        }
+        const int a = map_aa( (unsigned char) line[0] );
+        const char * p = line.c_str() + 1;
+        for( size_t i = 0; i < order.size(); i++ ) {
+            char * end;
+            long v = strtol( p, &end, 10 );
+            if( end == p )
+                fatal( "Problem parsing score matrix file." );
+            p = end;
+            const int b = order[i];
+            if( a >= 0 && b >= 0 )
+                out[(a << 5) + b] = v;
+        }
+    }
+}
+
+void matrix_constant( int match, int mismatch, int64_t * out ) {
+    // reference: src/matrices.c:447-460 -- code 0 keeps -1
+    matrix_clear( out );
+    for( int a = 1; a < 32; a++ )
+        for( int b = 1; b < 32; b++ )
+            out[(a << 5) + b] = (int8_t) (a == b ? match : mismatch);
+}
+
+}  // namespace ssa
+
+using namespace ssa;
+
+// ---- the query object ------------------------------------------------------------
+struct _query {
+    char * seq;          // mapped codes, NUL-terminated
+    size_t len;
+    char * header;
+    size_t headerlen;
+    int symtype;         // symbol type the codes were mapped with
+};
+
+static bool nucleotide_map( int symtype ) {
+    return !(symtype == AMINOACID || symtype == TRANS_DB);
+}
+
+// Maps ASCII to codes, removing unknown symbols with a warning; whitespace is
+// dropped silently (reference: src/query.c:102-130).
+static p_query make_query( const char * text, size_t n, char * header, size_t headerlen ) {
+    const bool nt = nucleotide_map( config().symtype );
+    p_query q = (p_query) calloc( 1, sizeof(struct _query) );
+    q->seq = (char *) malloc( n + 1 );
+    std::string unknown;
+    size_t k = 0;
+    for( size_t i = 0; i < n; i++ ) {
+        const unsigned char c = (unsigned char) text[i];
+        const int m = nt ? map_nt16( c ) : map_aa( c );
+        if( m >= 0 )
+            q->seq[k++] = (char) m;
+        else if( c != '\n' && c != ' ' && c != '\t' )
+            unknown += (char) c;
+    }
+    if( !unknown.empty() )
+        print_warning( "%zu unknown symbols found and removed: '%s'", unknown.size(), unknown.c_str() );
+    q->seq[k] = 0;
+    q->len = k;
+    q->header = header;
+    q->headerlen = headerlen;
+    q->symtype = config().symtype;
+    return q;
+}
+
+static p_query query_from_file( const char * filename ) {
+    // reference: src/query.c:187-264
+    if( strcmp( filename, "-" ) == 0 ) {
+        print_error( "Query not specified" );
+        return nullptr;
+    }
+    FILE * fp = fopen( filename, "r" );
+    if( !fp ) {
+        print_error( "Cannot open query file: %s", filename );
+        return nullptr;
+    }
+    char line[2048];
+    line[0] = 0;
+    if( !fgets( line, sizeof(line), fp ) ) {
+        print_error( "Could not initialise from query sequence" );
+        fclose( fp );
+        return nullptr;
+    }
+    size_t len = strlen( line );
+    if( len && line[len - 1] == '\n' ) {
+        line[len - 1] = 0;
+        len--;
+    }
+    char * header = nullptr;
+    size_t headerlen = 0;
+    if( line[0] == '>' ) {
+        header = (char *) malloc( len + 1 );
+        memcpy( header, line + 1, len );
+        header[len] = 0;
+        headerlen = len ? len - 1 : 0;
+        line[0] = 0;
+        if( !fgets( line, sizeof(line), fp ) ) {
+            print_error( "Could not read first line from query sequence" );
+            free( header );
+            fclose( fp );
+            return nullptr;
+        }
+    }
+    std::string seq;
+    while( line[0] && line[0] != '>' ) {
+        seq += line;
+        if( !fgets( line, sizeof(line), fp ) )
+            break;
+    }
+    fclose( fp );
+    return make_query( seq.data(), seq.size(), header, headerlen );
+}
+
+// ---- alignment lists -----------------------------------------------------------
+static p_alignment_list make_list( const std::vector<Hit> & hits, p_query q, bool with_cigar ) {
+    p_alignment_list l = (p_alignment_list) malloc( sizeof(alignment_list_t) );
+    l->len = hits.size();
+    l->alignments = (p_alignment *) malloc( std::max<size_t>( 1, hits.size() ) * sizeof(p_alignment) );
+    const bool nt = config().symtype == NUCLEOTIDE;
+    for( size_t k = 0; k < hits.size(); k++ ) {
+        const Hit & h = hits[k];
+        p_alignment a = (p_alignment) calloc( 1, sizeof(alignment_t) );
+        // the hit's database record is fetched and mapped again, as the
+        // reference does per hit (reference: src/algo/aligner.c:62-93)
+        p_seqinfo info = ssa_db_get_sequence( h.id );
+        if( !info )
+            fatal( "Could not get sequence from DB: %u", h.id );
+        a->db_seq.seq = (char *) malloc( info->seqlen + 1 );
+        for( size_t i = 0; i < info->seqlen; i++ ) {
+            int m = nt ? map_nt16( (unsigned char) info->seq[i] ) : map_aa( (unsigned char) info->seq[i] );
+            a->db_seq.seq[i] = (char) (m < 0 ? 0 : m);
+        }
+        a->db_seq.seq[info->seqlen] = 0;
+        a->db_seq.len = info->seqlen;
+        a->db_seq.ID = info->ID;
+        a->db_seq.strand = 0;
+        a->db_seq.frame = 0;
+        a->query.seq = q->seq;
+        a->query.len = q->len;
+        a->query.strand = 0;
+        a->query.frame = 0;
+        a->score = (long) h.score;
+        if( with_cigar && h.has_cigar ) {
+            a->alignment = (char *) malloc( h.cigar.size() + 1 );
+            memcpy( a->alignment, h.cigar.c_str(), h.cigar.size() + 1 );
+            a->alignment_len = h.cigar.size();
+            a->align_q_start = h.q_start;
+            a->align_q_end = h.q_end;
+            a->align_d_start = h.d_start;
+            a->align_d_end = h.d_end;
+        }
+        l->alignments[k] = a;
+    }
+    return l;
+}
+
+static SearchStats g_last_stats;
+
+// Checks shared by sw_align/nw_align (reference: src/libssa.c:196-219).
+static void test_configuration( p_query query ) {
+    const Config & c = config();
+    if( !c.gap_open && !c.gap_extend )
+        print_warning( "Gap opening and gap extension cost set to zero. Possible error." );
+    if( !c.matrix_set )
+        fatal( "Scoring not initialized." );
+    if( !query )
+        fatal( "Query not initialized." );
+    if( ssa_db_get_sequence_count() == 0 )
+        print_warning( "Database contains zero sequences. Possible error." );
+    if( !c.constant_scoring && c.symtype == NUCLEOTIDE )
+        fatal( "Nucleotide sequences can only be aligned using constant scores." );
+}
+
+static SearchRequest make_request( int algo, size_t hitcount, int bit_width, int align_type ) {
+    const Config & c = config();
+    if( bit_width != BIT_WIDTH_8 && bit_width != BIT_WIDTH_16 && bit_width != BIT_WIDTH_64 )
+        fatal( "\nunknown bit width provided: %d\n\n", bit_width );
+    if( c.symtype != AMINOACID && c.symtype != NUCLEOTIDE )
+        fatal( "Translated searches (symbol type %d) are not supported by the B200 build.", c.symtype );
+    if( c.symtype == NUCLEOTIDE && (c.strands & 2) )
+        fatal( "Searches of the complementary strand are not supported by the B200 build." );
+    SearchRequest r;
+    r.algo = algo;
+    r.bit_width = bit_width;
+    r.align_type = align_type;
+    r.hitcount = hitcount;
+    r.chunk_size = c.chunk_size;
+    // lane counts of the CPU schedule whose hit order is reproduced
+    // (reference: src/cpu_config.c:29-33, src/algo/8/search_8.c:41-56)
+    if( c.simd_mode >= COMPUTE_ON_AVX2 ) {
+        r.lanes8 = 32;
+        r.lanes16 = 16;
+    }
+    else if( c.simd_mode == COMPUTE_ON_SSE41 ) {
+        r.lanes8 = 16;
+        r.lanes16 = 8;
+    }
+    else {
+        if( bit_width == BIT_WIDTH_8 )
+            fatal( "\nAVX2 and SSE4.1 not enabled. No 8 bit search possible\n\n" );
+        r.lanes8 = 16;
+        r.lanes16 = 8;
+    }
+    r.gap_open = c.gap_open;
+    r.gap_extend = c.gap_extend;
+    r.matrix = c.matrix;
+    return r;
+}
+
+static std::vector<p_alignment_list> run_search( int algo, p_query * queries, size_t n, size_t hitcount,
+        int bit_width, int align_type ) {
+    for( size_t i = 0; i < n; i++ )
+        test_configuration( queries[i] );
+    SearchRequest req = make_request( algo, hitcount, bit_width, align_type );
+    std::vector<QueryCodes> qc( n );
+    for( size_t i = 0; i < n; i++ ) {
+        if( queries[i]->symtype != config().symtype )
+            fatal( "Query was read with a different symbol type than the current one." );
+        if( queries[i]->len == 0 )
+            fatal( "Query sequence is empty." );
+        qc[i] = QueryCodes{ (const uint8_t *) queries[i]->seq, (uint32_t) queries[i]->len };
+    }
+    std::vector<std::vector<Hit>> hits;
+    SearchStats st;
+    engine_search( req, qc, hits, st );
+    if( st.overflow8 || st.overflow16 )
+        print_info( "Overflow occurred: %ld sequences were re-aligned with 16 bit, and %ld sequences with 64 bit\n",
+                (long) st.overflow8, (long) st.overflow16 );
+    g_last_stats = st;
+    std::vector<p_alignment_list> out( n );
+    for( size_t i = 0; i < n; i++ )
+        out[i] = make_list( hits[i], queries[i], align_type == COMPUTE_ALIGNMENT );
+    return out;
+}
+
+// ---- libssa.h ---------------------------------------------------------------------
+// The C entry points are the library's only exported symbols.
+#pragma GCC visibility push( default )
+extern "C" {
+
+void set_output_mode( int mode ) {
+    config().output_mode = mode;
+}
+
+void set_simd_compute_mode( int mode ) {
+    config().simd_mode = mode;
+}
+
+void set_chunk_size( size_t size ) {
+    if( size == 0 ) {
+        print_error( "Only non zero chunk sizes are allowed. Using the default size of 1000 sequences.", size );
+        size = 1000;
+    }
+    config().chunk_size = size;
+}
+
+void set_thread_count( size_t count ) {
+    config().thread_count = count;
+}
+
+void init_score_matrix( int mode, const char * matrix ) {
+    Config & c = config();
+    if( mode == READ_FROM_FILE ) {
+        FILE * fp = fopen( matrix, "r" );
+        if( !fp )
+            fatal( "Cannot open score matrix file." );
+        std::string text;
+        char buf[4096];
+        size_t n;
+        while( (n = fread( buf, 1, sizeof(buf), fp )) > 0 )
+            text.append( buf, n );
+        fclose( fp );
+        matrix_from_string( text.c_str(), c.matrix );
+    }
+    else if( mode == READ_FROM_STRING ) {
+        if( !matrix )
+            fatal( "Cannot read score matrix string." );
+        matrix_from_string( matrix, c.matrix );
+    }
+    else if( mode == MATRIX_BUILDIN ) {
+        if( !matrix_builtin( matrix, c.matrix ) )
+            fatal( "Unknown matrix: %s", matrix );
+    }
+    else {
+        fatal( "Unknown mode for reading score matrices: %d", mode );
+    }
+    c.matrix_set = true;
+    c.constant_scoring = false;
+}
+
+void init_constant_scores( const int8_t p, const int8_t m ) {
+    Config & c = config();
+    matrix_constant( p, m, c.matrix );
+    c.matrix_set = true;
+    c.constant_scoring = true;
+}
+
+void init_gap_penalties( const int8_t gapO, const int8_t gapE ) {
+    config().gap_open = gapO;
+    config().gap_extend = gapE;
+}
+
+void init_symbol_translation( int type, int strands, int db_gencode, int q_gencode ) {
+    // reference: src/libssa.c:139-157 (the range checks read the previous
+    // symbol type, as there)
+    static const bool known[24] = { false, true, true, true, true, true, true, false, false, true, true, true, true,
+        true, true, true, true, false, false, false, false, true, true, true };
+    Config & c = config();
+    if( q_gencode < 1 || q_gencode > 23 || !known[q_gencode] )
+        fatal( "Illegal query genetic code specified." );
+    if( db_gencode < 1 || db_gencode > 23 || !known[db_gencode] )
+        fatal( "Illegal database genetic code specified." );
+    if( c.symtype < 0 || c.symtype > 4 )
+        fatal( "Illegal symbol type specified." );
+    if( c.symtype < 0 || c.symtype > 2 )
+        fatal( "Illegal strands specified." );
+    c.symtype = type;
+    c.strands = strands;
+    c.db_gencode = db_gencode;
+    c.q_gencode = q_gencode;
+}
+
+void init_db( const char * db_file ) {
+    ssa_db_close();
+    ssa_db_init( db_file );
+    engine_invalidate_database();
+    print_info( "DB read %lu sequences\n", (unsigned long) ssa_db_get_sequence_count() );
+}
+
+p_query init_sequence_fasta( int mode, const char * fasta ) {
+    if( mode == READ_FROM_FILE )
+        return query_from_file( fasta );
+    if( mode == READ_FROM_STRING )
+        return make_query( fasta, strlen( fasta ), nullptr, 0 );
+    fatal( "Unknown mode for reading query sequences: %d", mode );
+}
+
+void free_sequence( p_query p ) {
+    if( !p )
+        return;
+    free( p->seq );
+    free( p->header );
+    free( p );
+}
+
+p_alignment_list sw_align( p_query p, size_t hitcount, int bit_width, int align_type ) {
+    return run_search( 0, &p, 1, hitcount, bit_width, align_type )[0];
+}
+
+p_alignment_list nw_align( p_query p, size_t hitcount, int bit_width, int align_type ) {
+    return run_search( 1, &p, 1, hitcount, bit_width, align_type )[0];
+}
+
+void free_alignment( p_alignment_list alist ) {
+    if( !alist )
+        return;
+    for( size_t i = 0; i < alist->len; i++ ) {
+        p_alignment a = alist->alignments[i];
+        if( !a )
+            continue;
+        free( a->db_seq.seq );
+        free( a->alignment );
+        free( a );
+    }
+    free( alist->alignments );
+    free( alist );
+}
+
+void ssa_exit( void ) {
+    config().matrix_set = false;
+    ssa_db_close();
+    engine_shutdown();
+}
+
+// ---- libssa_b200.h extensions -------------------------------------------------------
+int ssa_align_batch( int algorithm, p_query * queries, size_t n_queries, size_t hitcount, int bit_width,
+        int align_type, p_alignment_list * results ) {
+    if( algorithm != SSA_SMITH_WATERMAN && algorithm != SSA_NEEDLEMAN_WUNSCH )
+        fatal( "\nUnknown search type: %d\n\n", algorithm );
+    if( n_queries == 0 )
+        return 0;
+    if( !queries || !results )
+        fatal( "Query not initialized." );
+    std::vector<p_alignment_list> l =
+            run_search( algorithm == SSA_SMITH_WATERMAN ? 0 : 1, queries, n_queries, hitcount, bit_width, align_type );
+    for( size_t i = 0; i < n_queries; i++ )
+        results[i] = l[i];
+    return 0;
+}
+
+void ssa_get_stats( ssa_stats_t * out ) {
+    if( !out )
+        return;
+    out->overflow_8_to_16 = g_last_stats.overflow8;
+    out->overflow_16_to_64 = g_last_stats.overflow16;
+    out->cells = g_last_stats.cells;
+    out->gpu_seconds = g_last_stats.seconds_gpu;
+    out->kernel_launches_total = engine_kernel_launches();
+}
+
+void ssa_db_refresh( void ) {
+    engine_invalidate_database();
+}
+
+size_t ssa_query_length( p_query p ) {
+    return p ? p->len : 0;
+}
+
+}  // extern "C"
+#pragma GCC visibility pop

@@ -1,0 +1,157 @@
+// device_common.cuh -- data structures shared by the host engine and the
+// sm_100a kernels of the libssa B200 build.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace ssa {
+
+// One (query, database sequence) unit of work of a saturating pass.  nb is
+// the number of 4-column blocks the sequence occupied in the previous pass
+// (its lane-schedule length there); 0 for the entry pass.
+struct PairTask {
+    uint32_t qslot;
+    uint32_t id;
+    int32_t nb_prev;
+    int32_t pad_;
+};
+
+// Device view of the packed database.  Codes are stored per sequence in ID
+// order; each sequence is followed by zero codes up to a multiple of 16 bytes.
+struct DbView {
+    const uint8_t * codes;
+    const uint64_t * offsets;     // per ID
+    const uint32_t * lens;        // per ID (0 = empty record, never searched)
+    uint32_t n_ids;
+};
+
+// Per-query data of a batch.  prof32 holds, for every query slot, the
+// 32 x qpad table prof[code][row] of substitution scores at the pass width
+// (matrix[(code << 5) + query[row]] truncated to 8 or 16 bits, or exact).
+struct QueryView {
+    const int32_t * prof32;
+    const uint64_t * prof32_off;  // per slot, in elements
+    const uint32_t * qlen;        // per slot
+    const uint32_t * qpad;        // per slot, rows of the profile
+    uint32_t n_slots;
+};
+
+// Result sink of a pass.  score[slot * n_ids + id] receives the pass's score.
+// Sequences the pass does not report (overflow, or a score outside the
+// reportable range) are appended to next[] with the block count they used.
+struct PassSink {
+    int32_t * score;
+    uint64_t score_stride;        // = n_ids
+    PairTask * next;
+    unsigned int * next_count;
+    uint32_t next_cap;
+    unsigned int * error_flags;   // bit 0: next[] overflow
+};
+
+enum ErrorBits : unsigned int {
+    ERR_REQUEUE_OVERFLOW = 1u,
+    ERR_SCRATCH_OVERFLOW = 2u,
+};
+
+
+// Parameters of the saturating-lane emulation kernel (emul_kernel.cu).
+struct EmulParams {
+    DbView db;
+    QueryView qv;
+    const PairTask * tasks;     // explicit task list, or nullptr
+    const uint32_t * order;     // implicit tasks: non-empty IDs, longest first
+    const uint32_t * slot_list; // implicit tasks over these slots (nullptr: all slots)
+    uint32_t n_sub;             // entries of slot_list
+    uint64_t n_tasks;
+    unsigned long long * counter;
+    int gap_open, gap_extend;
+    PassSink sink;
+    int4 * scratch;             // per warp: scratch_cols entries
+    uint32_t scratch_cols;
+};
+
+// Traceback work item and result (traceback_kernels.cu).
+struct TbHit {
+    uint32_t qslot;
+    uint32_t id;
+    int32_t score;      // search score
+    int32_t algo;       // 0 SW, 1 NW
+};
+
+struct TbRegion {
+    int32_t a_begin, a_end;   // query rows
+    int32_t b_begin, b_end;   // database columns
+    int32_t fwd_score;
+    int32_t status;           // 0 ok, 1 no positive cell, 2 reverse pass found nothing
+};
+
+struct TbParams {
+    DbView db;
+    const uint8_t * qcodes;     // per slot
+    const uint64_t * qoff;
+    const uint32_t * qlen;
+    const int64_t * matrix;     // 32x32 [(row << 5) + col]
+    int gap_open, gap_extend;
+    const TbHit * hits;
+    uint32_t n_hits;
+    TbRegion * regions;
+    int4 * scratch;             // per warp
+    uint32_t scratch_cols;
+    int32_t * last_h;           // per hit: forward pass last-row H (query-indexed)
+    int32_t * last_e;           // per hit: forward pass last-row vertical gap
+    const uint64_t * last_off;  // per hit offset into last_h / last_e
+    uint16_t * dirs;            // per hit direction words
+    const uint64_t * dir_off;   // per hit offset into dirs
+    char * ops;                 // per hit reversed op string
+    const uint64_t * ops_off;
+    uint32_t * ops_len;
+    unsigned int * error_flags;
+};
+
+// Kernel launchers.
+cudaError_t launch_emul( int algo, int width, const EmulParams & p, int grid, cudaStream_t st );
+cudaError_t launch_build_profile32( const uint8_t * qcodes, const uint64_t * qoff, const uint32_t * qlen,
+        const uint32_t * qpad, const uint64_t * prof_off, const int64_t * matrix, int width, int32_t * prof,
+        uint32_t n_slots, cudaStream_t st );
+cudaError_t launch_traceback( const TbParams & p, bool any_sw, int grid, cudaStream_t st );
+
+
+// ---- fast Smith-Waterman entry pass (sw_fast_kernel.cu) --------------------
+// Residue code used after a sequence's last 4-column block in the pair layout;
+// its profile row is -128, so it never changes a Smith-Waterman maximum.
+constexpr uint32_t FAST_PAD_CODE = 31;
+
+// Work item: one query slot against a range of database pairs.
+struct FastItem {
+    uint32_t slot;
+    uint32_t pair_begin;
+    uint32_t pair_end;
+    uint32_t pad_;
+};
+
+struct FastParams {
+    const uint8_t * pair_res;     // per pair: cols x (residue A, residue B)
+    const uint64_t * pair_off;    // byte offset of each pair (16-aligned)
+    const uint32_t * pair_cols;   // columns of each pair, a multiple of 8
+    const uint2 * pair_ids;       // database IDs (B = 0xffffffff when absent)
+    const int8_t * prof8;         // per slot: 32 x rows int8 scores
+    const uint64_t * prof8_off;   // per slot, bytes
+    uint32_t rows;                // profile rows of this launch's queries (passes x G x R)
+    uint32_t passes;
+    const FastItem * items;
+    uint32_t n_items;
+    unsigned * item_counter;
+    int gap_oe;                   // (int8) (gapO + gapE)
+    int gap_e;
+    PassSink sink;
+    int4 * scratch;               // per group: scratch_cols entries
+    uint32_t scratch_cols;
+};
+
+cudaError_t launch_sw_fast( int R, int G, const FastParams & p, int grid, cudaStream_t st );
+cudaError_t launch_build_profile8( const uint8_t * qcodes, const uint64_t * qoff, const uint32_t * qlen,
+        const uint32_t * slots, uint32_t n, uint32_t rows, const int64_t * matrix, int8_t * prof,
+        const uint64_t * prof_off, cudaStream_t st );
+
+}  // namespace ssa

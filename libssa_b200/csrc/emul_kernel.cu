@@ -1,0 +1,385 @@
+// emul_kernel.cu -- exact emulation of one libssa SIMD lane per database
+// sequence, at 8-bit, 16-bit or 64-bit semantics, for Smith-Waterman and
+// Needleman-Wunsch.
+//
+// The CPU library scores each database sequence in one lane of a saturating
+// int8/int16 vector kernel (reference: src/algo/simd/search_simd_sw.c:172-441,
+// src/algo/simd/search_simd_nw.c:180-516) or with scalar int64 code
+// (src/algo/64/smith_waterman_63.c:32-98, needleman_wunsch_64.c:32-98).  A
+// lane's result does not depend on its neighbours, so here one warp computes
+// one (query, sequence) pair with the lane's exact arithmetic: every add
+// saturates at the pass width, the 8/16-bit boundary values are the
+// reference's truncated and saturated chains, and the pad columns of the
+// sequence's last 4-column block are scored with residue code 0.  The warp
+// also reproduces the lane's overflow test at every block end and reports the
+// number of blocks the lane spent on the sequence, which the host needs to
+// replay the CPU channel schedule.
+//
+// Layout: warp lane k owns query rows [pass*256 + 8k, pass*256 + 8k + 8); the
+// sequence streams through the warp as a wavefront (lane k works on column
+// step-k), passing H, F and the column aggregates of its bottom row to lane
+// k+1 by shuffle.  Queries longer than 256 rows take several passes; the last
+// lane's bottom row of a pass is kept in a per-warp scratch row in global
+// memory and read back by lane 0 in the next pass.
+#include "device_common.cuh"
+
+#include <climits>
+
+namespace ssa {
+
+constexpr int EMUL_R = 8;                  // query rows per lane
+constexpr int EMUL_ROWS = 32 * EMUL_R;     // rows per pass
+
+template <int W>
+struct Width {
+    static constexpr int64_t MIN = (W == 64) ? INT64_MIN / 4 : -(int64_t(1) << (W - 1));
+    static constexpr int64_t MAX = (W == 64) ? INT64_MAX / 4 : (int64_t(1) << (W - 1)) - 1;
+    __device__ __forceinline__ static int32_t sat( int32_t x ) {
+        if constexpr( W == 64 ) {
+            return x;
+        }
+        else {
+            return min( max( x, (int32_t) MIN ), (int32_t) MAX );
+        }
+    }
+    __device__ __forceinline__ static int64_t sat64( int64_t x ) {
+        if constexpr( W == 64 ) {
+            return x;
+        }
+        else {
+            return x < MIN ? MIN : (x > MAX ? MAX : x);
+        }
+    }
+    __device__ __forceinline__ static int32_t trunc( int64_t x ) {
+        if constexpr( W == 8 )
+            return (int8_t) x;
+        else if constexpr( W == 16 )
+            return (int16_t) x;
+        else
+            return (int32_t) x;
+    }
+};
+
+// NW boundary values of the lane (reference: search_simd_nw.c:233-240,
+// 445-453, 494-502; needleman_wunsch_64.c:39-52).
+template <int W>
+struct NwBounds {
+    int gO, gE, gOE;
+    __device__ NwBounds( int go, int ge ) : gO( go ), gE( ge ) {
+        gOE = Width<W>::trunc( (int64_t) go + ge );
+        if constexpr( W == 64 )
+            gOE = go + ge;
+    }
+    // H(-1, j): the diagonal input of row 0 at column j + 1.
+    __device__ __forceinline__ int32_t top_h( int64_t j ) const {
+        int64_t col = j + 1;  // Hd(col)
+        if( col == 0 )
+            return 0;
+        if constexpr( W == 64 ) {
+            return (int32_t) (gO + col * gE);
+        }
+        else {
+            if( col <= 3 )
+                return Width<W>::trunc( gO + col * (int64_t) gE );
+            int64_t h3 = Width<W>::trunc( gO + 3 * (int64_t) gE );
+            return (int32_t) Width<W>::sat64( h3 + (col - 3) * (int64_t) gE );
+        }
+    }
+    // F entering row 0 at column c.
+    __device__ __forceinline__ int32_t top_f( int64_t c ) const {
+        if constexpr( W == 64 ) {
+            return (int32_t) (2 * (int64_t) gO + (c + 2) * gE);
+        }
+        else {
+            int64_t fd;
+            if( c <= 3 )
+                fd = Width<W>::trunc( gO + (c + 1) * (int64_t) gE );
+            else
+                fd = Width<W>::sat64( Width<W>::trunc( gO + 4 * (int64_t) gE ) + (c - 3) * (int64_t) gE );
+            return (int32_t) Width<W>::sat64( fd + gOE );
+        }
+    }
+    // H(i, -1) and E(i, -1).
+    __device__ __forceinline__ int32_t left_h( int64_t i ) const {
+        if constexpr( W == 64 )
+            return (int32_t) (gO + (i + 1) * gE);
+        else
+            return (int32_t) Width<W>::sat64( gOE + i * (int64_t) gE );
+    }
+    __device__ __forceinline__ int32_t left_e( int64_t i ) const {
+        if constexpr( W == 64 )
+            return (int32_t) (2 * (int64_t) gO + (i + 2) * gE);
+        else
+            return (int32_t) Width<W>::sat64( (int64_t) left_h( i ) + gOE );
+    }
+};
+
+template <int ALGO, int W>
+__global__ void __launch_bounds__( 256 ) emul_kernel( EmulParams p ) {
+    constexpr bool SW = (ALGO == 0);
+    constexpr int R = EMUL_R;
+    const int lane = threadIdx.x & 31;
+    const uint64_t warp_global = (blockIdx.x * (uint64_t) blockDim.x + threadIdx.x) >> 5;
+    int4 * scratch = p.scratch + warp_global * p.scratch_cols;
+
+    // Scalar parameters at the pass width (reference: search_simd_sw.c:319-320,
+    // search_simd_nw.c:360-373).
+    const int gE = p.gap_extend;
+    int gOE;
+    if constexpr( W == 64 )
+        gOE = p.gap_open + p.gap_extend;
+    else
+        gOE = Width<W>::trunc( (int64_t) p.gap_open + p.gap_extend );
+    const int32_t thresh = Width<W>::trunc( Width<W>::MIN - p.gap_open - p.gap_extend - 1 );
+    const NwBounds<W> nb( p.gap_open, p.gap_extend );
+    // SW values are biased by MIN at 8/16 bits (the reference's -128/-32768 is
+    // its zero); the 64-bit kernel is unbiased with an explicit floor at 0.
+    const int32_t SW_ZERO = (W == 64) ? 0 : (int32_t) Width<W>::MIN;
+
+    for( ;; ) {
+        unsigned long long t = 0;
+        if( lane == 0 )
+            t = atomicAdd( p.counter, 1ull );
+        t = __shfl_sync( 0xffffffffu, t, 0 );
+        if( t >= p.n_tasks )
+            break;
+        uint32_t slot, id;
+        if( p.tasks ) {
+            slot = p.tasks[t].qslot;
+            id = p.tasks[t].id;
+        }
+        else if( p.slot_list ) {
+            slot = p.slot_list[t % p.n_sub];
+            id = p.order[t / p.n_sub];
+        }
+        else {
+            slot = (uint32_t) (t % p.qv.n_slots);
+            id = p.order[t / p.qv.n_slots];
+        }
+        const uint32_t L = p.db.lens[id];
+        const uint32_t Lb = (L + 3u) & ~3u;          // pad to the block end
+        const uint8_t * dseq = p.db.codes + p.db.offsets[id];
+        const uint32_t Q = p.qv.qlen[slot];
+        const uint32_t qpad = p.qv.qpad[slot];
+        const int32_t * prof = p.qv.prof32 + p.qv.prof32_off[slot];
+        const uint32_t passes = (Q + EMUL_ROWS - 1) / EMUL_ROWS;
+
+        int32_t s_run = SW ? SW_ZERO : 0;            // last lane, final pass
+        int32_t blk_min = 0, blk_max = 0;
+        int first_ovf = -1;
+        int32_t nw_score = 0;
+
+        for( uint32_t pass = 0; pass < passes; pass++ ) {
+            const bool final_pass = (pass + 1 == passes);
+            const int64_t row0 = (int64_t) pass * EMUL_ROWS + lane * R;
+            const int nvalid = (int) max( (int64_t) 0, min( (int64_t) R, (int64_t) Q - row0 ) );
+            const int rstar = (int) ((int64_t) Q - 1 - row0);   // row Q-1 if in [0, R)
+
+            int32_t H[R], E[R];
+#pragma unroll
+            for( int r = 0; r < R; r++ ) {
+                if constexpr( SW ) {
+                    H[r] = SW_ZERO;
+                    E[r] = SW_ZERO;
+                }
+                else {
+                    H[r] = nb.left_h( row0 + r );
+                    E[r] = nb.left_e( row0 + r );
+                }
+            }
+            int32_t diag;
+            if constexpr( SW )
+                diag = SW_ZERO;
+            else
+                diag = (row0 == 0) ? 0 : nb.left_h( row0 - 1 );
+
+            int32_t out_h = 0, out_f = 0, out_a = 0, out_b = 0;
+            const uint32_t steps = Lb + 31;
+            for( uint32_t s = 0; s < steps; s++ ) {
+                int32_t up_h = __shfl_up_sync( 0xffffffffu, out_h, 1 );
+                int32_t up_f = __shfl_up_sync( 0xffffffffu, out_f, 1 );
+                int32_t up_a = __shfl_up_sync( 0xffffffffu, out_a, 1 );
+                int32_t up_b = __shfl_up_sync( 0xffffffffu, out_b, 1 );
+                const int64_t c = (int64_t) s - lane;
+                if( c < 0 || c >= (int64_t) Lb )
+                    continue;
+                if( lane == 0 ) {
+                    if( pass == 0 ) {
+                        if constexpr( SW ) {
+                            up_h = SW_ZERO;
+                            up_f = SW_ZERO;
+                            up_a = SW_ZERO;
+                        }
+                        else {
+                            up_h = nb.top_h( c );
+                            up_f = nb.top_f( c );
+                            up_a = 0;     // column max  (identity: block check also uses 0)
+                            up_b = 0;     // column min
+                        }
+                    }
+                    else if( (uint32_t) c < p.scratch_cols ) {
+                        int4 v = scratch[c];
+                        up_h = v.x;
+                        up_f = v.y;
+                        up_a = v.z;
+                        up_b = v.w;
+                    }
+                }
+                const int d = (c < (int64_t) L) ? dseq[c] : 0;
+                const int32_t * pr = prof + (uint64_t) d * qpad + row0;
+                int32_t v[R];
+#pragma unroll
+                for( int r = 0; r < R; r += 4 ) {
+                    int4 x = *reinterpret_cast<const int4 *>( pr + r );
+                    v[r] = x.x;
+                    v[r + 1] = x.y;
+                    v[r + 2] = x.z;
+                    v[r + 3] = x.w;
+                }
+                int32_t f = up_f;
+                int32_t hd = diag;
+                int32_t cmax = SW ? SW_ZERO : INT_MIN, cmin = INT_MAX;
+#pragma unroll
+                for( int r = 0; r < R; r++ ) {
+                    int32_t x;
+                    if constexpr( SW && W == 64 ) {
+                        // full_sw: max(hdiag + s, e, f, 0)
+                        x = max( max( hd + v[r], E[r] ), max( f, 0 ) );
+                    }
+                    else {
+                        // ALIGNCORE: H = sat(Hdiag + V); H = max(H, F); H = max(H, E)
+                        x = max( max( Width<W>::sat( hd + v[r] ), f ), E[r] );
+                    }
+                    if( r < nvalid ) {
+                        cmax = max( cmax, x );
+                        cmin = min( cmin, x );
+                    }
+                    if constexpr( !SW ) {
+                        if( r == rstar && c == (int64_t) L - 1 )
+                            nw_score = x;
+                    }
+                    hd = H[r];
+                    H[r] = x;
+                    int32_t y = Width<W>::sat( x + gOE );
+                    f = max( Width<W>::sat( f + gE ), y );
+                    E[r] = max( Width<W>::sat( E[r] + gE ), y );
+                }
+                diag = up_h;
+                out_h = H[R - 1];
+                out_f = f;
+                if constexpr( SW ) {
+                    out_a = max( up_a, cmax );
+                }
+                else {
+                    out_a = max( up_a, cmax );
+                    out_b = min( up_b, cmin );
+                }
+                if( lane == 31 ) {
+                    if( !final_pass ) {
+                        if( (uint32_t) c < p.scratch_cols )
+                            scratch[c] = make_int4( out_h, out_f, out_a, out_b );
+                        else
+                            atomicOr( p.sink.error_flags, ERR_SCRATCH_OVERFLOW );
+                    }
+                    else if( first_ovf < 0 ) {
+                        if constexpr( SW ) {
+                            s_run = max( s_run, out_a );
+                            if( (c & 3) == 3 && W != 64 && s_run == (int32_t) Width<W>::MAX )
+                                first_ovf = (int) (c >> 2);
+                        }
+                        else {
+                            blk_max = max( blk_max, out_a );
+                            blk_min = min( blk_min, out_b );
+                            if( (c & 3) == 3 ) {
+                                if( W != 64 && (blk_min < thresh || blk_max == (int32_t) Width<W>::MAX) )
+                                    first_ovf = (int) (c >> 2);
+                                blk_min = 0;
+                                blk_max = 0;
+                            }
+                        }
+                    }
+                }
+            }
+            __syncwarp();
+        }
+
+        // Collect the lane's report.
+        if constexpr( !SW ) {
+            const int owner = (int) (((int64_t) Q - 1 - (int64_t) (passes - 1) * EMUL_ROWS) / R);
+            nw_score = __shfl_sync( 0xffffffffu, nw_score, owner );
+        }
+        if( lane == 31 ) {
+            int32_t score;
+            bool ok;
+            if constexpr( SW ) {
+                score = (W == 64) ? s_run : (int32_t) (s_run - (int32_t) Width<W>::MIN);
+                ok = first_ovf < 0 && (W == 64 || (int64_t) score < ((int64_t) 1 << W) - 1);
+            }
+            else {
+                score = nw_score;
+                ok = first_ovf < 0 && (W == 64 || (score > (int32_t) Width<W>::MIN && score < (int32_t) Width<W>::MAX));
+            }
+            const int32_t nblocks = first_ovf >= 0 ? first_ovf + 1 : (int32_t) (Lb >> 2);
+            p.sink.score[(uint64_t) slot * p.sink.score_stride + id] = score;
+            if( !ok ) {
+                unsigned k = atomicAdd( p.sink.next_count, 1u );
+                if( k < p.sink.next_cap )
+                    p.sink.next[k] = PairTask{ slot, id, nblocks, 0 };
+                else
+                    atomicOr( p.sink.error_flags, ERR_REQUEUE_OVERFLOW );
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// Host-side launcher.
+cudaError_t launch_emul( int algo, int width, const EmulParams & p, int grid, cudaStream_t st ) {
+    dim3 block( 256 );
+#define SSA_EMUL_CASE( A, Wd ) \
+    if( algo == A && width == Wd ) { \
+        emul_kernel<A, Wd><<<grid, block, 0, st>>>( p ); \
+        return cudaGetLastError(); \
+    }
+    SSA_EMUL_CASE( 0, 8 )
+    SSA_EMUL_CASE( 0, 16 )
+    SSA_EMUL_CASE( 0, 64 )
+    SSA_EMUL_CASE( 1, 8 )
+    SSA_EMUL_CASE( 1, 16 )
+    SSA_EMUL_CASE( 1, 64 )
+#undef SSA_EMUL_CASE
+    return cudaErrorInvalidValue;
+}
+
+// prof32[slot][code][row] = matrix[(code << 5) + query[row]] at the pass width;
+// rows past the query are 0 (they never reach a result).
+__global__ void build_profile32_kernel( const uint8_t * qcodes, const uint64_t * qoff, const uint32_t * qlen,
+        const uint32_t * qpad, const uint64_t * prof_off, const int64_t * matrix, int width, int32_t * prof,
+        uint32_t n_slots ) {
+    const uint32_t slot = blockIdx.y;
+    if( slot >= n_slots )
+        return;
+    const uint32_t Q = qlen[slot], P = qpad[slot];
+    const uint8_t * q = qcodes + qoff[slot];
+    int32_t * out = prof + prof_off[slot];
+    for( uint64_t k = blockIdx.x * (uint64_t) blockDim.x + threadIdx.x; k < 32ull * P;
+            k += (uint64_t) gridDim.x * blockDim.x ) {
+        uint32_t code = (uint32_t) (k / P), row = (uint32_t) (k % P);
+        int32_t v = 0;
+        if( row < Q ) {
+            int64_t m = matrix[(code << 5) + q[row]];
+            v = (width == 8) ? (int32_t) (int8_t) m : (width == 16) ? (int32_t) (int16_t) m : (int32_t) m;
+        }
+        out[k] = v;
+    }
+}
+
+cudaError_t launch_build_profile32( const uint8_t * qcodes, const uint64_t * qoff, const uint32_t * qlen,
+        const uint32_t * qpad, const uint64_t * prof_off, const int64_t * matrix, int width, int32_t * prof,
+        uint32_t n_slots, cudaStream_t st ) {
+    dim3 grid( 64, n_slots );
+    build_profile32_kernel<<<grid, 256, 0, st>>>( qcodes, qoff, qlen, qpad, prof_off, matrix, width, prof, n_slots );
+    return cudaGetLastError();
+}
+
+}  // namespace ssa

@@ -1,0 +1,642 @@
+// engine.cu -- host orchestration of the GPU search.
+//
+// One search call (one query through sw_align/nw_align, or a batch through
+// the batched extension) runs as:
+//
+//   1. the database, read once through the libssa_extern_db.h plugin and
+//      mapped to residue codes, is resident in HBM (re-packed only after
+//      init_db or a change of symbol type);
+//   2. the queries of the batch are uploaded and their substitution profiles
+//      built on the device, one 32 x rows table per query and pass width;
+//   3. the entry pass scores every (query, non-empty sequence) pair; pairs the
+//      entry width cannot report go to a device-side re-queue list with the
+//      block count they used, and the next width runs on that list
+//      (8 -> 16 -> 64, reference: src/algo/8/search_8.c:94-124,
+//      src/algo/16/search_16.c:92-114);
+//   4. the final score of every pair and the re-queue lists come back to the
+//      host, which replays the CPU channel schedule and min-heap per query
+//      (replay.cpp) to get the exact CPU hit list;
+//   5. for COMPUTE_ALIGNMENT the hits go through the traceback kernels.
+#include "device_common.cuh"
+#include "ssa_internal.h"
+#include "libssa_extern_db.h"
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <thread>
+
+namespace ssa {
+
+#define CUDA_CHECK( expr ) \
+    do { \
+        cudaError_t e_ = (expr); \
+        if( e_ != cudaSuccess ) \
+            fatal( "CUDA error %s at %s:%d: %s", cudaGetErrorName( e_ ), __FILE__, __LINE__, cudaGetErrorString( e_ ) ); \
+    } while( 0 )
+
+// Grow-only device buffer.
+struct DevBuf {
+    void * p = nullptr;
+    size_t bytes = 0;
+    void * ensure( size_t n ) {
+        if( n > bytes ) {
+            if( p )
+                CUDA_CHECK( cudaFree( p ) );
+            p = nullptr;
+            size_t want = std::max( n, (size_t) 256 );
+            CUDA_CHECK( cudaMalloc( &p, want ) );
+            bytes = want;
+        }
+        return p;
+    }
+    void release() {
+        if( p )
+            cudaFree( p );
+        p = nullptr;
+        bytes = 0;
+    }
+    template <class T>
+    T * as() const {
+        return (T *) p;
+    }
+};
+
+struct PinnedBuf {
+    void * p = nullptr;
+    size_t bytes = 0;
+    void * ensure( size_t n ) {
+        if( n > bytes ) {
+            if( p )
+                CUDA_CHECK( cudaFreeHost( p ) );
+            p = nullptr;
+            size_t want = std::max( n, (size_t) 256 );
+            CUDA_CHECK( cudaMallocHost( &p, want ) );
+            bytes = want;
+        }
+        return p;
+    }
+    void release() {
+        if( p )
+            cudaFreeHost( p );
+        p = nullptr;
+        bytes = 0;
+    }
+};
+
+class Engine {
+public:
+    static Engine & get() {
+        static Engine e;
+        return e;
+    }
+
+    void init_device() {
+        if( ready_ )
+            return;
+        int dev = 0;
+        if( const char * s = getenv( "SSA_B200_DEVICE" ) )
+            dev = atoi( s );
+        int n = 0;
+        CUDA_CHECK( cudaGetDeviceCount( &n ) );
+        if( n <= 0 )
+            fatal( "No CUDA device available: the B200 libssa build has no CPU path." );
+        CUDA_CHECK( cudaSetDevice( dev ) );
+        cudaDeviceProp prop;
+        CUDA_CHECK( cudaGetDeviceProperties( &prop, dev ) );
+        if( prop.major < 10 )
+            fatal( "libssa B200 build needs an sm_100 device, found %s (sm_%d%d).", prop.name, prop.major,
+                    prop.minor );
+        sms_ = prop.multiProcessorCount;
+        CUDA_CHECK( cudaStreamCreateWithFlags( &stream_, cudaStreamNonBlocking ) );
+        CUDA_CHECK( cudaEventCreate( &ev0_ ) );
+        CUDA_CHECK( cudaEventCreate( &ev1_ ) );
+        device_ = dev;
+        ready_ = true;
+    }
+
+    // ---- database ------------------------------------------------------------
+    const HostDb & database() {
+        const Config & cfg = config();
+        if( db_.symtype != cfg.symtype || db_stale_ )
+            pack_database();
+        return db_;
+    }
+
+    void invalidate() { db_stale_ = true; }
+
+    void pack_database() {
+        const Config & cfg = config();
+        HostDb db;
+        const size_t n = ssa_db_get_sequence_count();
+        if( n > UINT32_MAX )
+            fatal( "Database has %zu sequences; at most %u are supported.", n, UINT32_MAX );
+        db.n_ids = (uint32_t) n;
+        db.len.assign( n, 0 );
+        db.off.assign( n, 0 );
+        const bool nt = cfg.symtype == NUCLEOTIDE;
+        if( cfg.symtype == TRANS_QUERY || cfg.symtype == TRANS_DB || cfg.symtype == TRANS_BOTH )
+            fatal( "Translated searches (symbol type %d) are not supported by the B200 build.", cfg.symtype );
+        uint64_t total = 0;
+        std::vector<p_seqinfo> infos( n );
+        for( size_t id = 0; id < n; id++ ) {
+            p_seqinfo info = ssa_db_get_sequence( id );
+            if( !info )
+                fatal( "Could not get sequence from DB: %zu", id );
+            infos[id] = info;
+            if( info->seqlen > (size_t) INT32_MAX / 2 )
+                fatal( "Database sequence %zu is too long (%zu residues).", id, info->seqlen );
+            db.len[id] = (uint32_t) info->seqlen;
+            db.off[id] = total;
+            total += (info->seqlen + 15) & ~(uint64_t) 15;
+            db.max_len = std::max( db.max_len, (uint32_t) info->seqlen );
+        }
+        db.codes.assign( total + 16, 0 );
+        uint64_t unknown = 0;
+        for( size_t id = 0; id < n; id++ ) {
+            // unknown symbols become code 0 (reference: src/util/util_sequence.c:298-318)
+            const char * s = infos[id]->seq;
+            uint8_t * o = db.codes.data() + db.off[id];
+            for( size_t k = 0; k < db.len[id]; k++ ) {
+                int m = nt ? map_nt16( (unsigned char) s[k] ) : map_aa( (unsigned char) s[k] );
+                if( m < 0 ) {
+                    m = 0;
+                    unknown++;
+                }
+                o[k] = (uint8_t) m;
+            }
+            db.residues += db.len[id];
+        }
+        if( unknown )
+            print_warning( "%llu unknown symbols found and set to zero", (unsigned long long) unknown );
+        db.nonempty_before.assign( (size_t) n + 1, 0 );
+        for( uint32_t id = 0; id < db.n_ids; id++ ) {
+            db.nonempty_before[id + 1] = db.nonempty_before[id] + (db.len[id] ? 1 : 0);
+            if( db.len[id] )
+                db.order_desc.push_back( id );
+        }
+        std::stable_sort( db.order_desc.begin(), db.order_desc.end(),
+                [&]( uint32_t a, uint32_t b ) { return db.len[a] > db.len[b]; } );
+        db.symtype = cfg.symtype;
+        db.generation = ++generation_;
+
+        init_device();
+        d_codes_.ensure( db.codes.size() );
+        d_off_.ensure( sizeof(uint64_t) * std::max<size_t>( 1, n ) );
+        d_len_.ensure( sizeof(uint32_t) * std::max<size_t>( 1, n ) );
+        d_order_.ensure( sizeof(uint32_t) * std::max<size_t>( 1, db.order_desc.size() ) );
+        CUDA_CHECK( cudaMemcpy( d_codes_.p, db.codes.data(), db.codes.size(), cudaMemcpyHostToDevice ) );
+        if( n ) {
+            CUDA_CHECK( cudaMemcpy( d_off_.p, db.off.data(), sizeof(uint64_t) * n, cudaMemcpyHostToDevice ) );
+            CUDA_CHECK( cudaMemcpy( d_len_.p, db.len.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice ) );
+        }
+        if( !db.order_desc.empty() )
+            CUDA_CHECK( cudaMemcpy( d_order_.p, db.order_desc.data(), sizeof(uint32_t) * db.order_desc.size(),
+                    cudaMemcpyHostToDevice ) );
+        db_ = std::move( db );
+        db_stale_ = false;
+        ranks_.clear();
+    }
+
+    DbView db_view() const {
+        DbView v;
+        v.codes = d_codes_.as<uint8_t>();
+        v.offsets = d_off_.as<uint64_t>();
+        v.lens = d_len_.as<uint32_t>();
+        v.n_ids = db_.n_ids;
+        return v;
+    }
+
+    const uint32_t * ranks( size_t chunk_size, int lanes ) {
+        for( auto & c : ranks_ )
+            if( c.chunk_size == chunk_size && c.lanes == lanes && c.generation == db_.generation )
+                return c.rank.data();
+        ScheduleCache c;
+        c.chunk_size = chunk_size;
+        c.lanes = lanes;
+        c.generation = db_.generation;
+        schedule_ranks( db_, chunk_size, lanes, c.rank );
+        ranks_.push_back( std::move( c ) );
+        return ranks_.back().rank.data();
+    }
+
+    // ---- search ----------------------------------------------------------------
+    void search( const SearchRequest & req, const std::vector<QueryCodes> & queries,
+            std::vector<std::vector<Hit>> & out, SearchStats & stats );
+
+    void shutdown() {
+        DevBuf * bufs[] = { &d_codes_, &d_off_, &d_len_, &d_order_, &d_qcodes_, &d_qoff_, &d_qlen_, &d_qpad_,
+            &d_prof_off_, &d_prof_, &d_matrix_, &d_score_, &d_list_a_, &d_list_b_, &d_counts_, &d_scratch_,
+            &d_tb_hits_, &d_tb_regions_, &d_tb_last_, &d_tb_last_off_, &d_tb_dirs_, &d_tb_dir_off_, &d_tb_ops_,
+            &d_tb_ops_off_, &d_tb_ops_len_ };
+        for( DevBuf * b : bufs )
+            b->release();
+        h_score_.release();
+        db_ = HostDb();
+        db_stale_ = true;
+        ranks_.clear();
+    }
+
+    uint64_t launches() const { return launches_.load(); }
+
+private:
+    Engine() = default;
+
+    void run_pass( int algo, int width, const SearchRequest & req, uint32_t n_slots, const PairTask * tasks,
+            uint64_t n_tasks, bool implicit, PairTask * next, unsigned * next_count, uint32_t next_cap );
+    void build_profiles( int width, uint32_t n_slots );
+    void traceback( const SearchRequest & req, const std::vector<QueryCodes> & queries, uint32_t slot0,
+            std::vector<std::vector<Hit>> & out );
+
+    bool ready_ = false;
+    int device_ = 0;
+    int sms_ = 148;
+    cudaStream_t stream_ = nullptr;
+    cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+    HostDb db_;
+    bool db_stale_ = true;
+    uint64_t generation_ = 0;
+    std::vector<ScheduleCache> ranks_;
+    std::atomic<uint64_t> launches_{ 0 };
+
+    // device buffers
+    DevBuf d_codes_, d_off_, d_len_, d_order_;
+    DevBuf d_qcodes_, d_qoff_, d_qlen_, d_qpad_, d_prof_off_, d_prof_, d_matrix_;
+    DevBuf d_score_, d_list_a_, d_list_b_, d_counts_, d_scratch_;
+    DevBuf d_tb_hits_, d_tb_regions_, d_tb_last_, d_tb_last_off_, d_tb_dirs_, d_tb_dir_off_, d_tb_ops_,
+            d_tb_ops_off_, d_tb_ops_len_;
+    PinnedBuf h_score_;
+
+    // per-batch query layout
+    std::vector<uint64_t> h_qoff_;
+    std::vector<uint32_t> h_qlen_, h_qpad_;
+    std::vector<uint64_t> h_prof_off_;
+    int prof_width_ = -1;
+    uint32_t prof_slots_ = 0;
+    uint32_t max_qlen_ = 0;
+
+    friend void engine_shutdown();
+};
+
+void Engine::build_profiles( int width, uint32_t n_slots ) {
+    if( prof_width_ == width && prof_slots_ == n_slots )
+        return;
+    launch_build_profile32( d_qcodes_.as<uint8_t>(), d_qoff_.as<uint64_t>(), d_qlen_.as<uint32_t>(),
+            d_qpad_.as<uint32_t>(), d_prof_off_.as<uint64_t>(), d_matrix_.as<int64_t>(), width,
+            d_prof_.as<int32_t>(), n_slots, stream_ );
+    CUDA_CHECK( cudaGetLastError() );
+    launches_++;
+    prof_width_ = width;
+    prof_slots_ = n_slots;
+}
+
+void Engine::run_pass( int algo, int width, const SearchRequest & req, uint32_t n_slots, const PairTask * tasks,
+        uint64_t n_tasks, bool implicit, PairTask * next, unsigned * next_count, uint32_t next_cap ) {
+    if( n_tasks == 0 )
+        return;
+    build_profiles( width, n_slots );
+    EmulParams p;
+    p.db = db_view();
+    p.qv.prof32 = d_prof_.as<int32_t>();
+    p.qv.prof32_off = d_prof_off_.as<uint64_t>();
+    p.qv.qlen = d_qlen_.as<uint32_t>();
+    p.qv.qpad = d_qpad_.as<uint32_t>();
+    p.qv.n_slots = n_slots;
+    p.tasks = implicit ? nullptr : tasks;
+    p.order = d_order_.as<uint32_t>();
+    p.n_tasks = n_tasks;
+    unsigned long long * counter = d_counts_.as<unsigned long long>() + 4;
+    CUDA_CHECK( cudaMemsetAsync( counter, 0, sizeof(unsigned long long), stream_ ) );
+    p.counter = counter;
+    p.gap_open = req.gap_open;
+    p.gap_extend = req.gap_extend;
+    p.sink.score = d_score_.as<int32_t>();
+    p.sink.score_stride = db_.n_ids;
+    p.sink.next = next;
+    p.sink.next_count = next_count;
+    p.sink.next_cap = next_cap;
+    p.sink.error_flags = d_counts_.as<unsigned>() + 2;
+    const int grid = sms_ * 2;
+    const uint32_t cols = ((db_.max_len + 3u) & ~3u) + 4;
+    if( max_qlen_ > 256 ) {
+        p.scratch = (int4 *) d_scratch_.ensure( (size_t) grid * 8 * cols * sizeof(int4) );
+        p.scratch_cols = cols;
+    }
+    else {
+        p.scratch = nullptr;
+        p.scratch_cols = 0;
+    }
+    CUDA_CHECK( launch_emul( algo, width, p, grid, stream_ ) );
+    launches_++;
+}
+
+void Engine::search( const SearchRequest & req, const std::vector<QueryCodes> & queries,
+        std::vector<std::vector<Hit>> & out, SearchStats & stats ) {
+    init_device();
+    const HostDb & db = database();
+    out.assign( queries.size(), {} );
+    if( queries.empty() )
+        return;
+    const uint64_t n_ne = db.order_desc.size();
+
+    // matrix on the device
+    d_matrix_.ensure( 1024 * sizeof(int64_t) );
+    CUDA_CHECK( cudaMemcpyAsync( d_matrix_.p, req.matrix, 1024 * sizeof(int64_t), cudaMemcpyHostToDevice, stream_ ) );
+
+    // sub-batches bounded by the per-pair result memory
+    const uint64_t pair_budget = (uint64_t) 1 << 28;
+    const uint64_t per_query = std::max<uint64_t>( 1, std::max<uint64_t>( n_ne, db.n_ids ) );
+    const size_t batch = (size_t) std::max<uint64_t>(
+            1, std::min<uint64_t>( std::min<uint64_t>( queries.size(), pair_budget / per_query ), 65535 ) );
+
+    CUDA_CHECK( cudaEventRecord( ev0_, stream_ ) );
+    for( size_t b0 = 0; b0 < queries.size(); b0 += batch ) {
+        const uint32_t nq = (uint32_t) std::min( batch, queries.size() - b0 );
+        // ---- upload queries
+        h_qoff_.assign( nq, 0 );
+        h_qlen_.assign( nq, 0 );
+        h_qpad_.assign( nq, 0 );
+        h_prof_off_.assign( nq, 0 );
+        uint64_t qtotal = 0, ptotal = 0;
+        max_qlen_ = 0;
+        for( uint32_t s = 0; s < nq; s++ ) {
+            const QueryCodes & q = queries[b0 + s];
+            h_qoff_[s] = qtotal;
+            h_qlen_[s] = q.len;
+            h_qpad_[s] = std::max<uint32_t>( 256, (q.len + 255u) & ~255u );
+            h_prof_off_[s] = ptotal;
+            qtotal += (q.len + 15u) & ~15u;
+            ptotal += 32ull * h_qpad_[s];
+            max_qlen_ = std::max( max_qlen_, q.len );
+            stats.cells += (uint64_t) q.len * db.residues;
+        }
+        std::vector<uint8_t> hq( qtotal + 16, 0 );
+        for( uint32_t s = 0; s < nq; s++ )
+            memcpy( hq.data() + h_qoff_[s], queries[b0 + s].codes, queries[b0 + s].len );
+        d_qcodes_.ensure( hq.size() );
+        d_qoff_.ensure( nq * sizeof(uint64_t) );
+        d_qlen_.ensure( nq * sizeof(uint32_t) );
+        d_qpad_.ensure( nq * sizeof(uint32_t) );
+        d_prof_off_.ensure( nq * sizeof(uint64_t) );
+        d_prof_.ensure( ptotal * sizeof(int32_t) );
+        CUDA_CHECK( cudaMemcpyAsync( d_qcodes_.p, hq.data(), hq.size(), cudaMemcpyHostToDevice, stream_ ) );
+        CUDA_CHECK( cudaMemcpyAsync( d_qoff_.p, h_qoff_.data(), nq * sizeof(uint64_t), cudaMemcpyHostToDevice, stream_ ) );
+        CUDA_CHECK( cudaMemcpyAsync( d_qlen_.p, h_qlen_.data(), nq * sizeof(uint32_t), cudaMemcpyHostToDevice, stream_ ) );
+        CUDA_CHECK( cudaMemcpyAsync( d_qpad_.p, h_qpad_.data(), nq * sizeof(uint32_t), cudaMemcpyHostToDevice, stream_ ) );
+        CUDA_CHECK( cudaMemcpyAsync( d_prof_off_.p, h_prof_off_.data(), nq * sizeof(uint64_t), cudaMemcpyHostToDevice,
+                stream_ ) );
+        prof_width_ = -1;
+
+        // ---- result and re-queue buffers
+        const uint64_t n_pairs = (uint64_t) nq * n_ne;
+        const size_t score_bytes = (size_t) nq * db.n_ids * sizeof(int32_t);
+        d_score_.ensure( std::max<size_t>( score_bytes, 4 ) );
+        const uint32_t cap = (uint32_t) std::min<uint64_t>( std::max<uint64_t>( n_pairs, 1 ), 0xffffffffull );
+        d_list_a_.ensure( (size_t) cap * sizeof(PairTask) );
+        d_list_b_.ensure( (size_t) cap * sizeof(PairTask) );
+        d_counts_.ensure( 8 * sizeof(unsigned long long) );
+        CUDA_CHECK( cudaMemsetAsync( d_counts_.p, 0, 8 * sizeof(unsigned long long), stream_ ) );
+        unsigned * cnt = d_counts_.as<unsigned>();   // [0] list a, [1] list b, [2] errors
+
+        // ---- passes
+        const int entry = req.bit_width;
+        std::vector<PairTask> list_entry, list_16;   // host copies for the replay
+        unsigned n_a = 0, n_b = 0;
+        run_pass( req.algo, entry, req, nq, nullptr, n_pairs, true, d_list_a_.as<PairTask>(), cnt + 0, cap );
+        if( entry != 64 ) {
+            CUDA_CHECK( cudaMemcpyAsync( &n_a, cnt + 0, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_ ) );
+            CUDA_CHECK( cudaStreamSynchronize( stream_ ) );
+            n_a = std::min( n_a, cap );
+            if( n_a ) {
+                const int w2 = (entry == 8) ? 16 : 64;
+                PairTask * nx = (w2 == 16) ? d_list_b_.as<PairTask>() : nullptr;
+                run_pass( req.algo, w2, req, nq, d_list_a_.as<PairTask>(), n_a, false, nx, cnt + 1, cap );
+                if( w2 == 16 ) {
+                    CUDA_CHECK( cudaMemcpyAsync( &n_b, cnt + 1, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_ ) );
+                    CUDA_CHECK( cudaStreamSynchronize( stream_ ) );
+                    n_b = std::min( n_b, cap );
+                    if( n_b )
+                        run_pass( req.algo, 64, req, nq, d_list_b_.as<PairTask>(), n_b, false, nullptr, cnt + 3, 0 );
+                }
+                list_entry.resize( n_a );
+                CUDA_CHECK( cudaMemcpyAsync( list_entry.data(), d_list_a_.p, n_a * sizeof(PairTask),
+                        cudaMemcpyDeviceToHost, stream_ ) );
+                if( n_b ) {
+                    list_16.resize( n_b );
+                    CUDA_CHECK( cudaMemcpyAsync( list_16.data(), d_list_b_.p, n_b * sizeof(PairTask),
+                            cudaMemcpyDeviceToHost, stream_ ) );
+                }
+            }
+        }
+        int32_t * hs = (int32_t *) h_score_.ensure( std::max<size_t>( score_bytes, 4 ) );
+        if( score_bytes )
+            CUDA_CHECK( cudaMemcpyAsync( hs, d_score_.p, score_bytes, cudaMemcpyDeviceToHost, stream_ ) );
+        unsigned err = 0;
+        CUDA_CHECK( cudaMemcpyAsync( &err, cnt + 2, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_ ) );
+        CUDA_CHECK( cudaStreamSynchronize( stream_ ) );
+        if( err )
+            fatal( "Internal error in the GPU search (flags 0x%x).", err );
+
+        // ---- host replay, one query per worker
+        std::vector<ReplayQuery> rq( nq );
+        for( uint32_t s = 0; s < nq; s++ )
+            rq[s].score = hs + (size_t) s * db.n_ids;
+        for( const PairTask & t : list_entry )
+            rq[t.qslot].ovf_entry.emplace_back( t.id, t.nb_prev );
+        for( const PairTask & t : list_16 )
+            rq[t.qslot].ovf16.emplace_back( t.id, t.nb_prev );
+        for( auto & r : rq ) {
+            std::sort( r.ovf_entry.begin(), r.ovf_entry.end() );
+            std::sort( r.ovf16.begin(), r.ovf16.end() );
+        }
+        const uint32_t * rank_entry = (entry == 64) ? nullptr : ranks( req.chunk_size, entry == 8 ? req.lanes8 : req.lanes16 );
+        {
+            const unsigned hw = std::max( 1u, std::thread::hardware_concurrency() );
+            const unsigned nthreads = std::min<unsigned>( hw, nq );
+            std::atomic<uint32_t> next{ 0 };
+            std::vector<ReplayCounts> counts( nq );
+            auto work = [&]() {
+                for( ;; ) {
+                    uint32_t s = next.fetch_add( 1 );
+                    if( s >= nq )
+                        break;
+                    replay_query( db, req, rq[s], rank_entry, out[b0 + s], counts[s] );
+                }
+            };
+            if( nthreads <= 1 ) {
+                work();
+            }
+            else {
+                std::vector<std::thread> th;
+                for( unsigned k = 0; k < nthreads; k++ )
+                    th.emplace_back( work );
+                for( auto & t : th )
+                    t.join();
+            }
+            for( const ReplayCounts & c : counts ) {
+                stats.overflow8 += c.overflow8;
+                stats.overflow16 += c.overflow16;
+            }
+        }
+        if( req.align_type == COMPUTE_ALIGNMENT )
+            traceback( req, queries, (uint32_t) b0, out );
+    }
+    CUDA_CHECK( cudaEventRecord( ev1_, stream_ ) );
+    CUDA_CHECK( cudaEventSynchronize( ev1_ ) );
+    float ms = 0;
+    CUDA_CHECK( cudaEventElapsedTime( &ms, ev0_, ev1_ ) );
+    stats.seconds_gpu += ms * 1e-3;
+    stats.kernel_launches = launches_.load();
+}
+
+void Engine::traceback( const SearchRequest & req, const std::vector<QueryCodes> & queries, uint32_t slot0,
+        std::vector<std::vector<Hit>> & out ) {
+    const uint32_t nq = (uint32_t) h_qlen_.size();
+    std::vector<TbHit> hits;
+    std::vector<std::pair<uint32_t, uint32_t>> where;   // (query index, hit index)
+    for( uint32_t s = 0; s < nq; s++ ) {
+        auto & hl = out[slot0 + s];
+        for( uint32_t k = 0; k < hl.size(); k++ ) {
+            hits.push_back( TbHit{ s, hl[k].id, (int32_t) hl[k].score, req.algo } );
+            where.emplace_back( slot0 + s, k );
+        }
+    }
+    const uint32_t nh = (uint32_t) hits.size();
+    if( nh == 0 )
+        return;
+    // value range guard: every DP value is bounded by (q + d) * max |step|
+    int64_t mabs = std::abs( (int64_t) req.gap_open ) + std::abs( (int64_t) req.gap_extend );
+    for( int k = 0; k < 1024; k++ )
+        mabs = std::max<int64_t>( mabs, std::llabs( req.matrix[k] ) );
+    std::vector<TbRegion> regions( nh );
+    std::vector<uint64_t> last_off( nh + 1, 0 ), dir_off( nh + 1, 0 ), ops_off( nh + 1, 0 );
+    for( uint32_t h = 0; h < nh; h++ ) {
+        const uint32_t A = h_qlen_[hits[h].qslot], B = db_.len[hits[h].id];
+        if( (int64_t) (A + B + 4) * (mabs + 1) * 2 > INT32_MAX )
+            fatal( "Alignment of %u x %u residues exceeds the supported score range.", A, B );
+        TbRegion rg{};
+        if( req.algo == 1 ) {
+            rg.a_begin = 0;
+            rg.a_end = (int32_t) A - 1;
+            rg.b_begin = 0;
+            rg.b_end = (int32_t) B - 1;
+            rg.status = (A && B) ? 0 : 1;
+        }
+        regions[h] = rg;
+        last_off[h + 1] = last_off[h] + A;
+        dir_off[h + 1] = dir_off[h] + (uint64_t) B * ((A + 7) / 8);
+        ops_off[h + 1] = ops_off[h] + A + B + 1;
+    }
+    TbParams p;
+    p.db = db_view();
+    p.qcodes = d_qcodes_.as<uint8_t>();
+    p.qoff = d_qoff_.as<uint64_t>();
+    p.qlen = d_qlen_.as<uint32_t>();
+    p.matrix = d_matrix_.as<int64_t>();
+    p.gap_open = req.gap_open;
+    p.gap_extend = req.gap_extend;
+    p.hits = (const TbHit *) d_tb_hits_.ensure( nh * sizeof(TbHit) );
+    p.n_hits = nh;
+    p.regions = (TbRegion *) d_tb_regions_.ensure( nh * sizeof(TbRegion) );
+    const int grid = sms_ * 2;
+    const uint32_t cols = db_.max_len + 4;
+    const bool multi = max_qlen_ > 256;
+    p.scratch = multi ? (int4 *) d_scratch_.ensure( (size_t) grid * 8 * cols * sizeof(int4) ) : nullptr;
+    p.scratch_cols = multi ? cols : 0;
+    int32_t * last = (int32_t *) d_tb_last_.ensure( 2 * last_off[nh] * sizeof(int32_t) + 16 );
+    p.last_h = last;
+    p.last_e = last + last_off[nh];
+    p.last_off = (const uint64_t *) d_tb_last_off_.ensure( (nh + 1) * sizeof(uint64_t) );
+    p.dirs = (uint16_t *) d_tb_dirs_.ensure( dir_off[nh] * sizeof(uint16_t) + 16 );
+    p.dir_off = (const uint64_t *) d_tb_dir_off_.ensure( (nh + 1) * sizeof(uint64_t) );
+    p.ops = (char *) d_tb_ops_.ensure( ops_off[nh] + 16 );
+    p.ops_off = (const uint64_t *) d_tb_ops_off_.ensure( (nh + 1) * sizeof(uint64_t) );
+    p.ops_len = (uint32_t *) d_tb_ops_len_.ensure( nh * sizeof(uint32_t) );
+    p.error_flags = d_counts_.as<unsigned>() + 2;
+    CUDA_CHECK( cudaMemcpyAsync( (void *) p.hits, hits.data(), nh * sizeof(TbHit), cudaMemcpyHostToDevice, stream_ ) );
+    CUDA_CHECK( cudaMemcpyAsync( p.regions, regions.data(), nh * sizeof(TbRegion), cudaMemcpyHostToDevice, stream_ ) );
+    CUDA_CHECK( cudaMemcpyAsync( (void *) p.last_off, last_off.data(), (nh + 1) * sizeof(uint64_t),
+            cudaMemcpyHostToDevice, stream_ ) );
+    CUDA_CHECK( cudaMemcpyAsync( (void *) p.dir_off, dir_off.data(), (nh + 1) * sizeof(uint64_t),
+            cudaMemcpyHostToDevice, stream_ ) );
+    CUDA_CHECK( cudaMemcpyAsync( (void *) p.ops_off, ops_off.data(), (nh + 1) * sizeof(uint64_t),
+            cudaMemcpyHostToDevice, stream_ ) );
+    CUDA_CHECK( launch_traceback( p, req.algo == 0, grid, stream_ ) );
+    launches_ += (req.algo == 0) ? 4 : 2;
+    std::vector<uint32_t> ops_len( nh );
+    std::vector<char> ops( ops_off[nh] + 1 );
+    CUDA_CHECK( cudaMemcpyAsync( regions.data(), p.regions, nh * sizeof(TbRegion), cudaMemcpyDeviceToHost, stream_ ) );
+    CUDA_CHECK( cudaMemcpyAsync( ops_len.data(), p.ops_len, nh * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream_ ) );
+    CUDA_CHECK( cudaMemcpyAsync( ops.data(), p.ops, ops_off[nh], cudaMemcpyDeviceToHost, stream_ ) );
+    unsigned err = 0;
+    CUDA_CHECK( cudaMemcpyAsync( &err, d_counts_.as<unsigned>() + 2, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_ ) );
+    CUDA_CHECK( cudaStreamSynchronize( stream_ ) );
+    if( err )
+        fatal( "Internal error in the GPU traceback (flags 0x%x).", err );
+    for( uint32_t h = 0; h < nh; h++ ) {
+        Hit & hit = out[where[h].first][where[h].second];
+        const TbRegion & rg = regions[h];
+        hit.has_cigar = true;
+        if( rg.status == 2 )
+            fatal( "Internal error in align function." );   // reference: src/algo/align.c:131
+        if( rg.status != 0 ) {
+            // no positive cell: the reference leaves the region undefined here
+            hit.q_start = hit.q_end = hit.d_start = hit.d_end = 0;
+            hit.cigar.clear();
+            continue;
+        }
+        hit.q_start = (uint32_t) rg.a_begin;
+        hit.q_end = (uint32_t) rg.a_end;
+        hit.d_start = (uint32_t) rg.b_begin;
+        hit.d_end = (uint32_t) rg.b_end;
+        // run-length encode the moves in alignment order; counts of 1 are
+        // omitted (reference: src/algo/cigar.c:221-263)
+        const char * mv = ops.data() + ops_off[h];
+        uint32_t n = std::min<uint64_t>( ops_len[h], ops_off[h + 1] - ops_off[h] );
+        std::string cig;
+        uint32_t k = n;
+        char buf[24];
+        while( k > 0 ) {
+            const char op = mv[k - 1];
+            uint32_t run = 0;
+            while( k > 0 && mv[k - 1] == op ) {
+                run++;
+                k--;
+            }
+            if( run > 1 ) {
+                snprintf( buf, sizeof(buf), "%u", run );
+                cig += buf;
+            }
+            cig += op;
+        }
+        hit.cigar = std::move( cig );
+    }
+}
+
+// ---- free functions ------------------------------------------------------------
+void engine_search( const SearchRequest & req, const std::vector<QueryCodes> & queries,
+        std::vector<std::vector<Hit>> & out, SearchStats & stats ) {
+    Engine::get().search( req, queries, out, stats );
+}
+
+const HostDb & engine_database() {
+    return Engine::get().database();
+}
+
+void engine_invalidate_database() {
+    Engine::get().invalidate();
+}
+
+void engine_shutdown() {
+    Engine::get().shutdown();
+}
+
+uint64_t engine_kernel_launches() {
+    return Engine::get().launches();
+}
+
+}  // namespace ssa

@@ -1,0 +1,131 @@
+// ssa_internal.h -- internal interfaces of the libssa B200 library.
+#pragma once
+
+#include <cstdint>
+#include <cstddef>
+#include <string>
+#include <vector>
+
+#include "libssa.h"
+
+namespace ssa {
+
+// ---- process-global settings (reference: src/libssa.c:35-36,
+//      src/util/util.c:34, src/algo/manager.c:38, src/util/util_sequence.c) ----
+struct Config {
+    int output_mode = OUTPUT_WARNING;
+    int simd_mode = COMPUTE_ON_AVX2;
+    size_t chunk_size = 1000;
+    size_t thread_count = (size_t) -1;
+    int8_t gap_open = 0;
+    int8_t gap_extend = 0;
+    int symtype = AMINOACID;
+    int strands = FORWARD_STRAND;
+    int db_gencode = 1;
+    int q_gencode = 1;
+    bool matrix_set = false;
+    bool constant_scoring = false;
+    int64_t matrix[1024];
+};
+
+Config & config();
+
+[[noreturn]] void fatal( const char * fmt, ... );
+void print_info( const char * fmt, ... );
+void print_warning( const char * fmt, ... );
+void print_error( const char * fmt, ... );
+
+// ---- residue maps (reference: src/util/util_sequence.c:38-88) ----------------
+int map_aa( unsigned char c );     // -1 if not an amino-acid symbol
+int map_nt16( unsigned char c );   // -1 if not a nucleotide symbol
+
+// ---- matrices (reference: src/matrices.c:335-568) ----------------------------
+void matrix_from_string( const char * text, int64_t * out );
+bool matrix_builtin( const char * name, int64_t * out );
+void matrix_constant( int match, int mismatch, int64_t * out );
+
+// ---- database packed on the host, mirrored into HBM --------------------------
+struct HostDb {
+    uint32_t n_ids = 0;
+    std::vector<uint32_t> len;          // per ID
+    std::vector<uint64_t> off;          // per ID into codes
+    std::vector<uint8_t> codes;         // mapped residues, each record padded to 16 B
+    std::vector<uint32_t> order_desc;   // non-empty IDs, longest first (stable)
+    std::vector<uint32_t> nonempty_before;   // per ID + 1: non-empty records with a smaller ID
+    uint64_t residues = 0;
+    uint32_t max_len = 0;
+    int symtype = -1;
+    uint64_t generation = 0;
+};
+
+// ---- hits and search requests -------------------------------------------------
+struct Hit {
+    int64_t score = 0;
+    uint32_t id = 0;
+    uint32_t q_start = 0, q_end = 0, d_start = 0, d_end = 0;
+    std::string cigar;
+    bool has_cigar = false;
+};
+
+struct SearchStats {
+    uint64_t overflow8 = 0;     // sequences re-aligned at 16 bit
+    uint64_t overflow16 = 0;    // sequences re-aligned at 64 bit
+    uint64_t cells = 0;         // query length x database residues, summed
+    uint64_t kernel_launches = 0;
+    double seconds_gpu = 0;
+};
+
+struct SearchRequest {
+    int algo = 0;               // 0 SW, 1 NW
+    int bit_width = 8;
+    int align_type = COMPUTE_SCORE;
+    size_t hitcount = 10;
+    size_t chunk_size = 1000;
+    int lanes8 = 32, lanes16 = 16;
+    int gap_open = 0, gap_extend = 0;
+    const int64_t * matrix = nullptr;
+};
+
+struct QueryCodes {
+    const uint8_t * codes;
+    uint32_t len;
+};
+
+// Runs the search of each query against the current database on the GPU and
+// returns the sorted hit list per query.
+void engine_search( const SearchRequest & req, const std::vector<QueryCodes> & queries,
+        std::vector<std::vector<Hit>> & out, SearchStats & stats );
+
+// The packed database (re-read through the plugin when stale).
+const HostDb & engine_database();
+void engine_invalidate_database();
+void engine_shutdown();
+uint64_t engine_kernel_launches();
+
+// ---- host replay of the CPU lane schedule and min-heap (replay.cpp) ----------
+struct ReplayQuery {
+    const int32_t * score;                          // per ID, final score
+    std::vector<std::pair<uint32_t, int32_t>> ovf_entry;   // (id, blocks) not reported by the entry pass
+    std::vector<std::pair<uint32_t, int32_t>> ovf16;       // (id, blocks) not reported by the 16-bit pass
+};
+
+// Chunk schedule ranks that do not depend on the query (entry pass without
+// overflow): rank[id] = report position of id inside its chunk.
+struct ScheduleCache {
+    size_t chunk_size = 0;
+    int lanes = 0;
+    uint64_t generation = 0;
+    std::vector<uint32_t> rank;
+};
+
+void schedule_ranks( const HostDb & db, size_t chunk_size, int lanes, std::vector<uint32_t> & rank );
+
+struct ReplayCounts {
+    uint64_t overflow8 = 0;     // searched sequences the 8-bit pass re-queued
+    uint64_t overflow16 = 0;    // searched sequences re-queued to 64 bit
+};
+
+void replay_query( const HostDb & db, const SearchRequest & req, const ReplayQuery & rq, const uint32_t * rank_entry,
+        std::vector<Hit> & hits, ReplayCounts & counts );
+
+}  // namespace ssa

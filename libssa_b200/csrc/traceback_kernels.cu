@@ -1,0 +1,455 @@
+// traceback_kernels.cu -- CIGAR traceback of the top hits on the GPU.
+//
+// For every hit the CPU library runs three scalar O(q*d) passes and a walk
+// (reference: src/algo/align.c:39-182, src/algo/cigar.c:48-346):
+//
+//   1. SW only: a forward local-alignment pass that finds the end cell, the
+//      first cell (database-row major) holding the maximum;
+//   2. SW only: a reverse pass from the end cell that finds the begin cell,
+//      the first cell (scanning rows and columns downwards) whose value
+//      reaches the score.  The reference resets its work rows only up to the
+//      database end index, so when the query end lies beyond it the reverse
+//      pass reads the forward pass's last-row values there; that is
+//      reproduced exactly;
+//   3. a direction pass over the matrix whose 4 flag bits collapse to the
+//      three observable traceback moves, stored here as 2 bits per cell in HBM;
+//   4. the walk from the end cell with the priority I > D > M.
+//
+// Each pass is a warp wavefront: lane k owns query rows [pass*256 + 8k, +8),
+// database columns stream through the warp, the bottom row of a lane goes to
+// the next lane by shuffle and the bottom row of a pass to a per-warp scratch
+// row in global memory.  All arithmetic is exact (int32, with the host
+// guaranteeing the range), matching the reference's int64 code.
+#include "device_common.cuh"
+
+#include <climits>
+
+namespace ssa {
+
+constexpr int TB_R = 8;
+constexpr int TB_ROWS = 32 * TB_R;
+
+__device__ __forceinline__ int32_t mget( const int64_t * m, int row, int col ) {
+    return (int32_t) m[(row << 5) + col];
+}
+
+// ---------------------------------------------------------------------------
+// 1. SW forward region pass (reference: src/algo/align.c:39-82).  The
+//    reference iterates database rows outer and query columns inner, scoring
+//    matrix[query][db]; the recurrence is symmetric, so the warp streams the
+//    database and keeps the query on lanes.  Key of the end cell: largest
+//    value, then smallest database index, then smallest query index.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__( 256 ) tb_forward_kernel( TbParams p ) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    int4 * scratch = p.scratch + (uint64_t) w * p.scratch_cols;
+    const int gO = p.gap_open, gE = p.gap_extend;
+    for( uint32_t h = w; h < p.n_hits; h += nwarps ) {
+        const TbHit hit = p.hits[h];
+        if( hit.algo != 0 )
+            continue;
+        const uint32_t A = p.qlen[hit.qslot];
+        const uint32_t B = p.db.lens[hit.id];
+        const uint8_t * a = p.qcodes + p.qoff[hit.qslot];
+        const uint8_t * b = p.db.codes + p.db.offsets[hit.id];
+        int32_t * lh = p.last_h + p.last_off[h];
+        int32_t * le = p.last_e + p.last_off[h];
+        const uint32_t passes = (A + TB_ROWS - 1) / TB_ROWS;
+        // best cell of this lane: value, db index, query index
+        int32_t best_v = 0;
+        int32_t best_i = INT_MAX, best_j = INT_MAX;
+        for( uint32_t pass = 0; pass < passes; pass++ ) {
+            const bool final_pass = (pass + 1 == passes);
+            const int32_t row0 = (int32_t) (pass * TB_ROWS + lane * TB_R);
+            const int nvalid = max( 0, min( TB_R, (int) A - row0 ) );
+            int32_t H[TB_R], E[TB_R];
+#pragma unroll
+            for( int r = 0; r < TB_R; r++ ) {
+                H[r] = 0;          // HH[j] = 0
+                E[r] = gO + gE;    // max(EE = gapO, HH + gapO) + gapE at row 0
+            }
+            int32_t diag = 0;
+            int32_t out_h = 0, out_f = 0;
+            for( uint32_t s = 0; s < B + 31; s++ ) {
+                int32_t up_h = __shfl_up_sync( 0xffffffffu, out_h, 1 );
+                int32_t up_f = __shfl_up_sync( 0xffffffffu, out_f, 1 );
+                const int32_t c = (int32_t) s - lane;
+                if( c < 0 || c >= (int32_t) B )
+                    continue;
+                if( lane == 0 ) {
+                    if( pass == 0 ) {
+                        up_h = 0;
+                        up_f = gO + gE;   // f starts at gapO: max(gapO, 0 + gapO) + gapE
+                    }
+                    else if( (uint32_t) c < p.scratch_cols ) {
+                        int4 v = scratch[c];
+                        up_h = v.x;
+                        up_f = v.y;
+                    }
+                }
+                int32_t f = up_f, hd = diag;
+                const int d = b[c];
+#pragma unroll
+                for( int r = 0; r < TB_R; r++ ) {
+                    if( r < nvalid ) {
+                        int32_t e_in = E[r];
+                        int32_t x = hd + mget( p.matrix, a[row0 + r], d );
+                        if( x < 0 )
+                            x = 0;
+                        if( f > x )
+                            x = f;
+                        if( e_in > x )
+                            x = e_in;
+                        if( c == (int32_t) B - 1 ) {
+                            lh[row0 + r] = x;
+                            le[row0 + r] = e_in;
+                        }
+                        if( x > best_v || (x == best_v && x > 0 && (c < best_i || (c == best_i && row0 + r < best_j))) ) {
+                            best_v = x;
+                            best_i = c;
+                            best_j = row0 + r;
+                        }
+                        hd = H[r];
+                        H[r] = x;
+                        f = max( f, x + gO ) + gE;
+                        E[r] = max( e_in, x + gO ) + gE;
+                    }
+                }
+                diag = up_h;
+                out_h = H[TB_R - 1];
+                out_f = f;
+                if( lane == 31 && !final_pass ) {
+                    if( (uint32_t) c < p.scratch_cols )
+                        scratch[c] = make_int4( out_h, out_f, 0, 0 );
+                    else
+                        atomicOr( p.error_flags, ERR_SCRATCH_OVERFLOW );
+                }
+            }
+            __syncwarp();
+        }
+        // reduce the best key over the warp
+        for( int o = 16; o > 0; o >>= 1 ) {
+            int32_t v = __shfl_xor_sync( 0xffffffffu, best_v, o );
+            int32_t bi = __shfl_xor_sync( 0xffffffffu, best_i, o );
+            int32_t bj = __shfl_xor_sync( 0xffffffffu, best_j, o );
+            if( v > best_v || (v == best_v && (bi < best_i || (bi == best_i && bj < best_j))) ) {
+                best_v = v;
+                best_i = bi;
+                best_j = bj;
+            }
+        }
+        if( lane == 0 ) {
+            TbRegion rg;
+            rg.fwd_score = best_v;
+            rg.a_end = best_j;
+            rg.b_end = best_i;
+            rg.a_begin = 0;
+            rg.b_begin = 0;
+            rg.status = (best_v > 0) ? 0 : 1;
+            p.regions[h] = rg;
+        }
+        __syncwarp();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// 2. SW reverse pass (reference: src/algo/align.c:84-131).  Both sequences
+//    are read backwards from the end cell: row j' = a_end - j, column
+//    i' = b_end - i.  The boundary row before column 0 is the reference's
+//    work row: -1 for query indices <= b_end, the forward pass's last row
+//    above that.  The begin cell is the first cell in (i' asc, j' asc) order
+//    whose value reaches the forward score.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__( 256 ) tb_reverse_kernel( TbParams p ) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    int4 * scratch = p.scratch + (uint64_t) w * p.scratch_cols;
+    const int gO = p.gap_open, gE = p.gap_extend;
+    for( uint32_t h = w; h < p.n_hits; h += nwarps ) {
+        const TbHit hit = p.hits[h];
+        if( hit.algo != 0 )
+            continue;
+        TbRegion rg = p.regions[h];
+        if( rg.status != 0 )
+            continue;
+        const int32_t score = rg.fwd_score;
+        const int32_t a_end = rg.a_end, b_end = rg.b_end;
+        const uint32_t A = (uint32_t) a_end + 1;     // rows j' = 0..a_end
+        const uint32_t B = (uint32_t) b_end + 1;     // cols i' = 0..b_end
+        const uint8_t * a = p.qcodes + p.qoff[hit.qslot];
+        const uint8_t * b = p.db.codes + p.db.offsets[hit.id];
+        const int32_t * lh = p.last_h + p.last_off[h];
+        const int32_t * le = p.last_e + p.last_off[h];
+        const uint32_t passes = (A + TB_ROWS - 1) / TB_ROWS;
+        int32_t hit_i = INT_MAX, hit_j = INT_MAX;   // first (i', j') reaching the score
+        for( uint32_t pass = 0; pass < passes; pass++ ) {
+            const bool final_pass = (pass + 1 == passes);
+            const int32_t row0 = (int32_t) (pass * TB_ROWS + lane * TB_R);
+            const int nvalid = max( 0, min( TB_R, (int) A - row0 ) );
+            int32_t H[TB_R], E[TB_R];
+#pragma unroll
+            for( int r = 0; r < TB_R; r++ ) {
+                const int32_t j = a_end - (row0 + r);     // query index
+                int32_t hh = -1, ee = -1;
+                if( r < nvalid && j > b_end ) {
+                    hh = lh[j];
+                    ee = le[j];
+                }
+                H[r] = hh;                                // HH(b_end + 1, j)
+                E[r] = max( ee, hh + gO ) + gE;           // EE(b_end, j)
+            }
+            // diagonal of the lane's first row at column 0: HH(b_end+1, j+1),
+            // or 0 for the end cell itself
+            int32_t diag;
+            {
+                const int32_t jprev = a_end - (row0 - 1);
+                if( row0 == 0 )
+                    diag = 0;
+                else
+                    diag = (jprev > b_end) ? lh[jprev] : -1;
+            }
+            int32_t out_h = 0, out_f = 0;
+            for( uint32_t s = 0; s < B + 31; s++ ) {
+                int32_t up_h = __shfl_up_sync( 0xffffffffu, out_h, 1 );
+                int32_t up_f = __shfl_up_sync( 0xffffffffu, out_f, 1 );
+                const int32_t c = (int32_t) s - lane;
+                if( c < 0 || c >= (int32_t) B )
+                    continue;
+                if( lane == 0 ) {
+                    if( pass == 0 ) {
+                        up_h = -1;                        // h starts at -1 per row
+                        up_f = max( -1, -1 + gO ) + gE;   // f = max(-1, h + gapO) + gapE
+                    }
+                    else if( (uint32_t) c < p.scratch_cols ) {
+                        int4 v = scratch[c];
+                        up_h = v.x;
+                        up_f = v.y;
+                    }
+                }
+                const int32_t i = b_end - c;              // database index
+                const int d = b[i];
+                int32_t f = up_f, hd = diag;              // lane 0 / pass 0: 0 at c == 0, then -1
+#pragma unroll
+                for( int r = 0; r < TB_R; r++ ) {
+                    if( r < nvalid ) {
+                        const int32_t j = a_end - (row0 + r);
+                        int32_t e_in = E[r];
+                        int32_t x = hd + mget( p.matrix, a[j], d );
+                        if( f > x )
+                            x = f;
+                        if( e_in > x )
+                            x = e_in;
+                        if( x >= score && (c < hit_i || (c == hit_i && row0 + r < hit_j)) ) {
+                            hit_i = c;
+                            hit_j = row0 + r;
+                        }
+                        hd = H[r];
+                        H[r] = x;
+                        f = max( f, x + gO ) + gE;
+                        E[r] = max( e_in, x + gO ) + gE;
+                    }
+                }
+                diag = up_h;
+                out_h = H[TB_R - 1];
+                out_f = f;
+                if( lane == 31 && !final_pass ) {
+                    if( (uint32_t) c < p.scratch_cols )
+                        scratch[c] = make_int4( out_h, out_f, 0, 0 );
+                    else
+                        atomicOr( p.error_flags, ERR_SCRATCH_OVERFLOW );
+                }
+            }
+            __syncwarp();
+        }
+        for( int o = 16; o > 0; o >>= 1 ) {
+            int32_t bi = __shfl_xor_sync( 0xffffffffu, hit_i, o );
+            int32_t bj = __shfl_xor_sync( 0xffffffffu, hit_j, o );
+            if( bi < hit_i || (bi == hit_i && bj < hit_j) ) {
+                hit_i = bi;
+                hit_j = bj;
+            }
+        }
+        if( lane == 0 ) {
+            if( hit_i == INT_MAX ) {
+                rg.status = 2;
+            }
+            else {
+                rg.b_begin = b_end - hit_i;
+                rg.a_begin = a_end - hit_j;
+            }
+            p.regions[h] = rg;
+        }
+        __syncwarp();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// 3. Direction pass (reference: src/algo/cigar.c:48-198).  Query rows on
+//    lanes, database columns streamed, exactly the reference orientation.
+//    Codes: 0 = M, 1 = D (UP|EXT_UP), 2 = I (LEFT|EXT_LEFT, takes priority).
+//    Stored for columns [b_begin, b_end] and all query rows of the lane, one
+//    16-bit word (8 rows x 2 bits) per lane and column.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__( 256 ) tb_directions_kernel( TbParams p ) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    int4 * scratch = p.scratch + (uint64_t) w * p.scratch_cols;
+    const int gO = p.gap_open, gE = p.gap_extend;
+    for( uint32_t h = w; h < p.n_hits; h += nwarps ) {
+        const TbHit hit = p.hits[h];
+        const TbRegion rg = p.regions[h];
+        if( rg.status != 0 )
+            continue;
+        const bool nw = hit.algo == 1;
+        const uint32_t A = (uint32_t) rg.a_end + 1;   // rows 0..a_end suffice
+        const uint32_t B = (uint32_t) rg.b_end + 1;   // columns 0..b_end
+        const uint32_t words = (A + TB_R - 1) / TB_R;
+        const uint8_t * a = p.qcodes + p.qoff[hit.qslot];
+        const uint8_t * b = p.db.codes + p.db.offsets[hit.id];
+        uint16_t * dir = p.dirs + p.dir_off[h];
+        const uint32_t passes = (A + TB_ROWS - 1) / TB_ROWS;
+        for( uint32_t pass = 0; pass < passes; pass++ ) {
+            const bool final_pass = (pass + 1 == passes);
+            const int32_t row0 = (int32_t) (pass * TB_ROWS + lane * TB_R);
+            const int nvalid = max( 0, min( TB_R, (int) A - row0 ) );
+            int32_t H[TB_R], E[TB_R];
+#pragma unroll
+            for( int r = 0; r < TB_R; r++ ) {
+                const int32_t i = row0 + r;
+                H[r] = nw ? gO + (i + 1) * gE : 0;
+                E[r] = nw ? 2 * gO + (i + 2) * gE : 0;
+            }
+            int32_t diag = nw ? ((row0 == 0) ? 0 : gO + row0 * gE) : 0;
+            int32_t out_h = 0, out_f = 0;
+            for( uint32_t s = 0; s < B + 31; s++ ) {
+                int32_t up_h = __shfl_up_sync( 0xffffffffu, out_h, 1 );
+                int32_t up_f = __shfl_up_sync( 0xffffffffu, out_f, 1 );
+                const int32_t j = (int32_t) s - lane;     // database index
+                if( j < 0 || j >= (int32_t) B )
+                    continue;
+                if( lane == 0 ) {
+                    if( pass == 0 ) {
+                        // H(-1, j) is the next column's row-0 diagonal
+                        up_h = nw ? gO + (j + 1) * gE : 0;
+                        up_f = nw ? 2 * gO + (j + 2) * gE : 0;
+                    }
+                    else if( (uint32_t) j < p.scratch_cols ) {
+                        int4 v = scratch[j];
+                        up_h = v.x;
+                        up_f = v.y;
+                    }
+                }
+                const int d = b[j];
+                int32_t f = up_f, hd = diag;
+                uint32_t code = 0;
+#pragma unroll
+                for( int r = 0; r < TB_R; r++ ) {
+                    if( r < nvalid ) {
+                        int32_t e = E[r];
+                        int32_t x = hd + mget( p.matrix, d, a[row0 + r] );
+                        unsigned flags = 0;
+                        if( f > x ) {
+                            flags |= 1u;     // UP
+                            x = f;
+                        }
+                        if( e > x ) {
+                            x = e;
+                            flags |= 2u;     // LEFT
+                        }
+                        if( !nw && x < 0 )
+                            x = 0;
+                        hd = H[r];
+                        H[r] = x;
+                        int32_t y = x + gO + gE;
+                        e += gE;
+                        f += gE;
+                        if( f > y )
+                            flags |= 4u;     // EXT_UP
+                        else
+                            f = y;
+                        if( e > y )
+                            flags |= 8u;     // EXT_LEFT
+                        else
+                            e = y;
+                        E[r] = e;
+                        const uint32_t op = (flags & 10u) ? 2u : ((flags & 5u) ? 1u : 0u);
+                        code |= op << (2 * r);
+                    }
+                }
+                diag = up_h;
+                out_h = H[TB_R - 1];
+                out_f = f;
+                if( j >= rg.b_begin && (uint32_t) (row0 / TB_R) < words )
+                    dir[(uint64_t) (j - rg.b_begin) * words + row0 / TB_R] = (uint16_t) code;
+                if( lane == 31 && !final_pass ) {
+                    if( (uint32_t) j < p.scratch_cols )
+                        scratch[j] = make_int4( out_h, out_f, 0, 0 );
+                    else
+                        atomicOr( p.error_flags, ERR_SCRATCH_OVERFLOW );
+                }
+            }
+            __syncwarp();
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// 4. Walk (reference: src/algo/cigar.c:300-334): one thread per hit writes the
+//    moves in traceback order (end to begin); the host run-length encodes.
+// ---------------------------------------------------------------------------
+__global__ void tb_walk_kernel( TbParams p ) {
+    const uint32_t h = blockIdx.x * blockDim.x + threadIdx.x;
+    if( h >= p.n_hits )
+        return;
+    const TbRegion rg = p.regions[h];
+    if( rg.status != 0 ) {
+        p.ops_len[h] = 0;
+        return;
+    }
+    const uint32_t words = ((uint32_t) rg.a_end + 1 + TB_R - 1) / TB_R;
+    const uint16_t * dir = p.dirs + p.dir_off[h];
+    char * out = p.ops + p.ops_off[h];
+    const uint64_t cap = p.ops_off[h + 1] - p.ops_off[h];
+    int64_t i = rg.a_end, j = rg.b_end;
+    uint64_t n = 0;
+    while( i >= rg.a_begin && j >= rg.b_begin && i >= 0 && j >= 0 ) {
+        const uint32_t word = dir[(uint64_t) (j - rg.b_begin) * words + (uint64_t) (i / TB_R)];
+        const uint32_t op = (word >> (2 * (i % TB_R))) & 3u;
+        char ch;
+        if( op == 2u ) {
+            j--;
+            ch = 'I';
+        }
+        else if( op == 1u ) {
+            i--;
+            ch = 'D';
+        }
+        else {
+            i--;
+            j--;
+            ch = 'M';
+        }
+        if( n < cap )
+            out[n] = ch;
+        n++;
+    }
+    p.ops_len[h] = (uint32_t) n;
+}
+
+cudaError_t launch_traceback( const TbParams & p, bool any_sw, int grid, cudaStream_t st ) {
+    if( p.n_hits == 0 )
+        return cudaSuccess;
+    if( any_sw ) {
+        tb_forward_kernel<<<grid, 256, 0, st>>>( p );
+        tb_reverse_kernel<<<grid, 256, 0, st>>>( p );
+    }
+    tb_directions_kernel<<<grid, 256, 0, st>>>( p );
+    tb_walk_kernel<<<(p.n_hits + 127) / 128, 128, 0, st>>>( p );
+    return cudaGetLastError();
+}
+
+}  // namespace ssa

@@ -1,0 +1,158 @@
+"""Generates the golden fixtures under tests/golden/ from the reference itself.
+
+    python tests/golden/make_golden.py [--reference /root/reference]
+
+Needs the reference sources (to build oracle/_ref/ref_run and to copy the FASTA
+fixtures of its own test suite).  Writes:
+
+* ``data/*``        -- the reference test-suite files the known-answer tests
+  read (copied unchanged from the reference's tests/testdata/);
+* ``matrices.json`` -- the reference's 32x32 score tables of every built-in
+  matrix, of constant scoring and of the file matrices in data/;
+* ``cases.json``    -- seeded synthetic search cases (inputs stored inline, or
+  regenerated from libssa_b200.workloads with the stored seed and checked by
+  hash) with the reference's complete answer: hit IDs, scores, CIGARs,
+  coordinates and overflow counts, at the 1-thread AVX2 or SSE settings.
+"""
+from __future__ import annotations
+
+import argparse
+import hashlib
+import json
+import os
+import shutil
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+import oracle  # noqa: E402
+from libssa_b200 import workloads as W  # noqa: E402
+
+DATA_FILES = ["AF091148.fas", "one_seq.fas", "NP_009305.1.fas", "test.fas", "short_db.fas", "tmp.fas",
+              "short_AA.fas", "short_nuc_db.fas", "blosum90.txt", "nuc_scoring_matrix.txt", "test_16_seq.fas",
+              "AF091148_selection.fas", "one_seq_db.fas", "test2.fas"]
+
+BUILTINS = ["blosum45", "blosum50", "blosum62", "blosum80", "blosum90", "pam30", "pam70", "pam250"]
+
+
+def digest(queries: list[bytes], flat: np.ndarray, offsets: np.ndarray) -> str:
+    h = hashlib.sha256()
+    for q in queries:
+        h.update(q + b"\0")
+    h.update(np.ascontiguousarray(offsets, dtype=np.uint64).tobytes())
+    h.update(np.ascontiguousarray(flat, dtype=np.uint8).tobytes())
+    return h.hexdigest()
+
+
+def run_case(case: dict, queries: list[bytes], records: list[bytes], tmp: str) -> list[dict]:
+    db = os.path.join(tmp, "db.sdb")
+    oracle.write_sdb(db, seqs=records)
+    return oracle.run_reference(db, [q.decode() for q in queries], algo=case["algo"], width=case["width"],
+                                align=case["align"], hits=case["hits"], symtype=case["symtype"],
+                                matrix=case["matrix"], gap=tuple(case["gap"]), chunk=case["chunk"],
+                                simd=case["simd"])
+
+
+def synthetic_cases() -> list[tuple[dict, list[bytes], list[bytes], bool]]:
+    """(case, queries, records, store_inline)."""
+    out = []
+    # config-shaped cases
+    w = W.sw_plain(seed=1, scale=1.0)
+    out.append(({"name": "sw_plain_full", "workload": "sw_plain", "seed": 1, "scale": 1.0}, w, False))
+    w = W.sw_plain(seed=11, scale=0.2)
+    out.append(({"name": "sw_plain_small", "workload": "sw_plain", "seed": 11, "scale": 0.2}, w, False))
+    w = W.nw_nucleotide(seed=12, scale=0.005, n_queries=4)
+    out.append(({"name": "nw_nucleotide_small", "workload": "nw_nucleotide", "seed": 12, "scale": 0.005,
+                 "n_queries": 4}, w, False))
+    w = W.sw_batched(seed=13, scale=0.004, n_queries=1024, n_db=500_000)
+    out.append(({"name": "sw_batched_small", "workload": "sw_batched", "seed": 13, "scale": 0.004}, w, False))
+    cases = []
+    for meta, w, inline in out:
+        case = dict(meta)
+        case.update({"algo": w.algo, "width": w.bit_width, "align": 1, "hits": w.hitcount, "symtype": w.symtype,
+                     "matrix": w.matrix, "gap": list(w.gap), "chunk": 1000, "simd": 2})
+        case["digest"] = digest(w.queries, w.db_flat, w.db_offsets)
+        cases.append((case, w.queries, w.db_records(), inline))
+
+    # tie- and overflow-heavy small cases across widths, schedules and chunking
+    rng = np.random.default_rng(2024)
+    k = 0
+    for algo in ("sw", "nw"):
+        for width in (8, 16, 64):
+            for simd in (2, 1):
+                if width == 8 and simd == 0:
+                    continue
+                nuc = bool(k % 2)
+                alpha = W.NT4 if nuc else W.AA20
+                qlen = int(rng.integers(20, 300))
+                q = W.random_residues(rng, qlen, alpha)
+                recs = []
+                for i in range(int(rng.integers(60, 400))):
+                    r = rng.random()
+                    if r < 0.15:
+                        recs.append(W.mutate(rng, q, alpha, 0.05, 0.02, (1, 4)))
+                    elif r < 0.2:
+                        recs.append(W.mutate(rng, np.tile(q, 3), alpha, 0.01, 0.0, (1, 1)))
+                    elif r < 0.22:
+                        recs.append(np.zeros(0, np.uint8))
+                    else:
+                        recs.append(W.random_residues(rng, int(rng.integers(1, 400)), alpha))
+                if nuc:
+                    matrix = "const:%d,%d" % (int(rng.integers(1, 6)), -int(rng.integers(1, 6)))
+                else:
+                    matrix = "builtin:" + ["blosum62", "blosum50", "pam250", "blosum90"][k % 4]
+                case = {"name": f"mixed_{algo}_{width}_{simd}", "algo": algo, "width": width, "align": 1,
+                        "hits": int(rng.integers(3, 15)), "symtype": 0 if nuc else 1, "matrix": matrix,
+                        "gap": [-int(rng.integers(1, 13)), -int(rng.integers(1, 3))],
+                        "chunk": int([1000, 50, 17, 1][k % 4]), "simd": simd}
+                recs_b = [r.tobytes() for r in recs]
+                case["digest"] = digest([q.tobytes()], np.frombuffer(b"".join(recs_b), np.uint8),
+                                        np.concatenate([[0], np.cumsum([len(r) for r in recs_b])]).astype(np.uint64))
+                cases.append((case, [q.tobytes()], recs_b, True))
+                k += 1
+    return cases
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reference", default="/root/reference")
+    args = ap.parse_args()
+    oracle.build(args.reference)
+    data = os.path.join(HERE, "data")
+    os.makedirs(data, exist_ok=True)
+    for f in DATA_FILES:
+        shutil.copyfile(os.path.join(args.reference, "tests", "testdata", f), os.path.join(data, f))
+
+    mats = {name: oracle.reference_matrix("builtin:" + name).tolist() for name in BUILTINS}
+    mats["const:5,-4"] = oracle.reference_matrix("const:5,-4").tolist()
+    mats["const:127,-128"] = oracle.reference_matrix("const:127,-128").tolist()
+    mats["file:blosum90.txt"] = oracle.reference_matrix("file:" + os.path.join(data, "blosum90.txt")).tolist()
+    mats["file:nuc_scoring_matrix.txt"] = oracle.reference_matrix(
+        "file:" + os.path.join(data, "nuc_scoring_matrix.txt")).tolist()
+    with open(os.path.join(HERE, "matrices.json"), "w") as f:
+        json.dump(mats, f)
+
+    import tempfile
+    out = []
+    with tempfile.TemporaryDirectory() as tmp:
+        for case, queries, records, inline in synthetic_cases():
+            res = run_case(case, queries, records, tmp)
+            case = dict(case)
+            case["expected"] = [{"ovf8": r["ovf8"], "ovf16": r["ovf16"],
+                                 "hits": [[h["id"], h["score"], h["cigar"], h["q_start"], h["q_end"], h["d_start"],
+                                           h["d_end"]] for h in r["hits"]]} for r in res]
+            if inline:
+                case["queries"] = [q.decode() for q in queries]
+                case["records"] = [r.decode() for r in records]
+            out.append(case)
+            print(case["name"], "queries", len(queries), "records", len(records))
+    with open(os.path.join(HERE, "cases.json"), "w") as f:
+        json.dump(out, f, indent=0)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,111 @@
+"""Parity of the GPU build with the reference, through the public C-ABI.
+
+Bit-exact: hit IDs, scores, order (ties included), CIGAR strings, coordinates
+and the 8->16 / 16->64 overflow counters.  Ground truth comes from the
+reference's own known-answer tests, from golden runs of the reference binary
+(tests/golden/cases.json) and from the oracle restatement on seeded inputs.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from helpers import DATA, case_inputs, first_fasta_sequence, golden_cases, oracle_search, product_search, \
+    product_setup, read_fasta
+from kats import KATS, matches
+from libssa_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def _query(kat):
+    kind, val = kat["query"]
+    return (first_fasta_sequence(os.path.join(DATA, val)) if kind == "file" else val).encode()
+
+
+@pytest.mark.parametrize("kat", KATS, ids=[k["source"] for k in KATS])
+def test_reference_kats(built_library, kat):
+    product_setup(kat["symtype"], kat["matrix"], kat["gap"], kat["chunk"], 2,
+                  db_file=os.path.join(DATA, kat["db"]))
+    q = _query(kat)
+    for algo, width, align, hits, simd, expected in kat["calls"]:
+        import libssa_b200 as L
+        L.set_simd_compute_mode(simd)
+        res, ovf = product_search(algo, width, align, hits, [q])
+        got = [(r[1], r[0], r[2]) for r in res[0]]
+        assert matches(expected, got, ovf[0]), (kat["source"], algo, width, simd, got, ovf)
+
+
+@pytest.mark.parametrize("case", golden_cases(), ids=[c["name"] for c in golden_cases()])
+def test_golden_reference_runs(built_library, case):
+    queries, records = case_inputs(case)
+    product_setup(case["symtype"], case["matrix"], tuple(case["gap"]), case["chunk"], case["simd"], records=records)
+    res, ovf = product_search(case["algo"], case["width"], case["align"], case["hits"], queries)
+    for qi in range(len(queries)):
+        exp = case["expected"][qi]
+        assert [list(r) for r in res[qi]] == exp["hits"], (case["name"], qi)
+        assert list(ovf[qi]) == [exp["ovf8"], exp["ovf16"]], (case["name"], qi)
+
+
+def test_batched_equals_single(built_library):
+    """Each query's result is the same alone and inside a batch."""
+    case = [c for c in golden_cases() if c["name"] == "sw_batched_small"][0]
+    queries, records = case_inputs(case)
+    product_setup(case["symtype"], case["matrix"], tuple(case["gap"]), case["chunk"], case["simd"], records=records)
+    single, _ = product_search(case["algo"], case["width"], 1, case["hits"], queries)
+    batched, _ = product_search(case["algo"], case["width"], 1, case["hits"], queries, batch=True)
+    assert single == batched
+    for qi in range(len(queries)):
+        assert [list(r) for r in batched[qi]] == case["expected"][qi]["hits"]
+
+
+def _random_case(seed):
+    rng = np.random.default_rng(seed)
+    nuc = bool(rng.random() < 0.4)
+    alpha = W.NT4 if nuc else W.AA20
+    q = W.random_residues(rng, int(rng.integers(1, 600)), alpha)
+    recs = []
+    for _ in range(int(rng.integers(1, 300))):
+        r = rng.random()
+        if r < 0.15:
+            recs.append(W.mutate(rng, q, alpha, 0.05, 0.02, (1, 5)).tobytes())
+        elif r < 0.18:
+            recs.append(W.mutate(rng, np.tile(q, int(rng.integers(2, 5))), alpha, 0.01, 0.0, (1, 1)).tobytes())
+        else:
+            recs.append(W.random_residues(rng, int(rng.integers(1, 700)), alpha).tobytes())
+    if nuc:
+        matrix = ("const", int(rng.integers(1, 8)), -int(rng.integers(1, 8)))
+    else:
+        matrix = ("builtin", ["blosum62", "blosum45", "pam30", "pam250", "blosum80"][int(rng.integers(0, 5))])
+    gap = (-int(rng.integers(0, 20)), -int(rng.integers(0, 4)))
+    return dict(algo=["sw", "nw"][int(rng.integers(0, 2))], width=int([8, 16, 64][int(rng.integers(0, 3))]),
+                align=1, hits=int(rng.integers(1, 20)), symtype=0 if nuc else 1, matrix=matrix, gap=gap,
+                chunk=int([1000, 64, 7][int(rng.integers(0, 3))]), simd=int([2, 1][int(rng.integers(0, 2))]),
+                query=q.tobytes(), records=recs)
+
+
+@pytest.mark.parametrize("seed", range(40))
+def test_random_against_oracle(built_library, seed):
+    c = _random_case(seed)
+    product_setup(c["symtype"], c["matrix"], c["gap"], c["chunk"], c["simd"], records=c["records"])
+    res, ovf = product_search(c["algo"], c["width"], c["align"], c["hits"], [c["query"]])
+    exp, eovf = oracle_search(c["algo"], c["width"], c["align"], c["hits"], c["symtype"], c["matrix"], c["gap"],
+                              c["chunk"], c["simd"], c["query"], c["records"])
+    assert res[0] == exp
+    assert tuple(ovf[0]) == tuple(eovf)
+
+
+def test_long_query_multi_pass(built_library):
+    """Queries longer than one 256-row pass and sequences with 8- and 16-bit
+    overflow, SW and NW, against the oracle."""
+    rng = np.random.default_rng(5)
+    q = W.random_residues(rng, 900, W.AA20)
+    recs = [W.mutate(rng, q, W.AA20, 0.02, 0.01, (1, 3)).tobytes() for _ in range(3)]
+    recs += [W.random_residues(rng, int(rng.integers(50, 1500)), W.AA20).tobytes() for _ in range(40)]
+    for algo, width in (("sw", 8), ("sw", 16), ("nw", 16), ("nw", 8)):
+        product_setup(1, ("builtin", "blosum62"), (-11, -1), 1000, 2, records=recs)
+        res, ovf = product_search(algo, width, 1, 8, [q.tobytes()])
+        exp, eovf = oracle_search(algo, width, 1, 8, 1, ("builtin", "blosum62"), (-11, -1), 1000, 2, q.tobytes(),
+                                  recs)
+        assert res[0] == exp, (algo, width)
+        assert tuple(ovf[0]) == tuple(eovf), (algo, width)
