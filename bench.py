@@ -1,0 +1,333 @@
+"""Benchmark of the libssa B200 build on the batched Smith-Waterman workload.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--scale S]
+
+Workload (``sw_batched``, synthetic, seeded): 1,024 protein queries with
+lognormal(median 300, sigma 0.7) lengths clipped to [30, 5000] against a
+500,000-sequence database (gamma(2, mean 350) lengths clipped to [20, 35000],
+1% near-identical 8,000-35,000 residue copies of a query); BLOSUM62, gaps
+11/1, 8-bit cascade entry, top 10 hits with CIGAR.  One step is one batched
+search of all 1,024 queries through ``ssa_align_batch`` (COMPUTE_ALIGNMENT).
+
+Metric: GCUPS = sum over queries of query length x database residues / time.
+* ``value``: device time of the search kernels (entry pass, overflow passes,
+  traceback; CUDA events on the library's streams), database resident in HBM;
+* ``e2e``: wall time of the public C-ABI call with host buffers (query upload,
+  result download, host schedule/heap replay and list building included);
+* ``roofline``: the entry-pass kernel against the measured packed-16x2
+  integer peak of the same device (9 lane operations per cell);
+* ``cpu_baseline``: the reference libssa (built from its sources into
+  oracle/_ref) on the host cores, on a sample of the same workload.
+
+With N > 1 (torchrun) every rank searches its own seeded 1,024-query batch
+against the full database (weak scaling, no collective on the data path);
+``value`` is all ranks' cells over the slowest rank's time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "GCUPS (batched SW search, 1,024 queries vs 500k sequences, top 10 with CIGAR)"
+ALGO_OPS_PER_CELL = 9          # 4 saturating adds + 5 maxes of the reference's ALIGNCORE
+
+
+# --------------------------------------------------------------------------
+# helpers
+# --------------------------------------------------------------------------
+class ClockSampler:
+    """Samples nvidia-smi SM clocks and throttle reasons while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=5)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    return world, rank, local, pg
+
+
+def reduce_max(pg, x: float) -> float:
+    if pg is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def reduce_sum(pg, x: float) -> float:
+    if pg is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    pg.all_reduce(t, op=pg.ReduceOp.SUM)
+    return float(t.item())
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+def make_workload(scale: float, query_seed: int):
+    from libssa_b200 import workloads as W
+    w = W.sw_batched(seed=3, scale=scale)
+    if query_seed != 3:
+        # a rank's own query batch of the same length distribution
+        import numpy as np
+        rng = np.random.default_rng(1000 + query_seed)
+        lens = W.lognormal_lengths(rng, len(w.queries), 300.0, 0.7)
+        w.queries = [W.random_residues(rng, int(L), W.AA20).tobytes() for L in lens]
+    return w
+
+
+def load_traffic() -> float | None:
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f).get("entry_pass_dram_bytes_per_cell")
+    except (OSError, ValueError):
+        return None
+
+
+# --------------------------------------------------------------------------
+# CPU baseline: the reference built from its sources (oracle/_ref/ref_run)
+# --------------------------------------------------------------------------
+def reference_sample(w, n_queries: int, threads: int, repeat: int = 1) -> tuple[float, float, str]:
+    """(GCUPS, seconds, description) of the reference on a query sample."""
+    import oracle
+    if not oracle.reference_available():
+        raise RuntimeError("oracle/_ref/ref_run is not built")
+    import numpy as np
+    lens = np.array([len(q) for q in w.queries])
+    # a representative sample: queries at evenly spaced length quantiles
+    order = np.argsort(lens)
+    pick = [int(order[int((i + 0.5) * len(order) / n_queries)]) for i in range(n_queries)]
+    qs = [w.queries[i].decode() for i in pick]
+    with tempfile.TemporaryDirectory() as td:
+        db = os.path.join(td, "db.sdb")
+        oracle.write_sdb(db, flat=w.db_flat, lengths=np.diff(w.db_offsets))
+        res = oracle.run_reference(db, qs, algo="sw", width=8, align=1, hits=10, symtype=1,
+                                   matrix="builtin:blosum62", gap=(-11, -1), chunk=1000, threads=threads, simd=2,
+                                   timing=True, repeat=repeat)
+    residues = int(w.db_offsets[-1])
+    secs = sum(r["seconds"] for r in res)
+    cells = sum(len(q) for q in qs) * residues
+    desc = (f"{n_queries} queries (lengths {sorted(len(q) for q in qs)}) of the workload vs the full "
+            f"{w.n_db}-sequence database, sw_align COMPUTE_ALIGNMENT, 8-bit entry, AVX2, {threads} threads")
+    return cells / secs / 1e9, secs, desc
+
+
+def run_reference_arm(args):
+    world, rank, local, pg = dist_setup()
+    if rank != 0:
+        return 0
+    w = make_workload(args.scale, 3)
+    threads = os.cpu_count() or 1
+    vals = []
+    desc = ""
+    for i in range(args.warmup + args.steps):
+        g, secs, desc = reference_sample(w, args.ref_queries, threads)
+        if i >= args.warmup:
+            vals.append((g, secs))
+    value = statistics.median(v[0] for v in vals)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": "GCUPS", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(1e3 * statistics.median(v[1] for v in vals), 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int8/int16/int64", "data": "synthetic (seeded)",
+        "config": {"workload": "sw_batched", "queries": len(w.queries), "db_sequences": w.n_db,
+                   "db_residues": int(w.db_offsets[-1]), "scale": args.scale},
+        "cpu_baseline": {"value": round(value, 3), "unit": "GCUPS", "cores": threads, "kind": "reference",
+                         "sample": desc},
+        "e2e": {"value": round(value, 3), "unit": "GCUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# --------------------------------------------------------------------------
+# the B200 arm
+# --------------------------------------------------------------------------
+def run_ours(args):
+    world, rank, local, pg = dist_setup()
+    os.environ["SSA_B200_DEVICE"] = str(local)
+    import libssa_b200 as L
+    if not L.libraries_built():
+        from libssa_b200 import build
+        build.build()
+    L.load()
+    w = make_workload(args.scale, 3 if rank == 0 else 3 + rank)
+    L.set_output_mode(L.OUTPUT_SILENT)
+    L.init_symbol_translation(L.AMINOACID, L.FORWARD_STRAND, 1, 1)
+    L.init_score_matrix(L.MATRIX_BUILDIN, "blosum62")
+    L.init_gap_penalties(-11, -1)
+    L.set_chunk_size(1000)
+    L.set_simd_compute_mode(L.COMPUTE_ON_AVX2)
+    L.load_db_memory(flat=w.db_flat, offsets=w.db_offsets)
+    qs = [L.init_sequence_fasta(L.READ_FROM_STRING, q.decode()) for q in w.queries]
+    cells = sum(len(q) for q in w.queries) * int(w.db_offsets[-1])
+
+    def step():
+        return L.align_batch(L.SSA_SMITH_WATERMAN, qs, 10, L.BIT_WIDTH_8, L.COMPUTE_ALIGNMENT)
+
+    for _ in range(args.warmup):
+        step()
+    peak_lane_ops, peak_ipc = L.int_peak()
+    barrier(pg)
+    launches0 = L.stats().kernel_launches_total
+    sampler = ClockSampler(local)
+    sampler.start()
+    wall, dev, entry, h2d, d2h = [], [], [], [], []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        step()
+        wall.append(time.perf_counter() - t0)
+        st = L.stats()
+        dev.append(st.kernel_seconds)
+        entry.append(st.entry_seconds)
+        h2d.append(st.h2d_bytes)
+        d2h.append(st.d2h_bytes)
+    clocks = sampler.stop()
+    launches = L.stats().kernel_launches_total - launches0
+    barrier(pg)
+    t_wall = reduce_max(pg, sum(wall))
+    t_dev = reduce_max(pg, sum(dev))
+    total_cells = reduce_sum(pg, float(cells)) * args.steps
+    value = total_cells / t_dev / 1e9
+    e2e = total_cells / t_wall / 1e9
+
+    if rank != 0:
+        return 0
+    # roofline of the entry pass: algorithmic lane operations per launch over
+    # its device time
+    t_entry = statistics.median(entry)
+    achieved = cells * ALGO_OPS_PER_CELL / t_entry / 1e12
+    peak = peak_lane_ops / 1e12
+    traffic_per_cell = load_traffic()
+    line = {
+        "metric": METRIC, "value": round(value, 2), "unit": "GCUPS", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(1e3 * t_dev / args.steps, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int16x2 (8-bit lane semantics), int32",
+        "data": "synthetic (seeded, BASELINE config 3 shapes)",
+        "config": {"workload": "sw_batched", "queries_per_gpu": len(w.queries), "db_sequences": w.n_db,
+                   "db_residues": int(w.db_offsets[-1]), "cells_per_step_per_gpu": cells,
+                   "matrix": "blosum62", "gap": [-11, -1], "bit_width": 8, "hits": 10,
+                   "align_type": "COMPUTE_ALIGNMENT", "scale": args.scale,
+                   "l2": "inputs larger than L2 (database codes %.2f GB)" % (int(w.db_offsets[-1]) / 1e9),
+                   "parallelism": f"{world} x independent query batch vs full database"},
+        "e2e": {"value": round(e2e, 2), "unit": "GCUPS", "h2d_bytes_per_step": int(statistics.median(h2d)),
+                "d2h_bytes_per_step": int(statistics.median(d2h))},
+        "roofline": {"bound": "int", "achieved": round(achieved, 3), "peak": round(peak, 3),
+                     "unit": "Tlaneop/s", "frac": round(achieved / peak, 4),
+                     "traffic": (round(traffic_per_cell * cells) if traffic_per_cell else None),
+                     "kernel": "sw_fast_kernel (entry pass)",
+                     "peak_source": "measured packed 16x2 max throughput on this device "
+                                    f"({peak_ipc:.2f} warp-inst/clk/SM), 9 lane ops per cell"},
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+        "timing": {"device_seconds": round(t_dev, 4), "wall_seconds": round(t_wall, 4),
+                   "entry_seconds_median": round(t_entry, 4)},
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        try:
+            g, secs, desc = reference_sample(w, args.ref_queries, os.cpu_count() or 1)
+            line["cpu_baseline"] = {"value": round(g, 3), "unit": "GCUPS", "cores": os.cpu_count() or 1,
+                                    "kind": "reference", "sample": desc}
+        except Exception as e:  # noqa: BLE001
+            line["cpu_baseline"] = {"value": None, "unit": "GCUPS", "cores": os.cpu_count() or 1,
+                                    "kind": "reference", "sample": f"unavailable: {e}"}
+    print(json.dumps(line), flush=True)
+    for q in qs:
+        L.free_sequence(q)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--scale", type=float, default=1.0, help="database and query count scale (1.0 = full)")
+    ap.add_argument("--ref-queries", type=int, default=4, help="queries in the reference CPU sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        sys.exit(run_reference_arm(args))
+    sys.exit(run_ours(args))
+
+
+if __name__ == "__main__":
+    main()

@@ -37,11 +37,21 @@ typedef struct {
     uint64_t overflow_8_to_16;       /* sequences re-aligned at 16 bit */
     uint64_t overflow_16_to_64;      /* sequences re-aligned at 64 bit */
     uint64_t cells;                  /* sum over queries of query length x database residues */
-    double gpu_seconds;              /* device time of the last call */
+    double gpu_seconds;              /* wall time of the last call's device pipeline, host replay included */
     uint64_t kernel_launches_total;  /* kernels launched by this process so far */
+    double entry_seconds;            /* device time of the entry pass (all database pairs) */
+    double kernel_seconds;           /* device time of entry pass, overflow passes and traceback */
+    uint64_t h2d_bytes;              /* host-to-device bytes of the last call */
+    uint64_t d2h_bytes;              /* device-to-host bytes of the last call */
 } ssa_stats_t;
 
 void ssa_get_stats( ssa_stats_t * out );
+
+/* Measured packed-16x2 integer max throughput of the current device, in
+ * lane operations per second (2 per instruction and thread), and the same as
+ * warp instructions per clock per SM.  The denominator of the search kernels'
+ * integer-pipe roofline.  Returns 0 on success. */
+int ssa_b200_int_peak( double * lane_ops_per_second, double * instructions_per_clock_per_sm );
 
 /* Marks the packed copy of the database stale, so the next search reads it
  * again through the plugin.  init_db() does this itself; call it after

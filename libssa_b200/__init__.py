@@ -36,7 +36,7 @@ EXPORTED = [
     "set_output_mode", "set_simd_compute_mode", "set_chunk_size", "set_thread_count", "init_score_matrix",
     "init_constant_scores", "init_gap_penalties", "init_symbol_translation", "init_db", "init_sequence_fasta",
     "free_sequence", "sw_align", "nw_align", "free_alignment", "ssa_exit", "ssa_align_batch", "ssa_get_stats",
-    "ssa_query_length", "ssa_db_refresh",
+    "ssa_query_length", "ssa_db_refresh", "ssa_b200_int_peak",
 ]
 
 
@@ -64,7 +64,8 @@ class AlignmentList(ctypes.Structure):
 class Stats(ctypes.Structure):
     _fields_ = [("overflow_8_to_16", ctypes.c_uint64), ("overflow_16_to_64", ctypes.c_uint64),
                 ("cells", ctypes.c_uint64), ("gpu_seconds", ctypes.c_double),
-                ("kernel_launches_total", ctypes.c_uint64)]
+                ("kernel_launches_total", ctypes.c_uint64), ("entry_seconds", ctypes.c_double),
+                ("kernel_seconds", ctypes.c_double), ("h2d_bytes", ctypes.c_uint64), ("d2h_bytes", ctypes.c_uint64)]
 
 
 P_LIST = ctypes.POINTER(AlignmentList)
@@ -110,6 +111,8 @@ def load():
     lib.ssa_align_batch.restype = ctypes.c_int
     lib.ssa_get_stats.argtypes = [ctypes.POINTER(Stats)]
     lib.ssa_db_refresh.argtypes = []
+    lib.ssa_b200_int_peak.argtypes = [ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
+    lib.ssa_b200_int_peak.restype = ctypes.c_int
     lib.ssa_query_length.argtypes = [ctypes.c_void_p]
     lib.ssa_query_length.restype = ctypes.c_size_t
     _plugin.ssa_db_b200_load_memory.argtypes = [ctypes.c_size_t, ctypes.c_char_p, ctypes.POINTER(ctypes.c_uint64)]
@@ -242,6 +245,15 @@ def stats() -> Stats:
     s = Stats()
     load().ssa_get_stats(ctypes.byref(s))
     return s
+
+
+def int_peak() -> tuple[float, float]:
+    """(lane operations per second, warp instructions per clock per SM) of
+    packed 16x2 max on the current device."""
+    a, b = ctypes.c_double(0), ctypes.c_double(0)
+    if load().ssa_b200_int_peak(ctypes.byref(a), ctypes.byref(b)) != 0:
+        raise RuntimeError("integer peak probe failed")
+    return a.value, b.value
 
 
 def query_length(q) -> int:

@@ -561,6 +561,10 @@ void ssa_get_stats( ssa_stats_t * out ) {
     out->cells = g_last_stats.cells;
     out->gpu_seconds = g_last_stats.seconds_gpu;
     out->kernel_launches_total = engine_kernel_launches();
+    out->entry_seconds = g_last_stats.entry_seconds;
+    out->kernel_seconds = g_last_stats.kernel_seconds;
+    out->h2d_bytes = g_last_stats.h2d_bytes;
+    out->d2h_bytes = g_last_stats.d2h_bytes;
 }
 
 void ssa_db_refresh( void ) {

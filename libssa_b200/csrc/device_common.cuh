@@ -122,14 +122,6 @@ cudaError_t launch_traceback( const TbParams & p, bool any_sw, int grid, cudaStr
 // its profile row is -128, so it never changes a Smith-Waterman maximum.
 constexpr uint32_t FAST_PAD_CODE = 31;
 
-// Work item: one query slot against a range of database pairs.
-struct FastItem {
-    uint32_t slot;
-    uint32_t pair_begin;
-    uint32_t pair_end;
-    uint32_t pad_;
-};
-
 struct FastParams {
     const uint8_t * pair_res;     // per pair: cols x (residue A, residue B)
     const uint64_t * pair_off;    // byte offset of each pair (16-aligned)
@@ -137,21 +129,28 @@ struct FastParams {
     const uint2 * pair_ids;       // database IDs (B = 0xffffffff when absent)
     const int8_t * prof8;         // per slot: 32 x rows int8 scores
     const uint64_t * prof8_off;   // per slot, bytes
-    uint32_t rows;                // profile rows of this launch's queries (passes x G x R)
-    uint32_t passes;
-    const FastItem * items;
-    uint32_t n_items;
-    unsigned * item_counter;
+    const uint16_t * slot_group;  // per slot: threads per pair G
+    const uint32_t * slot_rows;   // per slot: profile rows (passes x G x R)
+    // work units u = chunk * n_class + i: slot unit_slots[i] against pairs
+    // [chunk_bounds[chunk], chunk_bounds[chunk + 1])
+    const uint32_t * unit_slots;
+    uint32_t n_class;
+    const uint32_t * chunk_bounds;
+    uint64_t n_units;
+    unsigned long long * unit_counter;
     int gap_oe;                   // (int8) (gapO + gapE)
     int gap_e;
     PassSink sink;
-    int4 * scratch;               // per group: scratch_cols entries
+    int4 * scratch;               // per warp and group slot (4 per warp): scratch_cols entries
     uint32_t scratch_cols;
+    uint32_t slice_rows;          // largest G x R of the launch: rows of a warp's profile slice
 };
 
-cudaError_t launch_sw_fast( int R, int G, const FastParams & p, int grid, cudaStream_t st );
+constexpr int FAST_THREADS = 128;   // threads per CTA of the fast pass
+
+cudaError_t launch_sw_fast( int R, const FastParams & p, int grid, cudaStream_t st, int * blocks_per_sm );
 cudaError_t launch_build_profile8( const uint8_t * qcodes, const uint64_t * qoff, const uint32_t * qlen,
-        const uint32_t * slots, uint32_t n, uint32_t rows, const int64_t * matrix, int8_t * prof,
+        const uint32_t * slots, uint32_t n, const uint32_t * rows_of, const int64_t * matrix, int8_t * prof,
         const uint64_t * prof_off, cudaStream_t st );
 
 }  // namespace ssa

@@ -29,6 +29,7 @@
 #include <cstring>
 #include <mutex>
 #include <thread>
+#include <tuple>
 
 namespace ssa {
 
@@ -115,6 +116,13 @@ public:
         CUDA_CHECK( cudaStreamCreateWithFlags( &stream_, cudaStreamNonBlocking ) );
         CUDA_CHECK( cudaEventCreate( &ev0_ ) );
         CUDA_CHECK( cudaEventCreate( &ev1_ ) );
+        CUDA_CHECK( cudaEventCreateWithFlags( &ev_ready_, cudaEventDisableTiming ) );
+        for( auto & e : ev_phase_ )
+            CUDA_CHECK( cudaEventCreate( &e ) );
+        for( int i = 0; i < 4; i++ ) {
+            CUDA_CHECK( cudaStreamCreateWithFlags( &class_stream_[i], cudaStreamNonBlocking ) );
+            CUDA_CHECK( cudaEventCreateWithFlags( &ev_class_[i], cudaEventDisableTiming ) );
+        }
         device_ = dev;
         ready_ = true;
     }
@@ -183,6 +191,37 @@ public:
                 [&]( uint32_t a, uint32_t b ) { return db.len[a] > db.len[b]; } );
         db.symtype = cfg.symtype;
         db.generation = ++generation_;
+        db.mean_len = db.order_desc.empty() ? 0.0 : (double) db.residues / (double) db.order_desc.size();
+
+        // pairs of consecutive sequences in length order share the 16x2 lanes
+        // of the fast Smith-Waterman pass; columns past a sequence's last
+        // 4-column block hold the neutral pad code
+        const size_t n_pairs = (db.order_desc.size() + 1) / 2;
+        db.pair_cols.resize( n_pairs );
+        db.pair_a.resize( n_pairs );
+        db.pair_b.resize( n_pairs );
+        std::vector<uint64_t> pair_off( n_pairs + 1, 0 );
+        for( size_t pi = 0; pi < n_pairs; pi++ ) {
+            db.pair_a[pi] = db.order_desc[2 * pi];
+            db.pair_b[pi] = (2 * pi + 1 < db.order_desc.size()) ? db.order_desc[2 * pi + 1] : 0xffffffffu;
+            db.pair_cols[pi] = (db.len[db.pair_a[pi]] + 7u) & ~7u;
+            pair_off[pi + 1] = pair_off[pi] + 2ull * db.pair_cols[pi];
+        }
+        std::vector<uint8_t> pair_res( pair_off[n_pairs] + 16, (uint8_t) FAST_PAD_CODE );
+        for( size_t pi = 0; pi < n_pairs; pi++ ) {
+            uint8_t * out = pair_res.data() + pair_off[pi];
+            for( int half = 0; half < 2; half++ ) {
+                const uint32_t id = half ? db.pair_b[pi] : db.pair_a[pi];
+                if( id == 0xffffffffu )
+                    continue;
+                const uint32_t L = db.len[id], Lb = (L + 3u) & ~3u;
+                const uint8_t * src = db.codes.data() + db.off[id];
+                for( uint32_t j = 0; j < L; j++ )
+                    out[2 * j + half] = src[j];
+                for( uint32_t j = L; j < Lb; j++ )
+                    out[2 * j + half] = 0;   // the reference's pad inside the last block
+            }
+        }
 
         init_device();
         d_codes_.ensure( db.codes.size() );
@@ -197,6 +236,22 @@ public:
         if( !db.order_desc.empty() )
             CUDA_CHECK( cudaMemcpy( d_order_.p, db.order_desc.data(), sizeof(uint32_t) * db.order_desc.size(),
                     cudaMemcpyHostToDevice ) );
+        {
+            std::vector<uint2> ids( std::max<size_t>( 1, n_pairs ) );
+            for( size_t pi = 0; pi < n_pairs; pi++ )
+                ids[pi] = make_uint2( db.pair_a[pi], db.pair_b[pi] );
+            d_pair_res_.ensure( pair_res.size() );
+            d_pair_off_.ensure( sizeof(uint64_t) * (n_pairs + 1) );
+            d_pair_cols_.ensure( sizeof(uint32_t) * std::max<size_t>( 1, n_pairs ) );
+            d_pair_ids_.ensure( sizeof(uint2) * ids.size() );
+            CUDA_CHECK( cudaMemcpy( d_pair_res_.p, pair_res.data(), pair_res.size(), cudaMemcpyHostToDevice ) );
+            CUDA_CHECK( cudaMemcpy( d_pair_off_.p, pair_off.data(), sizeof(uint64_t) * (n_pairs + 1),
+                    cudaMemcpyHostToDevice ) );
+            if( n_pairs )
+                CUDA_CHECK( cudaMemcpy( d_pair_cols_.p, db.pair_cols.data(), sizeof(uint32_t) * n_pairs,
+                        cudaMemcpyHostToDevice ) );
+            CUDA_CHECK( cudaMemcpy( d_pair_ids_.p, ids.data(), sizeof(uint2) * ids.size(), cudaMemcpyHostToDevice ) );
+        }
         db_ = std::move( db );
         db_stale_ = false;
         ranks_.clear();
@@ -229,7 +284,9 @@ public:
             std::vector<std::vector<Hit>> & out, SearchStats & stats );
 
     void shutdown() {
-        DevBuf * bufs[] = { &d_codes_, &d_off_, &d_len_, &d_order_, &d_qcodes_, &d_qoff_, &d_qlen_, &d_qpad_,
+        DevBuf * bufs[] = { &d_codes_, &d_off_, &d_len_, &d_order_, &d_pair_res_, &d_pair_off_, &d_pair_cols_,
+            &d_pair_ids_, &d_prof8_, &d_prof8_off_, &d_rows_, &d_slots_, &d_bounds_, &d_group_,
+            &d_scratch_fast_[0], &d_scratch_fast_[1], &d_scratch_fast_[2], &d_scratch_fast_[3], &d_qcodes_, &d_qoff_, &d_qlen_, &d_qpad_,
             &d_prof_off_, &d_prof_, &d_matrix_, &d_score_, &d_list_a_, &d_list_b_, &d_counts_, &d_scratch_,
             &d_tb_hits_, &d_tb_regions_, &d_tb_last_, &d_tb_last_off_, &d_tb_dirs_, &d_tb_dir_off_, &d_tb_ops_,
             &d_tb_ops_off_, &d_tb_ops_len_ };
@@ -247,10 +304,12 @@ private:
     Engine() = default;
 
     void run_pass( int algo, int width, const SearchRequest & req, uint32_t n_slots, const PairTask * tasks,
-            uint64_t n_tasks, bool implicit, PairTask * next, unsigned * next_count, uint32_t next_cap );
+            uint64_t n_tasks, bool implicit, PairTask * next, unsigned * next_count, uint32_t next_cap,
+            const uint32_t * slot_list = nullptr, uint32_t n_sub = 0 );
+    void run_fast_entry( const SearchRequest & req, uint32_t nq, PairTask * next, unsigned * next_count, uint32_t cap );
     void build_profiles( int width, uint32_t n_slots );
     void traceback( const SearchRequest & req, const std::vector<QueryCodes> & queries, uint32_t slot0,
-            std::vector<std::vector<Hit>> & out );
+            std::vector<std::vector<Hit>> & out, SearchStats & stats );
 
     bool ready_ = false;
     int device_ = 0;
@@ -265,6 +324,14 @@ private:
 
     // device buffers
     DevBuf d_codes_, d_off_, d_len_, d_order_;
+    DevBuf d_pair_res_, d_pair_off_, d_pair_cols_, d_pair_ids_;
+    DevBuf d_prof8_, d_prof8_off_, d_rows_, d_slots_;
+    DevBuf d_scratch_fast_[4];
+    DevBuf d_bounds_, d_group_;
+    cudaStream_t class_stream_[4] = { nullptr, nullptr, nullptr, nullptr };
+    cudaEvent_t ev_class_[4] = { nullptr, nullptr, nullptr, nullptr };
+    cudaEvent_t ev_ready_ = nullptr;
+    cudaEvent_t ev_phase_[6] = {};   // batch start, entry pass done, cascade done, copies done, traceback
     DevBuf d_qcodes_, d_qoff_, d_qlen_, d_qpad_, d_prof_off_, d_prof_, d_matrix_;
     DevBuf d_score_, d_list_a_, d_list_b_, d_counts_, d_scratch_;
     DevBuf d_tb_hits_, d_tb_regions_, d_tb_last_, d_tb_last_off_, d_tb_dirs_, d_tb_dir_off_, d_tb_ops_,
@@ -295,7 +362,8 @@ void Engine::build_profiles( int width, uint32_t n_slots ) {
 }
 
 void Engine::run_pass( int algo, int width, const SearchRequest & req, uint32_t n_slots, const PairTask * tasks,
-        uint64_t n_tasks, bool implicit, PairTask * next, unsigned * next_count, uint32_t next_cap ) {
+        uint64_t n_tasks, bool implicit, PairTask * next, unsigned * next_count, uint32_t next_cap,
+        const uint32_t * slot_list, uint32_t n_sub ) {
     if( n_tasks == 0 )
         return;
     build_profiles( width, n_slots );
@@ -308,6 +376,8 @@ void Engine::run_pass( int algo, int width, const SearchRequest & req, uint32_t 
     p.qv.n_slots = n_slots;
     p.tasks = implicit ? nullptr : tasks;
     p.order = d_order_.as<uint32_t>();
+    p.slot_list = slot_list;
+    p.n_sub = n_sub;
     p.n_tasks = n_tasks;
     unsigned long long * counter = d_counts_.as<unsigned long long>() + 4;
     CUDA_CHECK( cudaMemsetAsync( counter, 0, sizeof(unsigned long long), stream_ ) );
@@ -332,6 +402,192 @@ void Engine::run_pass( int algo, int width, const SearchRequest & req, uint32_t 
     }
     CUDA_CHECK( launch_emul( algo, width, p, grid, stream_ ) );
     launches_++;
+}
+
+// The 16x2 pass reproduces the 8-bit Smith-Waterman lanes exactly when the
+// gap extension is not positive and the truncated 8-bit open+extend cost lies
+// in [-128, 0]; other parameters run the exact lane emulation.
+static bool fast_eligible( const SearchRequest & req ) {
+    if( req.algo != 0 || req.bit_width != 8 )
+        return false;
+    if( getenv( "SSA_B200_NO_FAST" ) )
+        return false;
+    const int goe8 = (int8_t) (req.gap_open + req.gap_extend);
+    return req.gap_extend <= 0 && goe8 <= 0;
+}
+
+struct FastShape {
+    int G, R, P;
+};
+
+constexpr uint32_t FAST_MAX_ROWS = 6144;    // 192 KiB of int8 profile per CTA
+
+// Threads per group G, rows per thread R and passes P for a query of Q rows:
+// the smallest estimated issue cost per database column, counting the
+// wavefront fill (G - 1 steps per pass) and a per-step overhead.
+static FastShape choose_shape( uint32_t Q, double mean_len ) {
+    FastShape best{ 0, 0, 0 };
+    double best_cost = 1e300;
+    const int Gs[] = { 8, 16, 32 };
+    const int Rs[] = { 8, 16, 24, 32 };
+    for( int G : Gs ) {
+        for( int R : Rs ) {
+            const uint32_t per = (uint32_t) (G * R);
+            const uint32_t P = (Q + per - 1) / per;
+            if( (uint64_t) P * per > FAST_MAX_ROWS )
+                continue;
+            const double cost = (double) P * G * (mean_len + G - 1) * (8.0 * R + 24.0);
+            if( cost < best_cost ) {
+                best_cost = cost;
+                best = FastShape{ G, R, (int) P };
+            }
+        }
+    }
+    return best;
+}
+
+void Engine::run_fast_entry( const SearchRequest & req, uint32_t nq, PairTask * next, unsigned * next_count,
+        uint32_t cap ) {
+    const uint32_t n_pairs = (uint32_t) db_.pair_cols.size();
+    if( n_pairs == 0 )
+        return;
+    // shape per slot; queries too long for the shared-memory profile run the
+    // exact lane emulation instead
+    std::vector<FastShape> shape( nq );
+    std::vector<uint32_t> rows_of( nq, 0 );
+    std::vector<uint32_t> fallback;
+    std::vector<std::vector<uint32_t>> by_r( 4 );   // R = 8, 16, 24, 32
+    for( uint32_t s = 0; s < nq; s++ ) {
+        shape[s] = choose_shape( h_qlen_[s], db_.mean_len );
+        if( shape[s].G == 0 ) {
+            fallback.push_back( s );
+            continue;
+        }
+        rows_of[s] = (uint32_t) (shape[s].G * shape[s].R * shape[s].P);
+        by_r[shape[s].R / 8 - 1].push_back( s );
+    }
+    // profiles: one 32 x rows int8 table per slot
+    std::vector<uint64_t> prof_off( nq, 0 );
+    uint64_t total = 0;
+    std::vector<uint32_t> slots;
+    for( auto & v : by_r )
+        for( uint32_t s : v ) {
+            prof_off[s] = total;
+            total += 32ull * rows_of[s];
+            slots.push_back( s );
+        }
+    const size_t n_shaped = slots.size();
+    for( uint32_t s : fallback )
+        slots.push_back( s );
+    d_prof8_.ensure( total + 16 );
+    d_prof8_off_.ensure( nq * sizeof(uint64_t) );
+    d_rows_.ensure( nq * sizeof(uint32_t) );
+    d_slots_.ensure( std::max<size_t>( 1, slots.size() ) * sizeof(uint32_t) );
+    CUDA_CHECK( cudaMemcpyAsync( d_prof8_off_.p, prof_off.data(), nq * sizeof(uint64_t), cudaMemcpyHostToDevice,
+            stream_ ) );
+    CUDA_CHECK( cudaMemcpyAsync( d_rows_.p, rows_of.data(), nq * sizeof(uint32_t), cudaMemcpyHostToDevice, stream_ ) );
+    CUDA_CHECK( cudaMemcpyAsync( d_slots_.p, slots.data(), slots.size() * sizeof(uint32_t), cudaMemcpyHostToDevice,
+            stream_ ) );
+    if( n_shaped ) {
+        CUDA_CHECK( launch_build_profile8( d_qcodes_.as<uint8_t>(), d_qoff_.as<uint64_t>(), d_qlen_.as<uint32_t>(),
+                d_slots_.as<uint32_t>(), (uint32_t) n_shaped, d_rows_.as<uint32_t>(), d_matrix_.as<int64_t>(),
+                d_prof8_.as<int8_t>(), d_prof8_off_.as<uint64_t>(), stream_ ) );
+        launches_++;
+    }
+
+    // work units: ranges of length-sorted pairs holding about equal numbers
+    // of columns (at least 4 pairs), the longest first; every query of a
+    // class gets every range.  A warp takes one unit at a time.
+    uint64_t total_cols = 0;
+    for( uint32_t c : db_.pair_cols )
+        total_cols += c;
+    const uint64_t want_units = (uint64_t) sms_ * 12 * 8;
+    const uint64_t target = std::max<uint64_t>( 1, total_cols * std::max<size_t>( 1, n_shaped ) / want_units );
+    std::vector<uint32_t> bounds{ 0 };
+    {
+        uint64_t acc = 0;
+        uint32_t cnt = 0;
+        for( uint32_t pi = 0; pi < n_pairs; pi++ ) {
+            acc += db_.pair_cols[pi];
+            cnt++;
+            if( acc >= target && cnt >= 4 ) {
+                bounds.push_back( pi + 1 );
+                acc = 0;
+                cnt = 0;
+            }
+        }
+        if( bounds.back() != n_pairs )
+            bounds.push_back( n_pairs );
+    }
+    const uint32_t n_chunks = (uint32_t) bounds.size() - 1;
+    std::vector<uint16_t> group_of( nq, 32 );
+    for( uint32_t s = 0; s < nq; s++ )
+        if( shape[s].G )
+            group_of[s] = (uint16_t) shape[s].G;
+    d_bounds_.ensure( bounds.size() * sizeof(uint32_t) );
+    d_group_.ensure( nq * sizeof(uint16_t) );
+    CUDA_CHECK( cudaMemcpyAsync( d_bounds_.p, bounds.data(), bounds.size() * sizeof(uint32_t), cudaMemcpyHostToDevice,
+            stream_ ) );
+    CUDA_CHECK( cudaMemcpyAsync( d_group_.p, group_of.data(), nq * sizeof(uint16_t), cudaMemcpyHostToDevice, stream_ ) );
+    CUDA_CHECK( cudaEventRecord( ev_ready_, stream_ ) );
+    const uint32_t cols_max = ((db_.max_len + 7u) & ~7u) + 8;
+    size_t class_first = 0;
+    for( int ri = 0; ri < 4; ri++ ) {
+        const std::vector<uint32_t> & cls = by_r[ri];
+        if( cls.empty() )
+            continue;
+        const int R = 8 * (ri + 1);
+        bool multi = false;
+        uint32_t slice_rows = 0;
+        for( uint32_t s : cls ) {
+            multi |= shape[s].P > 1;
+            slice_rows = std::max( slice_rows, (uint32_t) (shape[s].G * R) );
+        }
+        FastParams p{};
+        p.slice_rows = slice_rows;
+        int per_sm = 0;
+        CUDA_CHECK( launch_sw_fast( R, p, 0, class_stream_[ri], &per_sm ) );
+        const int grid = sms_ * std::max( 1, per_sm );
+        CUDA_CHECK( cudaStreamWaitEvent( class_stream_[ri], ev_ready_, 0 ) );
+        unsigned long long * unit_counter = d_counts_.as<unsigned long long>() + 8 + ri;   // bytes 64..95
+        CUDA_CHECK( cudaMemsetAsync( unit_counter, 0, sizeof(unsigned long long), class_stream_[ri] ) );
+        p.pair_res = d_pair_res_.as<uint8_t>();
+        p.pair_off = d_pair_off_.as<uint64_t>();
+        p.pair_cols = d_pair_cols_.as<uint32_t>();
+        p.pair_ids = d_pair_ids_.as<uint2>();
+        p.prof8 = d_prof8_.as<int8_t>();
+        p.prof8_off = d_prof8_off_.as<uint64_t>();
+        p.slot_group = d_group_.as<uint16_t>();
+        p.slot_rows = d_rows_.as<uint32_t>();
+        p.unit_slots = d_slots_.as<uint32_t>() + class_first;
+        p.n_class = (uint32_t) cls.size();
+        p.chunk_bounds = d_bounds_.as<uint32_t>();
+        p.n_units = (uint64_t) n_chunks * cls.size();
+        p.unit_counter = unit_counter;
+        p.gap_oe = (int8_t) (req.gap_open + req.gap_extend);
+        p.gap_e = req.gap_extend;
+        p.sink.score = d_score_.as<int32_t>();
+        p.sink.score_stride = db_.n_ids;
+        p.sink.next = next;
+        p.sink.next_count = next_count;
+        p.sink.next_cap = cap;
+        p.sink.error_flags = d_counts_.as<unsigned>() + 2;
+        if( multi ) {
+            p.scratch = (int4 *) d_scratch_fast_[ri].ensure( (size_t) grid * (FAST_THREADS / 32) * 4 * cols_max *
+                    sizeof(int4) );
+            p.scratch_cols = cols_max;
+        }
+        CUDA_CHECK( launch_sw_fast( R, p, grid, class_stream_[ri], nullptr ) );
+        launches_++;
+        CUDA_CHECK( cudaEventRecord( ev_class_[ri], class_stream_[ri] ) );
+        CUDA_CHECK( cudaStreamWaitEvent( stream_, ev_class_[ri], 0 ) );
+        class_first += cls.size();
+    }
+    if( !fallback.empty() ) {
+        const uint64_t n_ne = db_.order_desc.size();
+        run_pass( 0, 8, req, nq, nullptr, (uint64_t) fallback.size() * n_ne, true, next, next_count, cap,
+                d_slots_.as<uint32_t>() + n_shaped, (uint32_t) fallback.size() );
+    }
 }
 
 void Engine::search( const SearchRequest & req, const std::vector<QueryCodes> & queries,
@@ -383,6 +639,7 @@ void Engine::search( const SearchRequest & req, const std::vector<QueryCodes> & 
         d_qpad_.ensure( nq * sizeof(uint32_t) );
         d_prof_off_.ensure( nq * sizeof(uint64_t) );
         d_prof_.ensure( ptotal * sizeof(int32_t) );
+        stats.h2d_bytes += hq.size() + nq * (2 * sizeof(uint64_t) + 2 * sizeof(uint32_t));
         CUDA_CHECK( cudaMemcpyAsync( d_qcodes_.p, hq.data(), hq.size(), cudaMemcpyHostToDevice, stream_ ) );
         CUDA_CHECK( cudaMemcpyAsync( d_qoff_.p, h_qoff_.data(), nq * sizeof(uint64_t), cudaMemcpyHostToDevice, stream_ ) );
         CUDA_CHECK( cudaMemcpyAsync( d_qlen_.p, h_qlen_.data(), nq * sizeof(uint32_t), cudaMemcpyHostToDevice, stream_ ) );
@@ -398,15 +655,21 @@ void Engine::search( const SearchRequest & req, const std::vector<QueryCodes> & 
         const uint32_t cap = (uint32_t) std::min<uint64_t>( std::max<uint64_t>( n_pairs, 1 ), 0xffffffffull );
         d_list_a_.ensure( (size_t) cap * sizeof(PairTask) );
         d_list_b_.ensure( (size_t) cap * sizeof(PairTask) );
-        d_counts_.ensure( 8 * sizeof(unsigned long long) );
-        CUDA_CHECK( cudaMemsetAsync( d_counts_.p, 0, 8 * sizeof(unsigned long long), stream_ ) );
+        d_counts_.ensure( 16 * sizeof(unsigned long long) );
+        CUDA_CHECK( cudaMemsetAsync( d_counts_.p, 0, 16 * sizeof(unsigned long long), stream_ ) );
         unsigned * cnt = d_counts_.as<unsigned>();   // [0] list a, [1] list b, [2] errors
 
         // ---- passes
+        const bool timing = getenv( "SSA_B200_TIMING" ) != nullptr;
+        CUDA_CHECK( cudaEventRecord( ev_phase_[0], stream_ ) );
         const int entry = req.bit_width;
         std::vector<PairTask> list_entry, list_16;   // host copies for the replay
         unsigned n_a = 0, n_b = 0;
-        run_pass( req.algo, entry, req, nq, nullptr, n_pairs, true, d_list_a_.as<PairTask>(), cnt + 0, cap );
+        if( fast_eligible( req ) )
+            run_fast_entry( req, nq, d_list_a_.as<PairTask>(), cnt + 0, cap );
+        else
+            run_pass( req.algo, entry, req, nq, nullptr, n_pairs, true, d_list_a_.as<PairTask>(), cnt + 0, cap );
+        CUDA_CHECK( cudaEventRecord( ev_phase_[1], stream_ ) );
         if( entry != 64 ) {
             CUDA_CHECK( cudaMemcpyAsync( &n_a, cnt + 0, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_ ) );
             CUDA_CHECK( cudaStreamSynchronize( stream_ ) );
@@ -432,14 +695,18 @@ void Engine::search( const SearchRequest & req, const std::vector<QueryCodes> & 
                 }
             }
         }
+        CUDA_CHECK( cudaEventRecord( ev_phase_[2], stream_ ) );
+        stats.d2h_bytes += score_bytes + ((uint64_t) n_a + n_b) * sizeof(PairTask);
         int32_t * hs = (int32_t *) h_score_.ensure( std::max<size_t>( score_bytes, 4 ) );
         if( score_bytes )
             CUDA_CHECK( cudaMemcpyAsync( hs, d_score_.p, score_bytes, cudaMemcpyDeviceToHost, stream_ ) );
         unsigned err = 0;
         CUDA_CHECK( cudaMemcpyAsync( &err, cnt + 2, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_ ) );
+        CUDA_CHECK( cudaEventRecord( ev_phase_[3], stream_ ) );
         CUDA_CHECK( cudaStreamSynchronize( stream_ ) );
         if( err )
             fatal( "Internal error in the GPU search (flags 0x%x).", err );
+        const auto t_replay0 = std::chrono::steady_clock::now();
 
         // ---- host replay, one query per worker
         std::vector<ReplayQuery> rq( nq );
@@ -482,8 +749,26 @@ void Engine::search( const SearchRequest & req, const std::vector<QueryCodes> & 
                 stats.overflow16 += c.overflow16;
             }
         }
+        const auto t_replay1 = std::chrono::steady_clock::now();
+        CUDA_CHECK( cudaEventRecord( ev_phase_[4], stream_ ) );
         if( req.align_type == COMPUTE_ALIGNMENT )
-            traceback( req, queries, (uint32_t) b0, out );
+            traceback( req, queries, (uint32_t) b0, out, stats );
+        CUDA_CHECK( cudaEventRecord( ev_phase_[5], stream_ ) );
+        {
+            CUDA_CHECK( cudaEventSynchronize( ev_phase_[5] ) );
+            float ms[5];
+            for( int i = 0; i < 3; i++ )
+                CUDA_CHECK( cudaEventElapsedTime( &ms[i], ev_phase_[i], ev_phase_[i + 1] ) );
+            CUDA_CHECK( cudaEventElapsedTime( &ms[3], ev_phase_[4], ev_phase_[5] ) );
+            const double rep = std::chrono::duration<double, std::milli>( t_replay1 - t_replay0 ).count();
+            stats.entry_seconds += ms[0] * 1e-3;
+            stats.kernel_seconds += (ms[0] + ms[1] + ms[3]) * 1e-3;
+            if( timing )
+            fprintf( stderr,
+                    "[ssa timing] queries %u pairs %llu: entry %.3f ms, cascade %.3f ms (%u+%u re-queued), "
+                    "copies %.3f ms, replay %.3f ms, traceback %.3f ms\n",
+                    nq, (unsigned long long) n_pairs, ms[0], ms[1], n_a, n_b, ms[2], rep, ms[3] );
+        }
     }
     CUDA_CHECK( cudaEventRecord( ev1_, stream_ ) );
     CUDA_CHECK( cudaEventSynchronize( ev1_ ) );
@@ -494,7 +779,7 @@ void Engine::search( const SearchRequest & req, const std::vector<QueryCodes> & 
 }
 
 void Engine::traceback( const SearchRequest & req, const std::vector<QueryCodes> & queries, uint32_t slot0,
-        std::vector<std::vector<Hit>> & out ) {
+        std::vector<std::vector<Hit>> & out, SearchStats & stats ) {
     const uint32_t nq = (uint32_t) h_qlen_.size();
     std::vector<TbHit> hits;
     std::vector<std::pair<uint32_t, uint32_t>> where;   // (query index, hit index)
@@ -567,6 +852,8 @@ void Engine::traceback( const SearchRequest & req, const std::vector<QueryCodes>
             cudaMemcpyHostToDevice, stream_ ) );
     CUDA_CHECK( launch_traceback( p, req.algo == 0, grid, stream_ ) );
     launches_ += (req.algo == 0) ? 4 : 2;
+    stats.h2d_bytes += nh * (sizeof(TbHit) + sizeof(TbRegion) + 3 * sizeof(uint64_t));
+    stats.d2h_bytes += nh * (sizeof(TbRegion) + sizeof(uint32_t)) + ops_off[nh];
     std::vector<uint32_t> ops_len( nh );
     std::vector<char> ops( ops_off[nh] + 1 );
     CUDA_CHECK( cudaMemcpyAsync( regions.data(), p.regions, nh * sizeof(TbRegion), cudaMemcpyDeviceToHost, stream_ ) );

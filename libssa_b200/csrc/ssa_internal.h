@@ -52,6 +52,11 @@ struct HostDb {
     std::vector<uint8_t> codes;         // mapped residues, each record padded to 16 B
     std::vector<uint32_t> order_desc;   // non-empty IDs, longest first (stable)
     std::vector<uint32_t> nonempty_before;   // per ID + 1: non-empty records with a smaller ID
+    // length-sorted pairs for the 16x2 Smith-Waterman pass: IDs and padded
+    // column counts (the interleaved residues live only in HBM)
+    std::vector<uint32_t> pair_cols;
+    std::vector<uint32_t> pair_a, pair_b;   // pair_b = 0xffffffff when absent
+    double mean_len = 0;
     uint64_t residues = 0;
     uint32_t max_len = 0;
     int symtype = -1;
@@ -73,6 +78,10 @@ struct SearchStats {
     uint64_t cells = 0;         // query length x database residues, summed
     uint64_t kernel_launches = 0;
     double seconds_gpu = 0;
+    double entry_seconds = 0;
+    double kernel_seconds = 0;
+    uint64_t h2d_bytes = 0;
+    uint64_t d2h_bytes = 0;
 };
 
 struct SearchRequest {

@@ -30,6 +30,9 @@
 //     32-bit IADD (no borrow can cross halves) and the SW zero floor is a
 //     max with the bias;  per 16x2 cell pair: 4 half-rate DPX/PRMT and
 //     4 full-rate instructions;
+//   * every warp schedules itself: it takes (query, range of pairs) units from
+//     a global counter, keeps the current pass's rows of the query profile in
+//     its own shared-memory slice, and never waits on other warps;
 //   * queries longer than G*R rows take several passes; the bottom row of a
 //     pass goes through a per-group scratch row in global memory.
 #include "device_common.cuh"
@@ -76,64 +79,43 @@ struct ProfLoad {
     }
 };
 
-template <int R, int G>
-__global__ void __launch_bounds__( 256, 1 ) sw_fast_kernel( FastParams p ) {
+template <int R>
+__global__ void __launch_bounds__( 128, 3 ) sw_fast_kernel( FastParams p ) {
+    // one profile slice (32 codes x G*R rows, G <= 32) per warp
     extern __shared__ __align__( 16 ) int8_t sprof[];
-    __shared__ FastItem cur;
-    __shared__ unsigned pair_next;
-    __shared__ uint32_t loaded_slot;
-
-    constexpr int GPW = 32 / G;                  // groups per warp
     const int lane = threadIdx.x & 31;
-    const int k = lane % G;                      // thread within its group
-    const int g = lane / G;                      // group within the warp
+    const uint32_t warp_in_cta = threadIdx.x >> 5;
     const uint32_t warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const uint32_t rows = p.rows;
-    const uint32_t passes = p.passes;
+    int8_t * slice = sprof + (size_t) warp_in_cta * 32u * p.slice_rows;
     const uint32_t GOE32 = (uint32_t) ((int32_t) p.gap_oe * 65536 + (int32_t) p.gap_oe);
     const uint32_t GE2 = ((uint32_t) (uint16_t) (int16_t) p.gap_e << 16) | (uint16_t) (int16_t) p.gap_e;
     const uint32_t TH = FAST_BIAS + FAST_THRESHOLD;
-    int4 * scratch = p.scratch + ((uint64_t) warp_global * GPW + g) * p.scratch_cols;
+    uint64_t loaded_key = ~0ull;
 
-    if( threadIdx.x == 0 )
-        loaded_slot = 0xffffffffu;
     for( ;; ) {
-        __syncthreads();
-        if( threadIdx.x == 0 ) {
-            unsigned it = atomicAdd( p.item_counter, 1u );
-            if( it < p.n_items ) {
-                cur = p.items[it];
-            }
-            else {
-                cur.slot = 0xffffffffu;
-                cur.pair_begin = cur.pair_end = 0;
-            }
-            pair_next = cur.pair_begin;
-        }
-        __syncthreads();
-        if( cur.slot == 0xffffffffu )
+        // a work unit: one query slot against one range of pairs
+        unsigned long long u = 0;
+        if( lane == 0 )
+            u = atomicAdd( p.unit_counter, 1ull );
+        u = __shfl_sync( 0xffffffffu, u, 0 );
+        if( u >= p.n_units )
             break;
-        if( cur.slot != loaded_slot ) {
-            const uint4 * src = reinterpret_cast<const uint4 *>( p.prof8 + p.prof8_off[cur.slot] );
-            uint4 * dst = reinterpret_cast<uint4 *>( sprof );
-            const uint32_t n16 = 32u * rows / 16u;
-            for( uint32_t i = threadIdx.x; i < n16; i += blockDim.x )
-                dst[i] = src[i];
-            __syncthreads();
-            if( threadIdx.x == 0 )
-                loaded_slot = cur.slot;
-        }
-        const uint32_t slot = cur.slot;
+        const uint32_t slot = p.unit_slots[u % p.n_class];
+        const uint32_t chunk = (uint32_t) (u / p.n_class);
+        const uint32_t pair_begin = p.chunk_bounds[chunk], pair_end = p.chunk_bounds[chunk + 1];
+        const int G = (int) p.slot_group[slot];
+        const uint32_t GR = (uint32_t) (G * R);
+        const uint32_t rows = p.slot_rows[slot];
+        const uint32_t passes = rows / GR;
+        const int GPW = 32 / G;
+        const int k = lane % G;                      // thread within its group
+        const int g = lane / G;                      // group within the warp
+        const int8_t * prof = p.prof8 + p.prof8_off[slot];
+        int4 * scratch = p.scratch + ((uint64_t) warp_global * 4u + (uint32_t) g) * p.scratch_cols;
 
-        for( ;; ) {
-            unsigned b0 = 0;
-            if( lane == 0 )
-                b0 = atomicAdd( &pair_next, (unsigned) GPW );
-            b0 = __shfl_sync( 0xffffffffu, b0, 0 );
-            if( b0 >= cur.pair_end )
-                break;
-            const uint32_t pair = b0 + g;
-            const bool valid = pair < cur.pair_end;
+        for( uint32_t b0 = pair_begin; b0 < pair_end; b0 += (uint32_t) GPW ) {
+            const uint32_t pair = b0 + (uint32_t) g;
+            const bool valid = pair < pair_end;
             const uint32_t cols = valid ? p.pair_cols[pair] : 0u;
             const uint32_t max_cols = __reduce_max_sync( 0xffffffffu, cols );
             const uint8_t * res = p.pair_res + (valid ? p.pair_off[pair] : 0ull);
@@ -143,7 +125,20 @@ __global__ void __launch_bounds__( 256, 1 ) sw_fast_kernel( FastParams p ) {
 
             for( uint32_t pass = 0; pass < passes; pass++ ) {
                 const bool final_pass = (pass + 1 == passes);
-                const uint32_t row0 = pass * (uint32_t) (G * R) + (uint32_t) (k * R);
+                // stage this pass's rows of the profile in the warp's slice
+                const uint64_t key = ((uint64_t) slot << 16) | pass;
+                if( key != loaded_key ) {
+                    const uint32_t per_code = GR / 16u;
+                    const uint4 * src = reinterpret_cast<const uint4 *>( prof + (size_t) pass * GR );
+                    uint4 * dst = reinterpret_cast<uint4 *>( slice );
+                    for( uint32_t i = (uint32_t) lane; i < 32u * per_code; i += 32u ) {
+                        const uint32_t code = i / per_code, w = i % per_code;
+                        dst[i] = src[(size_t) code * (rows / 16u) + w];
+                    }
+                    loaded_key = key;
+                    __syncwarp();
+                }
+                const uint32_t row_in_slice = (uint32_t) (k * R);
                 uint32_t H[R], E[R];
 #pragma unroll
                 for( int r = 0; r < R; r++ ) {
@@ -152,8 +147,8 @@ __global__ void __launch_bounds__( 256, 1 ) sw_fast_kernel( FastParams p ) {
                 }
                 uint32_t diag = FAST_BIAS2, smax = FAST_BIAS2;
                 uint32_t out_h = FAST_BIAS2, out_f = FAST_BIAS2, out_s = FAST_BIAS2;
-                uint32_t rw = 0;
-                const uint32_t steps = max_cols + G - 1;
+                uint2 cur = make_uint2( 0u, 0u ), nxt = make_uint2( 0u, 0u );
+                const uint32_t steps = max_cols + (uint32_t) G - 1u;
                 for( uint32_t s = 0; s < steps; s++ ) {
                     uint32_t up_h = __shfl_up_sync( 0xffffffffu, out_h, 1, G );
                     uint32_t up_f = __shfl_up_sync( 0xffffffffu, out_f, 1, G );
@@ -167,33 +162,43 @@ __global__ void __launch_bounds__( 256, 1 ) sw_fast_kernel( FastParams p ) {
                             up_f = FAST_BIAS2;
                             up_s = FAST_BIAS2;
                         }
-                        else {
+                        else if( (uint32_t) c < p.scratch_cols ) {
                             int4 v = scratch[c];
                             up_h = (uint32_t) v.x;
                             up_f = (uint32_t) v.y;
                             up_s = (uint32_t) v.z;
                         }
                     }
-                    if( (c & 1) == 0 )
-                        rw = *reinterpret_cast<const uint32_t *>( res + 2 * (uint32_t) c );
+                    // residues: 4 columns (8 bytes) per word, the next word
+                    // loaded 4 columns ahead
+                    if( (c & 3) == 0 ) {
+                        if( c == 0 )
+                            nxt = *reinterpret_cast<const uint2 *>( res );
+                        cur = nxt;
+                        if( (uint32_t) c + 4u < cols )
+                            nxt = *reinterpret_cast<const uint2 *>( res + 2u * ((uint32_t) c + 4u) );
+                    }
+                    const uint32_t w = (c & 2) ? cur.y : cur.x;
                     const uint32_t sh = (uint32_t) (c & 1) * 16u;
-                    const uint32_t da = (rw >> sh) & 0xffu;
-                    const uint32_t db = (rw >> (sh + 8u)) & 0xffu;
+                    const uint32_t da = (w >> sh) & 0xffu;
+                    const uint32_t db = (w >> (sh + 8u)) & 0xffu;
                     uint32_t pa[R / 4], pb[R / 4];
-                    ProfLoad<R>::load( sprof + da * rows + row0, pa );
-                    ProfLoad<R>::load( sprof + db * rows + row0, pb );
+                    ProfLoad<R>::load( slice + da * GR + row_in_slice, pa );
+                    ProfLoad<R>::load( slice + db * GR + row_in_slice, pb );
                     uint32_t f = up_f, hd = diag;
 #pragma unroll
                     for( int r = 0; r < R; r++ ) {
+                        // off the row-to-row chain: a = max(Hdiag + V, E, 0)
                         const uint32_t v = prmt( pa[r >> 2], pb[r >> 2], sx_sel( r & 3 ) );
-                        uint32_t t = __vmaxs2( E[r], f );
-                        t = __vmaxs2( t, FAST_BIAS2 );                    // SW floor at 0
-                        const uint32_t h = __viaddmax_s16x2( hd, v, t );   // max(Hdiag + V, E, F, 0)
+                        const uint32_t e0 = __vmaxs2( E[r], FAST_BIAS2 );
+                        const uint32_t a = __viaddmax_s16x2( hd, v, e0 );
+                        // the chain through F: H = max(a, F), F' = max(F + gapE, H + gapO + gapE)
+                        const uint32_t h = __vmaxs2( a, f );
+                        const uint32_t hg = h + GOE32;                     // both halves, no borrow
+                        f = __viaddmax_s16x2( f, GE2, hg );
+                        E[r] = __viaddmax_s16x2( E[r], GE2, hg );
                         hd = H[r];
                         H[r] = h;
-                        const uint32_t hg = h + GOE32;                     // H + gapO + gapE, both halves
-                        E[r] = __viaddmax_s16x2( E[r], GE2, hg );
-                        f = __viaddmax_s16x2( f, GE2, hg );
                         smax = __vmaxs2( smax, h );
                     }
                     diag = up_h;
@@ -202,7 +207,10 @@ __global__ void __launch_bounds__( 256, 1 ) sw_fast_kernel( FastParams p ) {
                     out_s = __vmaxs2( up_s, smax );
                     if( k == G - 1 ) {
                         if( !final_pass ) {
-                            scratch[c] = make_int4( (int) out_h, (int) out_f, (int) out_s, 0 );
+                            if( (uint32_t) c < p.scratch_cols )
+                                scratch[c] = make_int4( (int) out_h, (int) out_f, (int) out_s, 0 );
+                            else
+                                atomicOr( p.sink.error_flags, ERR_SCRATCH_OVERFLOW );
                         }
                         else {
                             if( cross_lo < 0 && (out_s & 0xffffu) >= TH )
@@ -242,46 +250,44 @@ __global__ void __launch_bounds__( 256, 1 ) sw_fast_kernel( FastParams p ) {
     }
 }
 
-template <int R, int G>
-static cudaError_t launch_one( const FastParams & p, int grid, size_t smem, cudaStream_t st ) {
-    cudaError_t e = cudaFuncSetAttribute( sw_fast_kernel<R, G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-            (int) smem );
+// grid == 0: report the resident CTAs per SM in *blocks_per_sm without launching.
+template <int R>
+static cudaError_t launch_one( const FastParams & p, int grid, size_t smem, cudaStream_t st, int * blocks_per_sm ) {
+    cudaError_t e = cudaFuncSetAttribute( sw_fast_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem );
     if( e != cudaSuccess )
         return e;
-    sw_fast_kernel<R, G><<<grid, 256, smem, st>>>( p );
+    if( grid == 0 )
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor( blocks_per_sm, sw_fast_kernel<R>, FAST_THREADS, smem );
+    sw_fast_kernel<R><<<grid, FAST_THREADS, smem, st>>>( p );
     return cudaGetLastError();
 }
 
-cudaError_t launch_sw_fast( int R, int G, const FastParams & p, int grid, cudaStream_t st ) {
-    const size_t smem = 32ull * p.rows;
-#define SSA_FAST_CASE( RR, GG ) \
-    if( R == RR && G == GG ) \
-        return launch_one<RR, GG>( p, grid, smem, st );
-    SSA_FAST_CASE( 8, 8 )
-    SSA_FAST_CASE( 16, 8 )
-    SSA_FAST_CASE( 24, 8 )
-    SSA_FAST_CASE( 32, 8 )
-    SSA_FAST_CASE( 8, 16 )
-    SSA_FAST_CASE( 16, 16 )
-    SSA_FAST_CASE( 24, 16 )
-    SSA_FAST_CASE( 32, 16 )
-    SSA_FAST_CASE( 8, 32 )
-    SSA_FAST_CASE( 16, 32 )
-    SSA_FAST_CASE( 24, 32 )
-    SSA_FAST_CASE( 32, 32 )
-#undef SSA_FAST_CASE
-    return cudaErrorInvalidValue;
+cudaError_t launch_sw_fast( int R, const FastParams & p, int grid, cudaStream_t st, int * blocks_per_sm ) {
+    const size_t smem = (size_t) (FAST_THREADS / 32) * 32u * p.slice_rows;   // one slice per warp
+    switch( R ) {
+    case 8:
+        return launch_one<8>( p, grid, smem, st, blocks_per_sm );
+    case 16:
+        return launch_one<16>( p, grid, smem, st, blocks_per_sm );
+    case 24:
+        return launch_one<24>( p, grid, smem, st, blocks_per_sm );
+    case 32:
+        return launch_one<32>( p, grid, smem, st, blocks_per_sm );
+    default:
+        return cudaErrorInvalidValue;
+    }
 }
 
 // prof8[slot][code][row]: the query's 8-bit scores, -128 past the query and for
 // the neutral pad code used after a sequence's last 4-column block.
 __global__ void build_profile8_kernel( const uint8_t * qcodes, const uint64_t * qoff, const uint32_t * qlen,
-        const uint32_t * slots, uint32_t n, uint32_t rows, const int64_t * matrix, int8_t * prof,
+        const uint32_t * slots, uint32_t n, const uint32_t * rows_of, const int64_t * matrix, int8_t * prof,
         const uint64_t * prof_off ) {
     const uint32_t i = blockIdx.y;
     if( i >= n )
         return;
     const uint32_t slot = slots[i];
+    const uint32_t rows = rows_of[slot];
     const uint32_t Q = qlen[slot];
     const uint8_t * q = qcodes + qoff[slot];
     int8_t * out = prof + prof_off[slot];
@@ -296,12 +302,12 @@ __global__ void build_profile8_kernel( const uint8_t * qcodes, const uint64_t * 
 }
 
 cudaError_t launch_build_profile8( const uint8_t * qcodes, const uint64_t * qoff, const uint32_t * qlen,
-        const uint32_t * slots, uint32_t n, uint32_t rows, const int64_t * matrix, int8_t * prof,
+        const uint32_t * slots, uint32_t n, const uint32_t * rows_of, const int64_t * matrix, int8_t * prof,
         const uint64_t * prof_off, cudaStream_t st ) {
     if( n == 0 )
         return cudaSuccess;
     dim3 grid( 32, n );
-    build_profile8_kernel<<<grid, 256, 0, st>>>( qcodes, qoff, qlen, slots, n, rows, matrix, prof, prof_off );
+    build_profile8_kernel<<<grid, 256, 0, st>>>( qcodes, qoff, qlen, slots, n, rows_of, matrix, prof, prof_off );
     return cudaGetLastError();
 }
 

@@ -29,8 +29,23 @@ namespace ssa {
 constexpr int TB_R = 8;
 constexpr int TB_ROWS = 32 * TB_R;
 
-__device__ __forceinline__ int32_t mget( const int64_t * m, int row, int col ) {
-    return (int32_t) m[(row << 5) + col];
+// The 32x32 score table is staged in shared memory as int32 by every CTA.
+__device__ __forceinline__ void stage_matrix( const int64_t * m, int32_t * sm ) {
+    for( int i = threadIdx.x; i < 1024; i += blockDim.x )
+        sm[i] = (int32_t) m[i];
+    __syncthreads();
+}
+
+__device__ __forceinline__ int32_t mget( const int32_t * sm, int row, int col ) {
+    return sm[(row << 5) + col];
+}
+
+// The lane's R query codes (code 0 past the end) held in registers.
+__device__ __forceinline__ void load_rows( const uint8_t * a, int64_t first, int64_t step, int nvalid,
+        int (&code)[TB_R] ) {
+#pragma unroll
+    for( int r = 0; r < TB_R; r++ )
+        code[r] = (r < nvalid) ? a[first + step * r] : 0;
 }
 
 // ---------------------------------------------------------------------------
@@ -41,6 +56,8 @@ __device__ __forceinline__ int32_t mget( const int64_t * m, int row, int col ) {
 //    value, then smallest database index, then smallest query index.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__( 256 ) tb_forward_kernel( TbParams p ) {
+    __shared__ int32_t smat[1024];
+    stage_matrix( p.matrix, smat );
     const int lane = threadIdx.x & 31;
     const uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -64,6 +81,8 @@ __global__ void __launch_bounds__( 256 ) tb_forward_kernel( TbParams p ) {
             const bool final_pass = (pass + 1 == passes);
             const int32_t row0 = (int32_t) (pass * TB_ROWS + lane * TB_R);
             const int nvalid = max( 0, min( TB_R, (int) A - row0 ) );
+            int qa[TB_R];
+            load_rows( a, row0, 1, nvalid, qa );
             int32_t H[TB_R], E[TB_R];
 #pragma unroll
             for( int r = 0; r < TB_R; r++ ) {
@@ -95,7 +114,7 @@ __global__ void __launch_bounds__( 256 ) tb_forward_kernel( TbParams p ) {
                 for( int r = 0; r < TB_R; r++ ) {
                     if( r < nvalid ) {
                         int32_t e_in = E[r];
-                        int32_t x = hd + mget( p.matrix, a[row0 + r], d );
+                        int32_t x = hd + mget( smat, qa[r], d );
                         if( x < 0 )
                             x = 0;
                         if( f > x )
@@ -163,6 +182,8 @@ __global__ void __launch_bounds__( 256 ) tb_forward_kernel( TbParams p ) {
 //    whose value reaches the forward score.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__( 256 ) tb_reverse_kernel( TbParams p ) {
+    __shared__ int32_t smat[1024];
+    stage_matrix( p.matrix, smat );
     const int lane = threadIdx.x & 31;
     const uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -189,6 +210,8 @@ __global__ void __launch_bounds__( 256 ) tb_reverse_kernel( TbParams p ) {
             const bool final_pass = (pass + 1 == passes);
             const int32_t row0 = (int32_t) (pass * TB_ROWS + lane * TB_R);
             const int nvalid = max( 0, min( TB_R, (int) A - row0 ) );
+            int qa[TB_R];
+            load_rows( a, (int64_t) a_end - row0, -1, nvalid, qa );
             int32_t H[TB_R], E[TB_R];
 #pragma unroll
             for( int r = 0; r < TB_R; r++ ) {
@@ -235,9 +258,8 @@ __global__ void __launch_bounds__( 256 ) tb_reverse_kernel( TbParams p ) {
 #pragma unroll
                 for( int r = 0; r < TB_R; r++ ) {
                     if( r < nvalid ) {
-                        const int32_t j = a_end - (row0 + r);
                         int32_t e_in = E[r];
-                        int32_t x = hd + mget( p.matrix, a[j], d );
+                        int32_t x = hd + mget( smat, qa[r], d );
                         if( f > x )
                             x = f;
                         if( e_in > x )
@@ -294,6 +316,8 @@ __global__ void __launch_bounds__( 256 ) tb_reverse_kernel( TbParams p ) {
 //    16-bit word (8 rows x 2 bits) per lane and column.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__( 256 ) tb_directions_kernel( TbParams p ) {
+    __shared__ int32_t smat[1024];
+    stage_matrix( p.matrix, smat );
     const int lane = threadIdx.x & 31;
     const uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -316,6 +340,8 @@ __global__ void __launch_bounds__( 256 ) tb_directions_kernel( TbParams p ) {
             const bool final_pass = (pass + 1 == passes);
             const int32_t row0 = (int32_t) (pass * TB_ROWS + lane * TB_R);
             const int nvalid = max( 0, min( TB_R, (int) A - row0 ) );
+            int qa[TB_R];
+            load_rows( a, row0, 1, nvalid, qa );
             int32_t H[TB_R], E[TB_R];
 #pragma unroll
             for( int r = 0; r < TB_R; r++ ) {
@@ -350,7 +376,7 @@ __global__ void __launch_bounds__( 256 ) tb_directions_kernel( TbParams p ) {
                 for( int r = 0; r < TB_R; r++ ) {
                     if( r < nvalid ) {
                         int32_t e = E[r];
-                        int32_t x = hd + mget( p.matrix, d, a[row0 + r] );
+                        int32_t x = hd + mget( smat, d, qa[r] );
                         unsigned flags = 0;
                         if( f > x ) {
                             flags |= 1u;     // UP
