@@ -140,8 +140,15 @@ def barrier(pg):
         pg.barrier()
 
 
-def make_workload(scale: float, query_seed: int):
+def make_workload(scale: float, query_seed: int, kind: str = "sw_batched", n_queries: int | None = None):
     from libssa_b200 import workloads as W
+    if kind == "sw_plain":
+        # config 1's database (10,000 sequences) and n_queries queries of 375
+        import numpy as np
+        w = W.sw_plain(seed=1, scale=scale)
+        rng = np.random.default_rng(2000 + query_seed)
+        w.queries = [W.random_residues(rng, 375, W.AA20).tobytes() for _ in range(n_queries or 1)]
+        return w
     w = W.sw_batched(seed=3, scale=scale)
     if query_seed != 3:
         # a rank's own query batch of the same length distribution
@@ -228,7 +235,7 @@ def run_ours(args):
         from libssa_b200 import build
         build.build()
     L.load()
-    w = make_workload(args.scale, 3 if rank == 0 else 3 + rank)
+    w = make_workload(args.scale, 3 if rank == 0 else 3 + rank, args.workload, args.queries)
     L.set_output_mode(L.OUTPUT_SILENT)
     L.init_symbol_translation(L.AMINOACID, L.FORWARD_STRAND, 1, 1)
     L.init_score_matrix(L.MATRIX_BUILDIN, "blosum62")
@@ -300,6 +307,22 @@ def run_ours(args):
         "timing": {"device_seconds": round(t_dev, 4), "wall_seconds": round(t_wall, 4),
                    "entry_seconds_median": round(t_entry, 4)},
     }
+    if args.plain_queries > 0:
+        # the plain one-query-per-call path on a length-stratified query sample
+        import numpy as np
+        lens = np.array([len(q) for q in w.queries])
+        order = np.argsort(lens)
+        pick = [int(order[int((i + 0.5) * len(order) / args.plain_queries)]) for i in range(args.plain_queries)]
+        sample = [qs[i] for i in pick]
+        L.sw_align(sample[0], 10, L.BIT_WIDTH_8, L.COMPUTE_ALIGNMENT)
+        t0 = time.perf_counter()
+        for q in sample:
+            L.sw_align(q, 10, L.BIT_WIDTH_8, L.COMPUTE_ALIGNMENT)
+        t_plain = time.perf_counter() - t0
+        cells_plain = sum(len(w.queries[i]) for i in pick) * int(w.db_offsets[-1])
+        line["plain_gpu"] = {"value": round(cells_plain / t_plain / 1e9, 2), "unit": "GCUPS",
+                             "sample": f"{args.plain_queries} length-stratified queries, one sw_align call each "
+                                       "(COMPUTE_ALIGNMENT), wall time"}
     if world == 1 and not args.no_cpu_baseline:
         try:
             g, secs, desc = reference_sample(w, args.ref_queries, os.cpu_count() or 1)
@@ -323,6 +346,11 @@ def main():
     ap.add_argument("--scale", type=float, default=1.0, help="database and query count scale (1.0 = full)")
     ap.add_argument("--ref-queries", type=int, default=4, help="queries in the reference CPU sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--plain-queries", type=int, default=16,
+                    help="queries timed through the plain one-query-per-call path (0 = skip)")
+    ap.add_argument("--workload", default="sw_batched", choices=["sw_batched", "sw_plain"],
+                    help="sw_plain: config 1's 10,000-sequence database with --queries queries of 375")
+    ap.add_argument("--queries", type=int, default=None, help="query count for --workload sw_plain")
     args = ap.parse_args()
     if args.impl == "reference":
         sys.exit(run_reference_arm(args))

@@ -114,7 +114,7 @@ cudaError_t launch_emul( int algo, int width, const EmulParams & p, int grid, cu
 cudaError_t launch_build_profile32( const uint8_t * qcodes, const uint64_t * qoff, const uint32_t * qlen,
         const uint32_t * qpad, const uint64_t * prof_off, const int64_t * matrix, int width, int32_t * prof,
         uint32_t n_slots, cudaStream_t st );
-cudaError_t launch_traceback( const TbParams & p, bool any_sw, int grid, cudaStream_t st );
+cudaError_t launch_traceback( const TbParams & p, bool any_sw, int grid, cudaStream_t st, cudaEvent_t * ev );
 
 
 // ---- fast Smith-Waterman entry pass (sw_fast_kernel.cu) --------------------

@@ -118,7 +118,9 @@ template <int ALGO, int W>
 __global__ void __launch_bounds__( 256 ) emul_kernel( EmulParams p ) {
     constexpr bool SW = (ALGO == 0);
     constexpr int R = EMUL_R;
+    __shared__ int4 tiles[8][32];   // previous pass's boundary row, 32 columns ahead
     const int lane = threadIdx.x & 31;
+    int4 * tile = tiles[threadIdx.x >> 5];
     const uint64_t warp_global = (blockIdx.x * (uint64_t) blockDim.x + threadIdx.x) >> 5;
     int4 * scratch = p.scratch + warp_global * p.scratch_cols;
 
@@ -194,8 +196,19 @@ __global__ void __launch_bounds__( 256 ) emul_kernel( EmulParams p ) {
                 diag = (row0 == 0) ? 0 : nb.left_h( row0 - 1 );
 
             int32_t out_h = 0, out_f = 0, out_a = 0, out_b = 0;
+            int4 pf = make_int4( 0, 0, 0, 0 );
+            if( pass > 0 && (uint32_t) lane < p.scratch_cols && (uint32_t) lane < Lb )
+                pf = scratch[lane];
             const uint32_t steps = Lb + 31;
             for( uint32_t s = 0; s < steps; s++ ) {
+                if( pass > 0 && (s & 31u) == 0 ) {
+                    __syncwarp();
+                    tile[lane] = pf;
+                    __syncwarp();
+                    const uint32_t col = s + 32u + (uint32_t) lane;
+                    if( col < p.scratch_cols && col < Lb )
+                        pf = scratch[col];
+                }
                 int32_t up_h = __shfl_up_sync( 0xffffffffu, out_h, 1 );
                 int32_t up_f = __shfl_up_sync( 0xffffffffu, out_f, 1 );
                 int32_t up_a = __shfl_up_sync( 0xffffffffu, out_a, 1 );
@@ -217,8 +230,8 @@ __global__ void __launch_bounds__( 256 ) emul_kernel( EmulParams p ) {
                             up_b = 0;     // column min
                         }
                     }
-                    else if( (uint32_t) c < p.scratch_cols ) {
-                        int4 v = scratch[c];
+                    else {
+                        const int4 v = tile[s & 31u];
                         up_h = v.x;
                         up_f = v.y;
                         up_a = v.z;

@@ -119,6 +119,8 @@ public:
         CUDA_CHECK( cudaEventCreateWithFlags( &ev_ready_, cudaEventDisableTiming ) );
         for( auto & e : ev_phase_ )
             CUDA_CHECK( cudaEventCreate( &e ) );
+        for( auto & e : ev_tb_ )
+            CUDA_CHECK( cudaEventCreate( &e ) );
         for( int i = 0; i < 4; i++ ) {
             CUDA_CHECK( cudaStreamCreateWithFlags( &class_stream_[i], cudaStreamNonBlocking ) );
             CUDA_CHECK( cudaEventCreateWithFlags( &ev_class_[i], cudaEventDisableTiming ) );
@@ -331,7 +333,8 @@ private:
     cudaStream_t class_stream_[4] = { nullptr, nullptr, nullptr, nullptr };
     cudaEvent_t ev_class_[4] = { nullptr, nullptr, nullptr, nullptr };
     cudaEvent_t ev_ready_ = nullptr;
-    cudaEvent_t ev_phase_[6] = {};   // batch start, entry pass done, cascade done, copies done, traceback
+    cudaEvent_t ev_phase_[6] = {};
+    cudaEvent_t ev_tb_[5] = {};   // batch start, entry pass done, cascade done, copies done, traceback
     DevBuf d_qcodes_, d_qoff_, d_qlen_, d_qpad_, d_prof_off_, d_prof_, d_matrix_;
     DevBuf d_score_, d_list_a_, d_list_b_, d_counts_, d_scratch_;
     DevBuf d_tb_hits_, d_tb_regions_, d_tb_last_, d_tb_last_off_, d_tb_dirs_, d_tb_dir_off_, d_tb_ops_,
@@ -406,21 +409,24 @@ void Engine::run_pass( int algo, int width, const SearchRequest & req, uint32_t 
 
 // The 16x2 pass reproduces the 8-bit Smith-Waterman lanes exactly when the
 // gap extension is not positive and the truncated 8-bit open+extend cost lies
-// in [-128, 0]; other parameters run the exact lane emulation.
+// in [-128, gapE]; other parameters run the exact lane emulation.
 static bool fast_eligible( const SearchRequest & req ) {
     if( req.algo != 0 || req.bit_width != 8 )
         return false;
     if( getenv( "SSA_B200_NO_FAST" ) )
         return false;
+    // the kernel also uses gapO + gapE <= gapE (in 8-bit terms) to let the next
+    // row's F depend on Hdiag + V and E only
     const int goe8 = (int8_t) (req.gap_open + req.gap_extend);
-    return req.gap_extend <= 0 && goe8 <= 0;
+    return req.gap_extend <= 0 && goe8 <= 0 && goe8 <= req.gap_extend;
 }
 
 struct FastShape {
     int G, R, P;
 };
 
-constexpr uint32_t FAST_MAX_ROWS = 6144;    // 192 KiB of int8 profile per CTA
+constexpr uint32_t FAST_MAX_ROWS = 8192;    // longer queries run the lane emulation
+constexpr uint32_t FAST_MAX_PASS_ROWS = 512; // G x R: 16 KiB profile slice per warp
 
 // Threads per group G, rows per thread R and passes P for a query of Q rows:
 // the smallest estimated issue cost per database column, counting the
@@ -434,7 +440,7 @@ static FastShape choose_shape( uint32_t Q, double mean_len ) {
         for( int R : Rs ) {
             const uint32_t per = (uint32_t) (G * R);
             const uint32_t P = (Q + per - 1) / per;
-            if( (uint64_t) P * per > FAST_MAX_ROWS )
+            if( per > FAST_MAX_PASS_ROWS || (uint64_t) P * per > FAST_MAX_ROWS )
                 continue;
             const double cost = (double) P * G * (mean_len + G - 1) * (8.0 * R + 24.0);
             if( cost < best_cost ) {
@@ -501,7 +507,7 @@ void Engine::run_fast_entry( const SearchRequest & req, uint32_t nq, PairTask * 
     uint64_t total_cols = 0;
     for( uint32_t c : db_.pair_cols )
         total_cols += c;
-    const uint64_t want_units = (uint64_t) sms_ * 12 * 8;
+    const uint64_t want_units = (uint64_t) sms_ * 16 * 24;   // ~24 units per resident warp
     const uint64_t target = std::max<uint64_t>( 1, total_cols * std::max<size_t>( 1, n_shaped ) / want_units );
     std::vector<uint32_t> bounds{ 0 };
     {
@@ -850,7 +856,26 @@ void Engine::traceback( const SearchRequest & req, const std::vector<QueryCodes>
             cudaMemcpyHostToDevice, stream_ ) );
     CUDA_CHECK( cudaMemcpyAsync( (void *) p.ops_off, ops_off.data(), (nh + 1) * sizeof(uint64_t),
             cudaMemcpyHostToDevice, stream_ ) );
-    CUDA_CHECK( launch_traceback( p, req.algo == 0, grid, stream_ ) );
+    const bool timing = getenv( "SSA_B200_TIMING" ) != nullptr;
+    CUDA_CHECK( launch_traceback( p, req.algo == 0, grid, stream_, timing ? ev_tb_ : nullptr ) );
+    if( timing ) {
+        CUDA_CHECK( cudaEventSynchronize( ev_tb_[4] ) );
+        float t[4];
+        for( int i = 0; i < 4; i++ )
+            CUDA_CHECK( cudaEventElapsedTime( &t[i], ev_tb_[i], ev_tb_[i + 1] ) );
+        uint64_t max_cells = 0;
+        uint32_t max_a = 0, max_b = 0;
+        for( uint32_t h = 0; h < nh; h++ ) {
+            const uint64_t A = h_qlen_[hits[h].qslot], B = db_.len[hits[h].id];
+            if( A * B > max_cells ) {
+                max_cells = A * B;
+                max_a = (uint32_t) A;
+                max_b = (uint32_t) B;
+            }
+        }
+        fprintf( stderr, "[ssa timing] traceback %u hits: forward %.3f ms, reverse %.3f ms, directions %.3f ms, "
+                "walk %.3f ms; largest hit %u x %u\n", nh, t[0], t[1], t[2], t[3], max_a, max_b );
+    }
     launches_ += (req.algo == 0) ? 4 : 2;
     stats.h2d_bytes += nh * (sizeof(TbHit) + sizeof(TbRegion) + 3 * sizeof(uint64_t));
     stats.d2h_bytes += nh * (sizeof(TbRegion) + sizeof(uint32_t)) + ops_off[nh];

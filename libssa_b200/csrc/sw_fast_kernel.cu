@@ -26,10 +26,11 @@
 //   * the query profile (int8, 32 residue codes x padded rows) sits in shared
 //     memory; per cell a PRMT sign-extends the two sequences' scores into a
 //     16x2 word;
-//   * all values carry a +1024 bias per half, so H + gapO + gapE is a plain
-//     32-bit IADD (no borrow can cross halves) and the SW zero floor is a
-//     max with the bias;  per 16x2 cell pair: 4 half-rate DPX/PRMT and
-//     4 full-rate instructions;
+//   * all values carry a +1024 bias per half, so an add of gapO + gapE is a
+//     plain 32-bit IADD (no borrow can cross halves) and the SW zero floor is
+//     a max with the bias;  per 16x2 cell pair: 4 half-rate DPX/PRMT and
+//     5 full-rate instructions, with a one-instruction dependency from row to
+//     row;
 //   * every warp schedules itself: it takes (query, range of pairs) units from
 //     a global counter, keeps the current pass's rows of the query profile in
 //     its own shared-memory slice, and never waits on other warps;
@@ -80,13 +81,17 @@ struct ProfLoad {
 };
 
 template <int R>
-__global__ void __launch_bounds__( 128, 3 ) sw_fast_kernel( FastParams p ) {
+__global__ void __launch_bounds__( 128, 4 ) sw_fast_kernel( FastParams p ) {
     // one profile slice (32 codes x G*R rows, G <= 32) per warp
     extern __shared__ __align__( 16 ) int8_t sprof[];
     const int lane = threadIdx.x & 31;
     const uint32_t warp_in_cta = threadIdx.x >> 5;
     const uint32_t warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     int8_t * slice = sprof + (size_t) warp_in_cta * 32u * p.slice_rows;
+    // per warp: the previous pass's boundary row, G columns per group, staged
+    // ahead of use
+    int4 * tiles = reinterpret_cast<int4 *>( sprof + (size_t) (FAST_THREADS / 32) * 32u * p.slice_rows ) +
+            warp_in_cta * 32u;
     const uint32_t GOE32 = (uint32_t) ((int32_t) p.gap_oe * 65536 + (int32_t) p.gap_oe);
     const uint32_t GE2 = ((uint32_t) (uint16_t) (int16_t) p.gap_e << 16) | (uint16_t) (int16_t) p.gap_e;
     const uint32_t TH = FAST_BIAS + FAST_THRESHOLD;
@@ -147,56 +152,74 @@ __global__ void __launch_bounds__( 128, 3 ) sw_fast_kernel( FastParams p ) {
                 }
                 uint32_t diag = FAST_BIAS2, smax = FAST_BIAS2;
                 uint32_t out_h = FAST_BIAS2, out_f = FAST_BIAS2, out_s = FAST_BIAS2;
-                uint2 cur = make_uint2( 0u, 0u ), nxt = make_uint2( 0u, 0u );
+                // residues of columns c .. c+3 (two bytes each), refilled one
+                // column ahead every step
+                uint32_t q0 = 0, q1 = 0, q2 = 0, q3 = 0;
+                {
+                    const int32_t c0 = -k;
+                    auto fetch = [&]( int32_t col ) -> uint32_t {
+                        return (col >= 0 && (uint32_t) col < cols)
+                                ? (uint32_t) *reinterpret_cast<const uint16_t *>( res + 2u * (uint32_t) col ) : 0u;
+                    };
+                    q0 = fetch( c0 );
+                    q1 = fetch( c0 + 1 );
+                    q2 = fetch( c0 + 2 );
+                    q3 = fetch( c0 + 3 );
+                }
+                // boundary row of the previous pass: each lane of a group
+                // prefetches one column, published to the group's tile every G steps
+                int4 pf = make_int4( 0, 0, 0, 0 );
+                int4 * tile = tiles + g * G;
+                if( pass > 0 && (uint32_t) k < p.scratch_cols && (uint32_t) k < cols )
+                    pf = scratch[k];
                 const uint32_t steps = max_cols + (uint32_t) G - 1u;
                 for( uint32_t s = 0; s < steps; s++ ) {
+                    if( pass > 0 && (s % (uint32_t) G) == 0 ) {
+                        __syncwarp();
+                        tile[k] = pf;
+                        __syncwarp();
+                        const uint32_t col = s + (uint32_t) G + (uint32_t) k;
+                        if( col < p.scratch_cols && col < cols )
+                            pf = scratch[col];
+                    }
                     uint32_t up_h = __shfl_up_sync( 0xffffffffu, out_h, 1, G );
                     uint32_t up_f = __shfl_up_sync( 0xffffffffu, out_f, 1, G );
                     uint32_t up_s = __shfl_up_sync( 0xffffffffu, out_s, 1, G );
                     const int32_t c = (int32_t) s - k;
+                    const uint32_t w = q0;
+                    q0 = q1;
+                    q1 = q2;
+                    q2 = q3;
+                    {
+                        const int32_t col = c + 4;
+                        q3 = (col >= 0 && (uint32_t) col < cols)
+                                ? (uint32_t) *reinterpret_cast<const uint16_t *>( res + 2u * (uint32_t) col ) : 0u;
+                    }
                     if( c < 0 || (uint32_t) c >= cols )
                         continue;
                     if( k == 0 ) {
-                        if( pass == 0 ) {
-                            up_h = FAST_BIAS2;
-                            up_f = FAST_BIAS2;
-                            up_s = FAST_BIAS2;
-                        }
-                        else if( (uint32_t) c < p.scratch_cols ) {
-                            int4 v = scratch[c];
-                            up_h = (uint32_t) v.x;
-                            up_f = (uint32_t) v.y;
-                            up_s = (uint32_t) v.z;
-                        }
+                        const int4 v = tile[s % (uint32_t) G];
+                        up_h = pass ? (uint32_t) v.x : FAST_BIAS2;
+                        up_f = pass ? (uint32_t) v.y : FAST_BIAS2;
+                        up_s = pass ? (uint32_t) v.z : FAST_BIAS2;
                     }
-                    // residues: 4 columns (8 bytes) per word, the next word
-                    // loaded 4 columns ahead
-                    if( (c & 3) == 0 ) {
-                        if( c == 0 )
-                            nxt = *reinterpret_cast<const uint2 *>( res );
-                        cur = nxt;
-                        if( (uint32_t) c + 4u < cols )
-                            nxt = *reinterpret_cast<const uint2 *>( res + 2u * ((uint32_t) c + 4u) );
-                    }
-                    const uint32_t w = (c & 2) ? cur.y : cur.x;
-                    const uint32_t sh = (uint32_t) (c & 1) * 16u;
-                    const uint32_t da = (w >> sh) & 0xffu;
-                    const uint32_t db = (w >> (sh + 8u)) & 0xffu;
+                    const uint32_t da = w & 0xffu;
+                    const uint32_t db = w >> 8;
                     uint32_t pa[R / 4], pb[R / 4];
                     ProfLoad<R>::load( slice + da * GR + row_in_slice, pa );
                     ProfLoad<R>::load( slice + db * GR + row_in_slice, pb );
                     uint32_t f = up_f, hd = diag;
 #pragma unroll
                     for( int r = 0; r < R; r++ ) {
-                        // off the row-to-row chain: a = max(Hdiag + V, E, 0)
+                        // a = max(Hdiag + V, E, 0); since gapO <= 0 the next
+                        // row's F only needs a: F' = max(F + gapE, a + gapO + gapE),
+                        // so the row-to-row chain is one instruction
                         const uint32_t v = prmt( pa[r >> 2], pb[r >> 2], sx_sel( r & 3 ) );
                         const uint32_t e0 = __vmaxs2( E[r], FAST_BIAS2 );
                         const uint32_t a = __viaddmax_s16x2( hd, v, e0 );
-                        // the chain through F: H = max(a, F), F' = max(F + gapE, H + gapO + gapE)
-                        const uint32_t h = __vmaxs2( a, f );
-                        const uint32_t hg = h + GOE32;                     // both halves, no borrow
-                        f = __viaddmax_s16x2( f, GE2, hg );
-                        E[r] = __viaddmax_s16x2( E[r], GE2, hg );
+                        const uint32_t h = __vmaxs2( a, f );                // H = max(a, F)
+                        f = __viaddmax_s16x2( f, GE2, a + GOE32 );          // both halves, no borrow
+                        E[r] = __viaddmax_s16x2( E[r], GE2, h + GOE32 );
                         hd = H[r];
                         H[r] = h;
                         smax = __vmaxs2( smax, h );
@@ -263,7 +286,8 @@ static cudaError_t launch_one( const FastParams & p, int grid, size_t smem, cuda
 }
 
 cudaError_t launch_sw_fast( int R, const FastParams & p, int grid, cudaStream_t st, int * blocks_per_sm ) {
-    const size_t smem = (size_t) (FAST_THREADS / 32) * 32u * p.slice_rows;   // one slice per warp
+    // one profile slice and one 32-entry boundary tile per warp
+    const size_t smem = (size_t) (FAST_THREADS / 32) * (32u * p.slice_rows + 32u * sizeof(int4));
     switch( R ) {
     case 8:
         return launch_one<8>( p, grid, smem, st, blocks_per_sm );

@@ -29,15 +29,20 @@ namespace ssa {
 constexpr int TB_R = 8;
 constexpr int TB_ROWS = 32 * TB_R;
 
-// The 32x32 score table is staged in shared memory as int32 by every CTA.
-__device__ __forceinline__ void stage_matrix( const int64_t * m, int32_t * sm ) {
-    for( int i = threadIdx.x; i < 1024; i += blockDim.x )
-        sm[i] = (int32_t) m[i];
+// The 32x32 score table is staged in shared memory as int32 by every CTA,
+// laid out [database code][query code] so that the lanes of a warp (different
+// query rows, same database column) read different banks.  transposed = true
+// stores matrix[query][db] there (the region passes score [query][db]).
+__device__ __forceinline__ void stage_matrix( const int64_t * m, int32_t * sm, bool transposed ) {
+    for( int i = threadIdx.x; i < 1024; i += blockDim.x ) {
+        const int d = i >> 5, q = i & 31;
+        sm[i] = (int32_t) (transposed ? m[(q << 5) + d] : m[(d << 5) + q]);
+    }
     __syncthreads();
 }
 
-__device__ __forceinline__ int32_t mget( const int32_t * sm, int row, int col ) {
-    return sm[(row << 5) + col];
+__device__ __forceinline__ int32_t mget( const int32_t * sm, int dcode, int qcode ) {
+    return sm[(dcode << 5) + qcode];
 }
 
 // The lane's R query codes (code 0 past the end) held in registers.
@@ -48,6 +53,32 @@ __device__ __forceinline__ void load_rows( const uint8_t * a, int64_t first, int
         code[r] = (r < nvalid) ? a[first + step * r] : 0;
 }
 
+
+// The previous pass's boundary row is read by lane 0 one column per step; a
+// warp stages it in shared memory 32 columns ahead so that the read is never
+// a global-memory round trip on the step's critical path.
+struct BoundaryPrefetch {
+    int4 * tile;     // 32 entries of this warp
+    int4 pf;
+    __device__ void start( const int4 * scratch, uint32_t scratch_cols, uint32_t cols, bool active, int lane ) {
+        pf = make_int4( 0, 0, 0, 0 );
+        if( active && (uint32_t) lane < scratch_cols && (uint32_t) lane < cols )
+            pf = scratch[lane];
+    }
+    __device__ void step( const int4 * scratch, uint32_t scratch_cols, uint32_t cols, bool active, uint32_t s,
+            int lane ) {
+        if( active && (s & 31u) == 0 ) {
+            __syncwarp();
+            tile[lane] = pf;
+            __syncwarp();
+            const uint32_t col = s + 32u + (uint32_t) lane;
+            if( col < scratch_cols && col < cols )
+                pf = scratch[col];
+        }
+    }
+    __device__ int4 get( uint32_t s ) const { return tile[s & 31u]; }
+};
+
 // ---------------------------------------------------------------------------
 // 1. SW forward region pass (reference: src/algo/align.c:39-82).  The
 //    reference iterates database rows outer and query columns inner, scoring
@@ -56,8 +87,9 @@ __device__ __forceinline__ void load_rows( const uint8_t * a, int64_t first, int
 //    value, then smallest database index, then smallest query index.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__( 256 ) tb_forward_kernel( TbParams p ) {
+    __shared__ int4 tiles[8][32];
     __shared__ int32_t smat[1024];
-    stage_matrix( p.matrix, smat );
+    stage_matrix( p.matrix, smat, true );
     const int lane = threadIdx.x & 31;
     const uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -91,7 +123,10 @@ __global__ void __launch_bounds__( 256 ) tb_forward_kernel( TbParams p ) {
             }
             int32_t diag = 0;
             int32_t out_h = 0, out_f = 0;
+            BoundaryPrefetch bp{ tiles[threadIdx.x >> 5] };
+            bp.start( scratch, p.scratch_cols, B, pass > 0, lane );
             for( uint32_t s = 0; s < B + 31; s++ ) {
+                bp.step( scratch, p.scratch_cols, B, pass > 0, s, lane );
                 int32_t up_h = __shfl_up_sync( 0xffffffffu, out_h, 1 );
                 int32_t up_f = __shfl_up_sync( 0xffffffffu, out_f, 1 );
                 const int32_t c = (int32_t) s - lane;
@@ -102,8 +137,8 @@ __global__ void __launch_bounds__( 256 ) tb_forward_kernel( TbParams p ) {
                         up_h = 0;
                         up_f = gO + gE;   // f starts at gapO: max(gapO, 0 + gapO) + gapE
                     }
-                    else if( (uint32_t) c < p.scratch_cols ) {
-                        int4 v = scratch[c];
+                    else {
+                        const int4 v = bp.get( s );
                         up_h = v.x;
                         up_f = v.y;
                     }
@@ -114,7 +149,7 @@ __global__ void __launch_bounds__( 256 ) tb_forward_kernel( TbParams p ) {
                 for( int r = 0; r < TB_R; r++ ) {
                     if( r < nvalid ) {
                         int32_t e_in = E[r];
-                        int32_t x = hd + mget( smat, qa[r], d );
+                        int32_t x = hd + mget( smat, d, qa[r] );
                         if( x < 0 )
                             x = 0;
                         if( f > x )
@@ -182,8 +217,9 @@ __global__ void __launch_bounds__( 256 ) tb_forward_kernel( TbParams p ) {
 //    whose value reaches the forward score.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__( 256 ) tb_reverse_kernel( TbParams p ) {
+    __shared__ int4 tiles[8][32];
     __shared__ int32_t smat[1024];
-    stage_matrix( p.matrix, smat );
+    stage_matrix( p.matrix, smat, true );
     const int lane = threadIdx.x & 31;
     const uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -235,7 +271,17 @@ __global__ void __launch_bounds__( 256 ) tb_reverse_kernel( TbParams p ) {
                     diag = (jprev > b_end) ? lh[jprev] : -1;
             }
             int32_t out_h = 0, out_f = 0;
+            // columns past the first one holding a begin-cell candidate cannot
+            // change the result: stop once every lane has passed it
+            int32_t limit = __reduce_min_sync( 0xffffffffu, hit_i );
+            BoundaryPrefetch bp{ tiles[threadIdx.x >> 5] };
+            bp.start( scratch, p.scratch_cols, B, pass > 0, lane );
             for( uint32_t s = 0; s < B + 31; s++ ) {
+                if( (s & 7) == 0 )
+                    limit = __reduce_min_sync( 0xffffffffu, hit_i );
+                if( limit != INT_MAX && (int64_t) s > (int64_t) limit + 31 )
+                    break;
+                bp.step( scratch, p.scratch_cols, B, pass > 0, s, lane );
                 int32_t up_h = __shfl_up_sync( 0xffffffffu, out_h, 1 );
                 int32_t up_f = __shfl_up_sync( 0xffffffffu, out_f, 1 );
                 const int32_t c = (int32_t) s - lane;
@@ -246,8 +292,8 @@ __global__ void __launch_bounds__( 256 ) tb_reverse_kernel( TbParams p ) {
                         up_h = -1;                        // h starts at -1 per row
                         up_f = max( -1, -1 + gO ) + gE;   // f = max(-1, h + gapO) + gapE
                     }
-                    else if( (uint32_t) c < p.scratch_cols ) {
-                        int4 v = scratch[c];
+                    else {
+                        const int4 v = bp.get( s );
                         up_h = v.x;
                         up_f = v.y;
                     }
@@ -259,7 +305,7 @@ __global__ void __launch_bounds__( 256 ) tb_reverse_kernel( TbParams p ) {
                 for( int r = 0; r < TB_R; r++ ) {
                     if( r < nvalid ) {
                         int32_t e_in = E[r];
-                        int32_t x = hd + mget( smat, qa[r], d );
+                        int32_t x = hd + mget( smat, d, qa[r] );
                         if( f > x )
                             x = f;
                         if( e_in > x )
@@ -316,8 +362,9 @@ __global__ void __launch_bounds__( 256 ) tb_reverse_kernel( TbParams p ) {
 //    16-bit word (8 rows x 2 bits) per lane and column.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__( 256 ) tb_directions_kernel( TbParams p ) {
+    __shared__ int4 tiles[8][32];
     __shared__ int32_t smat[1024];
-    stage_matrix( p.matrix, smat );
+    stage_matrix( p.matrix, smat, false );
     const int lane = threadIdx.x & 31;
     const uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -351,7 +398,10 @@ __global__ void __launch_bounds__( 256 ) tb_directions_kernel( TbParams p ) {
             }
             int32_t diag = nw ? ((row0 == 0) ? 0 : gO + row0 * gE) : 0;
             int32_t out_h = 0, out_f = 0;
+            BoundaryPrefetch bp{ tiles[threadIdx.x >> 5] };
+            bp.start( scratch, p.scratch_cols, B, pass > 0, lane );
             for( uint32_t s = 0; s < B + 31; s++ ) {
+                bp.step( scratch, p.scratch_cols, B, pass > 0, s, lane );
                 int32_t up_h = __shfl_up_sync( 0xffffffffu, out_h, 1 );
                 int32_t up_f = __shfl_up_sync( 0xffffffffu, out_f, 1 );
                 const int32_t j = (int32_t) s - lane;     // database index
@@ -363,8 +413,8 @@ __global__ void __launch_bounds__( 256 ) tb_directions_kernel( TbParams p ) {
                         up_h = nw ? gO + (j + 1) * gE : 0;
                         up_f = nw ? 2 * gO + (j + 2) * gE : 0;
                     }
-                    else if( (uint32_t) j < p.scratch_cols ) {
-                        int4 v = scratch[j];
+                    else {
+                        const int4 v = bp.get( s );
                         up_h = v.x;
                         up_f = v.y;
                     }
@@ -466,15 +516,26 @@ __global__ void tb_walk_kernel( TbParams p ) {
     p.ops_len[h] = (uint32_t) n;
 }
 
-cudaError_t launch_traceback( const TbParams & p, bool any_sw, int grid, cudaStream_t st ) {
+// ev (optional): 5 events recorded around the four kernels.
+cudaError_t launch_traceback( const TbParams & p, bool any_sw, int grid, cudaStream_t st, cudaEvent_t * ev ) {
     if( p.n_hits == 0 )
         return cudaSuccess;
-    if( any_sw ) {
+    if( ev )
+        cudaEventRecord( ev[0], st );
+    if( any_sw )
         tb_forward_kernel<<<grid, 256, 0, st>>>( p );
+    if( ev )
+        cudaEventRecord( ev[1], st );
+    if( any_sw )
         tb_reverse_kernel<<<grid, 256, 0, st>>>( p );
-    }
+    if( ev )
+        cudaEventRecord( ev[2], st );
     tb_directions_kernel<<<grid, 256, 0, st>>>( p );
+    if( ev )
+        cudaEventRecord( ev[3], st );
     tb_walk_kernel<<<(p.n_hits + 127) / 128, 128, 0, st>>>( p );
+    if( ev )
+        cudaEventRecord( ev[4], st );
     return cudaGetLastError();
 }
 
