@@ -68,6 +68,45 @@ size_t ssa_query_length( p_query p );
  */
 int ssa_db_b200_load_memory( size_t count, const char * residues, const uint64_t * offsets );
 
+/*
+ * Allocation-free scoring.  No counterpart in the reference, whose searches
+ * allocate their buffers per call (src/algo/searcher.c:43,160).
+ *
+ * Scores one query against count database sequences that the caller already
+ * holds in device memory, with the exact 64-bit recurrences of a BIT_WIDTH_64
+ * search (same scores as sw_align/nw_align at BIT_WIDTH_64), writing
+ * d_scores[i] for sequence i.  Uses the global matrix and gap penalties.
+ * Residues are the library's codes: index into "-ABCDEFGHIKLMNPQRSTVWXYZU*OJ"
+ * for amino acids, into "-ACMGRSVTWYHKDBN" for nucleotides; sequence i is
+ * d_db_codes[d_db_offsets[i] .. + d_db_lengths[i]).  A sequence of length 0
+ * scores 0.
+ *
+ * It allocates no memory: for callers whose device memory is reserved by
+ * their own pool, or that cannot take cudaFree's device-wide synchronisation
+ * on a latency-bound path.  Its working buffers are fixed-size device arrays
+ * of the library (about 9.6 MiB per device), set up by the first call on each
+ * device -- make that first call, with the device current, before the phase
+ * that must not allocate and before any stream capture.  Sizes beyond the
+ * limits below are rejected with SSA_B200_NOALLOC_ETOOBIG; max_seq_len is the
+ * caller's bound on the database lengths.  The call runs on `stream` (a
+ * cudaStream_t; NULL = default stream) and returns when the scores are
+ * written.  Calls overlapping in time on one device (two host threads, or two
+ * streams) share the buffers and race.
+ */
+#define SSA_B200_NOALLOC_MAX_QUERY 4096u
+#define SSA_B200_NOALLOC_MAX_SEQ_LEN 4096u
+#define SSA_B200_NOALLOC_MAX_SEQS 262144u
+
+#define SSA_B200_NOALLOC_OK 0
+#define SSA_B200_NOALLOC_EINVAL 1      /* bad argument or no score matrix */
+#define SSA_B200_NOALLOC_ETOOBIG 2     /* a size above the limits above */
+#define SSA_B200_NOALLOC_ECUDA 3       /* CUDA error */
+#define SSA_B200_NOALLOC_ESEQLEN 4     /* a sequence exceeded SSA_B200_NOALLOC_MAX_SEQ_LEN */
+
+int ssa_b200_score64_noalloc( int algorithm, const uint8_t * d_query, uint32_t query_len,
+        const uint8_t * d_db_codes, const uint64_t * d_db_offsets, const uint32_t * d_db_lengths, uint32_t count,
+        uint32_t max_seq_len, int32_t * d_scores, void * stream );
+
 #ifdef __cplusplus
 }
 #endif

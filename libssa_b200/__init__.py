@@ -36,8 +36,12 @@ EXPORTED = [
     "set_output_mode", "set_simd_compute_mode", "set_chunk_size", "set_thread_count", "init_score_matrix",
     "init_constant_scores", "init_gap_penalties", "init_symbol_translation", "init_db", "init_sequence_fasta",
     "free_sequence", "sw_align", "nw_align", "free_alignment", "ssa_exit", "ssa_align_batch", "ssa_get_stats",
-    "ssa_query_length", "ssa_db_refresh", "ssa_b200_int_peak",
+    "ssa_query_length", "ssa_db_refresh", "ssa_b200_int_peak", "ssa_b200_score64_noalloc",
 ]
+
+# allocation-free scoring (include/libssa_b200.h)
+NOALLOC_MAX_QUERY, NOALLOC_MAX_SEQ_LEN, NOALLOC_MAX_SEQS = 4096, 4096, 262144
+NOALLOC_OK, NOALLOC_EINVAL, NOALLOC_ETOOBIG, NOALLOC_ECUDA, NOALLOC_ESEQLEN = 0, 1, 2, 3, 4
 
 
 class DbSeq(ctypes.Structure):
@@ -115,6 +119,10 @@ def load():
     lib.ssa_b200_int_peak.restype = ctypes.c_int
     lib.ssa_query_length.argtypes = [ctypes.c_void_p]
     lib.ssa_query_length.restype = ctypes.c_size_t
+    lib.ssa_b200_score64_noalloc.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p,
+                                             ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32,
+                                             ctypes.c_void_p, ctypes.c_void_p]
+    lib.ssa_b200_score64_noalloc.restype = ctypes.c_int
     _plugin.ssa_db_b200_load_memory.argtypes = [ctypes.c_size_t, ctypes.c_char_p, ctypes.POINTER(ctypes.c_uint64)]
     _plugin.ssa_db_b200_load_memory.restype = ctypes.c_int
     _plugin.ssa_db_get_sequence_count.restype = ctypes.c_size_t
@@ -254,6 +262,14 @@ def int_peak() -> tuple[float, float]:
     if load().ssa_b200_int_peak(ctypes.byref(a), ctypes.byref(b)) != 0:
         raise RuntimeError("integer peak probe failed")
     return a.value, b.value
+
+
+def score64_noalloc(algorithm: int, d_query: int, query_len: int, d_codes: int, d_offsets: int,
+                    d_lengths: int, count: int, max_seq_len: int, d_scores: int, stream: int = 0) -> int:
+    """ssa_b200_score64_noalloc() on raw device addresses; returns its status
+    code (NOALLOC_OK on success)."""
+    return int(load().ssa_b200_score64_noalloc(algorithm, d_query, query_len, d_codes, d_offsets, d_lengths,
+                                               count, max_seq_len, d_scores, stream or None))
 
 
 def query_length(q) -> int:

@@ -31,7 +31,8 @@ NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompil
               "--expt-relaxed-constexpr", "-I" + INCLUDE, "-I" + CSRC]
 CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-fvisibility=hidden", "-Wall", "-I" + INCLUDE, "-I" + CSRC]
 
-CU_SOURCES = ["engine.cu", "emul_kernel.cu", "traceback_kernels.cu", "diag_kernels.cu", "sw_fast_kernel.cu"]
+CU_SOURCES = ["engine.cu", "emul_kernel.cu", "traceback_kernels.cu", "diag_kernels.cu", "sw_fast_kernel.cu",
+              "noalloc.cu"]
 CPP_SOURCES = ["api.cpp", "replay.cpp"]
 HEADERS = ["device_common.cuh", "ssa_internal.h", "builtin_matrices.inc"]
 
