@@ -47,10 +47,11 @@ typedef struct {
 
 void ssa_get_stats( ssa_stats_t * out );
 
-/* Measured packed-16x2 integer max throughput of the current device, in
- * lane operations per second (2 per instruction and thread), and the same as
- * warp instructions per clock per SM.  The denominator of the search kernels'
- * integer-pipe roofline.  Returns 0 on success. */
+/* Measured integer ALU-pipe ceiling of the current device: the rate of the
+ * fused packed 16x2 add-max instruction, in operations per second (an add and
+ * a max in each 16-bit half of each thread: 4 per instruction and thread),
+ * and the same as warp instructions per clock per SM.  The denominator of the
+ * search kernels' integer-pipe roofline.  Returns 0 on success. */
 int ssa_b200_int_peak( double * lane_ops_per_second, double * instructions_per_clock_per_sm );
 
 /* Marks the packed copy of the database stale, so the next search reads it

@@ -256,8 +256,9 @@ def stats() -> Stats:
 
 
 def int_peak() -> tuple[float, float]:
-    """(lane operations per second, warp instructions per clock per SM) of
-    packed 16x2 max on the current device."""
+    """(operations per second, warp instructions per clock per SM) of the
+    fused packed 16x2 add-max on the current device: the integer ALU pipe's
+    ceiling, counting an add and a max per 16-bit half."""
     a, b = ctypes.c_double(0), ctypes.c_double(0)
     if load().ssa_b200_int_peak(ctypes.byref(a), ctypes.byref(b)) != 0:
         raise RuntimeError("integer peak probe failed")

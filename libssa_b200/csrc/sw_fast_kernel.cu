@@ -27,10 +27,11 @@
 //     memory; per cell a PRMT sign-extends the two sequences' scores into a
 //     16x2 word;
 //   * all values carry a +1024 bias per half, so an add of gapO + gapE is a
-//     plain 32-bit IADD (no borrow can cross halves) and the SW zero floor is
-//     a max with the bias;  per 16x2 cell pair: 4 half-rate DPX/PRMT and
-//     5 full-rate instructions, with a one-instruction dependency from row to
-//     row;
+//     plain 32-bit IADD (no borrow can cross halves: H never drops below the
+//     bias) and the SW zero floor is a max with the bias;  per 16x2 cell
+//     pair: one PRMT, three maxes, three fused add-max (all on the ALU pipe,
+//     16 lanes per clock per SM sub-partition) and two IADDs (ALU or FMA
+//     pipe), with a one-instruction dependency from row to row;
 //   * every warp schedules itself: it takes (query, range of pairs) units from
 //     a global counter, keeps the current pass's rows of the query profile in
 //     its own shared-memory slice, and never waits on other warps;
@@ -173,8 +174,9 @@ __global__ void __launch_bounds__( 128, 4 ) sw_fast_kernel( FastParams p ) {
                 if( pass > 0 && (uint32_t) k < p.scratch_cols && (uint32_t) k < cols )
                     pf = scratch[k];
                 const uint32_t steps = max_cols + (uint32_t) G - 1u;
+                const uint32_t gmask = (uint32_t) G - 1u;    // G is a power of two
                 for( uint32_t s = 0; s < steps; s++ ) {
-                    if( pass > 0 && (s % (uint32_t) G) == 0 ) {
+                    if( pass > 0 && (s & gmask) == 0 ) {
                         __syncwarp();
                         tile[k] = pf;
                         __syncwarp();
@@ -191,14 +193,15 @@ __global__ void __launch_bounds__( 128, 4 ) sw_fast_kernel( FastParams p ) {
                     q1 = q2;
                     q2 = q3;
                     {
-                        const int32_t col = c + 4;
-                        q3 = (col >= 0 && (uint32_t) col < cols)
-                                ? (uint32_t) *reinterpret_cast<const uint16_t *>( res + 2u * (uint32_t) col ) : 0u;
+                        // columns past the pair read its pad or the next pair's
+                        // residues (never used); the buffer has 16 bytes of slack
+                        const uint32_t col = min( (uint32_t) max( c + 4, 0 ), cols + 3u );
+                        q3 = (uint32_t) *reinterpret_cast<const uint16_t *>( res + 2u * col );
                     }
                     if( c < 0 || (uint32_t) c >= cols )
                         continue;
                     if( k == 0 ) {
-                        const int4 v = tile[s % (uint32_t) G];
+                        const int4 v = tile[s & gmask];
                         up_h = pass ? (uint32_t) v.x : FAST_BIAS2;
                         up_f = pass ? (uint32_t) v.y : FAST_BIAS2;
                         up_s = pass ? (uint32_t) v.z : FAST_BIAS2;
