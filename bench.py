@@ -118,22 +118,29 @@ def dist_setup():
     return world, rank, local, pg
 
 
-def reduce_max(pg, x: float) -> float:
+def _reduce(pg, x: float, op) -> float:
     if pg is None:
         return x
     import torch
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    device = "cuda" if pg.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=op)
     return float(t.item())
+
+
+def reduce_max(pg, x: float) -> float:
+    """Max over ranks (the job's time is the slowest rank's)."""
+    return _reduce(pg, x, pg.ReduceOp.MAX) if pg is not None else x
 
 
 def reduce_sum(pg, x: float) -> float:
-    if pg is None:
-        return x
-    import torch
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    pg.all_reduce(t, op=pg.ReduceOp.SUM)
-    return float(t.item())
+    """Sum over ranks (all ranks' cells)."""
+    return _reduce(pg, x, pg.ReduceOp.SUM) if pg is not None else x
+
+
+def job_throughput(pg, cells_per_step: float, steps: int, seconds: float) -> float:
+    """GCUPS of the whole job: every rank's cells over the slowest rank's time."""
+    return reduce_sum(pg, float(cells_per_step)) * steps / reduce_max(pg, seconds) / 1e9
 
 
 def barrier(pg):
@@ -158,6 +165,12 @@ def make_workload(scale: float, query_seed: int, kind: str = "sw_batched", n_que
         lens = W.lognormal_lengths(rng, len(w.queries), 300.0, 0.7)
         w.queries = [W.random_residues(rng, int(L), W.AA20).tobytes() for L in lens]
     return w
+
+
+def rank_workload(args, rank: int):
+    """A rank's shard of the job: its own seeded query batch (rank 0 the
+    canonical one) against the full database, which every rank holds."""
+    return make_workload(args.scale, 3 if rank == 0 else 3 + rank, args.workload, args.queries)
 
 
 def load_traffic() -> float | None:
@@ -236,7 +249,7 @@ def run_ours(args):
         from libssa_b200 import build
         build.build()
     L.load()
-    w = make_workload(args.scale, 3 if rank == 0 else 3 + rank, args.workload, args.queries)
+    w = rank_workload(args, rank)
     L.set_output_mode(L.OUTPUT_SILENT)
     L.init_symbol_translation(L.AMINOACID, L.FORWARD_STRAND, 1, 1)
     L.init_score_matrix(L.MATRIX_BUILDIN, "blosum62")

@@ -9,6 +9,9 @@ fixtures of its own test suite).  Writes:
   read (copied unchanged from the reference's tests/testdata/);
 * ``matrices.json`` -- the reference's 32x32 score tables of every built-in
   matrix, of constant scoring and of the file matrices in data/;
+* ``abi_layout.json`` -- sizes, field offsets and constants of the
+  reference's libssa.h / libssa_extern_db.h as its compiler sees them
+  (tests/c_client/abi_layout.c built against the reference's headers);
 * ``cases.json``    -- seeded synthetic search cases (inputs stored inline, or
   regenerated from libssa_b200.workloads with the stored seed and checked by
   hash) with the reference's complete answer: hit IDs, scores, CIGARs,
@@ -117,10 +120,27 @@ def synthetic_cases() -> list[tuple[dict, list[bytes], list[bytes], bool]]:
     return cases
 
 
+def write_abi_layout(reference: str) -> None:
+    import subprocess
+    import tempfile
+    src = os.path.join(os.path.dirname(HERE), "c_client", "abi_layout.c")
+    with tempfile.TemporaryDirectory() as tmp:
+        exe = os.path.join(tmp, "abi_layout")
+        subprocess.run(["gcc", "-I" + os.path.join(reference, "src"), "-o", exe, src], check=True)
+        out = subprocess.run([exe], check=True, capture_output=True, text=True).stdout
+    layout = json.loads(out)
+    with open(os.path.join(HERE, "abi_layout.json"), "w") as f:
+        json.dump(layout, f, indent=1)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--abi-only", action="store_true", help="only regenerate abi_layout.json")
     args = ap.parse_args()
+    write_abi_layout(args.reference)
+    if args.abi_only:
+        return
     oracle.build(args.reference)
     data = os.path.join(HERE, "data")
     os.makedirs(data, exist_ok=True)
