@@ -32,7 +32,7 @@ NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompil
 CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-fvisibility=hidden", "-Wall", "-I" + INCLUDE, "-I" + CSRC]
 
 CU_SOURCES = ["engine.cu", "emul_kernel.cu", "traceback_kernels.cu", "diag_kernels.cu", "sw_fast_kernel.cu",
-              "noalloc.cu"]
+              "noalloc.cu", "sw_qpair_kernel.cu"]
 CPP_SOURCES = ["api.cpp", "replay.cpp"]
 HEADERS = ["device_common.cuh", "ssa_internal.h", "builtin_matrices.inc"]
 

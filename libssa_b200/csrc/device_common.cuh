@@ -153,4 +153,38 @@ cudaError_t launch_build_profile8( const uint8_t * qcodes, const uint64_t * qoff
         const uint32_t * slots, uint32_t n, const uint32_t * rows_of, const int64_t * matrix, int8_t * prof,
         const uint64_t * prof_off, cudaStream_t st );
 
+// ---- query-pair Smith-Waterman entry pass (sw_qpair_kernel.cu) -------------
+// Two queries of similar length share each 32-bit register (low half query A,
+// high half query B) against one database sequence per group of QP_G threads.
+constexpr int QP_G = 4;               // threads per sequence
+constexpr int QP_GPW = 32 / QP_G;     // sequences per warp
+constexpr int QP_CODES = 28;          // residue codes with a profile row (AA 0..27, NT 0..15)
+constexpr int QP_THREADS_PER_CTA = 128;
+
+struct QPairParams {
+    DbView db;
+    const uint32_t * order;       // non-empty IDs, longest first
+    const uint32_t * prof;        // per query pair: QP_CODES x rows words (16x2: A low, B high)
+    const uint64_t * prof_off;    // per query pair, in words
+    const uint32_t * qp_slots;    // per query pair: slot A, slot B (0xffffffff when absent)
+    const uint32_t * qp_rows;     // per query pair: profile rows (passes x QP_G x R)
+    // work units u = chunk * n_class + i: query pair unit_pairs[i] against the
+    // sequences order[chunk_bounds[chunk] .. chunk_bounds[chunk + 1])
+    const uint32_t * unit_pairs;
+    uint32_t n_class;
+    const uint32_t * chunk_bounds;
+    uint64_t n_units;
+    unsigned long long * unit_counter;
+    int gap_oe;                   // (int8) (gapO + gapE)
+    int gap_e;
+    PassSink sink;
+    int4 * scratch;               // per warp and group: scratch_cols column pairs (H, F of two columns)
+    uint32_t scratch_cols;
+};
+
+cudaError_t launch_sw_qpair( int R, const QPairParams & p, int grid, cudaStream_t st, int * blocks_per_sm );
+cudaError_t launch_build_profile_qp( const uint8_t * qcodes, const uint64_t * qoff, const uint32_t * qlen,
+        const uint32_t * qp_slots, uint32_t n_qp, const uint32_t * qp_rows, const int64_t * matrix, uint32_t * prof,
+        const uint64_t * prof_off, cudaStream_t st );
+
 }  // namespace ssa

@@ -291,7 +291,7 @@ public:
             &d_scratch_fast_[0], &d_scratch_fast_[1], &d_scratch_fast_[2], &d_scratch_fast_[3], &d_qcodes_, &d_qoff_, &d_qlen_, &d_qpad_,
             &d_prof_off_, &d_prof_, &d_matrix_, &d_score_, &d_list_a_, &d_list_b_, &d_counts_, &d_scratch_,
             &d_tb_hits_, &d_tb_regions_, &d_tb_last_, &d_tb_last_off_, &d_tb_dirs_, &d_tb_dir_off_, &d_tb_ops_,
-            &d_tb_ops_off_, &d_tb_ops_len_ };
+            &d_tb_ops_off_, &d_tb_ops_len_, &d_qp_prof_, &d_qp_off_, &d_qp_rows_, &d_qp_slots_, &d_qp_units_ };
         for( DevBuf * b : bufs )
             b->release();
         h_score_.release();
@@ -309,6 +309,8 @@ private:
             uint64_t n_tasks, bool implicit, PairTask * next, unsigned * next_count, uint32_t next_cap,
             const uint32_t * slot_list = nullptr, uint32_t n_sub = 0 );
     void run_fast_entry( const SearchRequest & req, uint32_t nq, PairTask * next, unsigned * next_count, uint32_t cap );
+    void run_qpair_entry( const SearchRequest & req, uint32_t nq, PairTask * next, unsigned * next_count,
+            uint32_t cap );
     void build_profiles( int width, uint32_t n_slots );
     void traceback( const SearchRequest & req, const std::vector<QueryCodes> & queries, uint32_t slot0,
             std::vector<std::vector<Hit>> & out, SearchStats & stats );
@@ -330,6 +332,7 @@ private:
     DevBuf d_prof8_, d_prof8_off_, d_rows_, d_slots_;
     DevBuf d_scratch_fast_[4];
     DevBuf d_bounds_, d_group_;
+    DevBuf d_qp_prof_, d_qp_off_, d_qp_rows_, d_qp_slots_, d_qp_units_;
     cudaStream_t class_stream_[4] = { nullptr, nullptr, nullptr, nullptr };
     cudaEvent_t ev_class_[4] = { nullptr, nullptr, nullptr, nullptr };
     cudaEvent_t ev_ready_ = nullptr;
@@ -596,6 +599,165 @@ void Engine::run_fast_entry( const SearchRequest & req, uint32_t nq, PairTask * 
     }
 }
 
+// Batches: queries sorted by length are paired, the two queries of a pair
+// share the 16x2 lanes (sw_qpair_kernel.cu).  Rows per thread R for a pair of
+// Q rows (the longer query): the smallest estimated issue cost per column
+// pair, passes x (13 R + 40), with QP_G x R rows per pass.
+static int choose_qpair_rows( uint32_t Q, uint32_t * passes ) {
+    int best_r = 0;
+    double best_cost = 1e300;
+    for( int R : { 16, 20, 24, 28 } ) {
+        const uint32_t per = (uint32_t) (QP_G * R);
+        const uint32_t P = std::max<uint32_t>( 1, (Q + per - 1) / per );
+        if( (uint64_t) P * per > FAST_MAX_ROWS )
+            continue;
+        const double cost = (double) P * (13.0 * R + 40.0);
+        if( cost < best_cost ) {
+            best_cost = cost;
+            best_r = R;
+            *passes = P;
+        }
+    }
+    return best_r;
+}
+
+void Engine::run_qpair_entry( const SearchRequest & req, uint32_t nq, PairTask * next, unsigned * next_count,
+        uint32_t cap ) {
+    const uint32_t n_seq = (uint32_t) db_.order_desc.size();
+    if( n_seq == 0 )
+        return;
+    // pair the queries that fit, longest first; longer ones run the emulation
+    std::vector<uint32_t> fit, fallback;
+    for( uint32_t s = 0; s < nq; s++ )
+        (h_qlen_[s] <= FAST_MAX_ROWS ? fit : fallback).push_back( s );
+    std::stable_sort( fit.begin(), fit.end(), [&]( uint32_t a, uint32_t b ) { return h_qlen_[a] > h_qlen_[b]; } );
+    const uint32_t n_qp = (uint32_t) ((fit.size() + 1) / 2);
+    std::vector<uint32_t> qp_slots( 2 * std::max<uint32_t>( 1, n_qp ), 0xffffffffu );
+    std::vector<uint32_t> qp_rows( std::max<uint32_t>( 1, n_qp ), 0 );
+    std::vector<uint64_t> qp_off( std::max<uint32_t>( 1, n_qp ), 0 );
+    std::vector<std::vector<uint32_t>> by_r( 4 );     // R = 16, 20, 24, 28
+    uint64_t total = 0;
+    for( uint32_t i = 0; i < n_qp; i++ ) {
+        qp_slots[2 * i] = fit[2 * i];
+        if( 2 * i + 1 < fit.size() )
+            qp_slots[2 * i + 1] = fit[2 * i + 1];
+        uint32_t P = 1;
+        const int R = choose_qpair_rows( h_qlen_[fit[2 * i]], &P );
+        qp_rows[i] = P * (uint32_t) (QP_G * R);
+        by_r[R / 4 - 4].push_back( i );
+    }
+    // profiles: QP_CODES x rows words per pair (16-byte aligned: rows % 16 == 0)
+    for( int ri = 0; ri < 4; ri++ )
+        for( uint32_t i : by_r[ri] ) {
+            qp_off[i] = total;
+            total += (uint64_t) QP_CODES * qp_rows[i];
+        }
+    std::vector<uint32_t> units;                  // pairs grouped by class
+    for( auto & v : by_r )
+        units.insert( units.end(), v.begin(), v.end() );
+    d_qp_prof_.ensure( std::max<uint64_t>( total, 4 ) * sizeof(uint32_t) );
+    d_qp_off_.ensure( qp_off.size() * sizeof(uint64_t) );
+    d_qp_rows_.ensure( qp_rows.size() * sizeof(uint32_t) );
+    d_qp_slots_.ensure( qp_slots.size() * sizeof(uint32_t) );
+    d_qp_units_.ensure( std::max<size_t>( 1, units.size() ) * sizeof(uint32_t) );
+    CUDA_CHECK( cudaMemcpyAsync( d_qp_off_.p, qp_off.data(), qp_off.size() * sizeof(uint64_t), cudaMemcpyHostToDevice,
+            stream_ ) );
+    CUDA_CHECK( cudaMemcpyAsync( d_qp_rows_.p, qp_rows.data(), qp_rows.size() * sizeof(uint32_t),
+            cudaMemcpyHostToDevice, stream_ ) );
+    CUDA_CHECK( cudaMemcpyAsync( d_qp_slots_.p, qp_slots.data(), qp_slots.size() * sizeof(uint32_t),
+            cudaMemcpyHostToDevice, stream_ ) );
+    if( !units.empty() )
+        CUDA_CHECK( cudaMemcpyAsync( d_qp_units_.p, units.data(), units.size() * sizeof(uint32_t),
+                cudaMemcpyHostToDevice, stream_ ) );
+    if( n_qp ) {
+        CUDA_CHECK( launch_build_profile_qp( d_qcodes_.as<uint8_t>(), d_qoff_.as<uint64_t>(), d_qlen_.as<uint32_t>(),
+                d_qp_slots_.as<uint32_t>(), n_qp, d_qp_rows_.as<uint32_t>(), d_matrix_.as<int64_t>(),
+                d_qp_prof_.as<uint32_t>(), d_qp_off_.as<uint64_t>(), stream_ ) );
+        launches_++;
+    }
+
+    // work units: ranges of length-sorted sequences (multiples of QP_GPW)
+    // holding about equal numbers of columns, the longest first; every pair of
+    // a class gets every range.  A warp takes one unit at a time.
+    uint64_t total_cols = 0;
+    for( uint32_t id : db_.order_desc )
+        total_cols += (db_.len[id] + 3u) & ~3u;
+    const uint64_t want_units = (uint64_t) sms_ * 16 * 24;
+    const uint64_t target = std::max<uint64_t>( 1, total_cols * std::max<uint32_t>( 1, n_qp ) / want_units );
+    std::vector<uint32_t> bounds{ 0 };
+    {
+        uint64_t acc = 0;
+        for( uint32_t i = 0; i < n_seq; i++ ) {
+            acc += (db_.len[db_.order_desc[i]] + 3u) & ~3u;
+            if( acc >= target && (i + 1) % QP_GPW == 0 ) {
+                bounds.push_back( i + 1 );
+                acc = 0;
+            }
+        }
+        if( bounds.back() != n_seq )
+            bounds.push_back( n_seq );
+    }
+    const uint32_t n_chunks = (uint32_t) bounds.size() - 1;
+    d_bounds_.ensure( bounds.size() * sizeof(uint32_t) );
+    CUDA_CHECK( cudaMemcpyAsync( d_bounds_.p, bounds.data(), bounds.size() * sizeof(uint32_t), cudaMemcpyHostToDevice,
+            stream_ ) );
+    CUDA_CHECK( cudaEventRecord( ev_ready_, stream_ ) );
+    const uint32_t scratch_cols = (((db_.max_len + 3u) & ~3u) >> 1) + 2u;
+    size_t class_first = 0;
+    for( int ri = 0; ri < 4; ri++ ) {
+        const std::vector<uint32_t> & cls = by_r[ri];
+        if( cls.empty() )
+            continue;
+        const int R = 4 * (ri + 4);
+        bool multi = false;
+        for( uint32_t i : cls )
+            multi |= qp_rows[i] > (uint32_t) (QP_G * R);
+        QPairParams p{};
+        int per_sm = 0;
+        CUDA_CHECK( launch_sw_qpair( R, p, 0, class_stream_[ri], &per_sm ) );
+        const int grid = sms_ * std::max( 1, per_sm );
+        CUDA_CHECK( cudaStreamWaitEvent( class_stream_[ri], ev_ready_, 0 ) );
+        unsigned long long * unit_counter = d_counts_.as<unsigned long long>() + 8 + ri;   // bytes 64..95
+        CUDA_CHECK( cudaMemsetAsync( unit_counter, 0, sizeof(unsigned long long), class_stream_[ri] ) );
+        p.db = DbView{ d_codes_.as<uint8_t>(), d_off_.as<uint64_t>(), d_len_.as<uint32_t>(), db_.n_ids };
+        p.order = d_order_.as<uint32_t>();
+        p.prof = d_qp_prof_.as<uint32_t>();
+        p.prof_off = d_qp_off_.as<uint64_t>();
+        p.qp_slots = d_qp_slots_.as<uint32_t>();
+        p.qp_rows = d_qp_rows_.as<uint32_t>();
+        p.unit_pairs = d_qp_units_.as<uint32_t>() + class_first;
+        p.n_class = (uint32_t) cls.size();
+        p.chunk_bounds = d_bounds_.as<uint32_t>();
+        p.n_units = (uint64_t) n_chunks * cls.size();
+        p.unit_counter = unit_counter;
+        p.gap_oe = (int8_t) (req.gap_open + req.gap_extend);
+        p.gap_e = req.gap_extend;
+        p.sink.score = d_score_.as<int32_t>();
+        p.sink.score_stride = db_.n_ids;
+        p.sink.next = next;
+        p.sink.next_count = next_count;
+        p.sink.next_cap = cap;
+        p.sink.error_flags = d_counts_.as<unsigned>() + 2;
+        if( multi ) {
+            p.scratch = (int4 *) d_scratch_fast_[ri].ensure( (size_t) grid * (QP_THREADS_PER_CTA / 32) * QP_GPW *
+                    scratch_cols * sizeof(int4) );
+            p.scratch_cols = scratch_cols;
+        }
+        CUDA_CHECK( launch_sw_qpair( R, p, grid, class_stream_[ri], nullptr ) );
+        launches_++;
+        CUDA_CHECK( cudaEventRecord( ev_class_[ri], class_stream_[ri] ) );
+        CUDA_CHECK( cudaStreamWaitEvent( stream_, ev_class_[ri], 0 ) );
+        class_first += cls.size();
+    }
+    if( !fallback.empty() ) {
+        d_slots_.ensure( fallback.size() * sizeof(uint32_t) );
+        CUDA_CHECK( cudaMemcpyAsync( d_slots_.p, fallback.data(), fallback.size() * sizeof(uint32_t),
+                cudaMemcpyHostToDevice, stream_ ) );
+        run_pass( 0, 8, req, nq, nullptr, (uint64_t) fallback.size() * n_seq, true, next, next_count, cap,
+                d_slots_.as<uint32_t>(), (uint32_t) fallback.size() );
+    }
+}
+
 void Engine::search( const SearchRequest & req, const std::vector<QueryCodes> & queries,
         std::vector<std::vector<Hit>> & out, SearchStats & stats ) {
     init_device();
@@ -671,7 +833,9 @@ void Engine::search( const SearchRequest & req, const std::vector<QueryCodes> & 
         const int entry = req.bit_width;
         std::vector<PairTask> list_entry, list_16;   // host copies for the replay
         unsigned n_a = 0, n_b = 0;
-        if( fast_eligible( req ) )
+        if( fast_eligible( req ) && nq >= 2 && !getenv( "SSA_B200_NO_QPAIR" ) )
+            run_qpair_entry( req, nq, d_list_a_.as<PairTask>(), cnt + 0, cap );
+        else if( fast_eligible( req ) )
             run_fast_entry( req, nq, d_list_a_.as<PairTask>(), cnt + 0, cap );
         else
             run_pass( req.algo, entry, req, nq, nullptr, n_pairs, true, d_list_a_.as<PairTask>(), cnt + 0, cap );

@@ -1,0 +1,324 @@
+// sw_qpair_kernel.cu -- the Smith-Waterman 8-bit-entry search pass for
+// batches: two queries per register.
+//
+// Semantics are those of sw_fast_kernel.cu (exact 16-bit scores with a +1024
+// bias per half, the first column at which a running maximum reaches 255
+// gives the reference lane's overflow block; reference:
+// src/algo/simd/search_simd_sw.c:172-182, 369-382, 422-423).  What changes is
+// what shares a register: here the low half carries query A and the high half
+// query B of a length-sorted query pair, both against the same database
+// sequence.  The profile word of a (residue, row) is then one 16x2 value that
+// a 128-bit shared load delivers four rows at a time, so the cell update needs
+// no byte permute, and each database residue is read once for two queries.
+//
+// Mapping onto sm_100:
+//   * a group of QP_G = 4 threads computes one database sequence as a
+//     wavefront, thread k owning R query rows of the current pass in
+//     registers; eight groups (eight sequences of similar length) fill a warp;
+//   * a thread advances two columns per step and interleaves them row by row
+//     (cell (r, c) then cell (r - 1, c + 1)), which gives two independent
+//     dependency chains and lets H be updated in place without copies;
+//   * per 16x2 cell pair: one 3-way max, three fused add-max (ALU pipe), one
+//     IADD, and half a 3-way max for the running maximum;
+//   * H and F of the bottom rows of both columns go to thread k + 1 by
+//     shuffle; the running maximum is kept per thread and combined over the
+//     group only at the end of the sequence, together with the first column
+//     pair at which each thread's maximum reached 255;
+//   * queries longer than QP_G x R rows take several passes over a sequence;
+//     the bottom row's H and F go through a per-group scratch row in global
+//     memory, read back by thread 0 two steps ahead;
+//   * every warp schedules itself: (query pair, range of sequences) units from
+//     a global counter; the warp's shared-memory slice holds the current pass's
+//     rows of the query pair's profile.
+#include "device_common.cuh"
+
+#include <climits>
+
+namespace ssa {
+
+constexpr uint32_t QP_BIAS = 1024u;
+constexpr uint32_t QP_BIAS2 = (QP_BIAS << 16) | QP_BIAS;
+// adding this per half sets bit 15 exactly when the half is >= 1024 + 255
+// (halves stay in [0, 32767], so no carry crosses into the other half)
+constexpr uint32_t QP_CROSS_ADD = ((0x8000u - (QP_BIAS + 255u)) << 16) | (0x8000u - (QP_BIAS + 255u));
+constexpr int QP_THREADS = QP_THREADS_PER_CTA;
+
+template <int R>
+__global__ void __launch_bounds__( QP_THREADS, 4 ) sw_qpair_kernel( QPairParams p ) {
+    constexpr int G = QP_G;
+    constexpr uint32_t GR = (uint32_t) (G * R);
+    extern __shared__ __align__( 16 ) uint32_t qsm[];
+    const int lane = threadIdx.x & 31;
+    const uint32_t warp_in_cta = threadIdx.x >> 5;
+    const uint32_t warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    uint32_t * slice = qsm + warp_in_cta * (QP_CODES * GR);
+    const int k = lane & (G - 1);                // thread within its group
+    const int g = lane / G;                      // group within the warp
+    const uint32_t GOE32 = (uint32_t) ((int32_t) p.gap_oe * 65536 + (int32_t) p.gap_oe);
+    const uint32_t GE2 = ((uint32_t) (uint16_t) (int16_t) p.gap_e << 16) | (uint16_t) (int16_t) p.gap_e;
+    int4 * scratch = p.scratch + ((uint64_t) warp_global * QP_GPW + (uint32_t) g) * p.scratch_cols;
+    uint64_t loaded_key = ~0ull;
+
+    for( ;; ) {
+        unsigned long long u = 0;
+        if( lane == 0 )
+            u = atomicAdd( p.unit_counter, 1ull );
+        u = __shfl_sync( 0xffffffffu, u, 0 );
+        if( u >= p.n_units )
+            break;
+        const uint32_t qp = p.unit_pairs[u % p.n_class];
+        const uint32_t chunk = (uint32_t) (u / p.n_class);
+        const uint32_t seq_begin = p.chunk_bounds[chunk], seq_end = p.chunk_bounds[chunk + 1];
+        const uint32_t rows = p.qp_rows[qp];
+        const uint32_t passes = rows / GR;
+        const uint32_t * prof = p.prof + p.prof_off[qp];
+        const uint32_t slot_a = p.qp_slots[2 * qp], slot_b = p.qp_slots[2 * qp + 1];
+
+        for( uint32_t b0 = seq_begin; b0 < seq_end; b0 += (uint32_t) QP_GPW ) {
+            const uint32_t idx = b0 + (uint32_t) g;
+            const bool valid = idx < seq_end;
+            const uint32_t id = valid ? p.order[idx] : 0u;
+            const uint32_t L = valid ? p.db.lens[id] : 0u;
+            const uint32_t ncp = ((L + 3u) & ~3u) >> 1;          // column pairs up to the block end
+            const uint32_t max_ncp = __reduce_max_sync( 0xffffffffu, ncp );
+            const uint8_t * res = p.db.codes + (valid ? p.db.offsets[id] : 0ull);
+
+            // per thread over all passes: running maximum and the first column
+            // pair at which it reached 255 (per half)
+            uint32_t best = QP_BIAS2;
+            int cross_a = INT_MAX, cross_b = INT_MAX;
+
+            for( uint32_t pass = 0; pass < passes; pass++ ) {
+                const bool last_pass = (pass + 1 == passes);
+                const uint64_t key = ((uint64_t) qp << 24) | pass;
+                if( key != loaded_key ) {
+                    // this pass's rows of all residue codes: QP_CODES x GR words
+                    __syncwarp();
+                    constexpr uint32_t per_code = GR / 4u;
+                    const uint4 * src = reinterpret_cast<const uint4 *>( prof + (size_t) pass * GR );
+                    uint4 * dst = reinterpret_cast<uint4 *>( slice );
+                    for( uint32_t i = (uint32_t) lane; i < QP_CODES * per_code; i += 32u ) {
+                        const uint32_t code = i / per_code, w = i % per_code;
+                        dst[i] = src[(size_t) code * (rows / 4u) + w];
+                    }
+                    loaded_key = key;
+                    __syncwarp();
+                }
+                uint32_t H[R], E[R];
+#pragma unroll
+                for( int r = 0; r < R; r++ ) {
+                    H[r] = QP_BIAS2;
+                    E[r] = QP_BIAS2;
+                }
+                uint32_t diag = QP_BIAS2, smax = QP_BIAS2, seen = 0;
+                uint32_t out_h0 = QP_BIAS2, out_f0 = QP_BIAS2, out_h1 = QP_BIAS2, out_f1 = QP_BIAS2;
+                // residues of column pairs cp .. cp + 3 (two codes each), one pair
+                // fetched ahead every step; past the block end the reads stay
+                // inside the padded record or the next one (never used)
+                const uint32_t fetch_limit = ncp + 3u;
+                auto fetch = [&]( int32_t cp ) -> uint32_t {
+                    const uint32_t c = min( (uint32_t) max( cp, 0 ), fetch_limit );
+                    return (uint32_t) *reinterpret_cast<const uint16_t *>( res + 2u * c );
+                };
+                uint32_t q0 = fetch( -k ), q1 = fetch( 1 - k ), q2 = fetch( 2 - k ), q3 = fetch( 3 - k );
+                // thread 0: the previous pass's bottom row, two column pairs ahead
+                const bool reads_boundary = (k == 0) && pass > 0;
+                int4 bq0 = make_int4( 0, 0, 0, 0 ), bq1 = bq0;
+                if( reads_boundary ) {
+                    if( ncp > 0 )
+                        bq0 = scratch[0];
+                    if( ncp > 1 )
+                        bq1 = scratch[1];
+                }
+                const uint32_t steps = max_ncp + (uint32_t) G - 1u;
+                for( uint32_t s = 0; s < steps; s++ ) {
+                    uint32_t up_h0 = __shfl_up_sync( 0xffffffffu, out_h0, 1, G );
+                    uint32_t up_f0 = __shfl_up_sync( 0xffffffffu, out_f0, 1, G );
+                    uint32_t up_h1 = __shfl_up_sync( 0xffffffffu, out_h1, 1, G );
+                    uint32_t up_f1 = __shfl_up_sync( 0xffffffffu, out_f1, 1, G );
+                    const int32_t cp = (int32_t) s - k;
+                    const uint32_t w = q0;
+                    q0 = q1;
+                    q1 = q2;
+                    q2 = q3;
+                    q3 = fetch( cp + 4 );
+                    const int4 bnd = bq0;
+                    if( reads_boundary ) {
+                        bq0 = bq1;
+                        const uint32_t nxt = (uint32_t) cp + 2u;
+                        if( nxt < ncp && nxt < p.scratch_cols )
+                            bq1 = scratch[nxt];
+                    }
+                    if( cp < 0 || (uint32_t) cp >= ncp )
+                        continue;
+                    if( k == 0 ) {
+                        up_h0 = pass ? (uint32_t) bnd.x : QP_BIAS2;
+                        up_f0 = pass ? (uint32_t) bnd.y : QP_BIAS2;
+                        up_h1 = pass ? (uint32_t) bnd.z : QP_BIAS2;
+                        up_f1 = pass ? (uint32_t) bnd.w : QP_BIAS2;
+                    }
+                    const uint32_t * pa = slice + (w & 0xffu) * GR + (uint32_t) (k * R);
+                    const uint32_t * pb = slice + (w >> 8) * GR + (uint32_t) (k * R);
+                    // profile words four rows at a time, loaded as the rows come up
+                    uint4 xa = make_uint4( 0, 0, 0, 0 ), xb = xa;
+                    // column c = 2cp (cell A, row r) interleaved with column
+                    // c + 1 (cell B, row r - 1); H[r] keeps column c - 1 until
+                    // cell B of row r overwrites it with column c + 1
+                    uint32_t fa = up_f0, fb = up_f1;
+                    uint32_t hc_prev = 0, hc_prev2 = 0;     // column c, rows r - 1 and r - 2
+#pragma unroll
+                    for( int r = 0; r <= R; r++ ) {
+                        uint32_t ha = 0;
+                        if( r < R ) {
+                            if( (r & 3) == 0 )
+                                xa = *reinterpret_cast<const uint4 *>( pa + r );
+                            const uint32_t v = (r & 3) == 0 ? xa.x : (r & 3) == 1 ? xa.y : (r & 3) == 2 ? xa.z : xa.w;
+                            const uint32_t hd = (r == 0) ? diag : H[r - 1];
+                            const uint32_t t = __vimax3_s16x2( E[r], fa, QP_BIAS2 );
+                            ha = __viaddmax_s16x2( hd, v, t );
+                            const uint32_t hg = ha + GOE32;
+                            fa = __viaddmax_s16x2( fa, GE2, hg );
+                            E[r] = __viaddmax_s16x2( E[r], GE2, hg );
+                        }
+                        if( r >= 1 ) {
+                            const int rb = r - 1;
+                            if( (rb & 3) == 0 )
+                                xb = *reinterpret_cast<const uint4 *>( pb + rb );
+                            const uint32_t v = (rb & 3) == 0 ? xb.x : (rb & 3) == 1 ? xb.y : (rb & 3) == 2 ? xb.z : xb.w;
+                            const uint32_t hd = (rb == 0) ? up_h0 : hc_prev2;
+                            const uint32_t t = __vimax3_s16x2( E[rb], fb, QP_BIAS2 );
+                            const uint32_t hb = __viaddmax_s16x2( hd, v, t );
+                            const uint32_t hg = hb + GOE32;
+                            fb = __viaddmax_s16x2( fb, GE2, hg );
+                            E[rb] = __viaddmax_s16x2( E[rb], GE2, hg );
+                            H[rb] = hb;
+                            smax = (r < R) ? __vimax3_s16x2( smax, ha, hb ) : __vmaxs2( smax, hb );
+                        }
+                        else {
+                            smax = __vmaxs2( smax, ha );
+                        }
+                        hc_prev2 = hc_prev;
+                        hc_prev = ha;
+                    }
+                    diag = up_h1;
+                    out_h0 = hc_prev2;       // column c, row R - 1
+                    out_f0 = fa;
+                    out_h1 = H[R - 1];
+                    out_f1 = fb;
+                    // first column pair at which this thread's maximum reached 255
+                    const uint32_t ge = (smax + QP_CROSS_ADD) & 0x80008000u;
+                    if( ge != seen ) {
+                        if( (ge & 0x8000u) && !(seen & 0x8000u) )
+                            cross_a = min( cross_a, cp );
+                        if( (ge & 0x80000000u) && !(seen & 0x80000000u) )
+                            cross_b = min( cross_b, cp );
+                        seen = ge;
+                    }
+                    if( k == G - 1 && !last_pass ) {
+                        if( (uint32_t) cp < p.scratch_cols )
+                            scratch[cp] = make_int4( (int) out_h0, (int) out_f0, (int) out_h1, (int) out_f1 );
+                        else
+                            atomicOr( p.sink.error_flags, ERR_SCRATCH_OVERFLOW );
+                    }
+                }
+                best = __vmaxs2( best, smax );
+                __syncwarp();
+            }
+            // combine the group's threads: maximum and earliest crossing
+#pragma unroll
+            for( int o = 1; o < G; o <<= 1 ) {
+                best = __vmaxs2( best, __shfl_xor_sync( 0xffffffffu, best, o, G ) );
+                cross_a = min( cross_a, __shfl_xor_sync( 0xffffffffu, cross_a, o, G ) );
+                cross_b = min( cross_b, __shfl_xor_sync( 0xffffffffu, cross_b, o, G ) );
+            }
+            if( valid && k == 0 ) {
+                const uint32_t slots[2] = { slot_a, slot_b };
+                const int cross[2] = { cross_a, cross_b };
+                const uint32_t sv[2] = { best & 0xffffu, best >> 16 };
+#pragma unroll
+                for( int h = 0; h < 2; h++ ) {
+                    if( slots[h] == 0xffffffffu )
+                        continue;
+                    int32_t * dst = p.sink.score + (uint64_t) slots[h] * p.sink.score_stride + id;
+                    if( cross[h] == INT_MAX ) {
+                        *dst = (int32_t) (sv[h] - QP_BIAS);
+                    }
+                    else {
+                        // columns 2cp and 2cp + 1 lie in 4-column block cp / 2
+                        *dst = 255;
+                        unsigned q = atomicAdd( p.sink.next_count, 1u );
+                        if( q < p.sink.next_cap )
+                            p.sink.next[q] = PairTask{ slots[h], id, (cross[h] >> 1) + 1, 0 };
+                        else
+                            atomicOr( p.sink.error_flags, ERR_REQUEUE_OVERFLOW );
+                    }
+                }
+            }
+        }
+    }
+}
+
+// grid == 0: report the resident CTAs per SM in *blocks_per_sm without launching.
+template <int R>
+static cudaError_t launch_qp_one( const QPairParams & p, int grid, cudaStream_t st, int * blocks_per_sm ) {
+    const size_t smem = (size_t) (QP_THREADS / 32) * QP_CODES * QP_G * R * sizeof(uint32_t);
+    cudaError_t e = cudaFuncSetAttribute( sw_qpair_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            (int) smem );
+    if( e != cudaSuccess )
+        return e;
+    if( grid == 0 )
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor( blocks_per_sm, sw_qpair_kernel<R>, QP_THREADS, smem );
+    sw_qpair_kernel<R><<<grid, QP_THREADS, smem, st>>>( p );
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sw_qpair( int R, const QPairParams & p, int grid, cudaStream_t st, int * blocks_per_sm ) {
+    switch( R ) {
+    case 16:
+        return launch_qp_one<16>( p, grid, st, blocks_per_sm );
+    case 20:
+        return launch_qp_one<20>( p, grid, st, blocks_per_sm );
+    case 24:
+        return launch_qp_one<24>( p, grid, st, blocks_per_sm );
+    case 28:
+        return launch_qp_one<28>( p, grid, st, blocks_per_sm );
+    default:
+        return cudaErrorInvalidValue;
+    }
+}
+
+// prof[qp][code][row] = (A's 8-bit score, B's 8-bit score) as a 16x2 word;
+// rows past a query, and the absent query of an odd batch, score -128.
+__global__ void build_profile_qp_kernel( const uint8_t * qcodes, const uint64_t * qoff, const uint32_t * qlen,
+        const uint32_t * qp_slots, uint32_t n_qp, const uint32_t * qp_rows, const int64_t * matrix, uint32_t * prof,
+        const uint64_t * prof_off ) {
+    const uint32_t qp = blockIdx.y;
+    if( qp >= n_qp )
+        return;
+    const uint32_t rows = qp_rows[qp];
+    const uint32_t sa = qp_slots[2 * qp], sb = qp_slots[2 * qp + 1];
+    const uint32_t La = qlen[sa], Lb = (sb == 0xffffffffu) ? 0u : qlen[sb];
+    const uint8_t * qa = qcodes + qoff[sa];
+    const uint8_t * qb = (sb == 0xffffffffu) ? qa : qcodes + qoff[sb];
+    uint32_t * out = prof + prof_off[qp];
+    for( uint64_t x = blockIdx.x * (uint64_t) blockDim.x + threadIdx.x; x < (uint64_t) QP_CODES * rows;
+            x += (uint64_t) gridDim.x * blockDim.x ) {
+        const uint32_t code = (uint32_t) (x / rows), row = (uint32_t) (x % rows);
+        const int32_t a = row < La ? (int32_t) (int8_t) matrix[(code << 5) + qa[row]] : -128;
+        const int32_t b = row < Lb ? (int32_t) (int8_t) matrix[(code << 5) + qb[row]] : -128;
+        out[x] = ((uint32_t) (uint16_t) (int16_t) b << 16) | (uint16_t) (int16_t) a;
+    }
+}
+
+cudaError_t launch_build_profile_qp( const uint8_t * qcodes, const uint64_t * qoff, const uint32_t * qlen,
+        const uint32_t * qp_slots, uint32_t n_qp, const uint32_t * qp_rows, const int64_t * matrix, uint32_t * prof,
+        const uint64_t * prof_off, cudaStream_t st ) {
+    if( n_qp == 0 )
+        return cudaSuccess;
+    dim3 grid( 16, n_qp );
+    build_profile_qp_kernel<<<grid, 256, 0, st>>>( qcodes, qoff, qlen, qp_slots, n_qp, qp_rows, matrix, prof,
+            prof_off );
+    return cudaGetLastError();
+}
+
+}  // namespace ssa

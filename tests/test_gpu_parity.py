@@ -109,3 +109,40 @@ def test_long_query_multi_pass(built_library):
                                   recs)
         assert res[0] == exp, (algo, width)
         assert tuple(ovf[0]) == tuple(eovf), (algo, width)
+
+
+def _batch_case(seed):
+    rng = np.random.default_rng(1000 + seed)
+    nq = int(rng.integers(2, 10))
+    qs = [W.random_residues(rng, int(rng.integers(1, 1200)), W.AA20) for _ in range(nq)]
+    recs = []
+    for _ in range(int(rng.integers(20, 400))):
+        r = rng.random()
+        src = qs[int(rng.integers(0, nq))]
+        if r < 0.08:
+            recs.append(W.mutate(rng, src, W.AA20, 0.03, 0.01, (1, 4)).tobytes())
+        elif r < 0.1:
+            recs.append(W.mutate(rng, np.tile(src, int(rng.integers(2, 4))), W.AA20, 0.01, 0.0, (1, 1)).tobytes())
+        elif r < 0.12:
+            recs.append(b"")
+        else:
+            recs.append(W.random_residues(rng, int(rng.integers(1, 900)), W.AA20).tobytes())
+    gap = [(-11, -1), (-5, -2), (-10, 0), (0, 0)][int(rng.integers(0, 4))]
+    matrix = ("builtin", ["blosum62", "blosum45", "pam30"][int(rng.integers(0, 3))])
+    return dict(queries=[q.tobytes() for q in qs], records=recs, gap=gap, matrix=matrix,
+                chunk=int([1000, 50, 7][int(rng.integers(0, 3))]), hits=int(rng.integers(1, 15)),
+                simd=int([2, 1][int(rng.integers(0, 2))]))
+
+
+@pytest.mark.parametrize("seed", range(12))
+def test_batched_random_against_oracle(built_library, seed):
+    """Batches (query pairs share the 16x2 lanes) of 2-9 SW queries, 1-1200
+    residues, with overflowing copies and empty records, against the oracle
+    query by query."""
+    c = _batch_case(seed)
+    product_setup(1, c["matrix"], c["gap"], c["chunk"], c["simd"], records=c["records"])
+    batched, _ = product_search("sw", 8, 1, c["hits"], c["queries"], batch=True)
+    for qi, q in enumerate(c["queries"]):
+        exp, _ = oracle_search("sw", 8, 1, c["hits"], 1, c["matrix"], c["gap"], c["chunk"], c["simd"], q,
+                               c["records"])
+        assert batched[qi] == exp, (seed, qi, len(q))
