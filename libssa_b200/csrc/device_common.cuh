@@ -168,10 +168,12 @@ struct QPairParams {
     const uint64_t * prof_off;    // per query pair, in words
     const uint32_t * qp_slots;    // per query pair: slot A, slot B (0xffffffff when absent)
     const uint32_t * qp_rows;     // per query pair: profile rows (passes x QP_G x R)
-    // work units u = chunk * n_class + i: query pair unit_pairs[i] against the
-    // sequences order[chunk_bounds[chunk] .. chunk_bounds[chunk + 1])
+    // work units u = i * n_chunks + chunk: query pair unit_pairs[i] against the
+    // sequences order[chunk_bounds[chunk] .. chunk_bounds[chunk + 1]); the
+    // pairs come longest first, so the longest units start first
     const uint32_t * unit_pairs;
     uint32_t n_class;
+    uint32_t n_chunks;
     const uint32_t * chunk_bounds;
     uint64_t n_units;
     unsigned long long * unit_counter;

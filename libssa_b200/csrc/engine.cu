@@ -124,6 +124,8 @@ public:
         for( int i = 0; i < 4; i++ ) {
             CUDA_CHECK( cudaStreamCreateWithFlags( &class_stream_[i], cudaStreamNonBlocking ) );
             CUDA_CHECK( cudaEventCreateWithFlags( &ev_class_[i], cudaEventDisableTiming ) );
+            CUDA_CHECK( cudaEventCreate( &ev_cls_t_[2 * i] ) );
+            CUDA_CHECK( cudaEventCreate( &ev_cls_t_[2 * i + 1] ) );
         }
         device_ = dev;
         ready_ = true;
@@ -335,6 +337,7 @@ private:
     DevBuf d_qp_prof_, d_qp_off_, d_qp_rows_, d_qp_slots_, d_qp_units_;
     cudaStream_t class_stream_[4] = { nullptr, nullptr, nullptr, nullptr };
     cudaEvent_t ev_class_[4] = { nullptr, nullptr, nullptr, nullptr };
+    cudaEvent_t ev_cls_t_[8] = {};   // per class start / end, timed (SSA_B200_TIMING)
     cudaEvent_t ev_ready_ = nullptr;
     cudaEvent_t ev_phase_[6] = {};
     cudaEvent_t ev_tb_[5] = {};   // batch start, entry pass done, cascade done, copies done, traceback
@@ -601,23 +604,34 @@ void Engine::run_fast_entry( const SearchRequest & req, uint32_t nq, PairTask * 
 
 // Batches: queries sorted by length are paired, the two queries of a pair
 // share the 16x2 lanes (sw_qpair_kernel.cu).  Rows per thread R for a pair of
-// Q rows (the longer query): the smallest estimated issue cost per column
-// pair, passes x (13 R + 40), with QP_G x R rows per pass.
-static int choose_qpair_rows( uint32_t Q, uint32_t * passes ) {
+// Q rows (the longer query): the smallest estimated time per column pair,
+// passes x cost(R), with QP_G x R rows per pass.  cost(R) is the measured
+// device time of one pass per column pair on a B200 (relative units; 64
+// queries of 375 residues against 10,000 sequences, each R pinned): R = 16
+// pays for 2-way shared-memory bank conflicts inside a group, R = 28 for a
+// few spilled registers.
+static int choose_qpair_rows( uint32_t Q, uint32_t * passes, int pinned ) {
+    static const int rs[4] = { 16, 20, 24, 28 };
+    static const double cost[4] = { 4.28, 3.77, 4.56, 5.41 };
     int best_r = 0;
     double best_cost = 1e300;
-    for( int R : { 16, 20, 24, 28 } ) {
+    for( int i = 0; i < 4; i++ ) {
+        const int R = rs[i];
+        if( pinned && R != pinned )
+            continue;
         const uint32_t per = (uint32_t) (QP_G * R);
         const uint32_t P = std::max<uint32_t>( 1, (Q + per - 1) / per );
         if( (uint64_t) P * per > FAST_MAX_ROWS )
             continue;
-        const double cost = (double) P * (13.0 * R + 40.0);
-        if( cost < best_cost ) {
-            best_cost = cost;
+        const double c = (double) P * cost[i];
+        if( c < best_cost ) {
+            best_cost = c;
             best_r = R;
             *passes = P;
         }
     }
+    if( best_r == 0 && pinned )         // the pinned R does not fit this query
+        return choose_qpair_rows( Q, passes, 0 );
     return best_r;
 }
 
@@ -632,6 +646,9 @@ void Engine::run_qpair_entry( const SearchRequest & req, uint32_t nq, PairTask *
         (h_qlen_[s] <= FAST_MAX_ROWS ? fit : fallback).push_back( s );
     std::stable_sort( fit.begin(), fit.end(), [&]( uint32_t a, uint32_t b ) { return h_qlen_[a] > h_qlen_[b]; } );
     const uint32_t n_qp = (uint32_t) ((fit.size() + 1) / 2);
+    // SSA_B200_QP_R=16|20|24|28 pins R (tuning)
+    const char * pin = getenv( "SSA_B200_QP_R" );
+    const int pinned_r = pin ? atoi( pin ) : 0;
     std::vector<uint32_t> qp_slots( 2 * std::max<uint32_t>( 1, n_qp ), 0xffffffffu );
     std::vector<uint32_t> qp_rows( std::max<uint32_t>( 1, n_qp ), 0 );
     std::vector<uint64_t> qp_off( std::max<uint32_t>( 1, n_qp ), 0 );
@@ -642,7 +659,7 @@ void Engine::run_qpair_entry( const SearchRequest & req, uint32_t nq, PairTask *
         if( 2 * i + 1 < fit.size() )
             qp_slots[2 * i + 1] = fit[2 * i + 1];
         uint32_t P = 1;
-        const int R = choose_qpair_rows( h_qlen_[fit[2 * i]], &P );
+        const int R = choose_qpair_rows( h_qlen_[fit[2 * i]], &P, pinned_r );
         qp_rows[i] = P * (uint32_t) (QP_G * R);
         by_r[R / 4 - 4].push_back( i );
     }
@@ -652,9 +669,11 @@ void Engine::run_qpair_entry( const SearchRequest & req, uint32_t nq, PairTask *
             qp_off[i] = total;
             total += (uint64_t) QP_CODES * qp_rows[i];
         }
-    std::vector<uint32_t> units;                  // pairs grouped by class
-    for( auto & v : by_r )
+    std::vector<uint32_t> units;                  // pairs grouped by class, longest first
+    for( auto & v : by_r ) {
+        std::stable_sort( v.begin(), v.end(), [&]( uint32_t a, uint32_t b ) { return qp_rows[a] > qp_rows[b]; } );
         units.insert( units.end(), v.begin(), v.end() );
+    }
     d_qp_prof_.ensure( std::max<uint64_t>( total, 4 ) * sizeof(uint32_t) );
     d_qp_off_.ensure( qp_off.size() * sizeof(uint64_t) );
     d_qp_rows_.ensure( qp_rows.size() * sizeof(uint32_t) );
@@ -703,6 +722,7 @@ void Engine::run_qpair_entry( const SearchRequest & req, uint32_t nq, PairTask *
             stream_ ) );
     CUDA_CHECK( cudaEventRecord( ev_ready_, stream_ ) );
     const uint32_t scratch_cols = (((db_.max_len + 3u) & ~3u) >> 1) + 2u;
+    const bool timing = getenv( "SSA_B200_TIMING" ) != nullptr;
     size_t class_first = 0;
     for( int ri = 0; ri < 4; ri++ ) {
         const std::vector<uint32_t> & cls = by_r[ri];
@@ -727,6 +747,7 @@ void Engine::run_qpair_entry( const SearchRequest & req, uint32_t nq, PairTask *
         p.qp_rows = d_qp_rows_.as<uint32_t>();
         p.unit_pairs = d_qp_units_.as<uint32_t>() + class_first;
         p.n_class = (uint32_t) cls.size();
+        p.n_chunks = n_chunks;
         p.chunk_bounds = d_bounds_.as<uint32_t>();
         p.n_units = (uint64_t) n_chunks * cls.size();
         p.unit_counter = unit_counter;
@@ -743,11 +764,33 @@ void Engine::run_qpair_entry( const SearchRequest & req, uint32_t nq, PairTask *
                     scratch_cols * sizeof(int4) );
             p.scratch_cols = scratch_cols;
         }
+        if( timing )
+            CUDA_CHECK( cudaEventRecord( ev_cls_t_[2 * ri], class_stream_[ri] ) );
         CUDA_CHECK( launch_sw_qpair( R, p, grid, class_stream_[ri], nullptr ) );
         launches_++;
+        if( timing )
+            CUDA_CHECK( cudaEventRecord( ev_cls_t_[2 * ri + 1], class_stream_[ri] ) );
         CUDA_CHECK( cudaEventRecord( ev_class_[ri], class_stream_[ri] ) );
         CUDA_CHECK( cudaStreamWaitEvent( stream_, ev_class_[ri], 0 ) );
         class_first += cls.size();
+    }
+    if( timing ) {
+        for( int ri = 0; ri < 4; ri++ ) {
+            if( by_r[ri].empty() )
+                continue;
+            float ms = 0;
+            CUDA_CHECK( cudaEventSynchronize( ev_cls_t_[2 * ri + 1] ) );
+            CUDA_CHECK( cudaEventElapsedTime( &ms, ev_cls_t_[2 * ri], ev_cls_t_[2 * ri + 1] ) );
+            double cells = 0, padded = 0;
+            for( uint32_t i : by_r[ri] ) {
+                const uint32_t a = qp_slots[2 * i], b = qp_slots[2 * i + 1];
+                cells += (double) (h_qlen_[a] + (b == 0xffffffffu ? 0u : h_qlen_[b])) * (double) db_.residues;
+                padded += 2.0 * qp_rows[i] * (double) total_cols;
+            }
+            fprintf( stderr, "[ssa timing] qpair class R=%d: %zu pairs, %.3f ms, %.3e cells (%.1f%% of computed), "
+                    "%.1f GCUPS\n", 4 * (ri + 4), by_r[ri].size(), ms, cells, 100.0 * cells / padded,
+                    cells / (ms * 1e-3) / 1e9 );
+        }
     }
     if( !fallback.empty() ) {
         d_slots_.ensure( fallback.size() * sizeof(uint32_t) );

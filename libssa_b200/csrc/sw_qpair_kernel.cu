@@ -28,8 +28,9 @@
 //     the bottom row's H and F go through a per-group scratch row in global
 //     memory, read back by thread 0 two steps ahead;
 //   * every warp schedules itself: (query pair, range of sequences) units from
-//     a global counter; the warp's shared-memory slice holds the current pass's
-//     rows of the query pair's profile.
+//     a global counter, the longest query pairs first so that the last units
+//     to start are short ones; the warp's shared-memory slice holds the
+//     current pass's rows of the query pair's profile.
 #include "device_common.cuh"
 
 #include <climits>
@@ -66,8 +67,8 @@ __global__ void __launch_bounds__( QP_THREADS, 4 ) sw_qpair_kernel( QPairParams 
         u = __shfl_sync( 0xffffffffu, u, 0 );
         if( u >= p.n_units )
             break;
-        const uint32_t qp = p.unit_pairs[u % p.n_class];
-        const uint32_t chunk = (uint32_t) (u / p.n_class);
+        const uint32_t qp = p.unit_pairs[u / p.n_chunks];
+        const uint32_t chunk = (uint32_t) (u % p.n_chunks);
         const uint32_t seq_begin = p.chunk_bounds[chunk], seq_end = p.chunk_bounds[chunk + 1];
         const uint32_t rows = p.qp_rows[qp];
         const uint32_t passes = rows / GR;
