@@ -107,6 +107,7 @@ struct TbParams {
     const uint64_t * ops_off;
     uint32_t * ops_len;
     unsigned int * error_flags;
+    unsigned long long * hit_counters;   // forward, reverse, directions: next hit to take (start at 0)
 };
 
 // Kernel launchers.

@@ -1006,6 +1006,22 @@ void Engine::traceback( const SearchRequest & req, const std::vector<QueryCodes>
     const uint32_t nh = (uint32_t) hits.size();
     if( nh == 0 )
         return;
+    // largest alignments first: the kernels hand hits out in this order
+    {
+        std::vector<uint32_t> perm( nh );
+        for( uint32_t h = 0; h < nh; h++ )
+            perm[h] = h;
+        auto work = [&]( uint32_t h ) { return (uint64_t) h_qlen_[hits[h].qslot] * db_.len[hits[h].id]; };
+        std::stable_sort( perm.begin(), perm.end(), [&]( uint32_t a, uint32_t b ) { return work( a ) > work( b ); } );
+        std::vector<TbHit> hs( nh );
+        std::vector<std::pair<uint32_t, uint32_t>> ws( nh );
+        for( uint32_t h = 0; h < nh; h++ ) {
+            hs[h] = hits[perm[h]];
+            ws[h] = where[perm[h]];
+        }
+        hits.swap( hs );
+        where.swap( ws );
+    }
     // value range guard: every DP value is bounded by (q + d) * max |step|
     int64_t mabs = std::abs( (int64_t) req.gap_open ) + std::abs( (int64_t) req.gap_extend );
     for( int k = 0; k < 1024; k++ )
@@ -1055,6 +1071,8 @@ void Engine::traceback( const SearchRequest & req, const std::vector<QueryCodes>
     p.ops_off = (const uint64_t *) d_tb_ops_off_.ensure( (nh + 1) * sizeof(uint64_t) );
     p.ops_len = (uint32_t *) d_tb_ops_len_.ensure( nh * sizeof(uint32_t) );
     p.error_flags = d_counts_.as<unsigned>() + 2;
+    p.hit_counters = d_counts_.as<unsigned long long>() + 12;   // bytes 96..119
+    CUDA_CHECK( cudaMemsetAsync( p.hit_counters, 0, 3 * sizeof(unsigned long long), stream_ ) );
     CUDA_CHECK( cudaMemcpyAsync( (void *) p.hits, hits.data(), nh * sizeof(TbHit), cudaMemcpyHostToDevice, stream_ ) );
     CUDA_CHECK( cudaMemcpyAsync( p.regions, regions.data(), nh * sizeof(TbRegion), cudaMemcpyHostToDevice, stream_ ) );
     CUDA_CHECK( cudaMemcpyAsync( (void *) p.last_off, last_off.data(), (nh + 1) * sizeof(uint64_t),

@@ -79,6 +79,15 @@ struct BoundaryPrefetch {
     __device__ int4 get( uint32_t s ) const { return tile[s & 31u]; }
 };
 
+// Hits are handed out one per warp from a global counter, largest first (the
+// host sorts them), so that the longest alignments start first.
+__device__ __forceinline__ uint32_t next_hit( unsigned long long * counter, int lane ) {
+    unsigned long long v = 0;
+    if( lane == 0 )
+        v = atomicAdd( counter, 1ull );
+    return (uint32_t) __shfl_sync( 0xffffffffu, v, 0 );
+}
+
 // ---------------------------------------------------------------------------
 // 1. SW forward region pass (reference: src/algo/align.c:39-82).  The
 //    reference iterates database rows outer and query columns inner, scoring
@@ -92,10 +101,9 @@ __global__ void __launch_bounds__( 256 ) tb_forward_kernel( TbParams p ) {
     stage_matrix( p.matrix, smat, true );
     const int lane = threadIdx.x & 31;
     const uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
     int4 * scratch = p.scratch + (uint64_t) w * p.scratch_cols;
     const int gO = p.gap_open, gE = p.gap_extend;
-    for( uint32_t h = w; h < p.n_hits; h += nwarps ) {
+    for( uint32_t h = next_hit( p.hit_counters + 0, lane ); h < p.n_hits; h = next_hit( p.hit_counters + 0, lane ) ) {
         const TbHit hit = p.hits[h];
         if( hit.algo != 0 )
             continue;
@@ -222,10 +230,9 @@ __global__ void __launch_bounds__( 256 ) tb_reverse_kernel( TbParams p ) {
     stage_matrix( p.matrix, smat, true );
     const int lane = threadIdx.x & 31;
     const uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
     int4 * scratch = p.scratch + (uint64_t) w * p.scratch_cols;
     const int gO = p.gap_open, gE = p.gap_extend;
-    for( uint32_t h = w; h < p.n_hits; h += nwarps ) {
+    for( uint32_t h = next_hit( p.hit_counters + 1, lane ); h < p.n_hits; h = next_hit( p.hit_counters + 1, lane ) ) {
         const TbHit hit = p.hits[h];
         if( hit.algo != 0 )
             continue;
@@ -367,10 +374,9 @@ __global__ void __launch_bounds__( 256 ) tb_directions_kernel( TbParams p ) {
     stage_matrix( p.matrix, smat, false );
     const int lane = threadIdx.x & 31;
     const uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
     int4 * scratch = p.scratch + (uint64_t) w * p.scratch_cols;
     const int gO = p.gap_open, gE = p.gap_extend;
-    for( uint32_t h = w; h < p.n_hits; h += nwarps ) {
+    for( uint32_t h = next_hit( p.hit_counters + 2, lane ); h < p.n_hits; h = next_hit( p.hit_counters + 2, lane ) ) {
         const TbHit hit = p.hits[h];
         const TbRegion rg = p.regions[h];
         if( rg.status != 0 )
