@@ -354,9 +354,83 @@ def run_ours(args):
         except Exception as e:  # noqa: BLE001
             line["cpu_baseline"] = {"value": None, "unit": "GCUPS", "cores": os.cpu_count() or 1,
                                     "kind": "reference", "sample": f"unavailable: {e}"}
-    print(json.dumps(line), flush=True)
     for q in qs:
         L.free_sequence(q)
+    if world == 1 and args.served_queries > 0:
+        line["served"] = served_leg(args, L)
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# --------------------------------------------------------------------------
+# served: Poisson arrivals into the request loop (ssa_server_*)
+# --------------------------------------------------------------------------
+def served_leg(args, L) -> dict:
+    """Config 4: a resident 1,000,000-sequence database, queries arriving as a
+    Poisson process into the server; GCUPS over the wall time from the first
+    arrival to the last completion, and the submit-to-result latencies."""
+    import numpy as np
+    from libssa_b200 import workloads as W
+    w = W.sw_served_db(seed=4, scale=args.served_scale)
+    L.set_output_mode(L.OUTPUT_SILENT)
+    L.init_symbol_translation(L.AMINOACID, L.FORWARD_STRAND, 1, 1)
+    L.init_score_matrix(L.MATRIX_BUILDIN, "blosum62")
+    L.init_gap_penalties(-11, -1)
+    L.set_chunk_size(1000)
+    L.set_simd_compute_mode(L.COMPUTE_ON_AVX2)
+    L.load_db_memory(flat=w.db_flat, offsets=w.db_offsets)
+    texts = [q.decode() for q in W.served_queries(seed=40, n=args.served_queries)]
+    arrivals = W.poisson_arrivals(seed=41, rate=args.served_rate, n=len(texts))
+    qs = [L.init_sequence_fasta(L.READ_FROM_STRING, t) for t in texts]
+    server = L.Server(L.SSA_SMITH_WATERMAN, 10, L.BIT_WIDTH_8, L.COMPUTE_ALIGNMENT, slots=args.served_slots,
+                      segments=args.served_segments)
+    tickets = [None] * len(qs)
+    t0 = time.perf_counter()
+
+    def client():
+        for i, q in enumerate(qs):
+            delay = t0 + float(arrivals[i]) - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            tickets[i] = server.submit(q)
+
+    th = threading.Thread(target=client)
+    th.start()
+    th.join()
+    lat = []
+    for t in tickets:
+        _, latency = server.wait(t)
+        lat.append(latency)
+    wall = time.perf_counter() - t0
+    st = server.stats()
+    server.stop()
+    for q in qs:
+        L.free_sequence(q)
+    residues = int(w.db_offsets[-1])
+    cells = sum(len(t) for t in texts) * residues
+    lat_ms = np.array(lat) * 1e3
+    return {"value": round(cells / wall / 1e9, 2), "unit": "GCUPS",
+            "latency_ms": {"p50": round(float(np.percentile(lat_ms, 50)), 1),
+                           "p99": round(float(np.percentile(lat_ms, 99)), 1),
+                           "max": round(float(lat_ms.max()), 1)},
+            "config": {"workload": "sw_served", "db_sequences": w.n_db, "db_residues": residues,
+                       "queries": len(texts), "arrival_rate_qps": args.served_rate, "slots": args.served_slots,
+                       "segments": int(st.segments), "waves": int(st.waves), "hits": 10,
+                       "align_type": "COMPUTE_ALIGNMENT"},
+            "device_seconds": round(st.device_seconds, 3), "wall_seconds": round(wall, 3),
+            "timing": "wall time from the first arrival to the last completion; latency = submit to result"}
+
+
+def run_served_arm(args):
+    import libssa_b200 as L
+    L.load()
+    res = served_leg(args, L)
+    line = {"metric": "GCUPS (served SW search, 1,000,000 resident sequences, Poisson arrivals, top 10 with CIGAR)",
+            "value": res["value"], "unit": "GCUPS", "n_gpus": 1, "steps": 1, "warmup": 0,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "int16x2 (8-bit lane semantics), int32", "data": "synthetic (seeded, BASELINE config 4 shapes)",
+            **{k: v for k, v in res.items() if k not in ("value", "unit")}}
+    print(json.dumps(line), flush=True)
     return 0
 
 
@@ -371,12 +445,20 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--plain-queries", type=int, default=16,
                     help="queries timed through the plain one-query-per-call path (0 = skip)")
-    ap.add_argument("--workload", default="sw_batched", choices=["sw_batched", "sw_plain"],
+    ap.add_argument("--served-queries", type=int, default=64,
+                    help="requests of the served leg (config 4 database; 0 = skip)")
+    ap.add_argument("--served-rate", type=float, default=50.0, help="Poisson arrival rate of the served leg, 1/s")
+    ap.add_argument("--served-slots", type=int, default=64, help="resident query slots of the server")
+    ap.add_argument("--served-segments", type=int, default=8, help="database segments per scan turn")
+    ap.add_argument("--served-scale", type=float, default=1.0, help="served database scale (1.0 = 1M sequences)")
+    ap.add_argument("--workload", default="sw_batched", choices=["sw_batched", "sw_plain", "sw_served"],
                     help="sw_plain: config 1's 10,000-sequence database with --queries queries of 375")
     ap.add_argument("--queries", type=int, default=None, help="query count for --workload sw_plain")
     args = ap.parse_args()
     if args.impl == "reference":
         sys.exit(run_reference_arm(args))
+    if args.workload == "sw_served":
+        sys.exit(run_served_arm(args))
     sys.exit(run_ours(args))
 
 

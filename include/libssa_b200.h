@@ -70,6 +70,50 @@ size_t ssa_query_length( p_query p );
 int ssa_db_b200_load_memory( size_t count, const char * residues, const uint64_t * offsets );
 
 /*
+ * Serving.  No counterpart in the reference, which searches one query per call.
+ *
+ * A server keeps the database and `slots` query slots resident on the device
+ * and runs a request loop on its own thread: arriving queries are admitted into
+ * free slots (first come, first served, while the traceback memory of the
+ * admitted requests stays within `memory_budget` bytes; 0 = no limit) and
+ * folded into the running scan of the database, which proceeds in `segments`
+ * waves, each covering one segment for every occupied slot; a request is done
+ * after one full turn of the segments.  Each result equals what sw_align (or
+ * nw_align) returns for the query alone with the settings current at
+ * ssa_server_start (matrix, gaps, symbol type, chunk size, SIMD schedule),
+ * whatever else is in flight.  submit/wait may be called from any thread;
+ * other searches may run meanwhile (they take turns with the server's waves).
+ * The database must not change while a server runs.  A query must stay valid
+ * until its result list is freed with free_alignment (the list borrows the
+ * query's residues, as in sw_align).  Queries are limited to
+ * SSA_B200_SERVE_MAX_QUERY residues; submit returns -1 for longer ones.
+ */
+#define SSA_B200_SERVE_MAX_QUERY 8192u
+
+typedef struct ssa_server ssa_server;
+
+typedef struct {
+    uint64_t submitted, completed;
+    uint64_t waves;              /* segment waves run so far */
+    uint64_t cells;              /* query length x database residues of completed requests */
+    double busy_seconds;         /* wall time of the loop's waves and completions */
+    double device_seconds;       /* device time of the waves' entry passes and cascades */
+    uint32_t slots, segments;
+} ssa_server_stats_t;
+
+ssa_server * ssa_server_start( int algorithm, size_t hitcount, int bit_width, int align_type, size_t slots,
+        size_t segments, size_t memory_budget );
+/* Returns the request's ticket (>= 0), or -1. */
+long long ssa_server_submit( ssa_server * server, p_query query );
+/* Blocks until the request is done; returns its list (free with free_alignment)
+ * and, if latency_seconds is not NULL, the time from submit to completion. */
+p_alignment_list ssa_server_wait( ssa_server * server, long long ticket, double * latency_seconds );
+void ssa_server_get_stats( ssa_server * server, ssa_server_stats_t * out );
+/* Finishes every submitted request, frees the results nobody waited for, and
+ * releases the server. */
+void ssa_server_stop( ssa_server * server );
+
+/*
  * Allocation-free scoring.  No counterpart in the reference, whose searches
  * allocate their buffers per call (src/algo/searcher.c:43,160).
  *

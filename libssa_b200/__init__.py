@@ -37,6 +37,7 @@ EXPORTED = [
     "init_constant_scores", "init_gap_penalties", "init_symbol_translation", "init_db", "init_sequence_fasta",
     "free_sequence", "sw_align", "nw_align", "free_alignment", "ssa_exit", "ssa_align_batch", "ssa_get_stats",
     "ssa_query_length", "ssa_db_refresh", "ssa_b200_int_peak", "ssa_b200_score64_noalloc",
+    "ssa_server_start", "ssa_server_submit", "ssa_server_wait", "ssa_server_get_stats", "ssa_server_stop",
 ]
 
 # allocation-free scoring (include/libssa_b200.h)
@@ -123,6 +124,15 @@ def load():
                                              ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32,
                                              ctypes.c_void_p, ctypes.c_void_p]
     lib.ssa_b200_score64_noalloc.restype = ctypes.c_int
+    lib.ssa_server_start.argtypes = [ctypes.c_int, ctypes.c_size_t, ctypes.c_int, ctypes.c_int, ctypes.c_size_t,
+                                     ctypes.c_size_t, ctypes.c_size_t]
+    lib.ssa_server_start.restype = ctypes.c_void_p
+    lib.ssa_server_submit.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+    lib.ssa_server_submit.restype = ctypes.c_longlong
+    lib.ssa_server_wait.argtypes = [ctypes.c_void_p, ctypes.c_longlong, ctypes.POINTER(ctypes.c_double)]
+    lib.ssa_server_wait.restype = P_LIST
+    lib.ssa_server_get_stats.argtypes = [ctypes.c_void_p, ctypes.POINTER(ServerStats)]
+    lib.ssa_server_stop.argtypes = [ctypes.c_void_p]
     _plugin.ssa_db_b200_load_memory.argtypes = [ctypes.c_size_t, ctypes.c_char_p, ctypes.POINTER(ctypes.c_uint64)]
     _plugin.ssa_db_b200_load_memory.restype = ctypes.c_int
     _plugin.ssa_db_get_sequence_count.restype = ctypes.c_size_t
@@ -271,6 +281,52 @@ def score64_noalloc(algorithm: int, d_query: int, query_len: int, d_codes: int, 
     code (NOALLOC_OK on success)."""
     return int(load().ssa_b200_score64_noalloc(algorithm, d_query, query_len, d_codes, d_offsets, d_lengths,
                                                count, max_seq_len, d_scores, stream or None))
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_uint64), ("completed", ctypes.c_uint64), ("waves", ctypes.c_uint64),
+                ("cells", ctypes.c_uint64), ("busy_seconds", ctypes.c_double), ("device_seconds", ctypes.c_double),
+                ("slots", ctypes.c_uint32), ("segments", ctypes.c_uint32)]
+
+
+SERVE_MAX_QUERY = 8192
+
+
+class Server:
+    """The request loop of include/libssa_b200.h (ssa_server_*): queries are
+    admitted into resident slots and folded into the running database scan;
+    each result equals the query's sw_align/nw_align result alone."""
+
+    def __init__(self, algorithm: int, hitcount: int, bit_width: int, align_type: int, slots: int = 64,
+                 segments: int = 8, memory_budget: int = 0):
+        self._lib = load()
+        self._h = self._lib.ssa_server_start(algorithm, hitcount, bit_width, align_type, slots, segments,
+                                             memory_budget)
+
+    def submit(self, q) -> int:
+        t = int(self._lib.ssa_server_submit(self._h, q))
+        if t < 0:
+            raise ValueError("request refused")
+        return t
+
+    def wait(self, ticket: int) -> tuple[list[Hit], float]:
+        lat = ctypes.c_double(0)
+        lp = self._lib.ssa_server_wait(self._h, ticket, ctypes.byref(lat))
+        if not lp:
+            raise KeyError(ticket)
+        hits = _read_list(lp)
+        self._lib.free_alignment(lp)
+        return hits, lat.value
+
+    def stats(self) -> ServerStats:
+        st = ServerStats()
+        self._lib.ssa_server_get_stats(self._h, ctypes.byref(st))
+        return st
+
+    def stop(self) -> None:
+        if self._h:
+            self._lib.ssa_server_stop(self._h)
+            self._h = None
 
 
 def query_length(q) -> int:

@@ -7,6 +7,13 @@
 // prints an error and returns NULL.  The search itself is delegated to the
 // GPU engine (engine.cu); there is no CPU search path.
 #include "ssa_internal.h"
+
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <thread>
 #include "libssa_b200.h"
 #include "libssa_extern_db.h"
 
@@ -398,6 +405,131 @@ static std::vector<p_alignment_list> run_search( int algo, p_query * queries, si
     return out;
 }
 
+// ---- serving ------------------------------------------------------------------------
+// A server owns a fixed set of query slots resident on the device.  Its loop
+// thread repeats waves: admit waiting requests into free slots (first come,
+// first served, while their traceback memory fits the budget), run the entry
+// pass and cascade of every occupied slot over the next segment of the
+// database (the segments form a ring, so a request admitted at any wave starts
+// with the segment the loop is on and is done after one full turn), then finish
+// the requests that have seen every segment: replay of the CPU lane schedule,
+// heap, traceback, alignment list.  Per (query, sequence) the work is the same
+// as in sw_align/nw_align, so every result equals the one the query gets alone.
+struct ServeTicket {
+    p_query query = nullptr;
+    long long id = 0;
+    uint64_t mem = 0;
+    int slot = -1;
+    uint32_t waves = 0;
+    bool done = false;
+    std::chrono::steady_clock::time_point t_submit, t_done;
+    ReplayQuery lists;
+    p_alignment_list result = nullptr;
+};
+
+struct ServerImpl {
+    SearchRequest req;
+    std::vector<int64_t> matrix;       // the settings at start, kept for the server's lifetime
+    uint32_t slots = 0;
+    std::vector<uint32_t> seg;         // segment bounds over the length-sorted sequences
+    uint64_t budget = 0;
+    uint64_t max_db_len = 0;
+    uint64_t residues = 0;
+    std::mutex m;
+    std::condition_variable cv_work, cv_done;
+    std::deque<ServeTicket *> pending;
+    std::map<long long, ServeTicket *> tickets;
+    std::vector<ServeTicket *> owner;  // per slot
+    uint32_t occupied = 0;
+    uint64_t mem_in_use = 0;
+    long long next_id = 0;
+    bool stopping = false;
+    uint32_t cursor = 0;
+    std::thread loop_thread;
+    // statistics
+    uint64_t submitted = 0, completed = 0, waves = 0, cells = 0;
+    double busy_seconds = 0, device_seconds = 0;
+
+    void loop();
+};
+
+void ServerImpl::loop() {
+    const uint32_t n_seg = (uint32_t) seg.size() - 1;
+    for( ;; ) {
+        std::vector<ServeTicket *> admitted;
+        {
+            std::unique_lock<std::mutex> lk( m );
+            cv_work.wait( lk, [&] { return stopping || !pending.empty() || occupied > 0; } );
+            if( pending.empty() && occupied == 0 )
+                break;     // stopping and drained
+            while( !pending.empty() && occupied < slots ) {
+                ServeTicket * t = pending.front();
+                if( budget && occupied > 0 && mem_in_use + t->mem > budget )
+                    break;
+                pending.pop_front();
+                uint32_t s = 0;
+                while( owner[s] )
+                    s++;
+                owner[s] = t;
+                t->slot = (int) s;
+                occupied++;
+                mem_in_use += t->mem;
+                admitted.push_back( t );
+            }
+        }
+        const auto t0 = std::chrono::steady_clock::now();
+        for( ServeTicket * t : admitted )
+            engine_serve_load( (uint32_t) t->slot, (const uint8_t *) t->query->seq, (uint32_t) t->query->len );
+        std::vector<uint32_t> active;
+        for( uint32_t s = 0; s < slots; s++ )
+            if( owner[s] )
+                active.push_back( s );
+        std::vector<ServeOverflow> oe, o16;
+        SearchStats st;
+        engine_serve_wave( req, active, seg[cursor], seg[cursor + 1], oe, o16, st );
+        cursor = (cursor + 1) % n_seg;
+        for( const ServeOverflow & o : oe )
+            owner[o.slot]->lists.ovf_entry.emplace_back( o.id, o.nb );
+        for( const ServeOverflow & o : o16 )
+            owner[o.slot]->lists.ovf16.emplace_back( o.id, o.nb );
+        std::vector<uint32_t> done;
+        std::vector<ReplayQuery> rq;
+        for( uint32_t s : active ) {
+            ServeTicket * t = owner[s];
+            if( ++t->waves == n_seg ) {
+                done.push_back( s );
+                rq.push_back( std::move( t->lists ) );
+            }
+        }
+        std::vector<std::vector<Hit>> hits;
+        if( !done.empty() )
+            engine_serve_finish( req, done, rq, hits, st );
+        std::vector<p_alignment_list> lists( done.size() );
+        for( size_t i = 0; i < done.size(); i++ )
+            lists[i] = make_list( hits[done[i]], owner[done[i]]->query, req.align_type == COMPUTE_ALIGNMENT );
+        const auto t1 = std::chrono::steady_clock::now();
+        {
+            std::lock_guard<std::mutex> lk( m );
+            waves++;
+            busy_seconds += std::chrono::duration<double>( t1 - t0 ).count();
+            device_seconds += st.kernel_seconds;
+            for( size_t i = 0; i < done.size(); i++ ) {
+                ServeTicket * t = owner[done[i]];
+                t->result = lists[i];
+                t->done = true;
+                t->t_done = t1;
+                cells += (uint64_t) t->query->len * residues;
+                completed++;
+                mem_in_use -= t->mem;
+                owner[done[i]] = nullptr;
+                occupied--;
+            }
+        }
+        if( !done.empty() )
+            cv_done.notify_all();
+    }
+}
+
 // ---- libssa.h ---------------------------------------------------------------------
 // The C entry points are the library's only exported symbols.
 #pragma GCC visibility push( default )
@@ -573,6 +705,125 @@ void ssa_db_refresh( void ) {
 
 size_t ssa_query_length( p_query p ) {
     return p ? p->len : 0;
+}
+
+struct ssa_server {
+    ServerImpl impl;
+};
+
+ssa_server * ssa_server_start( int algorithm, size_t hitcount, int bit_width, int align_type, size_t slots,
+        size_t segments, size_t memory_budget ) {
+    if( algorithm != SSA_SMITH_WATERMAN && algorithm != SSA_NEEDLEMAN_WUNSCH )
+        fatal( "\nUnknown search type: %d\n\n", algorithm );
+    if( slots == 0 || slots > 4096 )
+        fatal( "Server slots must be in 1..4096 (got %zu).", slots );
+    const Config & c = config();
+    if( !c.matrix_set )
+        fatal( "Scoring not initialized." );
+    if( !c.constant_scoring && c.symtype == NUCLEOTIDE )
+        fatal( "Nucleotide sequences can only be aligned using constant scores." );
+    ssa_server * sv = new ssa_server();
+    ServerImpl & s = sv->impl;
+    s.req = make_request( algorithm == SSA_SMITH_WATERMAN ? 0 : 1, hitcount, bit_width, align_type );
+    s.matrix.assign( c.matrix, c.matrix + 1024 );
+    s.req.matrix = s.matrix.data();
+    s.slots = (uint32_t) slots;
+    s.budget = memory_budget;
+    s.owner.assign( slots, nullptr );
+    s.seg = engine_serve_open( s.req, (uint32_t) slots, (uint32_t) std::max<size_t>( 1, segments ) );
+    {
+        const HostDb & db = engine_database();
+        for( uint32_t l : db.len )
+            s.max_db_len = std::max<uint64_t>( s.max_db_len, l );
+        s.residues = db.residues;
+    }
+    s.loop_thread = std::thread( [&s] { s.loop(); } );
+    return sv;
+}
+
+long long ssa_server_submit( ssa_server * sv, p_query query ) {
+    if( !sv || !query )
+        fatal( "Query not initialized." );
+    ServerImpl & s = sv->impl;
+    if( query->symtype != config().symtype )
+        fatal( "Query was read with a different symbol type than the current one." );
+    if( query->len == 0 || query->len > SERVE_MAX_QUERY ) {
+        print_error( "Served queries must have 1..%u residues (got %zu).", SERVE_MAX_QUERY, query->len );
+        return -1;
+    }
+    ServeTicket * t = new ServeTicket();
+    t->query = query;
+    // traceback memory of the request's hits, bounded by the longest sequence:
+    // 2-bit directions (16 bits per 8 query rows and column), last rows, ops
+    if( s.req.align_type == COMPUTE_ALIGNMENT )
+        t->mem = (uint64_t) s.req.hitcount * (((query->len + 7) / 8) * 2 * s.max_db_len + 8 * query->len +
+                query->len + s.max_db_len);
+    t->t_submit = std::chrono::steady_clock::now();
+    {
+        std::lock_guard<std::mutex> lk( s.m );
+        if( s.stopping ) {
+            delete t;
+            return -1;
+        }
+        t->id = s.next_id++;
+        s.tickets[t->id] = t;
+        s.pending.push_back( t );
+        s.submitted++;
+    }
+    s.cv_work.notify_one();
+    return t->id;
+}
+
+p_alignment_list ssa_server_wait( ssa_server * sv, long long ticket, double * latency_seconds ) {
+    if( !sv )
+        return nullptr;
+    ServerImpl & s = sv->impl;
+    std::unique_lock<std::mutex> lk( s.m );
+    auto it = s.tickets.find( ticket );
+    if( it == s.tickets.end() )
+        return nullptr;
+    ServeTicket * t = it->second;
+    s.cv_done.wait( lk, [&] { return t->done; } );
+    p_alignment_list r = t->result;
+    if( latency_seconds )
+        *latency_seconds = std::chrono::duration<double>( t->t_done - t->t_submit ).count();
+    s.tickets.erase( it );
+    delete t;
+    return r;
+}
+
+void ssa_server_get_stats( ssa_server * sv, ssa_server_stats_t * out ) {
+    if( !sv || !out )
+        return;
+    ServerImpl & s = sv->impl;
+    std::lock_guard<std::mutex> lk( s.m );
+    out->submitted = s.submitted;
+    out->completed = s.completed;
+    out->waves = s.waves;
+    out->cells = s.cells;
+    out->busy_seconds = s.busy_seconds;
+    out->device_seconds = s.device_seconds;
+    out->slots = s.slots;
+    out->segments = (uint32_t) s.seg.size() - 1;
+}
+
+void ssa_server_stop( ssa_server * sv ) {
+    if( !sv )
+        return;
+    ServerImpl & s = sv->impl;
+    {
+        std::lock_guard<std::mutex> lk( s.m );
+        s.stopping = true;
+    }
+    s.cv_work.notify_all();
+    if( s.loop_thread.joinable() )
+        s.loop_thread.join();
+    for( auto & kv : s.tickets ) {      // results nobody waited for
+        if( kv.second->result )
+            free_alignment( kv.second->result );
+        delete kv.second;
+    }
+    delete sv;
 }
 
 }  // extern "C"

@@ -293,26 +293,41 @@ public:
             &d_scratch_fast_[0], &d_scratch_fast_[1], &d_scratch_fast_[2], &d_scratch_fast_[3], &d_qcodes_, &d_qoff_, &d_qlen_, &d_qpad_,
             &d_prof_off_, &d_prof_, &d_matrix_, &d_score_, &d_list_a_, &d_list_b_, &d_counts_, &d_scratch_,
             &d_tb_hits_, &d_tb_regions_, &d_tb_last_, &d_tb_last_off_, &d_tb_dirs_, &d_tb_dir_off_, &d_tb_ops_,
-            &d_tb_ops_off_, &d_tb_ops_len_, &d_qp_prof_, &d_qp_off_, &d_qp_rows_, &d_qp_slots_, &d_qp_units_ };
+            &d_tb_ops_off_, &d_tb_ops_len_, &d_qp_prof_, &d_qp_off_, &d_qp_rows_, &d_qp_slots_, &d_qp_units_,
+            &d_serve_score_ };
         for( DevBuf * b : bufs )
             b->release();
         h_score_.release();
         db_ = HostDb();
         db_stale_ = true;
         ranks_.clear();
+        serve_layout_ = false;
+        serve_slots_ = 0;
+        serve_codes_.clear();
     }
 
     uint64_t launches() const { return launches_.load(); }
+
+    // ---- serving: fixed query slots, waves over database segments ---------------
+    std::vector<uint32_t> serve_open( const SearchRequest & req, uint32_t slots, uint32_t segments );
+    void serve_restore( const SearchRequest & req );
+    void serve_load( uint32_t slot, const uint8_t * codes, uint32_t len );
+    void serve_wave( const SearchRequest & req, const std::vector<uint32_t> & active, uint32_t seq_lo,
+            uint32_t seq_hi, std::vector<PairTask> & ovf_entry, std::vector<PairTask> & ovf16, SearchStats & stats );
+    void serve_finish( const SearchRequest & req, const std::vector<uint32_t> & done,
+            std::vector<ReplayQuery> & rq, std::vector<std::vector<Hit>> & out, SearchStats & stats );
 
 private:
     Engine() = default;
 
     void run_pass( int algo, int width, const SearchRequest & req, uint32_t n_slots, const PairTask * tasks,
             uint64_t n_tasks, bool implicit, PairTask * next, unsigned * next_count, uint32_t next_cap,
-            const uint32_t * slot_list = nullptr, uint32_t n_sub = 0 );
+            const uint32_t * slot_list = nullptr, uint32_t n_sub = 0, uint32_t order_lo = 0 );
     void run_fast_entry( const SearchRequest & req, uint32_t nq, PairTask * next, unsigned * next_count, uint32_t cap );
     void run_qpair_entry( const SearchRequest & req, uint32_t nq, PairTask * next, unsigned * next_count,
-            uint32_t cap );
+            uint32_t cap, const std::vector<uint32_t> * slots = nullptr, uint32_t seq_lo = 0,
+            uint32_t seq_hi = UINT32_MAX );
+    int32_t * score_sink() { return serving_ ? d_serve_score_.as<int32_t>() : d_score_.as<int32_t>(); }
     void build_profiles( int width, uint32_t n_slots );
     void traceback( const SearchRequest & req, const std::vector<QueryCodes> & queries, uint32_t slot0,
             std::vector<std::vector<Hit>> & out, SearchStats & stats );
@@ -335,6 +350,12 @@ private:
     DevBuf d_scratch_fast_[4];
     DevBuf d_bounds_, d_group_;
     DevBuf d_qp_prof_, d_qp_off_, d_qp_rows_, d_qp_slots_, d_qp_units_;
+    // serving: fixed query slots and their own score rows
+    DevBuf d_serve_score_;
+    bool serving_ = false;           // passes write d_serve_score_
+    bool serve_layout_ = false;      // the query buffers hold the serving slots
+    uint32_t serve_slots_ = 0;
+    std::vector<std::vector<uint8_t>> serve_codes_;   // per slot, to restore the layout after a search
     cudaStream_t class_stream_[4] = { nullptr, nullptr, nullptr, nullptr };
     cudaEvent_t ev_class_[4] = { nullptr, nullptr, nullptr, nullptr };
     cudaEvent_t ev_cls_t_[8] = {};   // per class start / end, timed (SSA_B200_TIMING)
@@ -372,7 +393,7 @@ void Engine::build_profiles( int width, uint32_t n_slots ) {
 
 void Engine::run_pass( int algo, int width, const SearchRequest & req, uint32_t n_slots, const PairTask * tasks,
         uint64_t n_tasks, bool implicit, PairTask * next, unsigned * next_count, uint32_t next_cap,
-        const uint32_t * slot_list, uint32_t n_sub ) {
+        const uint32_t * slot_list, uint32_t n_sub, uint32_t order_lo ) {
     if( n_tasks == 0 )
         return;
     build_profiles( width, n_slots );
@@ -384,7 +405,7 @@ void Engine::run_pass( int algo, int width, const SearchRequest & req, uint32_t 
     p.qv.qpad = d_qpad_.as<uint32_t>();
     p.qv.n_slots = n_slots;
     p.tasks = implicit ? nullptr : tasks;
-    p.order = d_order_.as<uint32_t>();
+    p.order = d_order_.as<uint32_t>() + order_lo;
     p.slot_list = slot_list;
     p.n_sub = n_sub;
     p.n_tasks = n_tasks;
@@ -393,7 +414,7 @@ void Engine::run_pass( int algo, int width, const SearchRequest & req, uint32_t 
     p.counter = counter;
     p.gap_open = req.gap_open;
     p.gap_extend = req.gap_extend;
-    p.sink.score = d_score_.as<int32_t>();
+    p.sink.score = score_sink();
     p.sink.score_stride = db_.n_ids;
     p.sink.next = next;
     p.sink.next_count = next_count;
@@ -578,7 +599,7 @@ void Engine::run_fast_entry( const SearchRequest & req, uint32_t nq, PairTask * 
         p.unit_counter = unit_counter;
         p.gap_oe = (int8_t) (req.gap_open + req.gap_extend);
         p.gap_e = req.gap_extend;
-        p.sink.score = d_score_.as<int32_t>();
+        p.sink.score = score_sink();
         p.sink.score_stride = db_.n_ids;
         p.sink.next = next;
         p.sink.next_count = next_count;
@@ -636,14 +657,23 @@ static int choose_qpair_rows( uint32_t Q, uint32_t * passes, int pinned ) {
 }
 
 void Engine::run_qpair_entry( const SearchRequest & req, uint32_t nq, PairTask * next, unsigned * next_count,
-        uint32_t cap ) {
-    const uint32_t n_seq = (uint32_t) db_.order_desc.size();
+        uint32_t cap, const std::vector<uint32_t> * slots, uint32_t seq_lo, uint32_t seq_hi ) {
+    // the sequences order_desc[seq_lo, seq_hi) (all by default)
+    const uint32_t n_all = (uint32_t) db_.order_desc.size();
+    const uint32_t lo = std::min( seq_lo, n_all ), hi = std::min( seq_hi, n_all );
+    const uint32_t n_seq = hi - lo;
     if( n_seq == 0 )
         return;
     // pair the queries that fit, longest first; longer ones run the emulation
     std::vector<uint32_t> fit, fallback;
-    for( uint32_t s = 0; s < nq; s++ )
-        (h_qlen_[s] <= FAST_MAX_ROWS ? fit : fallback).push_back( s );
+    if( slots ) {
+        for( uint32_t s : *slots )
+            (h_qlen_[s] <= FAST_MAX_ROWS ? fit : fallback).push_back( s );
+    }
+    else {
+        for( uint32_t s = 0; s < nq; s++ )
+            (h_qlen_[s] <= FAST_MAX_ROWS ? fit : fallback).push_back( s );
+    }
     std::stable_sort( fit.begin(), fit.end(), [&]( uint32_t a, uint32_t b ) { return h_qlen_[a] > h_qlen_[b]; } );
     const uint32_t n_qp = (uint32_t) ((fit.size() + 1) / 2);
     // SSA_B200_QP_R=16|20|24|28 pins R (tuning)
@@ -699,15 +729,15 @@ void Engine::run_qpair_entry( const SearchRequest & req, uint32_t nq, PairTask *
     // holding about equal numbers of columns, the longest first; every pair of
     // a class gets every range.  A warp takes one unit at a time.
     uint64_t total_cols = 0;
-    for( uint32_t id : db_.order_desc )
-        total_cols += (db_.len[id] + 3u) & ~3u;
+    for( uint32_t i = lo; i < hi; i++ )
+        total_cols += (db_.len[db_.order_desc[i]] + 3u) & ~3u;
     const uint64_t want_units = (uint64_t) sms_ * 16 * 24;
     const uint64_t target = std::max<uint64_t>( 1, total_cols * std::max<uint32_t>( 1, n_qp ) / want_units );
     std::vector<uint32_t> bounds{ 0 };
     {
         uint64_t acc = 0;
         for( uint32_t i = 0; i < n_seq; i++ ) {
-            acc += (db_.len[db_.order_desc[i]] + 3u) & ~3u;
+            acc += (db_.len[db_.order_desc[lo + i]] + 3u) & ~3u;
             if( acc >= target && (i + 1) % QP_GPW == 0 ) {
                 bounds.push_back( i + 1 );
                 acc = 0;
@@ -723,6 +753,9 @@ void Engine::run_qpair_entry( const SearchRequest & req, uint32_t nq, PairTask *
     CUDA_CHECK( cudaEventRecord( ev_ready_, stream_ ) );
     const uint32_t scratch_cols = (((db_.max_len + 3u) & ~3u) >> 1) + 2u;
     const bool timing = getenv( "SSA_B200_TIMING" ) != nullptr;
+    uint64_t seg_residues = 0;
+    for( uint32_t i = lo; i < hi; i++ )
+        seg_residues += db_.len[db_.order_desc[i]];
     size_t class_first = 0;
     for( int ri = 0; ri < 4; ri++ ) {
         const std::vector<uint32_t> & cls = by_r[ri];
@@ -740,7 +773,7 @@ void Engine::run_qpair_entry( const SearchRequest & req, uint32_t nq, PairTask *
         unsigned long long * unit_counter = d_counts_.as<unsigned long long>() + 8 + ri;   // bytes 64..95
         CUDA_CHECK( cudaMemsetAsync( unit_counter, 0, sizeof(unsigned long long), class_stream_[ri] ) );
         p.db = DbView{ d_codes_.as<uint8_t>(), d_off_.as<uint64_t>(), d_len_.as<uint32_t>(), db_.n_ids };
-        p.order = d_order_.as<uint32_t>();
+        p.order = d_order_.as<uint32_t>() + lo;
         p.prof = d_qp_prof_.as<uint32_t>();
         p.prof_off = d_qp_off_.as<uint64_t>();
         p.qp_slots = d_qp_slots_.as<uint32_t>();
@@ -753,7 +786,7 @@ void Engine::run_qpair_entry( const SearchRequest & req, uint32_t nq, PairTask *
         p.unit_counter = unit_counter;
         p.gap_oe = (int8_t) (req.gap_open + req.gap_extend);
         p.gap_e = req.gap_extend;
-        p.sink.score = d_score_.as<int32_t>();
+        p.sink.score = score_sink();
         p.sink.score_stride = db_.n_ids;
         p.sink.next = next;
         p.sink.next_count = next_count;
@@ -784,7 +817,7 @@ void Engine::run_qpair_entry( const SearchRequest & req, uint32_t nq, PairTask *
             double cells = 0, padded = 0;
             for( uint32_t i : by_r[ri] ) {
                 const uint32_t a = qp_slots[2 * i], b = qp_slots[2 * i + 1];
-                cells += (double) (h_qlen_[a] + (b == 0xffffffffu ? 0u : h_qlen_[b])) * (double) db_.residues;
+                cells += (double) (h_qlen_[a] + (b == 0xffffffffu ? 0u : h_qlen_[b])) * (double) seg_residues;
                 padded += 2.0 * qp_rows[i] * (double) total_cols;
             }
             fprintf( stderr, "[ssa timing] qpair class R=%d: %zu pairs, %.3f ms, %.3e cells (%.1f%% of computed), "
@@ -797,7 +830,7 @@ void Engine::run_qpair_entry( const SearchRequest & req, uint32_t nq, PairTask *
         CUDA_CHECK( cudaMemcpyAsync( d_slots_.p, fallback.data(), fallback.size() * sizeof(uint32_t),
                 cudaMemcpyHostToDevice, stream_ ) );
         run_pass( 0, 8, req, nq, nullptr, (uint64_t) fallback.size() * n_seq, true, next, next_count, cap,
-                d_slots_.as<uint32_t>(), (uint32_t) fallback.size() );
+                d_slots_.as<uint32_t>(), (uint32_t) fallback.size(), lo );
     }
 }
 
@@ -805,6 +838,8 @@ void Engine::search( const SearchRequest & req, const std::vector<QueryCodes> & 
         std::vector<std::vector<Hit>> & out, SearchStats & stats ) {
     init_device();
     const HostDb & db = database();
+    serving_ = false;
+    serve_layout_ = false;      // the query buffers are reused for this batch
     out.assign( queries.size(), {} );
     if( queries.empty() )
         return;
@@ -1154,22 +1189,278 @@ void Engine::traceback( const SearchRequest & req, const std::vector<QueryCodes>
     }
 }
 
+// ---- serving -------------------------------------------------------------------
+// A server keeps a fixed number of query slots resident: slot s owns the codes at
+// s * SERVE_QSTRIDE, its int32 profile at s * 32 * SERVE_MAX_QUERY and the score
+// row s of d_serve_score_.  Each wave runs the entry pass and the cascade of every
+// occupied slot over one segment of the length-sorted database; a slot that has
+// seen every segment is finished (score rows to the host, schedule replay, heap,
+// traceback) and freed for the next request.
+constexpr uint32_t SERVE_QSTRIDE = SERVE_MAX_QUERY + 16;
+
+void Engine::serve_restore( const SearchRequest & req ) {
+    const uint32_t S = serve_slots_;
+    d_matrix_.ensure( 1024 * sizeof(int64_t) );
+    CUDA_CHECK( cudaMemcpyAsync( d_matrix_.p, req.matrix, 1024 * sizeof(int64_t), cudaMemcpyHostToDevice, stream_ ) );
+    h_qoff_.assign( S, 0 );
+    h_qlen_.assign( S, 0 );
+    h_qpad_.assign( S, 256 );
+    h_prof_off_.assign( S, 0 );
+    for( uint32_t s = 0; s < S; s++ ) {
+        const uint32_t len = (uint32_t) serve_codes_[s].size();
+        h_qoff_[s] = (uint64_t) s * SERVE_QSTRIDE;
+        h_qlen_[s] = len;
+        h_qpad_[s] = std::max<uint32_t>( 256, (len + 255u) & ~255u );
+        h_prof_off_[s] = (uint64_t) s * 32 * SERVE_MAX_QUERY;
+    }
+    d_qcodes_.ensure( (size_t) S * SERVE_QSTRIDE + 16 );
+    d_qoff_.ensure( S * sizeof(uint64_t) );
+    d_qlen_.ensure( S * sizeof(uint32_t) );
+    d_qpad_.ensure( S * sizeof(uint32_t) );
+    d_prof_off_.ensure( S * sizeof(uint64_t) );
+    d_prof_.ensure( (size_t) S * 32 * SERVE_MAX_QUERY * sizeof(int32_t) );
+    d_counts_.ensure( 16 * sizeof(unsigned long long) );
+    CUDA_CHECK( cudaMemcpyAsync( d_qoff_.p, h_qoff_.data(), S * sizeof(uint64_t), cudaMemcpyHostToDevice, stream_ ) );
+    CUDA_CHECK( cudaMemcpyAsync( d_qlen_.p, h_qlen_.data(), S * sizeof(uint32_t), cudaMemcpyHostToDevice, stream_ ) );
+    CUDA_CHECK( cudaMemcpyAsync( d_qpad_.p, h_qpad_.data(), S * sizeof(uint32_t), cudaMemcpyHostToDevice, stream_ ) );
+    CUDA_CHECK( cudaMemcpyAsync( d_prof_off_.p, h_prof_off_.data(), S * sizeof(uint64_t), cudaMemcpyHostToDevice,
+            stream_ ) );
+    for( uint32_t s = 0; s < S; s++ )
+        if( !serve_codes_[s].empty() )
+            CUDA_CHECK( cudaMemcpyAsync( d_qcodes_.as<uint8_t>() + h_qoff_[s], serve_codes_[s].data(),
+                    serve_codes_[s].size(), cudaMemcpyHostToDevice, stream_ ) );
+    CUDA_CHECK( cudaStreamSynchronize( stream_ ) );
+    prof_width_ = -1;
+    serve_layout_ = true;
+}
+
+std::vector<uint32_t> Engine::serve_open( const SearchRequest & req, uint32_t slots, uint32_t segments ) {
+    init_device();
+    const HostDb & db = database();
+    serve_slots_ = slots;
+    serve_codes_.assign( slots, {} );
+    d_serve_score_.ensure( std::max<size_t>( 4, (size_t) slots * db.n_ids * sizeof(int32_t) ) );
+    serve_layout_ = false;
+    serve_restore( req );
+    // the query-independent lane schedule of the entry width, computed once here
+    // rather than in the first request's latency
+    if( req.bit_width != 64 )
+        ranks( req.chunk_size, req.bit_width == 8 ? req.lanes8 : req.lanes16 );
+    // segments of the length-sorted sequences holding about equal residues
+    const uint32_t n = (uint32_t) db.order_desc.size();
+    segments = std::max<uint32_t>( 1, std::min<uint32_t>( segments, std::max<uint32_t>( 1, n ) ) );
+    std::vector<uint32_t> bounds{ 0 };
+    uint64_t acc = 0;
+    for( uint32_t i = 0; i < n && bounds.size() < segments; i++ ) {
+        acc += db.len[db.order_desc[i]];
+        if( acc * segments >= db.residues * (uint64_t) bounds.size() )
+            bounds.push_back( i + 1 );
+    }
+    if( bounds.back() != n )
+        bounds.push_back( n );
+    return bounds;
+}
+
+void Engine::serve_load( uint32_t slot, const uint8_t * codes, uint32_t len ) {
+    serve_codes_[slot].assign( codes, codes + len );
+    if( !serve_layout_ )
+        return;     // restored before the next wave
+    h_qlen_[slot] = len;
+    h_qpad_[slot] = std::max<uint32_t>( 256, (len + 255u) & ~255u );
+    CUDA_CHECK( cudaMemcpyAsync( d_qcodes_.as<uint8_t>() + h_qoff_[slot], codes, len, cudaMemcpyHostToDevice,
+            stream_ ) );
+    CUDA_CHECK( cudaMemcpyAsync( d_qlen_.as<uint32_t>() + slot, &h_qlen_[slot], sizeof(uint32_t),
+            cudaMemcpyHostToDevice, stream_ ) );
+    CUDA_CHECK( cudaMemcpyAsync( d_qpad_.as<uint32_t>() + slot, &h_qpad_[slot], sizeof(uint32_t),
+            cudaMemcpyHostToDevice, stream_ ) );
+    CUDA_CHECK( cudaStreamSynchronize( stream_ ) );
+    prof_width_ = -1;
+}
+
+void Engine::serve_wave( const SearchRequest & req, const std::vector<uint32_t> & active, uint32_t seq_lo,
+        uint32_t seq_hi, std::vector<PairTask> & ovf_entry, std::vector<PairTask> & ovf16, SearchStats & stats ) {
+    ovf_entry.clear();
+    ovf16.clear();
+    if( active.empty() || seq_hi <= seq_lo )
+        return;
+    if( !serve_layout_ )
+        serve_restore( req );
+    serving_ = true;
+    const uint32_t n_seg = seq_hi - seq_lo;
+    max_qlen_ = 0;
+    uint64_t seg_res = 0;
+    for( uint32_t i = seq_lo; i < seq_hi; i++ )
+        seg_res += db_.len[db_.order_desc[i]];
+    for( uint32_t s : active ) {
+        max_qlen_ = std::max( max_qlen_, h_qlen_[s] );
+        stats.cells += (uint64_t) h_qlen_[s] * seg_res;
+    }
+    const uint64_t n_pairs = (uint64_t) active.size() * n_seg;
+    const uint32_t cap = (uint32_t) std::min<uint64_t>( std::max<uint64_t>( n_pairs, 1 ), 0xffffffffull );
+    d_list_a_.ensure( (size_t) cap * sizeof(PairTask) );
+    d_list_b_.ensure( (size_t) cap * sizeof(PairTask) );
+    CUDA_CHECK( cudaMemsetAsync( d_counts_.p, 0, 16 * sizeof(unsigned long long), stream_ ) );
+    unsigned * cnt = d_counts_.as<unsigned>();
+    const int entry = req.bit_width;
+    CUDA_CHECK( cudaEventRecord( ev_phase_[0], stream_ ) );
+    if( fast_eligible( req ) ) {
+        run_qpair_entry( req, serve_slots_, d_list_a_.as<PairTask>(), cnt + 0, cap, &active, seq_lo, seq_hi );
+    }
+    else {
+        d_slots_.ensure( active.size() * sizeof(uint32_t) );
+        CUDA_CHECK( cudaMemcpyAsync( d_slots_.p, active.data(), active.size() * sizeof(uint32_t),
+                cudaMemcpyHostToDevice, stream_ ) );
+        run_pass( req.algo, entry, req, serve_slots_, nullptr, n_pairs, true, d_list_a_.as<PairTask>(), cnt + 0, cap,
+                d_slots_.as<uint32_t>(), (uint32_t) active.size(), seq_lo );
+    }
+    CUDA_CHECK( cudaEventRecord( ev_phase_[1], stream_ ) );
+    unsigned n_a = 0, n_b = 0;
+    if( entry != 64 ) {
+        CUDA_CHECK( cudaMemcpyAsync( &n_a, cnt + 0, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_ ) );
+        CUDA_CHECK( cudaStreamSynchronize( stream_ ) );
+        n_a = std::min( n_a, cap );
+        if( n_a ) {
+            const int w2 = (entry == 8) ? 16 : 64;
+            PairTask * nx = (w2 == 16) ? d_list_b_.as<PairTask>() : nullptr;
+            run_pass( req.algo, w2, req, serve_slots_, d_list_a_.as<PairTask>(), n_a, false, nx, cnt + 1, cap );
+            if( w2 == 16 ) {
+                CUDA_CHECK( cudaMemcpyAsync( &n_b, cnt + 1, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_ ) );
+                CUDA_CHECK( cudaStreamSynchronize( stream_ ) );
+                n_b = std::min( n_b, cap );
+                if( n_b )
+                    run_pass( req.algo, 64, req, serve_slots_, d_list_b_.as<PairTask>(), n_b, false, nullptr, cnt + 3,
+                            0 );
+            }
+            ovf_entry.resize( n_a );
+            CUDA_CHECK( cudaMemcpyAsync( ovf_entry.data(), d_list_a_.p, n_a * sizeof(PairTask),
+                    cudaMemcpyDeviceToHost, stream_ ) );
+            if( n_b ) {
+                ovf16.resize( n_b );
+                CUDA_CHECK( cudaMemcpyAsync( ovf16.data(), d_list_b_.p, n_b * sizeof(PairTask),
+                        cudaMemcpyDeviceToHost, stream_ ) );
+            }
+        }
+    }
+    unsigned err = 0;
+    CUDA_CHECK( cudaMemcpyAsync( &err, cnt + 2, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_ ) );
+    CUDA_CHECK( cudaEventRecord( ev_phase_[2], stream_ ) );
+    CUDA_CHECK( cudaStreamSynchronize( stream_ ) );
+    serving_ = false;
+    if( err )
+        fatal( "Internal error in the GPU search (flags 0x%x).", err );
+    float ms[2];
+    CUDA_CHECK( cudaEventElapsedTime( &ms[0], ev_phase_[0], ev_phase_[1] ) );
+    CUDA_CHECK( cudaEventElapsedTime( &ms[1], ev_phase_[1], ev_phase_[2] ) );
+    stats.entry_seconds += ms[0] * 1e-3;
+    stats.kernel_seconds += (ms[0] + ms[1]) * 1e-3;
+    stats.overflow8 += n_a;
+    stats.overflow16 += n_b;
+}
+
+void Engine::serve_finish( const SearchRequest & req, const std::vector<uint32_t> & done,
+        std::vector<ReplayQuery> & rq, std::vector<std::vector<Hit>> & out, SearchStats & stats ) {
+    out.assign( serve_slots_, {} );
+    if( done.empty() )
+        return;
+    if( !serve_layout_ )
+        serve_restore( req );
+    const uint32_t nd = (uint32_t) done.size();
+    const size_t row = (size_t) db_.n_ids;
+    int32_t * hs = (int32_t *) h_score_.ensure( std::max<size_t>( 4, nd * row * sizeof(int32_t) ) );
+    for( uint32_t i = 0; i < nd; i++ )
+        CUDA_CHECK( cudaMemcpyAsync( hs + i * row, d_serve_score_.as<int32_t>() + (size_t) done[i] * row,
+                row * sizeof(int32_t), cudaMemcpyDeviceToHost, stream_ ) );
+    CUDA_CHECK( cudaStreamSynchronize( stream_ ) );
+    stats.d2h_bytes += nd * row * sizeof(int32_t);
+    const int entry = req.bit_width;
+    const uint32_t * rank_entry =
+            (entry == 64) ? nullptr : ranks( req.chunk_size, entry == 8 ? req.lanes8 : req.lanes16 );
+    {
+        std::atomic<uint32_t> next{ 0 };
+        std::vector<ReplayCounts> counts( nd );
+        auto work = [&]() {
+            for( ;; ) {
+                const uint32_t i = next.fetch_add( 1 );
+                if( i >= nd )
+                    break;
+                rq[i].score = hs + i * row;
+                std::sort( rq[i].ovf_entry.begin(), rq[i].ovf_entry.end() );
+                std::sort( rq[i].ovf16.begin(), rq[i].ovf16.end() );
+                replay_query( db_, req, rq[i], rank_entry, out[done[i]], counts[i] );
+            }
+        };
+        const unsigned nthreads = std::min<unsigned>( std::max( 1u, std::thread::hardware_concurrency() ), nd );
+        std::vector<std::thread> th;
+        for( unsigned k = 1; k < nthreads; k++ )
+            th.emplace_back( work );
+        work();
+        for( auto & t : th )
+            t.join();
+    }
+    if( req.align_type == COMPUTE_ALIGNMENT ) {
+        max_qlen_ = 0;
+        for( uint32_t s : done )
+            max_qlen_ = std::max( max_qlen_, h_qlen_[s] );
+        traceback( req, {}, 0, out, stats );
+    }
+}
+
 // ---- free functions ------------------------------------------------------------
+// One engine per process; the search entry points and a server's waves take
+// turns on it.
+static std::mutex g_engine_mutex;
+
 void engine_search( const SearchRequest & req, const std::vector<QueryCodes> & queries,
         std::vector<std::vector<Hit>> & out, SearchStats & stats ) {
+    std::lock_guard<std::mutex> lock( g_engine_mutex );
     Engine::get().search( req, queries, out, stats );
 }
 
 const HostDb & engine_database() {
+    std::lock_guard<std::mutex> lock( g_engine_mutex );
     return Engine::get().database();
 }
 
 void engine_invalidate_database() {
+    std::lock_guard<std::mutex> lock( g_engine_mutex );
     Engine::get().invalidate();
 }
 
 void engine_shutdown() {
+    std::lock_guard<std::mutex> lock( g_engine_mutex );
     Engine::get().shutdown();
+}
+
+std::vector<uint32_t> engine_serve_open( const SearchRequest & req, uint32_t slots, uint32_t segments ) {
+    std::lock_guard<std::mutex> lock( g_engine_mutex );
+    return Engine::get().serve_open( req, slots, segments );
+}
+
+void engine_serve_load( uint32_t slot, const uint8_t * codes, uint32_t len ) {
+    std::lock_guard<std::mutex> lock( g_engine_mutex );
+    Engine::get().serve_load( slot, codes, len );
+}
+
+void engine_serve_wave( const SearchRequest & req, const std::vector<uint32_t> & active, uint32_t seq_lo,
+        uint32_t seq_hi, std::vector<ServeOverflow> & ovf_entry, std::vector<ServeOverflow> & ovf16,
+        SearchStats & stats ) {
+    std::vector<PairTask> a, b;
+    {
+        std::lock_guard<std::mutex> lock( g_engine_mutex );
+        Engine::get().serve_wave( req, active, seq_lo, seq_hi, a, b, stats );
+    }
+    ovf_entry.clear();
+    ovf16.clear();
+    for( const PairTask & t : a )
+        ovf_entry.push_back( ServeOverflow{ t.qslot, t.id, t.nb_prev } );
+    for( const PairTask & t : b )
+        ovf16.push_back( ServeOverflow{ t.qslot, t.id, t.nb_prev } );
+}
+
+void engine_serve_finish( const SearchRequest & req, const std::vector<uint32_t> & done,
+        std::vector<ReplayQuery> & rq, std::vector<std::vector<Hit>> & out, SearchStats & stats ) {
+    std::lock_guard<std::mutex> lock( g_engine_mutex );
+    Engine::get().serve_finish( req, done, rq, out, stats );
 }
 
 uint64_t engine_kernel_launches() {

@@ -113,10 +113,30 @@ uint64_t engine_kernel_launches();
 
 // ---- host replay of the CPU lane schedule and min-heap (replay.cpp) ----------
 struct ReplayQuery {
-    const int32_t * score;                          // per ID, final score
+    const int32_t * score = nullptr;                // per ID, final score
     std::vector<std::pair<uint32_t, int32_t>> ovf_entry;   // (id, blocks) not reported by the entry pass
     std::vector<std::pair<uint32_t, int32_t>> ovf16;       // (id, blocks) not reported by the 16-bit pass
 };
+
+// ---- serving (engine.cu): resident query slots, waves over database segments --
+constexpr uint32_t SERVE_MAX_QUERY = 8192;   // residues of a served query
+
+struct ServeOverflow {
+    uint32_t slot, id;
+    int32_t nb;      // blocks the lane spent on the sequence in that pass
+};
+
+// Sets up `slots` resident query slots for requests of `req`'s kind; returns the
+// bounds of `segments` ranges of the length-sorted non-empty sequences.
+std::vector<uint32_t> engine_serve_open( const SearchRequest & req, uint32_t slots, uint32_t segments );
+void engine_serve_load( uint32_t slot, const uint8_t * codes, uint32_t len );
+// Entry pass and cascade of the `active` slots over sequences [seq_lo, seq_hi).
+void engine_serve_wave( const SearchRequest & req, const std::vector<uint32_t> & active, uint32_t seq_lo,
+        uint32_t seq_hi, std::vector<ServeOverflow> & ovf_entry, std::vector<ServeOverflow> & ovf16,
+        SearchStats & stats );
+// Replay, heap and traceback of finished slots; out is indexed by slot.
+void engine_serve_finish( const SearchRequest & req, const std::vector<uint32_t> & done,
+        std::vector<ReplayQuery> & rq, std::vector<std::vector<Hit>> & out, SearchStats & stats );
 
 // Chunk schedule ranks that do not depend on the query (entry pass without
 // overflow): rank[id] = report position of id inside its chunk.
