@@ -18,7 +18,11 @@ Metric: GCUPS = sum over queries of query length x database residues / time.
   ceiling of the same device (fused 16x2 add-max: an add and a max per 16-bit
   half), 9 integer operations per cell;
 * ``cpu_baseline``: the reference libssa (built from its sources into
-  oracle/_ref) on the host cores, on a sample of the same workload.
+  oracle/_ref) on the host cores, on a sample of the same workload;
+* ``served``: config 4, 64 requests arriving as a Poisson process (50/s) into
+  the request loop (``ssa_server_*``) over a resident 1,000,000-sequence
+  database: GCUPS over first arrival to last result, p50/p99 latency.
+  ``--workload sw_served`` prints that leg alone as its own line.
 
 With N > 1 (torchrun) every rank searches its own seeded 1,024-query batch
 against the full database (weak scaling, no collective on the data path);
