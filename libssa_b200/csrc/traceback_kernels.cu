@@ -79,6 +79,34 @@ struct BoundaryPrefetch {
     __device__ int4 get( uint32_t s ) const { return tile[s & 31u]; }
 };
 
+// At step s lane k works on stream position s - k, so the warp needs the
+// database residues of positions s - 31 .. s.  They are staged in a 64-entry
+// ring in shared memory, each 32 positions loaded (one per lane) 32 steps
+// before use, so no step waits on a global load.  Position x is database index
+// x, or b_end - x for the reverse pass.
+struct ResidueRing {
+    uint8_t * ring;      // 64 entries of this warp
+    uint8_t pf;          // this lane's residue for the next refill
+    const uint8_t * b;
+    int32_t n;           // positions 0 .. n - 1
+    int32_t rev_end;     // -1: forward, else b_end of the reverse pass
+    __device__ uint8_t fetch( int32_t x ) const {
+        if( x < 0 || x >= n )
+            return 0;
+        return b[rev_end < 0 ? x : rev_end - x];
+    }
+    __device__ void start( int lane ) { pf = fetch( lane ); }
+    __device__ void step( uint32_t s, int lane ) {
+        if( (s & 31u) == 0 ) {
+            __syncwarp();
+            ring[(s + (uint32_t) lane) & 63u] = pf;
+            __syncwarp();
+            pf = fetch( (int32_t) s + 32 + lane );
+        }
+    }
+    __device__ int get( uint32_t s, int lane ) const { return ring[(s - (uint32_t) lane) & 63u]; }
+};
+
 // Hits are handed out one per warp from a global counter, largest first (the
 // host sorts them), so that the longest alignments start first.
 __device__ __forceinline__ uint32_t next_hit( unsigned long long * counter, int lane ) {
@@ -97,12 +125,14 @@ __device__ __forceinline__ uint32_t next_hit( unsigned long long * counter, int 
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__( 256 ) tb_forward_kernel( TbParams p ) {
     __shared__ int4 tiles[8][32];
+    __shared__ uint8_t rings[8][64];
     __shared__ int32_t smat[1024];
     stage_matrix( p.matrix, smat, true );
     const int lane = threadIdx.x & 31;
     const uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     int4 * scratch = p.scratch + (uint64_t) w * p.scratch_cols;
     const int gO = p.gap_open, gE = p.gap_extend;
+    const int gOE = gO + gE;
     for( uint32_t h = next_hit( p.hit_counters + 0, lane ); h < p.n_hits; h = next_hit( p.hit_counters + 0, lane ) ) {
         const TbHit hit = p.hits[h];
         if( hit.algo != 0 )
@@ -131,10 +161,14 @@ __global__ void __launch_bounds__( 256 ) tb_forward_kernel( TbParams p ) {
             }
             int32_t diag = 0;
             int32_t out_h = 0, out_f = 0;
+            int32_t pv = 0, pi = INT_MAX, pj = INT_MAX;     // this pass's first maximum
             BoundaryPrefetch bp{ tiles[threadIdx.x >> 5] };
             bp.start( scratch, p.scratch_cols, B, pass > 0, lane );
+            ResidueRing rr{ rings[threadIdx.x >> 5], 0, b, (int32_t) B, -1 };
+            rr.start( lane );
             for( uint32_t s = 0; s < B + 31; s++ ) {
                 bp.step( scratch, p.scratch_cols, B, pass > 0, s, lane );
+                rr.step( s, lane );
                 int32_t up_h = __shfl_up_sync( 0xffffffffu, out_h, 1 );
                 int32_t up_f = __shfl_up_sync( 0xffffffffu, out_f, 1 );
                 const int32_t c = (int32_t) s - lane;
@@ -152,32 +186,35 @@ __global__ void __launch_bounds__( 256 ) tb_forward_kernel( TbParams p ) {
                     }
                 }
                 int32_t f = up_f, hd = diag;
-                const int d = b[c];
+                const int d = rr.get( s, lane );
+                // branch-free rows: the row-to-row chain is a 3-way max, an
+                // add and a fused add-max; a lane visits its cells in (column,
+                // row) order, so within a pass the first maximum wins with a
+                // strict compare
+                int32_t e_last[TB_R];
 #pragma unroll
                 for( int r = 0; r < TB_R; r++ ) {
-                    if( r < nvalid ) {
-                        int32_t e_in = E[r];
-                        int32_t x = hd + mget( smat, d, qa[r] );
-                        if( x < 0 )
-                            x = 0;
-                        if( f > x )
-                            x = f;
-                        if( e_in > x )
-                            x = e_in;
-                        if( c == (int32_t) B - 1 ) {
-                            lh[row0 + r] = x;
-                            le[row0 + r] = e_in;
+                    const int32_t e_in = E[r];
+                    const int32_t t = max( hd + mget( smat, d, qa[r] ), 0 );
+                    const int32_t x = __vimax3_s32( t, f, e_in );
+                    const bool take = (r < nvalid) && x > pv;
+                    pv = take ? x : pv;
+                    pi = take ? c : pi;
+                    pj = take ? row0 + r : pj;
+                    e_last[r] = e_in;
+                    hd = H[r];
+                    H[r] = x;
+                    const int32_t y = x + gOE;
+                    f = __viaddmax_s32( f, gE, y );
+                    E[r] = __viaddmax_s32( e_in, gE, y );
+                }
+                if( c == (int32_t) B - 1 ) {
+#pragma unroll
+                    for( int r = 0; r < TB_R; r++ )
+                        if( r < nvalid ) {
+                            lh[row0 + r] = H[r];
+                            le[row0 + r] = e_last[r];
                         }
-                        if( x > best_v || (x == best_v && x > 0 && (c < best_i || (c == best_i && row0 + r < best_j))) ) {
-                            best_v = x;
-                            best_i = c;
-                            best_j = row0 + r;
-                        }
-                        hd = H[r];
-                        H[r] = x;
-                        f = max( f, x + gO ) + gE;
-                        E[r] = max( e_in, x + gO ) + gE;
-                    }
                 }
                 diag = up_h;
                 out_h = H[TB_R - 1];
@@ -188,6 +225,13 @@ __global__ void __launch_bounds__( 256 ) tb_forward_kernel( TbParams p ) {
                     else
                         atomicOr( p.error_flags, ERR_SCRATCH_OVERFLOW );
                 }
+            }
+            // this pass's first maximum against the earlier passes' (value desc,
+            // database index asc, query index asc)
+            if( pv > best_v || (pv == best_v && pv > 0 && (pi < best_i || (pi == best_i && pj < best_j))) ) {
+                best_v = pv;
+                best_i = pi;
+                best_j = pj;
             }
             __syncwarp();
         }
@@ -226,12 +270,14 @@ __global__ void __launch_bounds__( 256 ) tb_forward_kernel( TbParams p ) {
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__( 256 ) tb_reverse_kernel( TbParams p ) {
     __shared__ int4 tiles[8][32];
+    __shared__ uint8_t rings[8][64];
     __shared__ int32_t smat[1024];
     stage_matrix( p.matrix, smat, true );
     const int lane = threadIdx.x & 31;
     const uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     int4 * scratch = p.scratch + (uint64_t) w * p.scratch_cols;
     const int gO = p.gap_open, gE = p.gap_extend;
+    const int gOE = gO + gE;
     for( uint32_t h = next_hit( p.hit_counters + 1, lane ); h < p.n_hits; h = next_hit( p.hit_counters + 1, lane ) ) {
         const TbHit hit = p.hits[h];
         if( hit.algo != 0 )
@@ -283,12 +329,15 @@ __global__ void __launch_bounds__( 256 ) tb_reverse_kernel( TbParams p ) {
             int32_t limit = __reduce_min_sync( 0xffffffffu, hit_i );
             BoundaryPrefetch bp{ tiles[threadIdx.x >> 5] };
             bp.start( scratch, p.scratch_cols, B, pass > 0, lane );
+            ResidueRing rr{ rings[threadIdx.x >> 5], 0, b, (int32_t) B, b_end };
+            rr.start( lane );
             for( uint32_t s = 0; s < B + 31; s++ ) {
                 if( (s & 7) == 0 )
                     limit = __reduce_min_sync( 0xffffffffu, hit_i );
                 if( limit != INT_MAX && (int64_t) s > (int64_t) limit + 31 )
                     break;
                 bp.step( scratch, p.scratch_cols, B, pass > 0, s, lane );
+                rr.step( s, lane );
                 int32_t up_h = __shfl_up_sync( 0xffffffffu, out_h, 1 );
                 int32_t up_f = __shfl_up_sync( 0xffffffffu, out_f, 1 );
                 const int32_t c = (int32_t) s - lane;
@@ -305,27 +354,21 @@ __global__ void __launch_bounds__( 256 ) tb_reverse_kernel( TbParams p ) {
                         up_f = v.y;
                     }
                 }
-                const int32_t i = b_end - c;              // database index
-                const int d = b[i];
+                const int d = rr.get( s, lane );          // database index b_end - c
                 int32_t f = up_f, hd = diag;              // lane 0 / pass 0: 0 at c == 0, then -1
 #pragma unroll
                 for( int r = 0; r < TB_R; r++ ) {
-                    if( r < nvalid ) {
-                        int32_t e_in = E[r];
-                        int32_t x = hd + mget( smat, d, qa[r] );
-                        if( f > x )
-                            x = f;
-                        if( e_in > x )
-                            x = e_in;
-                        if( x >= score && (c < hit_i || (c == hit_i && row0 + r < hit_j)) ) {
-                            hit_i = c;
-                            hit_j = row0 + r;
-                        }
-                        hd = H[r];
-                        H[r] = x;
-                        f = max( f, x + gO ) + gE;
-                        E[r] = max( e_in, x + gO ) + gE;
-                    }
+                    const int32_t e_in = E[r];
+                    const int32_t x = __vimax3_s32( hd + mget( smat, d, qa[r] ), f, e_in );
+                    const bool take = (r < nvalid) && x >= score &&
+                            (c < hit_i || (c == hit_i && row0 + r < hit_j));
+                    hit_i = take ? c : hit_i;
+                    hit_j = take ? row0 + r : hit_j;
+                    hd = H[r];
+                    H[r] = x;
+                    const int32_t y = x + gOE;
+                    f = __viaddmax_s32( f, gE, y );
+                    E[r] = __viaddmax_s32( e_in, gE, y );
                 }
                 diag = up_h;
                 out_h = H[TB_R - 1];
@@ -370,12 +413,14 @@ __global__ void __launch_bounds__( 256 ) tb_reverse_kernel( TbParams p ) {
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__( 256 ) tb_directions_kernel( TbParams p ) {
     __shared__ int4 tiles[8][32];
+    __shared__ uint8_t rings[8][64];
     __shared__ int32_t smat[1024];
     stage_matrix( p.matrix, smat, false );
     const int lane = threadIdx.x & 31;
     const uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     int4 * scratch = p.scratch + (uint64_t) w * p.scratch_cols;
     const int gO = p.gap_open, gE = p.gap_extend;
+    const int gOE = gO + gE;
     for( uint32_t h = next_hit( p.hit_counters + 2, lane ); h < p.n_hits; h = next_hit( p.hit_counters + 2, lane ) ) {
         const TbHit hit = p.hits[h];
         const TbRegion rg = p.regions[h];
@@ -406,8 +451,11 @@ __global__ void __launch_bounds__( 256 ) tb_directions_kernel( TbParams p ) {
             int32_t out_h = 0, out_f = 0;
             BoundaryPrefetch bp{ tiles[threadIdx.x >> 5] };
             bp.start( scratch, p.scratch_cols, B, pass > 0, lane );
+            ResidueRing rr{ rings[threadIdx.x >> 5], 0, b, (int32_t) B, -1 };
+            rr.start( lane );
             for( uint32_t s = 0; s < B + 31; s++ ) {
                 bp.step( scratch, p.scratch_cols, B, pass > 0, s, lane );
+                rr.step( s, lane );
                 int32_t up_h = __shfl_up_sync( 0xffffffffu, out_h, 1 );
                 int32_t up_f = __shfl_up_sync( 0xffffffffu, out_f, 1 );
                 const int32_t j = (int32_t) s - lane;     // database index
@@ -425,42 +473,27 @@ __global__ void __launch_bounds__( 256 ) tb_directions_kernel( TbParams p ) {
                         up_f = v.y;
                     }
                 }
-                const int d = b[j];
+                const int d = rr.get( s, lane );
                 int32_t f = up_f, hd = diag;
                 uint32_t code = 0;
+                // flags as in the reference (strict compares in its order),
+                // computed beside a branch-free row-to-row chain
 #pragma unroll
                 for( int r = 0; r < TB_R; r++ ) {
-                    if( r < nvalid ) {
-                        int32_t e = E[r];
-                        int32_t x = hd + mget( smat, d, qa[r] );
-                        unsigned flags = 0;
-                        if( f > x ) {
-                            flags |= 1u;     // UP
-                            x = f;
-                        }
-                        if( e > x ) {
-                            x = e;
-                            flags |= 2u;     // LEFT
-                        }
-                        if( !nw && x < 0 )
-                            x = 0;
-                        hd = H[r];
-                        H[r] = x;
-                        int32_t y = x + gO + gE;
-                        e += gE;
-                        f += gE;
-                        if( f > y )
-                            flags |= 4u;     // EXT_UP
-                        else
-                            f = y;
-                        if( e > y )
-                            flags |= 8u;     // EXT_LEFT
-                        else
-                            e = y;
-                        E[r] = e;
-                        const uint32_t op = (flags & 10u) ? 2u : ((flags & 5u) ? 1u : 0u);
-                        code |= op << (2 * r);
-                    }
+                    const int32_t e = E[r];
+                    const int32_t x0 = hd + mget( smat, d, qa[r] );
+                    const bool up = f > x0;                      // UP
+                    const bool left = e > max( x0, f );          // LEFT
+                    const int32_t x = __vimax3_s32( nw ? x0 : max( x0, 0 ), f, e );
+                    hd = H[r];
+                    H[r] = x;
+                    const int32_t y = x + gOE;
+                    const bool ext_up = f + gE > y;              // EXT_UP
+                    const bool ext_left = e + gE > y;            // EXT_LEFT
+                    f = __viaddmax_s32( f, gE, y );
+                    E[r] = __viaddmax_s32( e, gE, y );
+                    const uint32_t op = (left || ext_left) ? 2u : ((up || ext_up) ? 1u : 0u);
+                    code |= (r < nvalid) ? op << (2 * r) : 0u;
                 }
                 diag = up_h;
                 out_h = H[TB_R - 1];
