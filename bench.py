@@ -425,6 +425,48 @@ def served_leg(args, L) -> dict:
             "timing": "wall time from the first arrival to the last completion; latency = submit to result"}
 
 
+def run_nw_arm(args):
+    """Config 2: 64 nucleotide queries vs 200,000 sequences, Needleman-Wunsch,
+    16-bit entry, constant scores 2/-3, gaps 5/2, top 20 with CIGAR; one step is
+    one batched search (ssa_align_batch)."""
+    import libssa_b200 as L
+    from libssa_b200 import workloads as W
+    L.load()
+    w = W.nw_nucleotide(seed=2, scale=args.scale, n_queries=64)
+    L.set_output_mode(L.OUTPUT_SILENT)
+    L.init_symbol_translation(L.NUCLEOTIDE, L.FORWARD_STRAND, 1, 1)
+    L.init_constant_scores(2, -3)
+    L.init_gap_penalties(-5, -2)
+    L.set_chunk_size(1000)
+    L.set_simd_compute_mode(L.COMPUTE_ON_AVX2)
+    L.load_db_memory(flat=w.db_flat, offsets=w.db_offsets)
+    qs = [L.init_sequence_fasta(L.READ_FROM_STRING, q.decode()) for q in w.queries]
+    cells = sum(len(q) for q in w.queries) * int(w.db_offsets[-1])
+    for _ in range(args.warmup):
+        L.align_batch(L.SSA_NEEDLEMAN_WUNSCH, qs, 20, L.BIT_WIDTH_16, L.COMPUTE_ALIGNMENT)
+    dev, wall = 0.0, 0.0
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        L.align_batch(L.SSA_NEEDLEMAN_WUNSCH, qs, 20, L.BIT_WIDTH_16, L.COMPUTE_ALIGNMENT)
+        wall += time.perf_counter() - t0
+        dev += L.stats().kernel_seconds
+    st = L.stats()
+    line = {"metric": "GCUPS (batched NW nucleotide search, 64 queries vs 200k sequences, top 20 with CIGAR)",
+            "value": round(cells * args.steps / dev / 1e9, 2), "unit": "GCUPS", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "int16 lanes (16-bit entry), int32", "data": "synthetic (seeded, BASELINE config 2 shapes)",
+            "config": {"workload": "nw_nucleotide", "queries": len(qs), "db_sequences": w.n_db,
+                       "db_residues": int(w.db_offsets[-1]), "cells_per_step": cells, "scale": args.scale},
+            "e2e": {"value": round(cells * args.steps / wall / 1e9, 2), "unit": "GCUPS"},
+            "timing": {"device_seconds": round(dev, 4), "wall_seconds": round(wall, 4),
+                       "entry_seconds_last": round(st.entry_seconds, 4),
+                       "overflow_16_to_64_last": int(st.overflow_16_to_64)}}
+    print(json.dumps(line), flush=True)
+    for q in qs:
+        L.free_sequence(q)
+    return 0
+
+
 def run_served_arm(args):
     import libssa_b200 as L
     L.load()
@@ -455,7 +497,7 @@ def main():
     ap.add_argument("--served-slots", type=int, default=64, help="resident query slots of the server")
     ap.add_argument("--served-segments", type=int, default=8, help="database segments per scan turn")
     ap.add_argument("--served-scale", type=float, default=1.0, help="served database scale (1.0 = 1M sequences)")
-    ap.add_argument("--workload", default="sw_batched", choices=["sw_batched", "sw_plain", "sw_served"],
+    ap.add_argument("--workload", default="sw_batched", choices=["sw_batched", "sw_plain", "sw_served", "nw_nucleotide"],
                     help="sw_plain: config 1's 10,000-sequence database with --queries queries of 375")
     ap.add_argument("--queries", type=int, default=None, help="query count for --workload sw_plain")
     args = ap.parse_args()
@@ -463,6 +505,8 @@ def main():
         sys.exit(run_reference_arm(args))
     if args.workload == "sw_served":
         sys.exit(run_served_arm(args))
+    if args.workload == "nw_nucleotide":
+        sys.exit(run_nw_arm(args))
     sys.exit(run_ours(args))
 
 

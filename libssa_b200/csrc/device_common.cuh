@@ -183,11 +183,21 @@ struct QPairParams {
     PassSink sink;
     int4 * scratch;               // per warp and group: scratch_cols column pairs (H, F of two columns)
     uint32_t scratch_cols;
+    // Needleman-Wunsch only (nw_qpair_kernel)
+    int gap_open;
+    const uint32_t * qlen;        // per slot
+    const uint32_t * qp_lmax;     // per query pair: longest sequence the kernel scores exactly
+    PairTask * redo;              // longer sequences: (slot, id) for the lane emulation
+    unsigned int * redo_count;
+    uint32_t redo_cap;
 };
 
 cudaError_t launch_sw_qpair( int R, const QPairParams & p, int grid, cudaStream_t st, int * blocks_per_sm );
+cudaError_t launch_nw_qpair( int R, const QPairParams & p, int grid, cudaStream_t st, int * blocks_per_sm );
+// width 8: (int8) scores, -128 past a query (Smith-Waterman 8-bit entry);
+// width 16: (int16) scores, 0 past a query (Needleman-Wunsch 16-bit entry)
 cudaError_t launch_build_profile_qp( const uint8_t * qcodes, const uint64_t * qoff, const uint32_t * qlen,
         const uint32_t * qp_slots, uint32_t n_qp, const uint32_t * qp_rows, const int64_t * matrix, uint32_t * prof,
-        const uint64_t * prof_off, cudaStream_t st );
+        const uint64_t * prof_off, int width, cudaStream_t st );
 
 }  // namespace ssa

@@ -294,7 +294,7 @@ public:
             &d_prof_off_, &d_prof_, &d_matrix_, &d_score_, &d_list_a_, &d_list_b_, &d_counts_, &d_scratch_,
             &d_tb_hits_, &d_tb_regions_, &d_tb_last_, &d_tb_last_off_, &d_tb_dirs_, &d_tb_dir_off_, &d_tb_ops_,
             &d_tb_ops_off_, &d_tb_ops_len_, &d_qp_prof_, &d_qp_off_, &d_qp_rows_, &d_qp_slots_, &d_qp_units_,
-            &d_serve_score_ };
+            &d_serve_score_, &d_qp_lmax_ };
         for( DevBuf * b : bufs )
             b->release();
         h_score_.release();
@@ -349,7 +349,7 @@ private:
     DevBuf d_prof8_, d_prof8_off_, d_rows_, d_slots_;
     DevBuf d_scratch_fast_[4];
     DevBuf d_bounds_, d_group_;
-    DevBuf d_qp_prof_, d_qp_off_, d_qp_rows_, d_qp_slots_, d_qp_units_;
+    DevBuf d_qp_prof_, d_qp_off_, d_qp_rows_, d_qp_slots_, d_qp_units_, d_qp_lmax_;
     // serving: fixed query slots and their own score rows
     DevBuf d_serve_score_;
     bool serving_ = false;           // passes write d_serve_score_
@@ -437,6 +437,15 @@ void Engine::run_pass( int algo, int width, const SearchRequest & req, uint32_t 
 // The 16x2 pass reproduces the 8-bit Smith-Waterman lanes exactly when the
 // gap extension is not positive and the truncated 8-bit open+extend cost lies
 // in [-128, gapE]; other parameters run the exact lane emulation.
+// Needleman-Wunsch at the 16-bit entry: the query-pair kernel scores exactly
+// the sequences short enough that no value can come near the int16 limits
+// (nw_qpair_kernel); it needs non-positive gap costs.
+static bool nw_fast_eligible( const SearchRequest & req ) {
+    if( req.algo != 1 || req.bit_width != 16 || getenv( "SSA_B200_NO_FAST" ) )
+        return false;
+    return req.gap_open <= 0 && req.gap_extend <= 0;
+}
+
 static bool fast_eligible( const SearchRequest & req ) {
     if( req.algo != 0 || req.bit_width != 8 )
         return false;
@@ -664,6 +673,7 @@ void Engine::run_qpair_entry( const SearchRequest & req, uint32_t nq, PairTask *
     const uint32_t n_seq = hi - lo;
     if( n_seq == 0 )
         return;
+    const bool nw = req.algo == 1;
     // pair the queries that fit, longest first; longer ones run the emulation
     std::vector<uint32_t> fit, fallback;
     if( slots ) {
@@ -693,6 +703,21 @@ void Engine::run_qpair_entry( const SearchRequest & req, uint32_t nq, PairTask *
         qp_rows[i] = P * (uint32_t) (QP_G * R);
         by_r[R / 4 - 4].push_back( i );
     }
+    // NW: per pair, the longest sequence whose matrix (padded rows and the last
+    // block's pad columns included) stays within +-30000: every step of a path
+    // changes a value by at most m, and a path has at most rows + L + 4 steps
+    // and two gap openings
+    std::vector<uint32_t> qp_lmax( std::max<uint32_t>( 1, n_qp ), 0 );
+    if( nw ) {
+        int64_t m = std::max<int64_t>( 1, std::llabs( (int64_t) req.gap_extend ) );
+        for( int c = 0; c < 1024; c++ )
+            m = std::max<int64_t>( m, std::llabs( (int64_t) (int16_t) req.matrix[c] ) );
+        const int64_t budget = 30000 - 2 * std::llabs( (int64_t) req.gap_open );
+        for( uint32_t i = 0; i < n_qp; i++ ) {
+            const int64_t l = budget / m - (int64_t) qp_rows[i] - 4;
+            qp_lmax[i] = (uint32_t) std::max<int64_t>( 0, l );
+        }
+    }
     // profiles: QP_CODES x rows words per pair (16-byte aligned: rows % 16 == 0)
     for( int ri = 0; ri < 4; ri++ )
         for( uint32_t i : by_r[ri] ) {
@@ -709,6 +734,12 @@ void Engine::run_qpair_entry( const SearchRequest & req, uint32_t nq, PairTask *
     d_qp_rows_.ensure( qp_rows.size() * sizeof(uint32_t) );
     d_qp_slots_.ensure( qp_slots.size() * sizeof(uint32_t) );
     d_qp_units_.ensure( std::max<size_t>( 1, units.size() ) * sizeof(uint32_t) );
+    d_qp_lmax_.ensure( qp_lmax.size() * sizeof(uint32_t) );
+    CUDA_CHECK( cudaMemcpyAsync( d_qp_lmax_.p, qp_lmax.data(), qp_lmax.size() * sizeof(uint32_t),
+            cudaMemcpyHostToDevice, stream_ ) );
+    unsigned * redo_count = d_counts_.as<unsigned>() + 5;
+    if( nw )
+        CUDA_CHECK( cudaMemsetAsync( redo_count, 0, sizeof(unsigned), stream_ ) );
     CUDA_CHECK( cudaMemcpyAsync( d_qp_off_.p, qp_off.data(), qp_off.size() * sizeof(uint64_t), cudaMemcpyHostToDevice,
             stream_ ) );
     CUDA_CHECK( cudaMemcpyAsync( d_qp_rows_.p, qp_rows.data(), qp_rows.size() * sizeof(uint32_t),
@@ -721,7 +752,7 @@ void Engine::run_qpair_entry( const SearchRequest & req, uint32_t nq, PairTask *
     if( n_qp ) {
         CUDA_CHECK( launch_build_profile_qp( d_qcodes_.as<uint8_t>(), d_qoff_.as<uint64_t>(), d_qlen_.as<uint32_t>(),
                 d_qp_slots_.as<uint32_t>(), n_qp, d_qp_rows_.as<uint32_t>(), d_matrix_.as<int64_t>(),
-                d_qp_prof_.as<uint32_t>(), d_qp_off_.as<uint64_t>(), stream_ ) );
+                d_qp_prof_.as<uint32_t>(), d_qp_off_.as<uint64_t>(), nw ? 16 : 8, stream_ ) );
         launches_++;
     }
 
@@ -767,7 +798,8 @@ void Engine::run_qpair_entry( const SearchRequest & req, uint32_t nq, PairTask *
             multi |= qp_rows[i] > (uint32_t) (QP_G * R);
         QPairParams p{};
         int per_sm = 0;
-        CUDA_CHECK( launch_sw_qpair( R, p, 0, class_stream_[ri], &per_sm ) );
+        CUDA_CHECK( nw ? launch_nw_qpair( R, p, 0, class_stream_[ri], &per_sm )
+                       : launch_sw_qpair( R, p, 0, class_stream_[ri], &per_sm ) );
         const int grid = sms_ * std::max( 1, per_sm );
         CUDA_CHECK( cudaStreamWaitEvent( class_stream_[ri], ev_ready_, 0 ) );
         unsigned long long * unit_counter = d_counts_.as<unsigned long long>() + 8 + ri;   // bytes 64..95
@@ -784,7 +816,8 @@ void Engine::run_qpair_entry( const SearchRequest & req, uint32_t nq, PairTask *
         p.chunk_bounds = d_bounds_.as<uint32_t>();
         p.n_units = (uint64_t) n_chunks * cls.size();
         p.unit_counter = unit_counter;
-        p.gap_oe = (int8_t) (req.gap_open + req.gap_extend);
+        // the 8-bit Smith-Waterman lanes add the int8 truncation of gapO + gapE
+        p.gap_oe = nw ? req.gap_open + req.gap_extend : (int8_t) (req.gap_open + req.gap_extend);
         p.gap_e = req.gap_extend;
         p.sink.score = score_sink();
         p.sink.score_stride = db_.n_ids;
@@ -797,9 +830,16 @@ void Engine::run_qpair_entry( const SearchRequest & req, uint32_t nq, PairTask *
                     scratch_cols * sizeof(int4) );
             p.scratch_cols = scratch_cols;
         }
+        p.gap_open = req.gap_open;
+        p.qlen = d_qlen_.as<uint32_t>();
+        p.qp_lmax = d_qp_lmax_.as<uint32_t>();
+        p.redo = d_list_b_.as<PairTask>();
+        p.redo_count = redo_count;
+        p.redo_cap = cap;
         if( timing )
             CUDA_CHECK( cudaEventRecord( ev_cls_t_[2 * ri], class_stream_[ri] ) );
-        CUDA_CHECK( launch_sw_qpair( R, p, grid, class_stream_[ri], nullptr ) );
+        CUDA_CHECK( nw ? launch_nw_qpair( R, p, grid, class_stream_[ri], nullptr )
+                       : launch_sw_qpair( R, p, grid, class_stream_[ri], nullptr ) );
         launches_++;
         if( timing )
             CUDA_CHECK( cudaEventRecord( ev_cls_t_[2 * ri + 1], class_stream_[ri] ) );
@@ -825,12 +865,21 @@ void Engine::run_qpair_entry( const SearchRequest & req, uint32_t nq, PairTask *
                     cells / (ms * 1e-3) / 1e9 );
         }
     }
+    if( nw ) {
+        // sequences beyond a pair's exact range: the 16-bit lane emulation
+        unsigned n_redo = 0;
+        CUDA_CHECK( cudaMemcpyAsync( &n_redo, redo_count, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_ ) );
+        CUDA_CHECK( cudaStreamSynchronize( stream_ ) );
+        n_redo = std::min( n_redo, cap );
+        if( n_redo )
+            run_pass( 1, 16, req, nq, d_list_b_.as<PairTask>(), n_redo, false, next, next_count, cap );
+    }
     if( !fallback.empty() ) {
         d_slots_.ensure( fallback.size() * sizeof(uint32_t) );
         CUDA_CHECK( cudaMemcpyAsync( d_slots_.p, fallback.data(), fallback.size() * sizeof(uint32_t),
                 cudaMemcpyHostToDevice, stream_ ) );
-        run_pass( 0, 8, req, nq, nullptr, (uint64_t) fallback.size() * n_seq, true, next, next_count, cap,
-                d_slots_.as<uint32_t>(), (uint32_t) fallback.size(), lo );
+        run_pass( req.algo, req.bit_width, req, nq, nullptr, (uint64_t) fallback.size() * n_seq, true, next,
+                next_count, cap, d_slots_.as<uint32_t>(), (uint32_t) fallback.size(), lo );
     }
 }
 
@@ -911,7 +960,7 @@ void Engine::search( const SearchRequest & req, const std::vector<QueryCodes> & 
         const int entry = req.bit_width;
         std::vector<PairTask> list_entry, list_16;   // host copies for the replay
         unsigned n_a = 0, n_b = 0;
-        if( fast_eligible( req ) && nq >= 2 && !getenv( "SSA_B200_NO_QPAIR" ) )
+        if( (fast_eligible( req ) && nq >= 2 && !getenv( "SSA_B200_NO_QPAIR" )) || nw_fast_eligible( req ) )
             run_qpair_entry( req, nq, d_list_a_.as<PairTask>(), cnt + 0, cap );
         else if( fast_eligible( req ) )
             run_fast_entry( req, nq, d_list_a_.as<PairTask>(), cnt + 0, cap );
@@ -1303,7 +1352,7 @@ void Engine::serve_wave( const SearchRequest & req, const std::vector<uint32_t> 
     unsigned * cnt = d_counts_.as<unsigned>();
     const int entry = req.bit_width;
     CUDA_CHECK( cudaEventRecord( ev_phase_[0], stream_ ) );
-    if( fast_eligible( req ) ) {
+    if( fast_eligible( req ) || nw_fast_eligible( req ) ) {
         run_qpair_entry( req, serve_slots_, d_list_a_.as<PairTask>(), cnt + 0, cap, &active, seq_lo, seq_hi );
     }
     else {

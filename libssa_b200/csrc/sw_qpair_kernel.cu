@@ -288,11 +288,302 @@ cudaError_t launch_sw_qpair( int R, const QPairParams & p, int grid, cudaStream_
     }
 }
 
-// prof[qp][code][row] = (A's 8-bit score, B's 8-bit score) as a 16x2 word;
-// rows past a query, and the absent query of an odd batch, score -128.
+// ---------------------------------------------------------------------------
+// Needleman-Wunsch, 16-bit entry (reference: src/algo/simd/search_simd_nw.c:
+// 180-516, boundaries :233-240, :445-453; the score is H of the last query
+// row at the sequence's last column).  The reference lane computes saturating
+// int16 values and re-queues the sequence when a block's minimum comes near
+// -32768 or its maximum reaches 32767.  The host passes, per query pair, the
+// longest sequence for which every value of the matrix (padded rows and the
+// last block's pad columns included) provably stays within +-30000: for those
+// the lane never saturates and never re-queues, so exact arithmetic gives its
+// score.  Longer sequences go to a list that the lane emulation runs.
+//
+// Values carry a +32768 bias per half and use unsigned 16x2 arithmetic, so
+// adding the 32-bit constant gapO + gapE to a word carries exactly once out of
+// the low half.  Same wavefront, two interleaved columns per step and profile
+// slices as sw_qpair_kernel; there is no zero floor and no running maximum.
+// ---------------------------------------------------------------------------
+constexpr uint32_t NWQ_BIAS = 32768u;
+
+__device__ __forceinline__ uint32_t nw_pack( int32_t v ) {
+    const uint32_t u = (uint32_t) (v + (int32_t) NWQ_BIAS) & 0xffffu;
+    return u | (u << 16);
+}
+
+// one step's rows: column c (cell A, row r) interleaved with column c + 1
+// (cell B, row r - 1); CAPTURE records H at the queries' last rows when one
+// of the two columns is the sequence's last
+template <int R, bool CAPTURE>
+__device__ __forceinline__ void nw_rows( uint32_t (&H)[R], uint32_t (&E)[R], const uint32_t * pa,
+        const uint32_t * pb, uint32_t diag, uint32_t up_h0, uint32_t & fa, uint32_t & fb, uint32_t GOE32,
+        uint32_t GE2, int32_t row0, bool last_a, bool last_b, int32_t qa_last, int32_t qb_last, uint32_t & cap_a,
+        uint32_t & cap_b, uint32_t & out_h0 ) {
+    uint4 xa = make_uint4( 0, 0, 0, 0 ), xb = xa;
+    uint32_t hc_prev = 0, hc_prev2 = 0;
+#pragma unroll
+    for( int r = 0; r <= R; r++ ) {
+        uint32_t ha = 0;
+        if( r < R ) {
+            if( (r & 3) == 0 )
+                xa = *reinterpret_cast<const uint4 *>( pa + r );
+            const uint32_t v = (r & 3) == 0 ? xa.x : (r & 3) == 1 ? xa.y : (r & 3) == 2 ? xa.z : xa.w;
+            const uint32_t hd = (r == 0) ? diag : H[r - 1];
+            ha = __viaddmax_u16x2( hd, v, __vmaxu2( E[r], fa ) );
+            const uint32_t hg = ha + GOE32;
+            fa = __viaddmax_u16x2( fa, GE2, hg );
+            E[r] = __viaddmax_u16x2( E[r], GE2, hg );
+            if constexpr( CAPTURE ) {
+                if( last_a && row0 + r == qa_last )
+                    cap_a = ha;
+                if( last_a && row0 + r == qb_last )
+                    cap_b = ha;
+            }
+        }
+        if( r >= 1 ) {
+            const int rb = r - 1;
+            if( (rb & 3) == 0 )
+                xb = *reinterpret_cast<const uint4 *>( pb + rb );
+            const uint32_t v = (rb & 3) == 0 ? xb.x : (rb & 3) == 1 ? xb.y : (rb & 3) == 2 ? xb.z : xb.w;
+            const uint32_t hd = (rb == 0) ? up_h0 : hc_prev2;
+            const uint32_t hb = __viaddmax_u16x2( hd, v, __vmaxu2( E[rb], fb ) );
+            const uint32_t hg = hb + GOE32;
+            fb = __viaddmax_u16x2( fb, GE2, hg );
+            E[rb] = __viaddmax_u16x2( E[rb], GE2, hg );
+            H[rb] = hb;
+            if constexpr( CAPTURE ) {
+                if( last_b && row0 + rb == qa_last )
+                    cap_a = hb;
+                if( last_b && row0 + rb == qb_last )
+                    cap_b = hb;
+            }
+        }
+        hc_prev2 = hc_prev;
+        hc_prev = ha;
+    }
+    out_h0 = hc_prev2;
+}
+
+template <int R>
+__global__ void __launch_bounds__( QP_THREADS, 4 ) nw_qpair_kernel( QPairParams p ) {
+    constexpr int G = QP_G;
+    constexpr uint32_t GR = (uint32_t) (G * R);
+    extern __shared__ __align__( 16 ) uint32_t qsm[];
+    const int lane = threadIdx.x & 31;
+    const uint32_t warp_in_cta = threadIdx.x >> 5;
+    const uint32_t warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    uint32_t * slice = qsm + warp_in_cta * (QP_CODES * GR);
+    const int k = lane & (G - 1);
+    const int g = lane / G;
+    const int gO = p.gap_open, gE = p.gap_e;
+    const uint32_t GOE32 = (uint32_t) ((int32_t) p.gap_oe * 65536 + (int32_t) p.gap_oe);
+    const uint32_t GE2 = ((uint32_t) (uint16_t) (int16_t) gE << 16) | (uint16_t) (int16_t) gE;
+    int4 * scratch = p.scratch + ((uint64_t) warp_global * QP_GPW + (uint32_t) g) * p.scratch_cols;
+    uint64_t loaded_key = ~0ull;
+    // exact NW boundaries (no saturation within the guarded range)
+    auto left_h = [&]( int32_t i ) { return gO + (i + 1) * gE; };           // H(i, -1)
+    auto left_e = [&]( int32_t i ) { return 2 * gO + (i + 2) * gE; };       // E entering column 0
+    auto top_h = [&]( int32_t j ) { return j < 0 ? 0 : gO + (j + 1) * gE; };   // H(-1, j)
+    auto top_f = [&]( int32_t c ) { return 2 * gO + (c + 2) * gE; };        // F entering row 0
+
+    for( ;; ) {
+        unsigned long long u = 0;
+        if( lane == 0 )
+            u = atomicAdd( p.unit_counter, 1ull );
+        u = __shfl_sync( 0xffffffffu, u, 0 );
+        if( u >= p.n_units )
+            break;
+        const uint32_t qp = p.unit_pairs[u / p.n_chunks];
+        const uint32_t chunk = (uint32_t) (u % p.n_chunks);
+        const uint32_t seq_begin = p.chunk_bounds[chunk], seq_end = p.chunk_bounds[chunk + 1];
+        const uint32_t rows = p.qp_rows[qp];
+        const uint32_t passes = rows / GR;
+        const uint32_t * prof = p.prof + p.prof_off[qp];
+        const uint32_t slot_a = p.qp_slots[2 * qp], slot_b = p.qp_slots[2 * qp + 1];
+        const int32_t qa_last = (int32_t) p.qlen[slot_a] - 1;
+        const int32_t qb_last = (slot_b == 0xffffffffu) ? -1 : (int32_t) p.qlen[slot_b] - 1;
+        const uint32_t lmax = p.qp_lmax[qp];
+
+        for( uint32_t b0 = seq_begin; b0 < seq_end; b0 += (uint32_t) QP_GPW ) {
+            const uint32_t idx = b0 + (uint32_t) g;
+            const bool valid = idx < seq_end;
+            const uint32_t id = valid ? p.order[idx] : 0u;
+            const uint32_t L = valid ? p.db.lens[id] : 0u;
+            const bool exact = valid && L <= lmax;
+            if( valid && !exact && k == 0 ) {
+                // beyond the guarded range: the lane emulation scores it
+                const uint32_t slots[2] = { slot_a, slot_b };
+                for( int h = 0; h < 2; h++ ) {
+                    if( slots[h] == 0xffffffffu )
+                        continue;
+                    const unsigned q = atomicAdd( p.redo_count, 1u );
+                    if( q < p.redo_cap )
+                        p.redo[q] = PairTask{ slots[h], id, 0, 0 };
+                    else
+                        atomicOr( p.sink.error_flags, ERR_REQUEUE_OVERFLOW );
+                }
+            }
+            const uint32_t ncp = exact ? (((L + 3u) & ~3u) >> 1) : 0u;
+            const uint32_t max_ncp = __reduce_max_sync( 0xffffffffu, ncp );
+            if( max_ncp == 0 )
+                continue;
+            const uint8_t * res = p.db.codes + (valid ? p.db.offsets[id] : 0ull);
+            const int32_t last_col = (int32_t) L - 1;
+            const int32_t cap_cp = last_col >> 1;
+            const bool last_is_a = (last_col & 1) == 0;
+            uint32_t cap_a = 0, cap_b = 0;
+
+            for( uint32_t pass = 0; pass < passes; pass++ ) {
+                const bool last_pass = (pass + 1 == passes);
+                const uint64_t key = ((uint64_t) qp << 24) | pass;
+                if( key != loaded_key ) {
+                    __syncwarp();
+                    constexpr uint32_t per_code = GR / 4u;
+                    const uint4 * src = reinterpret_cast<const uint4 *>( prof + (size_t) pass * GR );
+                    uint4 * dst = reinterpret_cast<uint4 *>( slice );
+                    for( uint32_t i = (uint32_t) lane; i < QP_CODES * per_code; i += 32u ) {
+                        const uint32_t code = i / per_code, w = i % per_code;
+                        dst[i] = src[(size_t) code * (rows / 4u) + w];
+                    }
+                    loaded_key = key;
+                    __syncwarp();
+                }
+                const int32_t row0 = (int32_t) (pass * GR) + k * R;
+                // does this thread hold a query's last row in this pass?
+                const bool holds_last = (qa_last >= row0 && qa_last < row0 + R) ||
+                        (qb_last >= row0 && qb_last < row0 + R);
+                uint32_t H[R], E[R];
+#pragma unroll
+                for( int r = 0; r < R; r++ ) {
+                    H[r] = nw_pack( left_h( row0 + r ) );
+                    E[r] = nw_pack( left_e( row0 + r ) );
+                }
+                uint32_t diag = nw_pack( row0 == 0 ? 0 : left_h( row0 - 1 ) );
+                uint32_t out_h0 = 0, out_f0 = 0, out_h1 = 0, out_f1 = 0;
+                const uint32_t fetch_limit = ncp + 3u;
+                auto fetch = [&]( int32_t cp ) -> uint32_t {
+                    const uint32_t c = min( (uint32_t) max( cp, 0 ), fetch_limit );
+                    return (uint32_t) *reinterpret_cast<const uint16_t *>( res + 2u * c );
+                };
+                uint32_t q0 = fetch( -k ), q1 = fetch( 1 - k ), q2 = fetch( 2 - k ), q3 = fetch( 3 - k );
+                const bool reads_boundary = (k == 0) && pass > 0;
+                int4 bq0 = make_int4( 0, 0, 0, 0 ), bq1 = bq0;
+                if( reads_boundary ) {
+                    if( ncp > 0 )
+                        bq0 = scratch[0];
+                    if( ncp > 1 )
+                        bq1 = scratch[1];
+                }
+                const uint32_t steps = max_ncp + (uint32_t) G - 1u;
+                for( uint32_t s = 0; s < steps; s++ ) {
+                    uint32_t up_h0 = __shfl_up_sync( 0xffffffffu, out_h0, 1, G );
+                    uint32_t up_f0 = __shfl_up_sync( 0xffffffffu, out_f0, 1, G );
+                    uint32_t up_h1 = __shfl_up_sync( 0xffffffffu, out_h1, 1, G );
+                    uint32_t up_f1 = __shfl_up_sync( 0xffffffffu, out_f1, 1, G );
+                    const int32_t cp = (int32_t) s - k;
+                    const uint32_t w = q0;
+                    q0 = q1;
+                    q1 = q2;
+                    q2 = q3;
+                    q3 = fetch( cp + 4 );
+                    const int4 bnd = bq0;
+                    if( reads_boundary ) {
+                        bq0 = bq1;
+                        const uint32_t nxt = (uint32_t) cp + 2u;
+                        if( nxt < ncp && nxt < p.scratch_cols )
+                            bq1 = scratch[nxt];
+                    }
+                    if( cp < 0 || (uint32_t) cp >= ncp )
+                        continue;
+                    if( k == 0 ) {
+                        if( pass ) {
+                            up_h0 = (uint32_t) bnd.x;
+                            up_f0 = (uint32_t) bnd.y;
+                            up_h1 = (uint32_t) bnd.z;
+                            up_f1 = (uint32_t) bnd.w;
+                        }
+                        else {
+                            const int32_t c = 2 * cp;
+                            up_h0 = nw_pack( top_h( c ) );
+                            up_f0 = nw_pack( top_f( c ) );
+                            up_h1 = nw_pack( top_h( c + 1 ) );
+                            up_f1 = nw_pack( top_f( c + 1 ) );
+                        }
+                    }
+                    const uint32_t * pa = slice + (w & 0xffu) * GR + (uint32_t) (k * R);
+                    const uint32_t * pb = slice + (w >> 8) * GR + (uint32_t) (k * R);
+                    uint32_t fa = up_f0, fb = up_f1;
+                    if( holds_last && cp == cap_cp )
+                        nw_rows<R, true>( H, E, pa, pb, diag, up_h0, fa, fb, GOE32, GE2, row0, last_is_a, !last_is_a,
+                                qa_last, qb_last, cap_a, cap_b, out_h0 );
+                    else
+                        nw_rows<R, false>( H, E, pa, pb, diag, up_h0, fa, fb, GOE32, GE2, row0, false, false,
+                                qa_last, qb_last, cap_a, cap_b, out_h0 );
+                    diag = up_h1;
+                    out_f0 = fa;
+                    out_h1 = H[R - 1];
+                    out_f1 = fb;
+                    if( k == G - 1 && !last_pass ) {
+                        if( (uint32_t) cp < p.scratch_cols )
+                            scratch[cp] = make_int4( (int) out_h0, (int) out_f0, (int) out_h1, (int) out_f1 );
+                        else
+                            atomicOr( p.sink.error_flags, ERR_SCRATCH_OVERFLOW );
+                    }
+                }
+                __syncwarp();
+            }
+            // the threads holding the last rows report (values are > 0 with the bias)
+#pragma unroll
+            for( int o = 1; o < G; o <<= 1 ) {
+                cap_a = max( cap_a, __shfl_xor_sync( 0xffffffffu, cap_a, o, G ) );
+                cap_b = max( cap_b, __shfl_xor_sync( 0xffffffffu, cap_b, o, G ) );
+            }
+            if( exact && k == 0 ) {
+                p.sink.score[(uint64_t) slot_a * p.sink.score_stride + id] =
+                        (int32_t) (cap_a & 0xffffu) - (int32_t) NWQ_BIAS;
+                if( slot_b != 0xffffffffu )
+                    p.sink.score[(uint64_t) slot_b * p.sink.score_stride + id] =
+                            (int32_t) (cap_b >> 16) - (int32_t) NWQ_BIAS;
+            }
+        }
+    }
+}
+
+template <int R>
+static cudaError_t launch_nw_one( const QPairParams & p, int grid, cudaStream_t st, int * blocks_per_sm ) {
+    const size_t smem = (size_t) (QP_THREADS / 32) * QP_CODES * QP_G * R * sizeof(uint32_t);
+    cudaError_t e = cudaFuncSetAttribute( nw_qpair_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            (int) smem );
+    if( e != cudaSuccess )
+        return e;
+    if( grid == 0 )
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor( blocks_per_sm, nw_qpair_kernel<R>, QP_THREADS, smem );
+    nw_qpair_kernel<R><<<grid, QP_THREADS, smem, st>>>( p );
+    return cudaGetLastError();
+}
+
+cudaError_t launch_nw_qpair( int R, const QPairParams & p, int grid, cudaStream_t st, int * blocks_per_sm ) {
+    switch( R ) {
+    case 16:
+        return launch_nw_one<16>( p, grid, st, blocks_per_sm );
+    case 20:
+        return launch_nw_one<20>( p, grid, st, blocks_per_sm );
+    case 24:
+        return launch_nw_one<24>( p, grid, st, blocks_per_sm );
+    case 28:
+        return launch_nw_one<28>( p, grid, st, blocks_per_sm );
+    default:
+        return cudaErrorInvalidValue;
+    }
+}
+
+// prof[qp][code][row] = (A's score, B's score) as a 16x2 word at the entry
+// width; rows past a query, and the absent query of an odd batch, score -128
+// (8-bit Smith-Waterman: never raises a maximum) or 0 (16-bit
+// Needleman-Wunsch: rows below a query do not feed back into it).
 __global__ void build_profile_qp_kernel( const uint8_t * qcodes, const uint64_t * qoff, const uint32_t * qlen,
         const uint32_t * qp_slots, uint32_t n_qp, const uint32_t * qp_rows, const int64_t * matrix, uint32_t * prof,
-        const uint64_t * prof_off ) {
+        const uint64_t * prof_off, int width ) {
     const uint32_t qp = blockIdx.y;
     if( qp >= n_qp )
         return;
@@ -305,20 +596,28 @@ __global__ void build_profile_qp_kernel( const uint8_t * qcodes, const uint64_t 
     for( uint64_t x = blockIdx.x * (uint64_t) blockDim.x + threadIdx.x; x < (uint64_t) QP_CODES * rows;
             x += (uint64_t) gridDim.x * blockDim.x ) {
         const uint32_t code = (uint32_t) (x / rows), row = (uint32_t) (x % rows);
-        const int32_t a = row < La ? (int32_t) (int8_t) matrix[(code << 5) + qa[row]] : -128;
-        const int32_t b = row < Lb ? (int32_t) (int8_t) matrix[(code << 5) + qb[row]] : -128;
+        const int32_t pad = (width == 8) ? -128 : 0;
+        int32_t a = pad, b = pad;
+        if( row < La ) {
+            const int64_t m = matrix[(code << 5) + qa[row]];
+            a = (width == 8) ? (int32_t) (int8_t) m : (int32_t) (int16_t) m;
+        }
+        if( row < Lb ) {
+            const int64_t m = matrix[(code << 5) + qb[row]];
+            b = (width == 8) ? (int32_t) (int8_t) m : (int32_t) (int16_t) m;
+        }
         out[x] = ((uint32_t) (uint16_t) (int16_t) b << 16) | (uint16_t) (int16_t) a;
     }
 }
 
 cudaError_t launch_build_profile_qp( const uint8_t * qcodes, const uint64_t * qoff, const uint32_t * qlen,
         const uint32_t * qp_slots, uint32_t n_qp, const uint32_t * qp_rows, const int64_t * matrix, uint32_t * prof,
-        const uint64_t * prof_off, cudaStream_t st ) {
+        const uint64_t * prof_off, int width, cudaStream_t st ) {
     if( n_qp == 0 )
         return cudaSuccess;
     dim3 grid( 16, n_qp );
     build_profile_qp_kernel<<<grid, 256, 0, st>>>( qcodes, qoff, qlen, qp_slots, n_qp, qp_rows, matrix, prof,
-            prof_off );
+            prof_off, width );
     return cudaGetLastError();
 }
 

@@ -146,3 +146,48 @@ def test_batched_random_against_oracle(built_library, seed):
         exp, _ = oracle_search("sw", 8, 1, c["hits"], 1, c["matrix"], c["gap"], c["chunk"], c["simd"], q,
                                c["records"])
         assert batched[qi] == exp, (seed, qi, len(q))
+
+
+def _nw_batch_case(seed):
+    rng = np.random.default_rng(2000 + seed)
+    nuc = seed % 2 == 0
+    alpha = W.NT4 if nuc else W.AA20
+    nq = int(rng.integers(1, 7))
+    qs = [W.random_residues(rng, int(rng.integers(1, 900)), alpha) for _ in range(nq)]
+    recs = []
+    for _ in range(int(rng.integers(20, 250))):
+        r = rng.random()
+        src = qs[int(rng.integers(0, nq))]
+        if r < 0.1:
+            recs.append(W.mutate(rng, src, alpha, 0.05, 0.02, (1, 5)).tobytes())
+        elif r < 0.14:
+            # long enough that some pairs fall outside the exact 16-bit range
+            recs.append(W.random_residues(rng, int(rng.integers(3000, 9000)), alpha).tobytes())
+        else:
+            recs.append(W.random_residues(rng, int(rng.integers(1, 1500)), alpha).tobytes())
+    if nuc:
+        matrix = ("const", int(rng.integers(1, 6)), -int(rng.integers(1, 6)))
+    else:
+        matrix = ("builtin", ["blosum62", "pam30"][int(rng.integers(0, 2))])
+    gap = [(-5, -2), (-11, -1), (-2, -3), (-40, -4)][int(rng.integers(0, 4))]
+    return dict(queries=[q.tobytes() for q in qs], records=recs, gap=gap, matrix=matrix, symtype=0 if nuc else 1,
+                chunk=int([1000, 33][int(rng.integers(0, 2))]), hits=int(rng.integers(1, 12)),
+                simd=int([2, 1][int(rng.integers(0, 2))]))
+
+
+@pytest.mark.parametrize("seed", range(8))
+def test_nw16_batched_against_oracle(built_library, seed):
+    """Needleman-Wunsch at the 16-bit entry through the query-pair kernel
+    (single queries and batches), including sequences beyond its exact range
+    that go to the lane emulation, against the oracle query by query."""
+    c = _nw_batch_case(seed)
+    product_setup(c["symtype"], c["matrix"], c["gap"], c["chunk"], c["simd"], records=c["records"])
+    batched, _ = product_search("nw", 16, 1, c["hits"], c["queries"], batch=True)
+    single, ovf = product_search("nw", 16, 1, c["hits"], c["queries"][:1])
+    for qi, q in enumerate(c["queries"]):
+        exp, eovf = oracle_search("nw", 16, 1, c["hits"], c["symtype"], c["matrix"], c["gap"], c["chunk"], c["simd"],
+                                  q, c["records"])
+        assert batched[qi] == exp, (seed, qi, len(q))
+        if qi == 0:
+            assert single[0] == exp
+            assert tuple(ovf[0]) == tuple(eovf)
