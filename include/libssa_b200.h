@@ -62,6 +62,12 @@ void ssa_db_refresh( void );
 /* Number of residue codes of a query after mapping. */
 size_t ssa_query_length( p_query p );
 
+/* Translation table of NCBI genetic code `code` (1-6, 9-16, 21-25) as
+ * translated searches use it: out[a*256 + b*16 + c] is the amino-acid code of
+ * the nucleotide triple (a, b, c), nucleotide codes 0-15 (IUPAC bit masks).
+ * Returns 0, or -1 for a code that does not exist. */
+int ssa_b200_translation_table( int code, uint8_t * out );
+
 /*
  * Database plugin extension implemented by libsdb_b200 (the plugin that ships
  * with this build): installs count records from memory, record i being

@@ -38,6 +38,7 @@ EXPORTED = [
     "free_sequence", "sw_align", "nw_align", "free_alignment", "ssa_exit", "ssa_align_batch", "ssa_get_stats",
     "ssa_query_length", "ssa_db_refresh", "ssa_b200_int_peak", "ssa_b200_score64_noalloc",
     "ssa_server_start", "ssa_server_submit", "ssa_server_wait", "ssa_server_get_stats", "ssa_server_stop",
+    "ssa_b200_translation_table",
 ]
 
 # allocation-free scoring (include/libssa_b200.h)
@@ -133,6 +134,8 @@ def load():
     lib.ssa_server_wait.restype = P_LIST
     lib.ssa_server_get_stats.argtypes = [ctypes.c_void_p, ctypes.POINTER(ServerStats)]
     lib.ssa_server_stop.argtypes = [ctypes.c_void_p]
+    lib.ssa_b200_translation_table.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_uint8)]
+    lib.ssa_b200_translation_table.restype = ctypes.c_int
     _plugin.ssa_db_b200_load_memory.argtypes = [ctypes.c_size_t, ctypes.c_char_p, ctypes.POINTER(ctypes.c_uint64)]
     _plugin.ssa_db_b200_load_memory.restype = ctypes.c_int
     _plugin.ssa_db_get_sequence_count.restype = ctypes.c_size_t
@@ -203,9 +206,16 @@ class Hit:
     dlen: int
     qlen: int
     db_seq: bytes = b""
+    strand: int = 0      # alignment_t.db_seq.strand
+    frame: int = 0       # alignment_t.db_seq.frame
+    qstrand: int = 0     # alignment_t.query.strand
+    qframe: int = 0      # alignment_t.query.frame
 
     def key(self):
         return (self.id, self.score, self.cigar, self.q_start, self.q_end, self.d_start, self.d_end)
+
+    def key_frames(self):
+        return self.key() + (self.strand, self.frame, self.qstrand, self.qframe)
 
 
 def _read_list(lp) -> list[Hit]:
@@ -216,7 +226,8 @@ def _read_list(lp) -> list[Hit]:
         cig = a.alignment.decode() if a.alignment is not None else None
         seq = ctypes.string_at(a.db_seq.seq, a.db_seq.len) if a.db_seq.seq else b""
         out.append(Hit(int(a.db_seq.ID), int(a.score), cig, int(a.align_q_start), int(a.align_q_end),
-                       int(a.align_d_start), int(a.align_d_end), int(a.db_seq.len), int(a.query.len), seq))
+                       int(a.align_d_start), int(a.align_d_end), int(a.db_seq.len), int(a.query.len), seq,
+                       int(a.db_seq.strand), int(a.db_seq.frame), int(a.query.strand), int(a.query.frame)))
     return out
 
 
@@ -327,6 +338,15 @@ class Server:
         if self._h:
             self._lib.ssa_server_stop(self._h)
             self._h = None
+
+
+def translation_table(code: int) -> list[int]:
+    """Amino-acid code of every nucleotide triple (a, b, c), codes 0-15, index
+    a*256 + b*16 + c, under NCBI genetic code `code`."""
+    out = (ctypes.c_uint8 * 4096)()
+    if load().ssa_b200_translation_table(code, out) != 0:
+        raise ValueError(f"no genetic code {code}")
+    return list(out)
 
 
 def query_length(q) -> int:

@@ -192,18 +192,159 @@ void matrix_constant( int match, int mismatch, int64_t * out ) {
             out[(a << 5) + b] = (int8_t) (a == b ? match : mismatch);
 }
 
+// ---- genetic codes and translation (reference: src/util/util_sequence.c:88-260,
+//      298-392) ----------------------------------------------------------------------
+// NCBI translation tables 1-25, one amino acid per codon with the codons in
+// TCAG order (TTT, TTC, TTA, TTG, TCT, ...); tables 7, 8 and 17-20 do not exist.
+static const char * const NCBI_CODES[25] = {
+    "FFLLSSSSYY**CC*WLLLLPPPPHHQQRRRRIIIMTTTTNNKKSSRRVVVVAAAADDEEGGGG",
+    "FFLLSSSSYY**CCWWLLLLPPPPHHQQRRRRIIMMTTTTNNKKSS**VVVVAAAADDEEGGGG",
+    "FFLLSSSSYY**CCWWTTTTPPPPHHQQRRRRIIMMTTTTNNKKSSRRVVVVAAAADDEEGGGG",
+    "FFLLSSSSYY**CCWWLLLLPPPPHHQQRRRRIIIMTTTTNNKKSSRRVVVVAAAADDEEGGGG",
+    "FFLLSSSSYY**CCWWLLLLPPPPHHQQRRRRIIMMTTTTNNKKSSSSVVVVAAAADDEEGGGG",
+    "FFLLSSSSYYQQCC*WLLLLPPPPHHQQRRRRIIIMTTTTNNKKSSRRVVVVAAAADDEEGGGG",
+    nullptr,
+    nullptr,
+    "FFLLSSSSYY**CCWWLLLLPPPPHHQQRRRRIIIMTTTTNNNKSSSSVVVVAAAADDEEGGGG",
+    "FFLLSSSSYY**CCCWLLLLPPPPHHQQRRRRIIIMTTTTNNKKSSRRVVVVAAAADDEEGGGG",
+    "FFLLSSSSYY**CC*WLLLLPPPPHHQQRRRRIIIMTTTTNNKKSSRRVVVVAAAADDEEGGGG",
+    "FFLLSSSSYY**CC*WLLLSPPPPHHQQRRRRIIIMTTTTNNKKSSRRVVVVAAAADDEEGGGG",
+    "FFLLSSSSYY**CCWWLLLLPPPPHHQQRRRRIIMMTTTTNNKKSSGGVVVVAAAADDEEGGGG",
+    "FFLLSSSSYYY*CCWWLLLLPPPPHHQQRRRRIIIMTTTTNNNKSSSSVVVVAAAADDEEGGGG",
+    "FFLLSSSSYY*QCC*WLLLLPPPPHHQQRRRRIIIMTTTTNNKKSSRRVVVVAAAADDEEGGGG",
+    "FFLLSSSSYY*LCC*WLLLLPPPPHHQQRRRRIIIMTTTTNNKKSSRRVVVVAAAADDEEGGGG",
+    nullptr,
+    nullptr,
+    nullptr,
+    nullptr,
+    "FFLLSSSSYY**CCWWLLLLPPPPHHQQRRRRIIMMTTTTNNNKSSSSVVVVAAAADDEEGGGG",
+    "FFLLSS*SYY*LCC*WLLLLPPPPHHQQRRRRIIIMTTTTNNKKSSRRVVVVAAAADDEEGGGG",
+    "FF*LSSSSYY**CC*WLLLLPPPPHHQQRRRRIIIMTTTTNNKKSSRRVVVVAAAADDEEGGGG",
+    "FFLLSSSSYY**CCWWLLLLPPPPHHQQRRRRIIIMTTTTNNKKSSSKVVVVAAAADDEEGGGG",
+    "FFLLSSSSYY**CCGWLLLLPPPPHHQQRRRRIIIMTTTTNNKKSSRRVVVVAAAADDEEGGGG",
+};
+
+// Amino-acid code of every triple (a, b, c) of nt16 codes (bit 0 A, 1 C, 2 G,
+// 3 T): the amino acid all concrete codons the IUPAC codes allow agree on, B
+// when they give D and N, Z when they give E and Q, X otherwise (and for a
+// code without bases).
+void translation_table( int code_no, uint8_t * table ) {
+    static const int tcag[4] = { 2, 1, 3, 0 };   // base bit -> TCAG position
+    const char * code = (code_no >= 1 && code_no <= 25) ? NCBI_CODES[code_no - 1] : nullptr;
+    if( !code )
+        fatal( "Illegal genetic code %d.", code_no );
+    for( int t = 0; t < 4096; t++ ) {
+        const int m[3] = { t >> 8, (t >> 4) & 15, t & 15 };
+        bool seen[128] = {};
+        int n = 0;
+        char one = 'X';
+        for( int i = 0; i < 4; i++ )
+            for( int j = 0; j < 4; j++ )
+                for( int k = 0; k < 4; k++ ) {
+                    if( !((m[0] >> i) & 1) || !((m[1] >> j) & 1) || !((m[2] >> k) & 1) )
+                        continue;
+                    const char x = code[tcag[i] * 16 + tcag[j] * 4 + tcag[k]];
+                    if( !seen[(int) x] ) {
+                        seen[(int) x] = true;
+                        n++;
+                        one = x;
+                    }
+                }
+        char aa = 'X';
+        if( n == 1 )
+            aa = one;
+        else if( n == 2 && seen['D'] && seen['N'] )
+            aa = 'B';
+        else if( n == 2 && seen['E'] && seen['Q'] )
+            aa = 'Z';
+        table[t] = (uint8_t) map_aa( (unsigned char) aa );
+    }
+}
+
+uint32_t units_per_record( int symtype, int strands ) {
+    return (symtype == NUCLEOTIDE && (strands & 2)) ? 2u : 1u;
+}
+
+// complement of an nt16 code: A <-> T, C <-> G bit by bit
+uint8_t nt_complement( uint8_t x ) {
+    return (uint8_t) (((x & 1) << 3) | ((x & 2) << 1) | ((x & 4) >> 1) | ((x & 8) >> 3));
+}
+
+// Protein of one strand (0 forward, 1 reverse complement) and frame (0-2) of a
+// mapped nucleotide sequence: codon k starts at frame + 3k on that strand.
+void translate( const char * dna, size_t n, int strand, int frame, const uint8_t * table, std::vector<char> & out ) {
+    const size_t len = (n > (size_t) frame) ? (n - frame) / 3 : 0;
+    out.assign( len + 1, 0 );
+    for( size_t k = 0; k < len; k++ ) {
+        int c;
+        if( strand == 0 ) {
+            const size_t p = frame + 3 * k;
+            c = (dna[p] << 8) | (dna[p + 1] << 4) | dna[p + 2];
+        }
+        else {
+            const size_t p = n - 1 - frame - 3 * k;
+            c = (nt_complement( (uint8_t) dna[p] ) << 8) | (nt_complement( (uint8_t) dna[p - 1] ) << 4) |
+                    nt_complement( (uint8_t) dna[p - 2] );
+        }
+        out[k] = (char) table[c & 4095];
+    }
+}
+
 }  // namespace ssa
 
 using namespace ssa;
 
 // ---- the query object ------------------------------------------------------------
+// One sequence a search runs for the query: the mapped residues themselves, a
+// strand of a nucleotide query, or a translated frame (reference:
+// src/query.c:132-160, src/algo/searcher.c:58-85).
+struct QueryFrame {
+    std::vector<char> seq;   // codes, NUL-terminated
+    int strand;
+    int frame;
+};
+
 struct _query {
     char * seq;          // mapped codes, NUL-terminated
     size_t len;
     char * header;
     size_t headerlen;
     int symtype;         // symbol type the codes were mapped with
+    std::vector<QueryFrame> * frames;   // sequences searched, in the reference's query order
 };
+
+// Strands of a nucleotide query, or translated frames, as the settings at read
+// time ask for; otherwise the mapped sequence alone.
+static void make_frames( p_query q ) {
+    const Config & c = config();
+    q->frames = new std::vector<QueryFrame>();
+    if( c.symtype == NUCLEOTIDE ) {
+        if( c.strands & 1 )
+            q->frames->push_back( QueryFrame{ std::vector<char>( q->seq, q->seq + q->len + 1 ), 0, 0 } );
+        if( c.strands & 2 ) {
+            std::vector<char> rc( q->len + 1, 0 );
+            for( size_t i = 0; i < q->len; i++ )
+                rc[i] = (char) nt_complement( (uint8_t) q->seq[q->len - 1 - i] );
+            q->frames->push_back( QueryFrame{ std::move( rc ), 1, 0 } );
+        }
+    }
+    else if( c.symtype == TRANS_QUERY || c.symtype == TRANS_BOTH ) {
+        uint8_t table[4096];
+        translation_table( c.q_gencode, table );
+        for( int st = 0; st < 2; st++ ) {
+            if( !((st + 1) & c.strands) )
+                continue;
+            for( int f = 0; f < 3; f++ ) {
+                QueryFrame qf{ {}, st, f };
+                translate( q->seq, q->len, st, f, table, qf.seq );
+                q->frames->push_back( std::move( qf ) );
+            }
+        }
+    }
+    else {
+        q->frames->push_back( QueryFrame{ std::vector<char>( q->seq, q->seq + q->len + 1 ), 0, 0 } );
+    }
+}
 
 static bool nucleotide_map( int symtype ) {
     return !(symtype == AMINOACID || symtype == TRANS_DB);
@@ -232,6 +373,7 @@ static p_query make_query( const char * text, size_t n, char * header, size_t he
     q->header = header;
     q->headerlen = headerlen;
     q->symtype = config().symtype;
+    make_frames( q );
     return q;
 }
 
@@ -293,10 +435,13 @@ static p_alignment_list make_list( const std::vector<Hit> & hits, p_query q, boo
         const Hit & h = hits[k];
         p_alignment a = (p_alignment) calloc( 1, sizeof(alignment_t) );
         // the hit's database record is fetched and mapped again, as the
-        // reference does per hit (reference: src/algo/aligner.c:62-93)
+        // reference does per hit (reference: src/algo/aligner.c:62-93); a
+        // reverse-complement unit is mapped forward there too (us_prepare_sequence
+        // only reverses for strand 2, which the database units never carry)
         p_seqinfo info = ssa_db_get_sequence( h.id );
         if( !info )
             fatal( "Could not get sequence from DB: %u", h.id );
+        const QueryFrame & qf = (*q->frames)[h.q_index];
         a->db_seq.seq = (char *) malloc( info->seqlen + 1 );
         for( size_t i = 0; i < info->seqlen; i++ ) {
             int m = nt ? map_nt16( (unsigned char) info->seq[i] ) : map_aa( (unsigned char) info->seq[i] );
@@ -305,12 +450,14 @@ static p_alignment_list make_list( const std::vector<Hit> & hits, p_query q, boo
         a->db_seq.seq[info->seqlen] = 0;
         a->db_seq.len = info->seqlen;
         a->db_seq.ID = info->ID;
-        a->db_seq.strand = 0;
-        a->db_seq.frame = 0;
-        a->query.seq = q->seq;
-        a->query.len = q->len;
-        a->query.strand = 0;
-        a->query.frame = 0;
+        // the reference stores the unit's frame in strand and its strand in
+        // frame (reference: src/algo/aligner.c:76-77)
+        a->db_seq.strand = h.db_frame;
+        a->db_seq.frame = h.db_strand;
+        a->query.seq = const_cast<char *>( qf.seq.data() );
+        a->query.len = qf.seq.size() - 1;
+        a->query.strand = qf.strand;
+        a->query.frame = qf.frame;
         a->score = (long) h.score;
         if( with_cigar && h.has_cigar ) {
             a->alignment = (char *) malloc( h.cigar.size() + 1 );
@@ -347,10 +494,14 @@ static SearchRequest make_request( int algo, size_t hitcount, int bit_width, int
     const Config & c = config();
     if( bit_width != BIT_WIDTH_8 && bit_width != BIT_WIDTH_16 && bit_width != BIT_WIDTH_64 )
         fatal( "\nunknown bit width provided: %d\n\n", bit_width );
-    if( c.symtype != AMINOACID && c.symtype != NUCLEOTIDE )
-        fatal( "Translated searches (symbol type %d) are not supported by the B200 build.", c.symtype );
-    if( c.symtype == NUCLEOTIDE && (c.strands & 2) )
-        fatal( "Searches of the complementary strand are not supported by the B200 build." );
+    // the reference crashes in every search of a translated database (its
+    // translated units are built and aligned from uninitialised buffers), so
+    // there is no behaviour to reproduce
+    if( c.symtype == TRANS_DB || c.symtype == TRANS_BOTH )
+        fatal( "Searches of a translated database (symbol type %d) are not supported by the B200 build.",
+                c.symtype );
+    if( c.symtype != AMINOACID && c.symtype != NUCLEOTIDE && c.symtype != TRANS_QUERY )
+        fatal( "Illegal symbol type specified." );
     SearchRequest r;
     r.algo = algo;
     r.bit_width = bit_width;
@@ -384,17 +535,25 @@ static std::vector<p_alignment_list> run_search( int algo, p_query * queries, si
     for( size_t i = 0; i < n; i++ )
         test_configuration( queries[i] );
     SearchRequest req = make_request( algo, hitcount, bit_width, align_type );
-    std::vector<QueryCodes> qc( n );
+    // every strand or frame of a query is searched as its own sequence; the
+    // engine merges a query's frames into one heap as the reference does
+    std::vector<QueryCodes> qc;
+    std::vector<uint32_t> groups( n );
     for( size_t i = 0; i < n; i++ ) {
         if( queries[i]->symtype != config().symtype )
             fatal( "Query was read with a different symbol type than the current one." );
         if( queries[i]->len == 0 )
             fatal( "Query sequence is empty." );
-        qc[i] = QueryCodes{ (const uint8_t *) queries[i]->seq, (uint32_t) queries[i]->len };
+        for( const QueryFrame & f : *queries[i]->frames ) {
+            if( f.seq.size() <= 1 )
+                fatal( "Query frame (strand %d, frame %d) is empty.", f.strand, f.frame );
+            qc.push_back( QueryCodes{ (const uint8_t *) f.seq.data(), (uint32_t) (f.seq.size() - 1) } );
+        }
+        groups[i] = (uint32_t) queries[i]->frames->size();
     }
     std::vector<std::vector<Hit>> hits;
     SearchStats st;
-    engine_search( req, qc, hits, st );
+    engine_search( req, qc, groups, hits, st );
     if( st.overflow8 || st.overflow16 )
         print_info( "Overflow occurred: %ld sequences were re-aligned with 16 bit, and %ld sequences with 64 bit\n",
                 (long) st.overflow8, (long) st.overflow16 );
@@ -637,6 +796,7 @@ void free_sequence( p_query p ) {
         return;
     free( p->seq );
     free( p->header );
+    delete p->frames;
     free( p );
 }
 
@@ -707,6 +867,13 @@ size_t ssa_query_length( p_query p ) {
     return p ? p->len : 0;
 }
 
+int ssa_b200_translation_table( int code, uint8_t * out ) {
+    if( code < 1 || code > 25 || !NCBI_CODES[code - 1] || !out )
+        return -1;
+    translation_table( code, out );
+    return 0;
+}
+
 struct ssa_server {
     ServerImpl impl;
 };
@@ -722,6 +889,8 @@ ssa_server * ssa_server_start( int algorithm, size_t hitcount, int bit_width, in
         fatal( "Scoring not initialized." );
     if( !c.constant_scoring && c.symtype == NUCLEOTIDE )
         fatal( "Nucleotide sequences can only be aligned using constant scores." );
+    if( !(c.symtype == AMINOACID || (c.symtype == NUCLEOTIDE && c.strands == FORWARD_STRAND)) )
+        fatal( "The server runs protein and forward-strand nucleotide searches only." );
     ssa_server * sv = new ssa_server();
     ServerImpl & s = sv->impl;
     s.req = make_request( algorithm == SSA_SMITH_WATERMAN ? 0 : 1, hitcount, bit_width, align_type );

@@ -134,7 +134,7 @@ public:
     // ---- database ------------------------------------------------------------
     const HostDb & database() {
         const Config & cfg = config();
-        if( db_.symtype != cfg.symtype || db_stale_ )
+        if( db_.symtype != cfg.symtype || db_.upi != units_per_record( cfg.symtype, cfg.strands ) || db_stale_ )
             pack_database();
         return db_;
     }
@@ -144,36 +144,45 @@ public:
     void pack_database() {
         const Config & cfg = config();
         HostDb db;
-        const size_t n = ssa_db_get_sequence_count();
-        if( n > UINT32_MAX )
-            fatal( "Database has %zu sequences; at most %u are supported.", n, UINT32_MAX );
+        const size_t n_rec = ssa_db_get_sequence_count();
+        const uint32_t upi = units_per_record( cfg.symtype, cfg.strands );
+        if( (uint64_t) n_rec * upi > UINT32_MAX )
+            fatal( "Database has %zu sequences; at most %u are supported.", n_rec, UINT32_MAX / upi );
+        const size_t n = n_rec * upi;
+        db.n_records = (uint32_t) n_rec;
+        db.upi = upi;
         db.n_ids = (uint32_t) n;
         db.len.assign( n, 0 );
         db.off.assign( n, 0 );
         const bool nt = cfg.symtype == NUCLEOTIDE;
-        if( cfg.symtype == TRANS_QUERY || cfg.symtype == TRANS_DB || cfg.symtype == TRANS_BOTH )
-            fatal( "Translated searches (symbol type %d) are not supported by the B200 build.", cfg.symtype );
+        if( cfg.symtype == TRANS_DB || cfg.symtype == TRANS_BOTH )
+            fatal( "Searches of a translated database (symbol type %d) are not supported by the B200 build.",
+                    cfg.symtype );
         uint64_t total = 0;
-        std::vector<p_seqinfo> infos( n );
-        for( size_t id = 0; id < n; id++ ) {
+        std::vector<p_seqinfo> infos( n_rec );
+        for( size_t id = 0; id < n_rec; id++ ) {
             p_seqinfo info = ssa_db_get_sequence( id );
             if( !info )
                 fatal( "Could not get sequence from DB: %zu", id );
             infos[id] = info;
             if( info->seqlen > (size_t) INT32_MAX / 2 )
                 fatal( "Database sequence %zu is too long (%zu residues).", id, info->seqlen );
-            db.len[id] = (uint32_t) info->seqlen;
-            db.off[id] = total;
-            total += (info->seqlen + 15) & ~(uint64_t) 15;
+            for( uint32_t k = 0; k < upi; k++ ) {
+                const size_t u = id * upi + k;
+                db.len[u] = (uint32_t) info->seqlen;
+                db.off[u] = total;
+                total += (info->seqlen + 15) & ~(uint64_t) 15;
+            }
             db.max_len = std::max( db.max_len, (uint32_t) info->seqlen );
         }
         db.codes.assign( total + 16, 0 );
         uint64_t unknown = 0;
-        for( size_t id = 0; id < n; id++ ) {
+        for( size_t id = 0; id < n_rec; id++ ) {
             // unknown symbols become code 0 (reference: src/util/util_sequence.c:298-318)
             const char * s = infos[id]->seq;
-            uint8_t * o = db.codes.data() + db.off[id];
-            for( size_t k = 0; k < db.len[id]; k++ ) {
+            const size_t L = infos[id]->seqlen;
+            uint8_t * o = db.codes.data() + db.off[id * upi];
+            for( size_t k = 0; k < L; k++ ) {
                 int m = nt ? map_nt16( (unsigned char) s[k] ) : map_aa( (unsigned char) s[k] );
                 if( m < 0 ) {
                     m = 0;
@@ -181,7 +190,13 @@ public:
                 }
                 o[k] = (uint8_t) m;
             }
-            db.residues += db.len[id];
+            if( upi == 2 ) {
+                // the reverse complement unit (reference: src/util/util_sequence.c:420-437)
+                uint8_t * rc = db.codes.data() + db.off[id * upi + 1];
+                for( size_t k = 0; k < L; k++ )
+                    rc[k] = nt_complement( o[L - 1 - k] );
+            }
+            db.residues += (uint64_t) L * upi;
         }
         if( unknown )
             print_warning( "%llu unknown symbols found and set to zero", (unsigned long long) unknown );
@@ -194,6 +209,7 @@ public:
         std::stable_sort( db.order_desc.begin(), db.order_desc.end(),
                 [&]( uint32_t a, uint32_t b ) { return db.len[a] > db.len[b]; } );
         db.symtype = cfg.symtype;
+        db.strands = cfg.strands;
         db.generation = ++generation_;
         db.mean_len = db.order_desc.empty() ? 0.0 : (double) db.residues / (double) db.order_desc.size();
 
@@ -285,7 +301,7 @@ public:
 
     // ---- search ----------------------------------------------------------------
     void search( const SearchRequest & req, const std::vector<QueryCodes> & queries,
-            std::vector<std::vector<Hit>> & out, SearchStats & stats );
+            const std::vector<uint32_t> & groups, std::vector<std::vector<Hit>> & out, SearchStats & stats );
 
     void shutdown() {
         DevBuf * bufs[] = { &d_codes_, &d_off_, &d_len_, &d_order_, &d_pair_res_, &d_pair_off_, &d_pair_cols_,
@@ -329,8 +345,8 @@ private:
             uint32_t seq_hi = UINT32_MAX );
     int32_t * score_sink() { return serving_ ? d_serve_score_.as<int32_t>() : d_score_.as<int32_t>(); }
     void build_profiles( int width, uint32_t n_slots );
-    void traceback( const SearchRequest & req, const std::vector<QueryCodes> & queries, uint32_t slot0,
-            std::vector<std::vector<Hit>> & out, SearchStats & stats );
+    void traceback( const SearchRequest & req, std::vector<std::vector<Hit>> & out,
+            const std::vector<std::pair<uint32_t, uint32_t>> & lists, SearchStats & stats );
 
     bool ready_ = false;
     int device_ = 0;
@@ -884,12 +900,21 @@ void Engine::run_qpair_entry( const SearchRequest & req, uint32_t nq, PairTask *
 }
 
 void Engine::search( const SearchRequest & req, const std::vector<QueryCodes> & queries,
-        std::vector<std::vector<Hit>> & out, SearchStats & stats ) {
+        const std::vector<uint32_t> & groups_in, std::vector<std::vector<Hit>> & out, SearchStats & stats ) {
     init_device();
     const HostDb & db = database();
     serving_ = false;
     serve_layout_ = false;      // the query buffers are reused for this batch
-    out.assign( queries.size(), {} );
+    // groups of query sequences (strands or frames of one query)
+    std::vector<uint32_t> groups = groups_in;
+    if( groups.empty() )
+        groups.assign( queries.size(), 1u );
+    std::vector<uint64_t> gstart( groups.size() + 1, 0 );
+    for( size_t g = 0; g < groups.size(); g++ )
+        gstart[g + 1] = gstart[g] + groups[g];
+    if( gstart.back() != queries.size() )
+        fatal( "Internal error: query groups do not cover the queries." );
+    out.assign( groups.size(), {} );
     if( queries.empty() )
         return;
     const uint64_t n_ne = db.order_desc.size();
@@ -905,8 +930,13 @@ void Engine::search( const SearchRequest & req, const std::vector<QueryCodes> & 
             1, std::min<uint64_t>( std::min<uint64_t>( queries.size(), pair_budget / per_query ), 65535 ) );
 
     CUDA_CHECK( cudaEventRecord( ev0_, stream_ ) );
-    for( size_t b0 = 0; b0 < queries.size(); b0 += batch ) {
-        const uint32_t nq = (uint32_t) std::min( batch, queries.size() - b0 );
+    for( size_t g0 = 0; g0 < groups.size(); ) {
+        // whole groups, at most `batch` query sequences (at least one group)
+        size_t g1 = g0 + 1;
+        while( g1 < groups.size() && gstart[g1 + 1] - gstart[g0] <= batch )
+            g1++;
+        const size_t b0 = gstart[g0];
+        const uint32_t nq = (uint32_t) (gstart[g1] - b0);
         // ---- upload queries
         h_qoff_.assign( nq, 0 );
         h_qlen_.assign( nq, 0 );
@@ -1005,7 +1035,7 @@ void Engine::search( const SearchRequest & req, const std::vector<QueryCodes> & 
             fatal( "Internal error in the GPU search (flags 0x%x).", err );
         const auto t_replay0 = std::chrono::steady_clock::now();
 
-        // ---- host replay, one query per worker
+        // ---- host replay, one query (group of query sequences) per worker
         std::vector<ReplayQuery> rq( nq );
         for( uint32_t s = 0; s < nq; s++ )
             rq[s].score = hs + (size_t) s * db.n_ids;
@@ -1019,16 +1049,22 @@ void Engine::search( const SearchRequest & req, const std::vector<QueryCodes> & 
         }
         const uint32_t * rank_entry = (entry == 64) ? nullptr : ranks( req.chunk_size, entry == 8 ? req.lanes8 : req.lanes16 );
         {
+            const uint32_t ng = (uint32_t) (g1 - g0);
             const unsigned hw = std::max( 1u, std::thread::hardware_concurrency() );
-            const unsigned nthreads = std::min<unsigned>( hw, nq );
+            const unsigned nthreads = std::min<unsigned>( hw, ng );
             std::atomic<uint32_t> next{ 0 };
-            std::vector<ReplayCounts> counts( nq );
+            std::vector<ReplayCounts> counts( ng );
             auto work = [&]() {
                 for( ;; ) {
-                    uint32_t s = next.fetch_add( 1 );
-                    if( s >= nq )
+                    const uint32_t i = next.fetch_add( 1 );
+                    if( i >= ng )
                         break;
-                    replay_query( db, req, rq[s], rank_entry, out[b0 + s], counts[s] );
+                    const size_t g = g0 + i;
+                    const uint32_t s0 = (uint32_t) (gstart[g] - b0);
+                    if( groups[g] == 1 && db.upi == 1 )
+                        replay_query( db, req, rq[s0], rank_entry, out[g], counts[i] );
+                    else
+                        replay_frames( db, req, &rq[s0], groups[g], out[g], counts[i] );
                 }
             };
             if( nthreads <= 1 ) {
@@ -1048,8 +1084,12 @@ void Engine::search( const SearchRequest & req, const std::vector<QueryCodes> & 
         }
         const auto t_replay1 = std::chrono::steady_clock::now();
         CUDA_CHECK( cudaEventRecord( ev_phase_[4], stream_ ) );
-        if( req.align_type == COMPUTE_ALIGNMENT )
-            traceback( req, queries, (uint32_t) b0, out, stats );
+        if( req.align_type == COMPUTE_ALIGNMENT ) {
+            std::vector<std::pair<uint32_t, uint32_t>> lists;   // (out index, slot of its first sequence)
+            for( size_t g = g0; g < g1; g++ )
+                lists.emplace_back( (uint32_t) g, (uint32_t) (gstart[g] - b0) );
+            traceback( req, out, lists, stats );
+        }
         CUDA_CHECK( cudaEventRecord( ev_phase_[5], stream_ ) );
         {
             CUDA_CHECK( cudaEventSynchronize( ev_phase_[5] ) );
@@ -1066,6 +1106,7 @@ void Engine::search( const SearchRequest & req, const std::vector<QueryCodes> & 
                     "copies %.3f ms, replay %.3f ms, traceback %.3f ms\n",
                     nq, (unsigned long long) n_pairs, ms[0], ms[1], n_a, n_b, ms[2], rep, ms[3] );
         }
+        g0 = g1;
     }
     CUDA_CHECK( cudaEventRecord( ev1_, stream_ ) );
     CUDA_CHECK( cudaEventSynchronize( ev1_ ) );
@@ -1075,16 +1116,19 @@ void Engine::search( const SearchRequest & req, const std::vector<QueryCodes> & 
     stats.kernel_launches = launches_.load();
 }
 
-void Engine::traceback( const SearchRequest & req, const std::vector<QueryCodes> & queries, uint32_t slot0,
-        std::vector<std::vector<Hit>> & out, SearchStats & stats ) {
-    const uint32_t nq = (uint32_t) h_qlen_.size();
+void Engine::traceback( const SearchRequest & req, std::vector<std::vector<Hit>> & out,
+        const std::vector<std::pair<uint32_t, uint32_t>> & lists, SearchStats & stats ) {
     std::vector<TbHit> hits;
-    std::vector<std::pair<uint32_t, uint32_t>> where;   // (query index, hit index)
-    for( uint32_t s = 0; s < nq; s++ ) {
-        auto & hl = out[slot0 + s];
+    std::vector<std::pair<uint32_t, uint32_t>> where;   // (list index, hit index)
+    for( const auto & l : lists ) {
+        auto & hl = out[l.first];
         for( uint32_t k = 0; k < hl.size(); k++ ) {
-            hits.push_back( TbHit{ s, hl[k].id, (int32_t) hl[k].score, req.algo } );
-            where.emplace_back( slot0 + s, k );
+            // the hit's query sequence; the database record's first unit (the
+            // reference aligns a reverse-complement hit on the forward strand:
+            // src/util/util_sequence.c:360-375)
+            const uint32_t fwd_unit = hl[k].unit - hl[k].unit % db_.upi;
+            hits.push_back( TbHit{ l.second + hl[k].q_index, fwd_unit, (int32_t) hl[k].score, req.algo } );
+            where.emplace_back( l.first, k );
         }
     }
     const uint32_t nh = (uint32_t) hits.size();
@@ -1450,7 +1494,10 @@ void Engine::serve_finish( const SearchRequest & req, const std::vector<uint32_t
         max_qlen_ = 0;
         for( uint32_t s : done )
             max_qlen_ = std::max( max_qlen_, h_qlen_[s] );
-        traceback( req, {}, 0, out, stats );
+        std::vector<std::pair<uint32_t, uint32_t>> lists;
+        for( uint32_t sl : done )
+            lists.emplace_back( sl, sl );
+        traceback( req, out, lists, stats );
     }
 }
 
@@ -1460,9 +1507,9 @@ void Engine::serve_finish( const SearchRequest & req, const std::vector<uint32_t
 static std::mutex g_engine_mutex;
 
 void engine_search( const SearchRequest & req, const std::vector<QueryCodes> & queries,
-        std::vector<std::vector<Hit>> & out, SearchStats & stats ) {
+        const std::vector<uint32_t> & groups, std::vector<std::vector<Hit>> & out, SearchStats & stats ) {
     std::lock_guard<std::mutex> lock( g_engine_mutex );
-    Engine::get().search( req, queries, out, stats );
+    Engine::get().search( req, queries, groups, out, stats );
 }
 
 const HostDb & engine_database() {

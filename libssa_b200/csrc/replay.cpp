@@ -56,8 +56,9 @@ void schedule_ranks( const HostDb & db, size_t chunk_size, int lanes, std::vecto
     std::vector<uint32_t> ids;
     std::vector<int32_t> nb;
     std::vector<uint32_t> order;
-    for( uint64_t start = 0; start < db.n_ids; start += chunk_size ) {
-        const uint64_t end = std::min<uint64_t>( db.n_ids, start + chunk_size );
+    const uint64_t cs = (uint64_t) chunk_size * db.upi;    // a chunk of records, in units
+    for( uint64_t start = 0; start < db.n_ids; start += cs ) {
+        const uint64_t end = std::min<uint64_t>( db.n_ids, start + cs );
         ids.clear();
         nb.clear();
         for( uint64_t id = start; id < end; id++ ) {
@@ -78,8 +79,9 @@ namespace {
 // (reference: src/util/minheap.c:50-91).
 struct MinHeap {
     struct Elem {
-        uint32_t id;
+        uint32_t id;       // database unit
         int64_t score;
+        uint32_t q = 0;    // query strand or frame
     };
     size_t alloc;
     std::vector<Elem> a;
@@ -89,10 +91,10 @@ struct MinHeap {
     bool full() const { return a.size() >= alloc; }
     int64_t root() const { return a[0].score; }
 
-    void add( uint32_t id, int64_t score ) {
+    void add( uint32_t id, int64_t score, uint32_t q = 0 ) {
         if( alloc == 0 )
             return;
-        Elem n{ id, score };
+        Elem n{ id, score, q };
         if( a.size() < alloc ) {
             size_t i = a.size();
             a.push_back( n );
@@ -141,7 +143,7 @@ struct BlockMap {
 void replay_query( const HostDb & db, const SearchRequest & req, const ReplayQuery & rq, const uint32_t * rank_entry,
         std::vector<Hit> & hits, ReplayCounts & counts ) {
     MinHeap heap( req.hitcount );
-    const size_t cs = req.chunk_size ? req.chunk_size : 1000;
+    const size_t cs = (req.chunk_size ? req.chunk_size : 1000) * (size_t) db.upi;   // records -> units
     const int lanes_entry = req.bit_width == 8 ? req.lanes8 : req.lanes16;
     BlockMap ovfE{ rq.ovf_entry }, ovf16{ rq.ovf16 };
 
@@ -245,7 +247,115 @@ void replay_query( const HostDb & db, const SearchRequest & req, const ReplayQue
     hits.resize( e.size() );
     for( size_t k = 0; k < e.size(); k++ ) {
         hits[k].score = e[k].score;
-        hits[k].id = e[k].id;
+        hits[k].unit = e[k].id;
+        hits[k].id = e[k].id / db.upi;
+        hits[k].db_strand = (uint8_t) (e[k].id % db.upi);
+    }
+}
+
+// A query searched as several sequences (strands, or translated frames): the
+// reference runs every chunk once per query sequence into the same heap, then
+// re-runs the chunk's overflow list, which holds the overflowing units of all
+// query sequences in report order, at 16 bits for every query sequence, and its
+// 16-bit overflow list at 64 bits for every query sequence
+// (src/algo/8/search_8.c:94-124, src/algo/16/search_16.c:92-114,
+// src/algo/64/search_64.c:44-56).  Every report carries the pair's exact
+// score, which the GPU passes leave in the score rows.
+void replay_frames( const HostDb & db, const SearchRequest & req, const ReplayQuery * rq, uint32_t F,
+        std::vector<Hit> & hits, ReplayCounts & counts ) {
+    MinHeap heap( req.hitcount );
+    const size_t cs = (req.chunk_size ? req.chunk_size : 1000) * (size_t) db.upi;
+    const int lanes_entry = req.bit_width == 8 ? req.lanes8 : req.lanes16;
+    std::vector<BlockMap> ovfE, ovf16;
+    for( uint32_t q = 0; q < F; q++ ) {
+        ovfE.push_back( BlockMap{ rq[q].ovf_entry } );
+        ovf16.push_back( BlockMap{ rq[q].ovf16 } );
+    }
+    auto blocks = [&]( uint32_t u ) { return (int32_t) ((db.len[u] + 3) / 4); };
+    std::vector<uint32_t> units, order, ovf_chunk, list64;
+    std::vector<int32_t> nb;
+    for( uint64_t start = 0; start < db.n_ids; start += cs ) {
+        const uint64_t end = std::min<uint64_t>( db.n_ids, start + cs );
+        if( db.nonempty_before[end] == db.nonempty_before[start] )
+            break;
+        units.clear();
+        for( uint64_t u = start; u < end; u++ )
+            if( db.len[u] )
+                units.push_back( (uint32_t) u );
+        if( req.bit_width == 64 ) {
+            for( uint32_t q = 0; q < F; q++ )
+                for( uint32_t u : units )
+                    heap.add( u, rq[q].score[u], q );
+            continue;
+        }
+        ovf_chunk.clear();
+        for( uint32_t q = 0; q < F; q++ ) {
+            nb.clear();
+            for( uint32_t u : units ) {
+                int32_t b;
+                nb.push_back( ovfE[q].find( u, b ) ? b : blocks( u ) );
+            }
+            simulate_lanes( lanes_entry, nb, order );
+            for( uint32_t k : order ) {
+                const uint32_t u = units[k];
+                int32_t b;
+                if( ovfE[q].find( u, b ) )
+                    ovf_chunk.push_back( u );
+                else
+                    heap.add( u, rq[q].score[u], q );
+            }
+        }
+        if( ovf_chunk.empty() )
+            continue;
+        if( req.bit_width == 8 ) {
+            counts.overflow8 += ovf_chunk.size();
+            list64.clear();
+            for( uint32_t q = 0; q < F; q++ ) {
+                // a pair that did not overflow at 8 bits reports at 16 bits too
+                nb.clear();
+                for( uint32_t u : ovf_chunk ) {
+                    int32_t b8, b16;
+                    nb.push_back( (ovfE[q].find( u, b8 ) && ovf16[q].find( u, b16 )) ? b16 : blocks( u ) );
+                }
+                simulate_lanes( req.lanes16, nb, order );
+                for( uint32_t k : order ) {
+                    const uint32_t u = ovf_chunk[k];
+                    int32_t b8, b16;
+                    if( ovfE[q].find( u, b8 ) && ovf16[q].find( u, b16 ) )
+                        list64.push_back( u );
+                    else
+                        heap.add( u, rq[q].score[u], q );
+                }
+            }
+            counts.overflow16 += list64.size();
+            for( uint32_t q = 0; q < F; q++ )
+                for( uint32_t u : list64 )
+                    heap.add( u, rq[q].score[u], q );
+        }
+        else {
+            counts.overflow16 += ovf_chunk.size();
+            for( uint32_t q = 0; q < F; q++ )
+                for( uint32_t u : ovf_chunk )
+                    heap.add( u, rq[q].score[u], q );
+        }
+    }
+    // score, then database ID, both descending; entries equal in both keep
+    // their heap order (the reference's qsort of the heap array is a stable
+    // merge sort: src/util/minheap.c:93-106)
+    std::vector<MinHeap::Elem> e = heap.a;
+    std::stable_sort( e.begin(), e.end(), [&]( const MinHeap::Elem & x, const MinHeap::Elem & y ) {
+        if( x.score != y.score )
+            return x.score > y.score;
+        return x.id / db.upi > y.id / db.upi;
+    } );
+    hits.clear();
+    hits.resize( e.size() );
+    for( size_t k = 0; k < e.size(); k++ ) {
+        hits[k].score = e[k].score;
+        hits[k].unit = e[k].id;
+        hits[k].id = e[k].id / db.upi;
+        hits[k].db_strand = (uint8_t) (e[k].id % db.upi);
+        hits[k].q_index = e[k].q;
     }
 }
 

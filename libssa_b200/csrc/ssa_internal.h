@@ -45,8 +45,16 @@ bool matrix_builtin( const char * name, int64_t * out );
 void matrix_constant( int match, int mismatch, int64_t * out );
 
 // ---- database packed on the host, mirrored into HBM --------------------------
+// The database as the searches see it: units.  A record (database ID) gives
+// `upi` consecutive units, unit id * upi + k: its mapped residues (k = 0) and,
+// for nucleotide searches of the complementary strand, their reverse
+// complement (k = 1), as the reference's chunks hold them
+// (src/db_adapter.c:47-70, 118-135, 212-239).  The per-unit arrays below say
+// "ID" for the unit index; with upi = 1 units are records.
 struct HostDb {
-    uint32_t n_ids = 0;
+    uint32_t n_ids = 0;                 // units
+    uint32_t n_records = 0;             // database IDs
+    uint32_t upi = 1;                   // units per record
     std::vector<uint32_t> len;          // per ID
     std::vector<uint64_t> off;          // per ID into codes
     std::vector<uint8_t> codes;         // mapped residues, each record padded to 16 B
@@ -60,13 +68,21 @@ struct HostDb {
     uint64_t residues = 0;
     uint32_t max_len = 0;
     int symtype = -1;
+    int strands = -1;
     uint64_t generation = 0;
 };
+
+// units per record for the current settings
+uint32_t units_per_record( int symtype, int strands );
+uint8_t nt_complement( uint8_t x );
 
 // ---- hits and search requests -------------------------------------------------
 struct Hit {
     int64_t score = 0;
-    uint32_t id = 0;
+    uint32_t id = 0;            // database record (ID)
+    uint32_t unit = 0;          // database unit (record x units per record + strand)
+    uint32_t q_index = 0;       // strand or frame of the query (its search order)
+    uint8_t db_strand = 0, db_frame = 0;
     uint32_t q_start = 0, q_end = 0, d_start = 0, d_end = 0;
     std::string cigar;
     bool has_cigar = false;
@@ -101,9 +117,11 @@ struct QueryCodes {
 };
 
 // Runs the search of each query against the current database on the GPU and
-// returns the sorted hit list per query.
+// returns the sorted hit list per query.  groups[g] consecutive entries of
+// `queries` are the strands or frames of query g, merged into one hit list
+// (empty groups: one entry per query).
 void engine_search( const SearchRequest & req, const std::vector<QueryCodes> & queries,
-        std::vector<std::vector<Hit>> & out, SearchStats & stats );
+        const std::vector<uint32_t> & groups, std::vector<std::vector<Hit>> & out, SearchStats & stats );
 
 // The packed database (re-read through the plugin when stale).
 const HostDb & engine_database();
@@ -154,6 +172,8 @@ struct ReplayCounts {
     uint64_t overflow16 = 0;    // searched sequences re-queued to 64 bit
 };
 
+void replay_frames( const HostDb & db, const SearchRequest & req, const ReplayQuery * rq, uint32_t F,
+        std::vector<Hit> & hits, ReplayCounts & counts );
 void replay_query( const HostDb & db, const SearchRequest & req, const ReplayQuery & rq, const uint32_t * rank_entry,
         std::vector<Hit> & hits, ReplayCounts & counts );
 

@@ -11,6 +11,9 @@
  * Usage:
  *   ref_run [options] --db DB --queries FASTA --out OUT.json
  *   ref_run --dump-matrix SPEC            (prints the 32x32 int64 table)
+ *   ref_run --dump-translation CODE       (prints the amino-acid code of every
+ *                                          nucleotide triple (a,b,c), codes 0-15,
+ *                                          under genetic code CODE, 4096 values)
  *
  * Options:
  *   --algo sw|nw        --width 8|16|64     --align 0|1     --hits K
@@ -37,6 +40,7 @@
 
 #include "libssa.h"
 #include "matrices.h"
+#include "util/util_sequence.h"
 
 static double now_s( void ) {
     struct timespec ts;
@@ -177,6 +181,25 @@ int main( int argc, char ** argv ) {
             printf( "[" );
             for( int k = 0; k < SCORE_MATRIX_DIM * SCORE_MATRIX_DIM; k++ )
                 printf( "%s%ld", k ? "," : "", (long) score_matrix_64[k] );
+            printf( "]\n" );
+            return 0;
+        }
+        else if( !strcmp( a, "--dump-translation" ) ) {
+            // translate the 4096 nucleotide triples with the reference's own
+            // translation of a query sequence (frame 0, forward strand)
+            const int gc = atoi( v );
+            us_init_translation( gc, gc );
+            sequence_t dna = { malloc( 3 * 4096 + 1 ), 3 * 4096 };
+            for( int t = 0; t < 4096; t++ ) {
+                dna.seq[3 * t] = (char) (t >> 8);
+                dna.seq[3 * t + 1] = (char) ((t >> 4) & 15);
+                dna.seq[3 * t + 2] = (char) (t & 15);
+            }
+            sequence_t prot = { NULL, 0 };
+            us_translate_sequence( 0, dna, 0, 0, &prot );
+            printf( "[" );
+            for( size_t k = 0; k < prot.len; k++ )
+                printf( "%s%d", k ? "," : "", (int) prot.seq[k] );
             printf( "]\n" );
             return 0;
         }

@@ -9,6 +9,10 @@ fixtures of its own test suite).  Writes:
   read (copied unchanged from the reference's tests/testdata/);
 * ``matrices.json`` -- the reference's 32x32 score tables of every built-in
   matrix, of constant scoring and of the file matrices in data/;
+* ``genetic_codes.json`` -- the reference's amino acid for every nucleotide
+  triple under each genetic code (ref_run --dump-translation);
+* ``frame_cases.json`` -- searches of query strands and translated query
+  frames with the reference's complete answer, strand and frame fields included;
 * ``abi_layout.json`` -- sizes, field offsets and constants of the
   reference's libssa.h / libssa_extern_db.h as its compiler sees them
   (tests/c_client/abi_layout.c built against the reference's headers);
@@ -120,6 +124,120 @@ def synthetic_cases() -> list[tuple[dict, list[bytes], list[bytes], bool]]:
     return cases
 
 
+def frame_cases() -> list[tuple[dict, list[bytes], list[bytes]]]:
+    """Searches with query strands or translated query frames: nucleotide
+    queries on the forward, complementary and both strands, and translated
+    queries (3 or 6 frames, several genetic codes) against protein sequences."""
+    rng = np.random.default_rng(77)
+    out = []
+    k = 0
+    for symtype, strands_list in ((0, (1, 2, 3)), (2, (1, 2, 3))):
+        for strands in strands_list:
+            for algo, width, simd in (("sw", 8, 2), ("nw", 16, 1), ("sw", 64, 2), ("sw", 16, 2)):
+                qlen = int(rng.integers(30, 400))
+                q = W.random_residues(rng, qlen, W.NT4)
+                if symtype == 0:
+                    alpha = W.NT4
+                    src = q
+                else:
+                    alpha = W.AA20
+                    # protein records, some of them translations-like copies
+                    src = W.random_residues(rng, max(10, qlen // 3), W.AA20)
+                recs = []
+                for i in range(int(rng.integers(40, 250))):
+                    r = rng.random()
+                    if r < 0.12:
+                        recs.append(W.mutate(rng, src, alpha, 0.05, 0.02, (1, 3)))
+                    elif r < 0.15:
+                        recs.append(W.mutate(rng, np.tile(src, 4), alpha, 0.01, 0.0, (1, 1)))
+                    elif r < 0.17:
+                        recs.append(np.zeros(0, np.uint8))
+                    else:
+                        recs.append(W.random_residues(rng, int(rng.integers(1, 500)), alpha))
+                if symtype == 0:
+                    matrix = "const:%d,%d" % (int(rng.integers(1, 6)), -int(rng.integers(1, 6)))
+                    gencode = [1, 1]
+                else:
+                    matrix = "builtin:" + ["blosum62", "pam30"][k % 2]
+                    gencode = [[1, 1], [2, 1], [11, 1], [5, 1]][k % 4]
+                case = {"name": f"frames_{symtype}_{strands}_{algo}_{width}", "algo": algo, "width": width,
+                        "align": 1, "hits": int(rng.integers(3, 14)), "symtype": symtype, "strands": strands,
+                        "gencode": gencode, "matrix": matrix,
+                        "gap": [-int(rng.integers(1, 13)), -int(rng.integers(1, 3))],
+                        "chunk": int([1000, 40, 7][k % 3]), "simd": simd}
+                out.append((case, [q.tobytes()], [r.tobytes() for r in recs]))
+                k += 1
+    # translated queries against copies of their own frames' translations, so
+    # that 8-bit lanes overflow in several frames of the same chunk
+    with open(os.path.join(HERE, "genetic_codes.json")) as f:
+        table = json.load(f)["1"]
+    nt_code = {c: i for i, c in enumerate("-ACMGRSVTWYHKDBN")}
+    compl = {"A": "T", "C": "G", "G": "C", "T": "A"}
+    aa = "-ABCDEFGHIKLMNPQRSTVWXYZU*OJ"
+    for strands, algo, width in ((3, "sw", 8), (1, "sw", 8), (2, "nw", 8)):
+        q = W.random_residues(rng, 240, W.NT4).tobytes().decode()
+        frames = []
+        for st in (0, 1):
+            seq = q if st == 0 else "".join(compl[c] for c in reversed(q))
+            for fr in range(3):
+                codes = [nt_code[c] for c in seq[fr:]]
+                frames.append("".join(aa[table[(codes[i] << 8) | (codes[i + 1] << 4) | codes[i + 2]]]
+                                      for i in range(0, len(codes) - 2, 3)).replace("*", "W"))
+        recs = []
+        for i in range(160):
+            r = rng.random()
+            fr = frames[int(rng.integers(0, 6))]
+            src = np.frombuffer(fr.encode(), np.uint8)
+            if r < 0.2:
+                recs.append(W.mutate(rng, np.tile(src, 3), W.AA20, 0.02, 0.0, (1, 1)))
+            elif r < 0.3:
+                recs.append(W.mutate(rng, src, W.AA20, 0.05, 0.02, (1, 3)))
+            else:
+                recs.append(W.random_residues(rng, int(rng.integers(5, 300)), W.AA20))
+        case = {"name": f"frames_ovf_2_{strands}_{algo}_{width}", "algo": algo, "width": width, "align": 1,
+                "hits": 12, "symtype": 2, "strands": strands, "gencode": [1, 1], "matrix": "builtin:blosum62",
+                "gap": [-11, -1], "chunk": 25, "simd": 2}
+        out.append((case, [q.encode()], [r.tobytes() for r in recs]))
+    return out
+
+
+def write_frame_cases() -> None:
+    import tempfile
+    res_all = []
+    with tempfile.TemporaryDirectory() as tmp:
+        for case, queries, records in frame_cases():
+            db = os.path.join(tmp, "db.sdb")
+            oracle.write_sdb(db, seqs=records)
+            res = oracle.run_reference(db, [q.decode() for q in queries], algo=case["algo"], width=case["width"],
+                                       align=case["align"], hits=case["hits"], symtype=case["symtype"],
+                                       strands=case["strands"], gencode=tuple(case["gencode"]),
+                                       matrix=case["matrix"], gap=tuple(case["gap"]), chunk=case["chunk"],
+                                       simd=case["simd"])
+            case = dict(case)
+            case["queries"] = [q.decode() for q in queries]
+            case["records"] = [r.decode() for r in records]
+            case["expected"] = [{"ovf8": r["ovf8"], "ovf16": r["ovf16"],
+                                 "hits": [[h["id"], h["score"], h["cigar"], h["q_start"], h["q_end"], h["d_start"],
+                                           h["d_end"], h["strand"], h["frame"], h["qstrand"], h["qframe"]]
+                                          for h in r["hits"]]} for r in res]
+            res_all.append(case)
+            print(case["name"], "records", len(records))
+    with open(os.path.join(HERE, "frame_cases.json"), "w") as f:
+        json.dump(res_all, f, indent=0)
+
+
+def write_genetic_codes() -> None:
+    """The reference's translation of every nucleotide triple, per genetic code."""
+    import subprocess
+    codes = {}
+    for gc in [1, 2, 3, 4, 5, 6, 9, 10, 11, 12, 13, 14, 15, 16, 21, 22, 23]:
+        out = subprocess.run([oracle.REF_RUN, "--dump-translation", str(gc)], check=True, capture_output=True,
+                             text=True).stdout
+        codes[str(gc)] = json.loads(out)
+    with open(os.path.join(HERE, "genetic_codes.json"), "w") as f:
+        json.dump(codes, f)
+
+
 def write_abi_layout(reference: str) -> None:
     import subprocess
     import tempfile
@@ -137,11 +255,17 @@ def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
     ap.add_argument("--abi-only", action="store_true", help="only regenerate abi_layout.json")
+    ap.add_argument("--frames-only", action="store_true",
+                    help="only regenerate frame_cases.json and genetic_codes.json")
     args = ap.parse_args()
     write_abi_layout(args.reference)
     if args.abi_only:
         return
     oracle.build(args.reference)
+    write_genetic_codes()
+    write_frame_cases()
+    if args.frames_only:
+        return
     data = os.path.join(HERE, "data")
     os.makedirs(data, exist_ok=True)
     for f in DATA_FILES:

@@ -43,6 +43,11 @@ def golden_matrices() -> dict:
         return json.load(f)
 
 
+def frame_cases() -> list[dict]:
+    with open(os.path.join(GOLDEN, "frame_cases.json")) as f:
+        return json.load(f)
+
+
 def golden_cases() -> list[dict]:
     with open(os.path.join(GOLDEN, "cases.json")) as f:
         return json.load(f)
@@ -103,10 +108,12 @@ def oracle_search(algo, width, align, hits, symtype, matrix, gap, chunk, simd, q
 # --------------------------------------------------------------------------
 # product (GPU) through the C-ABI
 # --------------------------------------------------------------------------
-def product_setup(symtype, matrix, gap, chunk, simd, records: list[bytes] | None = None, db_file: str | None = None):
+def product_setup(symtype, matrix, gap, chunk, simd, records: list[bytes] | None = None, db_file: str | None = None,
+                  strands: int = 1, gencode: tuple[int, int] = (1, 1)):
+    """gencode: (query, database) genetic codes."""
     import libssa_b200 as L
     L.set_output_mode(L.OUTPUT_SILENT)
-    L.init_symbol_translation(symtype, L.FORWARD_STRAND, 1, 1)
+    L.init_symbol_translation(symtype, strands, gencode[1], gencode[0])
     if isinstance(matrix, str):
         kind, arg = matrix.split(":", 1)
         matrix = ("const", *map(int, arg.split(","))) if kind == "const" else (kind, arg)
@@ -124,7 +131,7 @@ def product_setup(symtype, matrix, gap, chunk, simd, records: list[bytes] | None
         L.load_db_memory(records)
 
 
-def product_search(algo, width, align, hits, queries: list[bytes], batch: bool = False):
+def product_search(algo, width, align, hits, queries: list[bytes], batch: bool = False, frames: bool = False):
     import libssa_b200 as L
     qs = [L.init_sequence_fasta(L.READ_FROM_STRING, q.decode("latin-1")) for q in queries]
     try:
@@ -144,5 +151,8 @@ def product_search(algo, width, align, hits, queries: list[bytes], batch: bool =
     finally:
         for q in qs:
             L.free_sequence(q)
-    out = [[(h.id, h.score, h.cigar, h.q_start, h.q_end, h.d_start, h.d_end) for h in lst] for lst in lists]
+    if frames:
+        out = [[h.key_frames() for h in lst] for lst in lists]
+    else:
+        out = [[(h.id, h.score, h.cigar, h.q_start, h.q_end, h.d_start, h.d_end) for h in lst] for lst in lists]
     return out, ovf

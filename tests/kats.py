@@ -156,3 +156,19 @@ def matches(expected: dict, hits: list[tuple], ovf: tuple[int, int] | None) -> b
     if expected["ovf"] is not None and ovf is not None and tuple(expected["ovf"]) != tuple(ovf):
         return False
     return True
+
+KATS.append({
+    # tests/algo/test_searcher.c:247-325 (test_searcher_translate_*): a nucleotide
+    # query translated in 6 frames (genetic code 3) against one protein sequence,
+    # constant scores 1/-1, gaps 1/1, chunk = hit count = 6; the heap, sorted,
+    # holds one entry per frame
+    "source": "tests/algo/test_searcher.c:247-325 (test_searcher_translate)",
+    "db": "short_AA.fas", "query": ("string", "ATGCCCAAAATTGACTTGAATAGGGGCGTGAGGAGGGGTTTTCAATACTATTTTTTG"),
+    "symtype": 2, "strands": 3, "gencode": (3, 3),
+    "matrix": ("const", 1, -1), "gap": (-1, -1), "chunk": 6,
+    "calls": [
+        (algo, w, 0, 6, simd, {"hits": [(s, 0) for s in exp], "ovf": None})
+        for w, simd in ((64, 2), (16, 0), (8, 1))
+        for algo, exp in (("nw", [-109, -109, -110, -110, -110, -113]), ("sw", [2, 2, 2, 2, 2, 1]))
+    ],
+})

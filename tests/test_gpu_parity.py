@@ -26,7 +26,8 @@ def _query(kat):
 @pytest.mark.parametrize("kat", KATS, ids=[k["source"] for k in KATS])
 def test_reference_kats(built_library, kat):
     product_setup(kat["symtype"], kat["matrix"], kat["gap"], kat["chunk"], 2,
-                  db_file=os.path.join(DATA, kat["db"]))
+                  db_file=os.path.join(DATA, kat["db"]), strands=kat.get("strands", 1),
+                  gencode=kat.get("gencode", (1, 1)))
     q = _query(kat)
     for algo, width, align, hits, simd, expected in kat["calls"]:
         import libssa_b200 as L
@@ -191,3 +192,25 @@ def test_nw16_batched_against_oracle(built_library, seed):
         if qi == 0:
             assert single[0] == exp
             assert tuple(ovf[0]) == tuple(eovf)
+
+
+from helpers import frame_cases  # noqa: E402
+
+
+@pytest.mark.parametrize("case", frame_cases(), ids=[c["name"] for c in frame_cases()])
+def test_strands_and_translated_frames(built_library, case):
+    """Nucleotide queries on one or both strands and translated queries (3 or
+    6 frames, several genetic codes): hits, tie order, CIGARs, coordinates,
+    the strand and frame fields of every hit and the overflow counters equal
+    the reference's, alone and in a batch."""
+    queries, records = case_inputs(case)
+    product_setup(case["symtype"], case["matrix"], tuple(case["gap"]), case["chunk"], case["simd"], records=records,
+                  strands=case["strands"], gencode=tuple(case["gencode"]))
+    res, ovf = product_search(case["algo"], case["width"], case["align"], case["hits"], queries, frames=True)
+    for qi in range(len(queries)):
+        exp = case["expected"][qi]
+        assert [list(r) for r in res[qi]] == exp["hits"], (case["name"], qi)
+        assert list(ovf[qi]) == [exp["ovf8"], exp["ovf16"]], (case["name"], qi)
+    batched, _ = product_search(case["algo"], case["width"], case["align"], case["hits"], queries * 3, batch=True,
+                                frames=True)
+    assert all(b == res[0] for b in batched)
