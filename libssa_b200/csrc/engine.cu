@@ -1125,7 +1125,7 @@ void Engine::traceback( const SearchRequest & req, std::vector<std::vector<Hit>>
         for( uint32_t k = 0; k < hl.size(); k++ ) {
             // the hit's query sequence; the database record's first unit (the
             // reference aligns a reverse-complement hit on the forward strand:
-            // src/util/util_sequence.c:360-375)
+            // src/util/util_sequence.c:384-402)
             const uint32_t fwd_unit = hl[k].unit - hl[k].unit % db_.upi;
             hits.push_back( TbHit{ l.second + hl[k].q_index, fwd_unit, (int32_t) hl[k].score, req.algo } );
             where.emplace_back( l.first, k );
