@@ -494,9 +494,8 @@ static SearchRequest make_request( int algo, size_t hitcount, int bit_width, int
     const Config & c = config();
     if( bit_width != BIT_WIDTH_8 && bit_width != BIT_WIDTH_16 && bit_width != BIT_WIDTH_64 )
         fatal( "\nunknown bit width provided: %d\n\n", bit_width );
-    // the reference crashes in every search of a translated database (its
-    // translated units are built and aligned from uninitialised buffers), so
-    // there is no behaviour to reproduce
+    // the reference crashes (segmentation fault) in the searches of a
+    // translated database, so there is no behaviour to reproduce
     if( c.symtype == TRANS_DB || c.symtype == TRANS_BOTH )
         fatal( "Searches of a translated database (symbol type %d) are not supported by the B200 build.",
                 c.symtype );
