@@ -467,6 +467,59 @@ def run_nw_arm(args):
     return 0
 
 
+def run_pairs_arm(args):
+    """Config 5: long pairs, each a query of 5,000-30,000 residues and a mutated
+    copy of it (85-99% identity, 1% indel events of length 1-20), BLOSUM62, gaps
+    11/1, 16-bit entry, full CIGAR.  One step aligns every pair with
+    Smith-Waterman and with Needleman-Wunsch through ssa_align_pairs (query i
+    against database sequence i alone)."""
+    import libssa_b200 as L
+    from libssa_b200 import workloads as W
+    L.load()
+    pairs = W.long_pairs(seed=5, n_pairs=args.pairs)
+    L.set_output_mode(L.OUTPUT_SILENT)
+    L.init_symbol_translation(L.AMINOACID, L.FORWARD_STRAND, 1, 1)
+    L.init_score_matrix(L.MATRIX_BUILDIN, "blosum62")
+    L.init_gap_penalties(-11, -1)
+    L.set_chunk_size(1000)
+    L.set_simd_compute_mode(L.COMPUTE_ON_AVX2)
+    L.load_db_memory([b for _, b in pairs])
+    qs = [L.init_sequence_fasta(L.READ_FROM_STRING, a.decode()) for a, _ in pairs]
+    ids = list(range(len(pairs)))
+    cells_one = sum(len(a) * len(b) for a, b in pairs)
+    cells = 2 * cells_one
+    algos = (L.SSA_SMITH_WATERMAN, L.SSA_NEEDLEMAN_WUNSCH)
+    for _ in range(args.warmup):
+        for algo in algos:
+            L.align_pairs(algo, qs, ids, L.BIT_WIDTH_16, L.COMPUTE_ALIGNMENT)
+    dev, wall, score_dev = 0.0, 0.0, 0.0
+    per_algo = {0: 0.0, 1: 0.0}
+    for _ in range(args.steps):
+        for algo in algos:
+            t0 = time.perf_counter()
+            L.align_pairs(algo, qs, ids, L.BIT_WIDTH_16, L.COMPUTE_ALIGNMENT)
+            wall += time.perf_counter() - t0
+            st = L.stats()
+            dev += st.gpu_seconds
+            score_dev += st.entry_seconds
+            per_algo[algo] += st.gpu_seconds
+    line = {"metric": "GCUPS (long-pair SW and NW alignments with CIGAR, 5k-30k residues per side)",
+            "value": round(cells * args.steps / dev / 1e9, 2), "unit": "GCUPS", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "int32", "data": "synthetic (seeded, BASELINE config 5 shapes)",
+            "config": {"workload": "long_pairs", "pairs": len(pairs), "algorithms": ["sw", "nw"],
+                       "cells_per_step": cells, "bit_width": 16},
+            "e2e": {"value": round(cells * args.steps / wall / 1e9, 2), "unit": "GCUPS"},
+            "timing": {"device_seconds": round(dev, 4), "wall_seconds": round(wall, 4),
+                       "sw_seconds": round(per_algo[0], 4), "nw_seconds": round(per_algo[1], 4),
+                       "pair_score_seconds": round(score_dev, 4),
+                       "pair_score_gcups": round(cells * args.steps / score_dev / 1e9, 2)}}
+    print(json.dumps(line), flush=True)
+    for q in qs:
+        L.free_sequence(q)
+    return 0
+
+
 def run_served_arm(args):
     import libssa_b200 as L
     L.load()
@@ -497,9 +550,10 @@ def main():
     ap.add_argument("--served-slots", type=int, default=64, help="resident query slots of the server")
     ap.add_argument("--served-segments", type=int, default=8, help="database segments per scan turn")
     ap.add_argument("--served-scale", type=float, default=1.0, help="served database scale (1.0 = 1M sequences)")
-    ap.add_argument("--workload", default="sw_batched", choices=["sw_batched", "sw_plain", "sw_served", "nw_nucleotide"],
+    ap.add_argument("--workload", default="sw_batched", choices=["sw_batched", "sw_plain", "sw_served", "nw_nucleotide", "long_pairs"],
                     help="sw_plain: config 1's 10,000-sequence database with --queries queries of 375")
     ap.add_argument("--queries", type=int, default=None, help="query count for --workload sw_plain")
+    ap.add_argument("--pairs", type=int, default=4096, help="pair count for --workload long_pairs")
     args = ap.parse_args()
     if args.impl == "reference":
         sys.exit(run_reference_arm(args))
@@ -507,6 +561,8 @@ def main():
         sys.exit(run_served_arm(args))
     if args.workload == "nw_nucleotide":
         sys.exit(run_nw_arm(args))
+    if args.workload == "long_pairs":
+        sys.exit(run_pairs_arm(args))
     sys.exit(run_ours(args))
 
 

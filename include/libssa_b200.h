@@ -32,6 +32,29 @@ extern "C" {
 int ssa_align_batch( int algorithm, p_query * queries, size_t n_queries, size_t hitcount, int bit_width,
         int align_type, p_alignment_list * results );
 
+/*
+ * Long-pair batch: queries[i] is aligned against the database sequence with ID
+ * db_ids[i] (0-based, in plugin order) and nothing else.  results[i] receives
+ * exactly the list that sw_align/nw_align(queries[i], 1, bit_width,
+ * align_type) returns against a database holding only that sequence: one hit
+ * with its score (and CIGAR and coordinates for COMPUTE_ALIGNMENT), or an
+ * empty list for an empty sequence; db_seq.ID is db_ids[i].  A reference
+ * caller does this with one init_db and one sw_align/nw_align per pair
+ * (src/libssa.c:126-132, :229-251).  One warp scores each pair exactly, which
+ * is what every entry width of the reference reports for one sequence, as
+ * long as the width holds the score table and gap costs untruncated.  Returns
+ * 0; -1 (message on stderr) for settings outside that: a table entry or
+ * gapO + gapE outside the width's range, positive gap costs, a translated or
+ * two-strand setup, an ID past the database.  Other errors follow fatal().
+ */
+int ssa_align_pairs( int algorithm, p_query * queries, const size_t * db_ids, size_t n_pairs, int bit_width,
+        int align_type, p_alignment_list * results );
+
+/* Device memory (bytes) for the direction matrices of one traceback wave: the
+ * hits of a call whose matrices do not fit together are traced back in
+ * several waves.  0 (the default) = the free device memory less a reserve. */
+void ssa_b200_set_traceback_memory( size_t bytes );
+
 /* Counters of the last search call. */
 typedef struct {
     uint64_t overflow_8_to_16;       /* sequences re-aligned at 16 bit */

@@ -38,7 +38,7 @@ EXPORTED = [
     "free_sequence", "sw_align", "nw_align", "free_alignment", "ssa_exit", "ssa_align_batch", "ssa_get_stats",
     "ssa_query_length", "ssa_db_refresh", "ssa_b200_int_peak", "ssa_b200_score64_noalloc",
     "ssa_server_start", "ssa_server_submit", "ssa_server_wait", "ssa_server_get_stats", "ssa_server_stop",
-    "ssa_b200_translation_table",
+    "ssa_b200_translation_table", "ssa_align_pairs", "ssa_b200_set_traceback_memory",
 ]
 
 # allocation-free scoring (include/libssa_b200.h)
@@ -115,6 +115,10 @@ def load():
     lib.ssa_align_batch.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p), ctypes.c_size_t,
                                     ctypes.c_size_t, ctypes.c_int, ctypes.c_int, ctypes.POINTER(P_LIST)]
     lib.ssa_align_batch.restype = ctypes.c_int
+    lib.ssa_align_pairs.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_size_t),
+                                    ctypes.c_size_t, ctypes.c_int, ctypes.c_int, ctypes.POINTER(P_LIST)]
+    lib.ssa_align_pairs.restype = ctypes.c_int
+    lib.ssa_b200_set_traceback_memory.argtypes = [ctypes.c_size_t]
     lib.ssa_get_stats.argtypes = [ctypes.POINTER(Stats)]
     lib.ssa_db_refresh.argtypes = []
     lib.ssa_b200_int_peak.argtypes = [ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
@@ -268,6 +272,34 @@ def align_batch(algorithm: int, queries: list, hitcount: int, bit_width: int, al
         out.append(_read_list(res[i]))
         lib.free_alignment(res[i])
     return out
+
+
+def align_pairs(algorithm: int, queries: list, db_ids: list[int], bit_width: int, align_type: int) -> list[list[Hit]]:
+    """Long-pair batch: query handle i against database sequence db_ids[i] alone.
+
+    Each list equals sw_align / nw_align(queries[i], 1, ...) against a database
+    holding only that sequence (one hit, or none for an empty sequence), with the
+    hit's ID db_ids[i].  Raises ValueError for settings the call refuses.
+    """
+    lib = load()
+    n = len(queries)
+    if len(db_ids) != n:
+        raise ValueError("one database ID per query")
+    qarr = (ctypes.c_void_p * max(1, n))(*queries)
+    ids = (ctypes.c_size_t * max(1, n))(*db_ids)
+    res = (P_LIST * max(1, n))()
+    if lib.ssa_align_pairs(algorithm, qarr, ids, n, bit_width, align_type, res) != 0:
+        raise ValueError("ssa_align_pairs refused the settings or IDs")
+    out = []
+    for i in range(n):
+        out.append(_read_list(res[i]))
+        lib.free_alignment(res[i])
+    return out
+
+
+def set_traceback_memory(nbytes: int) -> None:
+    """Direction-matrix memory of one traceback wave (0 = automatic)."""
+    load().ssa_b200_set_traceback_memory(nbytes)
 
 
 def stats() -> Stats:

@@ -844,6 +844,75 @@ int ssa_align_batch( int algorithm, p_query * queries, size_t n_queries, size_t 
     return 0;
 }
 
+// Long pairs: queries[i] against database sequence db_ids[i] alone.  The
+// reference's equivalent is init_db of that one sequence and
+// sw_align / nw_align( queries[i], 1, bit_width, align_type ) per pair; every
+// entry width of the reference reports the exact score there (a saturated lane
+// is searched again at the next width), which is what the pair kernel computes,
+// provided the narrow lanes hold the score table and gap costs untruncated.
+int ssa_align_pairs( int algorithm, p_query * queries, const size_t * db_ids, size_t n_pairs, int bit_width,
+        int align_type, p_alignment_list * results ) {
+    if( algorithm != SSA_SMITH_WATERMAN && algorithm != SSA_NEEDLEMAN_WUNSCH )
+        fatal( "\nUnknown search type: %d\n\n", algorithm );
+    if( n_pairs == 0 )
+        return 0;
+    if( !queries || !db_ids || !results )
+        fatal( "Query not initialized." );
+    for( size_t i = 0; i < n_pairs; i++ )
+        test_configuration( queries[i] );
+    const Config & c = config();
+    SearchRequest req = make_request( algorithm == SSA_SMITH_WATERMAN ? 0 : 1, 1, bit_width, align_type );
+    if( c.symtype == TRANS_QUERY || (c.symtype == NUCLEOTIDE && c.strands != FORWARD_STRAND) ) {
+        print_error( "ssa_align_pairs: translated or two-strand searches are not supported" );
+        return -1;
+    }
+    if( c.gap_open > 0 || c.gap_extend > 0 ) {
+        print_error( "ssa_align_pairs: positive gap costs are not supported" );
+        return -1;
+    }
+    const int64_t lo = bit_width == BIT_WIDTH_8 ? INT8_MIN : bit_width == BIT_WIDTH_16 ? INT16_MIN : INT64_MIN;
+    const int64_t hi = bit_width == BIT_WIDTH_8 ? INT8_MAX : bit_width == BIT_WIDTH_16 ? INT16_MAX : INT64_MAX;
+    bool fits = (int64_t) c.gap_open + c.gap_extend >= lo;
+    for( int k = 0; k < 1024; k++ )
+        fits = fits && c.matrix[k] >= lo && c.matrix[k] <= hi;
+    if( !fits ) {
+        print_error( "ssa_align_pairs: the score matrix or the gap costs do not fit the %d-bit entry width", bit_width );
+        return -1;
+    }
+    const HostDb & db = engine_database();
+    if( db.upi != 1 ) {
+        print_error( "ssa_align_pairs: translated or two-strand searches are not supported" );
+        return -1;
+    }
+    std::vector<QueryCodes> qc( n_pairs );
+    std::vector<uint32_t> units( n_pairs );
+    for( size_t i = 0; i < n_pairs; i++ ) {
+        if( queries[i]->symtype != c.symtype )
+            fatal( "Query was read with a different symbol type than the current one." );
+        if( queries[i]->len == 0 )
+            fatal( "Query sequence is empty." );
+        const QueryFrame & f = (*queries[i]->frames)[0];
+        qc[i] = QueryCodes{ (const uint8_t *) f.seq.data(), (uint32_t) (f.seq.size() - 1) };
+        if( db_ids[i] >= db.n_records ) {
+            print_error( "ssa_align_pairs: database ID %zu out of range (%zu sequences)", db_ids[i],
+                    (size_t) db.n_records );
+            return -1;
+        }
+        units[i] = (uint32_t) db_ids[i];
+    }
+    std::vector<std::vector<Hit>> hits;
+    SearchStats st;
+    engine_align_pairs( req, qc, units, hits, st );
+    g_last_stats = st;
+    for( size_t i = 0; i < n_pairs; i++ )
+        results[i] = make_list( hits[i], queries[i], align_type == COMPUTE_ALIGNMENT );
+    return 0;
+}
+
+void ssa_b200_set_traceback_memory( size_t bytes ) {
+    engine_set_traceback_memory( (uint64_t) bytes );
+}
+
 void ssa_get_stats( ssa_stats_t * out ) {
     if( !out )
         return;

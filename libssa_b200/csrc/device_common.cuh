@@ -86,6 +86,9 @@ struct TbRegion {
     int32_t status;           // 0 ok, 1 no positive cell, 2 reverse pass found nothing
 };
 
+// Query rows per 16-bit direction word (2 bits per cell).
+constexpr int TB_WORD_ROWS = 8;
+
 struct TbParams {
     DbView db;
     const uint8_t * qcodes;     // per slot
@@ -115,7 +118,8 @@ cudaError_t launch_emul( int algo, int width, const EmulParams & p, int grid, cu
 cudaError_t launch_build_profile32( const uint8_t * qcodes, const uint64_t * qoff, const uint32_t * qlen,
         const uint32_t * qpad, const uint64_t * prof_off, const int64_t * matrix, int width, int32_t * prof,
         uint32_t n_slots, cudaStream_t st );
-cudaError_t launch_traceback( const TbParams & p, bool any_sw, int grid, cudaStream_t st, cudaEvent_t * ev );
+cudaError_t launch_tb_regions( const TbParams & p, int grid, cudaStream_t st, cudaEvent_t * ev );
+cudaError_t launch_tb_paths( const TbParams & p, int grid, cudaStream_t st, cudaEvent_t * ev );
 
 
 // ---- fast Smith-Waterman entry pass (sw_fast_kernel.cu) --------------------
@@ -199,5 +203,30 @@ cudaError_t launch_nw_qpair( int R, const QPairParams & p, int grid, cudaStream_
 cudaError_t launch_build_profile_qp( const uint8_t * qcodes, const uint64_t * qoff, const uint32_t * qlen,
         const uint32_t * qp_slots, uint32_t n_qp, const uint32_t * qp_rows, const int64_t * matrix, uint32_t * prof,
         const uint64_t * prof_off, int width, cudaStream_t st );
+
+// ---- long pairs (pair_kernel.cu) ---------------------------------------------
+// One warp scores one (query, database sequence) pair exactly in int32: lane k
+// owns PAIR_R query rows of a stripe of 32 x PAIR_R rows.
+constexpr int PAIR_R = 16;
+constexpr int PAIR_THREADS = 256;
+
+struct PairScoreParams {
+    DbView db;
+    const uint8_t * qcodes;       // per query slot: codes at qoff[slot]
+    const uint64_t * qoff;
+    const uint32_t * qlen;
+    const uint32_t * pair_slot;   // per pair, in work order (largest first): query slot
+    const uint32_t * pair_unit;   // per pair: database unit
+    uint32_t n_pairs;
+    const int64_t * matrix;       // 32 x 32, [database code][query code]
+    int gap_open, gap_extend;
+    int32_t * score;              // per pair, in work order
+    int4 * scratch;               // per warp: scratch_cols boundary columns (H, F)
+    uint32_t scratch_cols;
+    unsigned long long * counter;
+    unsigned * error_flags;
+};
+
+cudaError_t launch_pair_score( int algo, const PairScoreParams & p, int grid, cudaStream_t st, int * blocks_per_sm );
 
 }  // namespace ssa

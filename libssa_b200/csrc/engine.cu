@@ -302,6 +302,10 @@ public:
     // ---- search ----------------------------------------------------------------
     void search( const SearchRequest & req, const std::vector<QueryCodes> & queries,
             const std::vector<uint32_t> & groups, std::vector<std::vector<Hit>> & out, SearchStats & stats );
+    // query i against database unit units[i] alone
+    void align_pairs( const SearchRequest & req, const std::vector<QueryCodes> & queries,
+            const std::vector<uint32_t> & units, std::vector<std::vector<Hit>> & out, SearchStats & stats );
+    void set_traceback_budget( uint64_t bytes ) { tb_budget_ = bytes; }
 
     void shutdown() {
         DevBuf * bufs[] = { &d_codes_, &d_off_, &d_len_, &d_order_, &d_pair_res_, &d_pair_off_, &d_pair_cols_,
@@ -310,7 +314,7 @@ public:
             &d_prof_off_, &d_prof_, &d_matrix_, &d_score_, &d_list_a_, &d_list_b_, &d_counts_, &d_scratch_,
             &d_tb_hits_, &d_tb_regions_, &d_tb_last_, &d_tb_last_off_, &d_tb_dirs_, &d_tb_dir_off_, &d_tb_ops_,
             &d_tb_ops_off_, &d_tb_ops_len_, &d_qp_prof_, &d_qp_off_, &d_qp_rows_, &d_qp_slots_, &d_qp_units_,
-            &d_serve_score_, &d_qp_lmax_ };
+            &d_serve_score_, &d_qp_lmax_, &d_pair_slot_, &d_pair_unit_, &d_pair_score_ };
         for( DevBuf * b : bufs )
             b->release();
         h_score_.release();
@@ -347,6 +351,8 @@ private:
     void build_profiles( int width, uint32_t n_slots );
     void traceback( const SearchRequest & req, std::vector<std::vector<Hit>> & out,
             const std::vector<std::pair<uint32_t, uint32_t>> & lists, SearchStats & stats );
+    uint64_t traceback_budget();
+    void upload_queries( const QueryCodes * queries, uint32_t nq, bool profiles, SearchStats & stats );
 
     bool ready_ = false;
     int device_ = 0;
@@ -383,6 +389,8 @@ private:
     DevBuf d_tb_hits_, d_tb_regions_, d_tb_last_, d_tb_last_off_, d_tb_dirs_, d_tb_dir_off_, d_tb_ops_,
             d_tb_ops_off_, d_tb_ops_len_;
     PinnedBuf h_score_;
+    DevBuf d_pair_slot_, d_pair_unit_, d_pair_score_;
+    uint64_t tb_budget_ = 0;         // traceback direction memory per wave (0 = automatic)
 
     // per-batch query layout
     std::vector<uint64_t> h_qoff_;
@@ -938,40 +946,9 @@ void Engine::search( const SearchRequest & req, const std::vector<QueryCodes> & 
         const size_t b0 = gstart[g0];
         const uint32_t nq = (uint32_t) (gstart[g1] - b0);
         // ---- upload queries
-        h_qoff_.assign( nq, 0 );
-        h_qlen_.assign( nq, 0 );
-        h_qpad_.assign( nq, 0 );
-        h_prof_off_.assign( nq, 0 );
-        uint64_t qtotal = 0, ptotal = 0;
-        max_qlen_ = 0;
-        for( uint32_t s = 0; s < nq; s++ ) {
-            const QueryCodes & q = queries[b0 + s];
-            h_qoff_[s] = qtotal;
-            h_qlen_[s] = q.len;
-            h_qpad_[s] = std::max<uint32_t>( 256, (q.len + 255u) & ~255u );
-            h_prof_off_[s] = ptotal;
-            qtotal += (q.len + 15u) & ~15u;
-            ptotal += 32ull * h_qpad_[s];
-            max_qlen_ = std::max( max_qlen_, q.len );
-            stats.cells += (uint64_t) q.len * db.residues;
-        }
-        std::vector<uint8_t> hq( qtotal + 16, 0 );
-        for( uint32_t s = 0; s < nq; s++ )
-            memcpy( hq.data() + h_qoff_[s], queries[b0 + s].codes, queries[b0 + s].len );
-        d_qcodes_.ensure( hq.size() );
-        d_qoff_.ensure( nq * sizeof(uint64_t) );
-        d_qlen_.ensure( nq * sizeof(uint32_t) );
-        d_qpad_.ensure( nq * sizeof(uint32_t) );
-        d_prof_off_.ensure( nq * sizeof(uint64_t) );
-        d_prof_.ensure( ptotal * sizeof(int32_t) );
-        stats.h2d_bytes += hq.size() + nq * (2 * sizeof(uint64_t) + 2 * sizeof(uint32_t));
-        CUDA_CHECK( cudaMemcpyAsync( d_qcodes_.p, hq.data(), hq.size(), cudaMemcpyHostToDevice, stream_ ) );
-        CUDA_CHECK( cudaMemcpyAsync( d_qoff_.p, h_qoff_.data(), nq * sizeof(uint64_t), cudaMemcpyHostToDevice, stream_ ) );
-        CUDA_CHECK( cudaMemcpyAsync( d_qlen_.p, h_qlen_.data(), nq * sizeof(uint32_t), cudaMemcpyHostToDevice, stream_ ) );
-        CUDA_CHECK( cudaMemcpyAsync( d_qpad_.p, h_qpad_.data(), nq * sizeof(uint32_t), cudaMemcpyHostToDevice, stream_ ) );
-        CUDA_CHECK( cudaMemcpyAsync( d_prof_off_.p, h_prof_off_.data(), nq * sizeof(uint64_t), cudaMemcpyHostToDevice,
-                stream_ ) );
-        prof_width_ = -1;
+        upload_queries( queries.data() + b0, nq, true, stats );
+        for( uint32_t q = 0; q < nq; q++ )
+            stats.cells += (uint64_t) h_qlen_[q] * db.residues;
 
         // ---- result and re-queue buffers
         const uint64_t n_pairs = (uint64_t) nq * n_ne;
@@ -1116,6 +1093,53 @@ void Engine::search( const SearchRequest & req, const std::vector<QueryCodes> & 
     stats.kernel_launches = launches_.load();
 }
 
+// Query codes of one batch to the device (slot s = queries[s]); profiles: also
+// size the int32 profile buffer of the lane emulation.
+void Engine::upload_queries( const QueryCodes * queries, uint32_t nq, bool profiles, SearchStats & stats ) {
+    h_qoff_.assign( nq, 0 );
+    h_qlen_.assign( nq, 0 );
+    h_qpad_.assign( nq, 0 );
+    h_prof_off_.assign( nq, 0 );
+    uint64_t qtotal = 0, ptotal = 0;
+    max_qlen_ = 0;
+    for( uint32_t s = 0; s < nq; s++ ) {
+        const QueryCodes & q = queries[s];
+        h_qoff_[s] = qtotal;
+        h_qlen_[s] = q.len;
+        h_qpad_[s] = std::max<uint32_t>( 256, (q.len + 255u) & ~255u );
+        h_prof_off_[s] = ptotal;
+        qtotal += (q.len + 15u) & ~15u;
+        ptotal += 32ull * h_qpad_[s];
+        max_qlen_ = std::max( max_qlen_, q.len );
+    }
+    std::vector<uint8_t> hq( qtotal + 16, 0 );
+    for( uint32_t s = 0; s < nq; s++ )
+        memcpy( hq.data() + h_qoff_[s], queries[s].codes, queries[s].len );
+    d_qcodes_.ensure( hq.size() );
+    d_qoff_.ensure( nq * sizeof(uint64_t) );
+    d_qlen_.ensure( nq * sizeof(uint32_t) );
+    d_qpad_.ensure( nq * sizeof(uint32_t) );
+    d_prof_off_.ensure( nq * sizeof(uint64_t) );
+    if( profiles )
+        d_prof_.ensure( ptotal * sizeof(int32_t) );
+    stats.h2d_bytes += hq.size() + nq * (2 * sizeof(uint64_t) + 2 * sizeof(uint32_t));
+    CUDA_CHECK( cudaMemcpyAsync( d_qcodes_.p, hq.data(), hq.size(), cudaMemcpyHostToDevice, stream_ ) );
+    CUDA_CHECK( cudaMemcpyAsync( d_qoff_.p, h_qoff_.data(), nq * sizeof(uint64_t), cudaMemcpyHostToDevice, stream_ ) );
+    CUDA_CHECK( cudaMemcpyAsync( d_qlen_.p, h_qlen_.data(), nq * sizeof(uint32_t), cudaMemcpyHostToDevice, stream_ ) );
+    CUDA_CHECK( cudaMemcpyAsync( d_qpad_.p, h_qpad_.data(), nq * sizeof(uint32_t), cudaMemcpyHostToDevice, stream_ ) );
+    CUDA_CHECK( cudaMemcpyAsync( d_prof_off_.p, h_prof_off_.data(), nq * sizeof(uint64_t), cudaMemcpyHostToDevice,
+            stream_ ) );
+    prof_width_ = -1;
+}
+
+// Largest magnitude of one DP step: a score-table entry or a gap cost.
+static int64_t max_abs_step( const SearchRequest & req ) {
+    int64_t m = std::llabs( (int64_t) req.gap_open ) + std::llabs( (int64_t) req.gap_extend );
+    for( int k = 0; k < 1024; k++ )
+        m = std::max<int64_t>( m, std::llabs( req.matrix[k] ) );
+    return m;
+}
+
 void Engine::traceback( const SearchRequest & req, std::vector<std::vector<Hit>> & out,
         const std::vector<std::pair<uint32_t, uint32_t>> & lists, SearchStats & stats ) {
     std::vector<TbHit> hits;
@@ -1151,11 +1175,9 @@ void Engine::traceback( const SearchRequest & req, std::vector<std::vector<Hit>>
         where.swap( ws );
     }
     // value range guard: every DP value is bounded by (q + d) * max |step|
-    int64_t mabs = std::abs( (int64_t) req.gap_open ) + std::abs( (int64_t) req.gap_extend );
-    for( int k = 0; k < 1024; k++ )
-        mabs = std::max<int64_t>( mabs, std::llabs( req.matrix[k] ) );
+    const int64_t mabs = max_abs_step( req );
     std::vector<TbRegion> regions( nh );
-    std::vector<uint64_t> last_off( nh + 1, 0 ), dir_off( nh + 1, 0 ), ops_off( nh + 1, 0 );
+    std::vector<uint64_t> last_off( nh + 1, 0 );
     for( uint32_t h = 0; h < nh; h++ ) {
         const uint32_t A = h_qlen_[hits[h].qslot], B = db_.len[hits[h].id];
         if( (int64_t) (A + B + 4) * (mabs + 1) * 2 > INT32_MAX )
@@ -1170,10 +1192,8 @@ void Engine::traceback( const SearchRequest & req, std::vector<std::vector<Hit>>
         }
         regions[h] = rg;
         last_off[h + 1] = last_off[h] + A;
-        dir_off[h + 1] = dir_off[h] + (uint64_t) B * ((A + 7) / 8);
-        ops_off[h + 1] = ops_off[h] + A + B + 1;
     }
-    TbParams p;
+    TbParams p{};
     p.db = db_view();
     p.qcodes = d_qcodes_.as<uint8_t>();
     p.qoff = d_qoff_.as<uint64_t>();
@@ -1181,41 +1201,169 @@ void Engine::traceback( const SearchRequest & req, std::vector<std::vector<Hit>>
     p.matrix = d_matrix_.as<int64_t>();
     p.gap_open = req.gap_open;
     p.gap_extend = req.gap_extend;
-    p.hits = (const TbHit *) d_tb_hits_.ensure( nh * sizeof(TbHit) );
-    p.n_hits = nh;
-    p.regions = (TbRegion *) d_tb_regions_.ensure( nh * sizeof(TbRegion) );
+    p.error_flags = d_counts_.as<unsigned>() + 2;
+    p.hit_counters = d_counts_.as<unsigned long long>() + 12;   // bytes 96..119
     const int grid = sms_ * 2;
     const uint32_t cols = db_.max_len + 4;
     const bool multi = max_qlen_ > 256;
     p.scratch = multi ? (int4 *) d_scratch_.ensure( (size_t) grid * 8 * cols * sizeof(int4) ) : nullptr;
     p.scratch_cols = multi ? cols : 0;
-    int32_t * last = (int32_t *) d_tb_last_.ensure( 2 * last_off[nh] * sizeof(int32_t) + 16 );
-    p.last_h = last;
-    p.last_e = last + last_off[nh];
-    p.last_off = (const uint64_t *) d_tb_last_off_.ensure( (nh + 1) * sizeof(uint64_t) );
-    p.dirs = (uint16_t *) d_tb_dirs_.ensure( dir_off[nh] * sizeof(uint16_t) + 16 );
-    p.dir_off = (const uint64_t *) d_tb_dir_off_.ensure( (nh + 1) * sizeof(uint64_t) );
-    p.ops = (char *) d_tb_ops_.ensure( ops_off[nh] + 16 );
-    p.ops_off = (const uint64_t *) d_tb_ops_off_.ensure( (nh + 1) * sizeof(uint64_t) );
-    p.ops_len = (uint32_t *) d_tb_ops_len_.ensure( nh * sizeof(uint32_t) );
-    p.error_flags = d_counts_.as<unsigned>() + 2;
-    p.hit_counters = d_counts_.as<unsigned long long>() + 12;   // bytes 96..119
-    CUDA_CHECK( cudaMemsetAsync( p.hit_counters, 0, 3 * sizeof(unsigned long long), stream_ ) );
-    CUDA_CHECK( cudaMemcpyAsync( (void *) p.hits, hits.data(), nh * sizeof(TbHit), cudaMemcpyHostToDevice, stream_ ) );
-    CUDA_CHECK( cudaMemcpyAsync( p.regions, regions.data(), nh * sizeof(TbRegion), cudaMemcpyHostToDevice, stream_ ) );
-    CUDA_CHECK( cudaMemcpyAsync( (void *) p.last_off, last_off.data(), (nh + 1) * sizeof(uint64_t),
-            cudaMemcpyHostToDevice, stream_ ) );
-    CUDA_CHECK( cudaMemcpyAsync( (void *) p.dir_off, dir_off.data(), (nh + 1) * sizeof(uint64_t),
-            cudaMemcpyHostToDevice, stream_ ) );
-    CUDA_CHECK( cudaMemcpyAsync( (void *) p.ops_off, ops_off.data(), (nh + 1) * sizeof(uint64_t),
-            cudaMemcpyHostToDevice, stream_ ) );
     const bool timing = getenv( "SSA_B200_TIMING" ) != nullptr;
-    CUDA_CHECK( launch_traceback( p, req.algo == 0, grid, stream_, timing ? ev_tb_ : nullptr ) );
+    float t_fwd = 0, t_rev = 0, t_dir = 0, t_walk = 0;
+    auto check_errors = [&]() {
+        unsigned err = 0;
+        CUDA_CHECK( cudaMemcpyAsync( &err, d_counts_.as<unsigned>() + 2, sizeof(unsigned), cudaMemcpyDeviceToHost,
+                stream_ ) );
+        CUDA_CHECK( cudaStreamSynchronize( stream_ ) );
+        if( err )
+            fatal( "Internal error in the GPU traceback (flags 0x%x).", err );
+    };
+
+    // ---- region phase (Smith-Waterman): end cell and begin cell of every hit
+    if( req.algo == 0 ) {
+        p.hits = (const TbHit *) d_tb_hits_.ensure( nh * sizeof(TbHit) );
+        p.n_hits = nh;
+        p.regions = (TbRegion *) d_tb_regions_.ensure( nh * sizeof(TbRegion) );
+        int32_t * last = (int32_t *) d_tb_last_.ensure( 2 * last_off[nh] * sizeof(int32_t) + 16 );
+        p.last_h = last;
+        p.last_e = last + last_off[nh];
+        p.last_off = (const uint64_t *) d_tb_last_off_.ensure( (nh + 1) * sizeof(uint64_t) );
+        CUDA_CHECK( cudaMemsetAsync( p.hit_counters, 0, 3 * sizeof(unsigned long long), stream_ ) );
+        CUDA_CHECK( cudaMemcpyAsync( (void *) p.hits, hits.data(), nh * sizeof(TbHit), cudaMemcpyHostToDevice, stream_ ) );
+        CUDA_CHECK( cudaMemcpyAsync( p.regions, regions.data(), nh * sizeof(TbRegion), cudaMemcpyHostToDevice,
+                stream_ ) );
+        CUDA_CHECK( cudaMemcpyAsync( (void *) p.last_off, last_off.data(), (nh + 1) * sizeof(uint64_t),
+                cudaMemcpyHostToDevice, stream_ ) );
+        CUDA_CHECK( launch_tb_regions( p, grid, stream_, timing ? ev_tb_ : nullptr ) );
+        launches_ += 2;
+        CUDA_CHECK( cudaMemcpyAsync( regions.data(), p.regions, nh * sizeof(TbRegion), cudaMemcpyDeviceToHost,
+                stream_ ) );
+        check_errors();
+        if( timing ) {
+            CUDA_CHECK( cudaEventElapsedTime( &t_fwd, ev_tb_[0], ev_tb_[1] ) );
+            CUDA_CHECK( cudaEventElapsedTime( &t_rev, ev_tb_[1], ev_tb_[2] ) );
+        }
+        stats.h2d_bytes += nh * (sizeof(TbHit) + sizeof(TbRegion) + sizeof(uint64_t));
+        stats.d2h_bytes += nh * sizeof(TbRegion);
+    }
+
+    // ---- path phase: direction words (2 bits per cell of rows 0..a_end and
+    // columns b_begin..b_end) and the walk, in waves whose direction words fit
+    // the traceback memory; the largest hits are spread over the waves
+    std::vector<uint64_t> dir_words( nh, 0 ), ops_bytes( nh, 0 );
+    uint64_t total_dir = 0;
+    for( uint32_t h = 0; h < nh; h++ ) {
+        const TbRegion & rg = regions[h];
+        if( rg.status == 2 )
+            fatal( "Internal error in align function." );   // reference: src/algo/align.c:131
+        if( rg.status != 0 )
+            continue;
+        dir_words[h] = (uint64_t) (rg.b_end - rg.b_begin + 1) * (uint64_t) ((rg.a_end + TB_WORD_ROWS) / TB_WORD_ROWS);
+        ops_bytes[h] = (uint64_t) (rg.a_end - rg.a_begin + 1) + (uint64_t) (rg.b_end - rg.b_begin + 1) + 1;
+        total_dir += dir_words[h] * sizeof(uint16_t);
+    }
+    const uint64_t budget = traceback_budget();
+    std::vector<std::vector<uint32_t>> waves;
+    {
+        std::vector<uint64_t> load;
+        for( uint32_t h = 0; h < nh; h++ ) {
+            const uint64_t need = dir_words[h] * sizeof(uint16_t);
+            int best = -1;
+            for( size_t w = 0; w < waves.size(); w++ )
+                if( load[w] + need <= budget && (best < 0 || load[w] < load[best]) )
+                    best = (int) w;
+            if( best < 0 ) {
+                waves.emplace_back();
+                load.push_back( 0 );
+                best = (int) waves.size() - 1;
+            }
+            waves[best].push_back( h );
+            load[best] += need;
+        }
+    }
+    for( const std::vector<uint32_t> & wave : waves ) {
+        const uint32_t nw = (uint32_t) wave.size();
+        std::vector<TbHit> whits( nw );
+        std::vector<TbRegion> wregs( nw );
+        std::vector<uint64_t> wdir( nw + 1, 0 ), wops( nw + 1, 0 );
+        for( uint32_t k = 0; k < nw; k++ ) {
+            whits[k] = hits[wave[k]];
+            wregs[k] = regions[wave[k]];
+            wdir[k + 1] = wdir[k] + dir_words[wave[k]];
+            wops[k + 1] = wops[k] + ops_bytes[wave[k]];
+        }
+        p.hits = (const TbHit *) d_tb_hits_.ensure( nw * sizeof(TbHit) );
+        p.n_hits = nw;
+        p.regions = (TbRegion *) d_tb_regions_.ensure( nw * sizeof(TbRegion) );
+        p.dirs = (uint16_t *) d_tb_dirs_.ensure( wdir[nw] * sizeof(uint16_t) + 16 );
+        p.dir_off = (const uint64_t *) d_tb_dir_off_.ensure( (nw + 1) * sizeof(uint64_t) );
+        p.ops = (char *) d_tb_ops_.ensure( wops[nw] + 16 );
+        p.ops_off = (const uint64_t *) d_tb_ops_off_.ensure( (nw + 1) * sizeof(uint64_t) );
+        p.ops_len = (uint32_t *) d_tb_ops_len_.ensure( nw * sizeof(uint32_t) );
+        CUDA_CHECK( cudaMemsetAsync( p.hit_counters, 0, 3 * sizeof(unsigned long long), stream_ ) );
+        CUDA_CHECK( cudaMemcpyAsync( (void *) p.hits, whits.data(), nw * sizeof(TbHit), cudaMemcpyHostToDevice,
+                stream_ ) );
+        CUDA_CHECK( cudaMemcpyAsync( p.regions, wregs.data(), nw * sizeof(TbRegion), cudaMemcpyHostToDevice, stream_ ) );
+        CUDA_CHECK( cudaMemcpyAsync( (void *) p.dir_off, wdir.data(), (nw + 1) * sizeof(uint64_t),
+                cudaMemcpyHostToDevice, stream_ ) );
+        CUDA_CHECK( cudaMemcpyAsync( (void *) p.ops_off, wops.data(), (nw + 1) * sizeof(uint64_t),
+                cudaMemcpyHostToDevice, stream_ ) );
+        CUDA_CHECK( launch_tb_paths( p, grid, stream_, timing ? ev_tb_ + 2 : nullptr ) );
+        launches_ += 2;
+        std::vector<uint32_t> ops_len( nw );
+        std::vector<char> ops( wops[nw] + 1 );
+        CUDA_CHECK( cudaMemcpyAsync( ops_len.data(), p.ops_len, nw * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                stream_ ) );
+        CUDA_CHECK( cudaMemcpyAsync( ops.data(), p.ops, wops[nw], cudaMemcpyDeviceToHost, stream_ ) );
+        check_errors();
+        if( timing ) {
+            float a = 0, b = 0;
+            CUDA_CHECK( cudaEventElapsedTime( &a, ev_tb_[2], ev_tb_[3] ) );
+            CUDA_CHECK( cudaEventElapsedTime( &b, ev_tb_[3], ev_tb_[4] ) );
+            t_dir += a;
+            t_walk += b;
+        }
+        stats.h2d_bytes += nw * (sizeof(TbHit) + sizeof(TbRegion) + 2 * sizeof(uint64_t));
+        stats.d2h_bytes += nw * sizeof(uint32_t) + wops[nw];
+        for( uint32_t k = 0; k < nw; k++ ) {
+            const uint32_t h = wave[k];
+            Hit & hit = out[where[h].first][where[h].second];
+            const TbRegion & rg = regions[h];
+            hit.has_cigar = true;
+            if( rg.status != 0 ) {
+                // no positive cell: the reference leaves the region undefined here
+                hit.q_start = hit.q_end = hit.d_start = hit.d_end = 0;
+                hit.cigar.clear();
+                continue;
+            }
+            hit.q_start = (uint32_t) rg.a_begin;
+            hit.q_end = (uint32_t) rg.a_end;
+            hit.d_start = (uint32_t) rg.b_begin;
+            hit.d_end = (uint32_t) rg.b_end;
+            // run-length encode the moves in alignment order; counts of 1 are
+            // omitted (reference: src/algo/cigar.c:221-263)
+            const char * mv = ops.data() + wops[k];
+            uint32_t n = (uint32_t) std::min<uint64_t>( ops_len[k], wops[k + 1] - wops[k] );
+            std::string cig;
+            uint32_t i = n;
+            char buf[24];
+            while( i > 0 ) {
+                const char op = mv[i - 1];
+                uint32_t run = 0;
+                while( i > 0 && mv[i - 1] == op ) {
+                    run++;
+                    i--;
+                }
+                if( run > 1 ) {
+                    snprintf( buf, sizeof(buf), "%u", run );
+                    cig += buf;
+                }
+                cig += op;
+            }
+            hit.cigar = std::move( cig );
+        }
+    }
     if( timing ) {
-        CUDA_CHECK( cudaEventSynchronize( ev_tb_[4] ) );
-        float t[4];
-        for( int i = 0; i < 4; i++ )
-            CUDA_CHECK( cudaEventElapsedTime( &t[i], ev_tb_[i], ev_tb_[i + 1] ) );
         uint64_t max_cells = 0;
         uint32_t max_a = 0, max_b = 0;
         for( uint32_t h = 0; h < nh; h++ ) {
@@ -1227,59 +1375,143 @@ void Engine::traceback( const SearchRequest & req, std::vector<std::vector<Hit>>
             }
         }
         fprintf( stderr, "[ssa timing] traceback %u hits: forward %.3f ms, reverse %.3f ms, directions %.3f ms, "
-                "walk %.3f ms; largest hit %u x %u\n", nh, t[0], t[1], t[2], t[3], max_a, max_b );
+                "walk %.3f ms in %zu wave(s) (%.3f GB of directions); largest hit %u x %u\n", nh, t_fwd, t_rev,
+                t_dir, t_walk, waves.size(), total_dir * 1e-9, max_a, max_b );
     }
-    launches_ += (req.algo == 0) ? 4 : 2;
-    stats.h2d_bytes += nh * (sizeof(TbHit) + sizeof(TbRegion) + 3 * sizeof(uint64_t));
-    stats.d2h_bytes += nh * (sizeof(TbRegion) + sizeof(uint32_t)) + ops_off[nh];
-    std::vector<uint32_t> ops_len( nh );
-    std::vector<char> ops( ops_off[nh] + 1 );
-    CUDA_CHECK( cudaMemcpyAsync( regions.data(), p.regions, nh * sizeof(TbRegion), cudaMemcpyDeviceToHost, stream_ ) );
-    CUDA_CHECK( cudaMemcpyAsync( ops_len.data(), p.ops_len, nh * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream_ ) );
-    CUDA_CHECK( cudaMemcpyAsync( ops.data(), p.ops, ops_off[nh], cudaMemcpyDeviceToHost, stream_ ) );
-    unsigned err = 0;
-    CUDA_CHECK( cudaMemcpyAsync( &err, d_counts_.as<unsigned>() + 2, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_ ) );
-    CUDA_CHECK( cudaStreamSynchronize( stream_ ) );
-    if( err )
-        fatal( "Internal error in the GPU traceback (flags 0x%x).", err );
-    for( uint32_t h = 0; h < nh; h++ ) {
-        Hit & hit = out[where[h].first][where[h].second];
-        const TbRegion & rg = regions[h];
-        hit.has_cigar = true;
-        if( rg.status == 2 )
-            fatal( "Internal error in align function." );   // reference: src/algo/align.c:131
-        if( rg.status != 0 ) {
-            // no positive cell: the reference leaves the region undefined here
-            hit.q_start = hit.q_end = hit.d_start = hit.d_end = 0;
-            hit.cigar.clear();
-            continue;
-        }
-        hit.q_start = (uint32_t) rg.a_begin;
-        hit.q_end = (uint32_t) rg.a_end;
-        hit.d_start = (uint32_t) rg.b_begin;
-        hit.d_end = (uint32_t) rg.b_end;
-        // run-length encode the moves in alignment order; counts of 1 are
-        // omitted (reference: src/algo/cigar.c:221-263)
-        const char * mv = ops.data() + ops_off[h];
-        uint32_t n = std::min<uint64_t>( ops_len[h], ops_off[h + 1] - ops_off[h] );
-        std::string cig;
-        uint32_t k = n;
-        char buf[24];
-        while( k > 0 ) {
-            const char op = mv[k - 1];
-            uint32_t run = 0;
-            while( k > 0 && mv[k - 1] == op ) {
-                run++;
-                k--;
-            }
-            if( run > 1 ) {
-                snprintf( buf, sizeof(buf), "%u", run );
-                cig += buf;
-            }
-            cig += op;
-        }
-        hit.cigar = std::move( cig );
+}
+
+// Device memory for the direction words of one traceback wave: the setting of
+// ssa_b200_set_traceback_memory, else the free device memory (plus what the
+// direction buffer holds already) less a reserve.
+uint64_t Engine::traceback_budget() {
+    if( tb_budget_ )
+        return tb_budget_;
+    size_t free_b = 0, total_b = 0;
+    CUDA_CHECK( cudaMemGetInfo( &free_b, &total_b ) );
+    const uint64_t avail = (uint64_t) free_b + d_tb_dirs_.bytes;
+    const uint64_t reserve = std::max<uint64_t>( (uint64_t) 4 << 30, (uint64_t) total_b / 16 );
+    const uint64_t floor = (uint64_t) 256 << 20;
+    return avail > reserve + floor ? avail - reserve : floor;
+}
+
+// ---- long pairs -------------------------------------------------------------------
+// Query i against database unit units[i] alone: what sw_align / nw_align return
+// for the query against a database holding only that sequence (one hit, or
+// none for an empty sequence).  One warp scores each pair exactly
+// (pair_kernel.cu); the hits then go through the traceback like a search's.
+void Engine::align_pairs( const SearchRequest & req, const std::vector<QueryCodes> & queries,
+        const std::vector<uint32_t> & units, std::vector<std::vector<Hit>> & out, SearchStats & stats ) {
+    const HostDb & db = database();
+    serving_ = false;
+    serve_layout_ = false;      // the query buffers are reused for this batch
+    const uint32_t n = (uint32_t) queries.size();
+    out.assign( n, {} );
+    if( n == 0 )
+        return;
+    if( units.size() != n )
+        fatal( "Internal error: pairs without a database sequence." );
+    const int64_t mabs = max_abs_step( req );
+    std::vector<uint32_t> work;     // pairs with a non-empty sequence, largest first
+    uint32_t max_b = 0, max_a = 0;
+    for( uint32_t i = 0; i < n; i++ ) {
+        if( units[i] >= db.n_ids )
+            fatal( "Internal error: database unit %u out of range.", units[i] );
+        const uint32_t A = queries[i].len, B = db.len[units[i]];
+        if( (int64_t) (A + B + 4) * (mabs + 1) * 2 > INT32_MAX )
+            fatal( "Alignment of %u x %u residues exceeds the supported score range.", A, B );
+        stats.cells += (uint64_t) A * B;
+        if( B == 0 )
+            continue;       // the reference never searches an empty sequence
+        work.push_back( i );
+        max_b = std::max( max_b, B );
+        max_a = std::max( max_a, A );
     }
+    std::stable_sort( work.begin(), work.end(), [&]( uint32_t x, uint32_t y ) {
+        return (uint64_t) queries[x].len * db.len[units[x]] > (uint64_t) queries[y].len * db.len[units[y]];
+    } );
+    const bool timing = getenv( "SSA_B200_TIMING" ) != nullptr;
+    CUDA_CHECK( cudaEventRecord( ev0_, stream_ ) );
+    d_matrix_.ensure( 1024 * sizeof(int64_t) );
+    CUDA_CHECK( cudaMemcpyAsync( d_matrix_.p, req.matrix, 1024 * sizeof(int64_t), cudaMemcpyHostToDevice, stream_ ) );
+    upload_queries( queries.data(), n, false, stats );
+    d_counts_.ensure( 16 * sizeof(unsigned long long) );
+    CUDA_CHECK( cudaMemsetAsync( d_counts_.p, 0, 16 * sizeof(unsigned long long), stream_ ) );
+    const uint32_t nw = (uint32_t) work.size();
+    if( nw ) {
+        std::vector<uint32_t> hs( nw ), hu( nw );
+        for( uint32_t k = 0; k < nw; k++ ) {
+            hs[k] = work[k];
+            hu[k] = units[work[k]];
+        }
+        PairScoreParams p{};
+        p.db = db_view();
+        p.qcodes = d_qcodes_.as<uint8_t>();
+        p.qoff = d_qoff_.as<uint64_t>();
+        p.qlen = d_qlen_.as<uint32_t>();
+        p.pair_slot = (const uint32_t *) d_pair_slot_.ensure( nw * sizeof(uint32_t) );
+        p.pair_unit = (const uint32_t *) d_pair_unit_.ensure( nw * sizeof(uint32_t) );
+        p.n_pairs = nw;
+        p.matrix = d_matrix_.as<int64_t>();
+        p.gap_open = req.gap_open;
+        p.gap_extend = req.gap_extend;
+        p.score = (int32_t *) d_pair_score_.ensure( nw * sizeof(int32_t) );
+        p.counter = d_counts_.as<unsigned long long>() + 15;      // bytes 120..127
+        p.error_flags = d_counts_.as<unsigned>() + 2;
+        int per_sm = 0;
+        CUDA_CHECK( launch_pair_score( req.algo, p, 0, stream_, &per_sm ) );
+        const int grid = sms_ * std::max( 1, per_sm );
+        if( max_a > (uint32_t) (32 * PAIR_R) ) {
+            p.scratch_cols = max_b;
+            p.scratch = (int4 *) d_scratch_.ensure( (size_t) grid * (PAIR_THREADS / 32) * max_b * sizeof(int4) );
+        }
+        CUDA_CHECK( cudaMemcpyAsync( (void *) p.pair_slot, hs.data(), nw * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                stream_ ) );
+        CUDA_CHECK( cudaMemcpyAsync( (void *) p.pair_unit, hu.data(), nw * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                stream_ ) );
+        stats.h2d_bytes += 2 * nw * sizeof(uint32_t);
+        CUDA_CHECK( cudaEventRecord( ev_phase_[0], stream_ ) );
+        CUDA_CHECK( launch_pair_score( req.algo, p, grid, stream_, nullptr ) );
+        launches_++;
+        CUDA_CHECK( cudaEventRecord( ev_phase_[1], stream_ ) );
+        std::vector<int32_t> sc( nw );
+        unsigned err = 0;
+        CUDA_CHECK( cudaMemcpyAsync( sc.data(), p.score, nw * sizeof(int32_t), cudaMemcpyDeviceToHost, stream_ ) );
+        CUDA_CHECK( cudaMemcpyAsync( &err, p.error_flags, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_ ) );
+        CUDA_CHECK( cudaStreamSynchronize( stream_ ) );
+        if( err )
+            fatal( "Internal error in the GPU pair scores (flags 0x%x).", err );
+        stats.d2h_bytes += nw * sizeof(int32_t);
+        float ms = 0;
+        CUDA_CHECK( cudaEventElapsedTime( &ms, ev_phase_[0], ev_phase_[1] ) );
+        stats.entry_seconds += ms * 1e-3;
+        stats.kernel_seconds += ms * 1e-3;
+        if( timing )
+            fprintf( stderr, "[ssa timing] pair scores: %u pairs, %.3f ms\n", nw, ms );
+        for( uint32_t k = 0; k < nw; k++ ) {
+            const uint32_t i = work[k];
+            Hit h;
+            h.score = sc[k];
+            h.unit = units[i];
+            h.id = units[i] / db.upi;
+            h.q_index = 0;
+            out[i].push_back( h );
+        }
+    }
+    if( req.align_type == COMPUTE_ALIGNMENT && nw ) {
+        std::vector<std::pair<uint32_t, uint32_t>> lists;
+        for( uint32_t i = 0; i < n; i++ )
+            if( !out[i].empty() )
+                lists.emplace_back( i, i );
+        const auto t0 = std::chrono::steady_clock::now();
+        traceback( req, out, lists, stats );
+        stats.kernel_seconds += std::chrono::duration<double>( std::chrono::steady_clock::now() - t0 ).count();
+    }
+    CUDA_CHECK( cudaEventRecord( ev1_, stream_ ) );
+    CUDA_CHECK( cudaEventSynchronize( ev1_ ) );
+    float ms = 0;
+    CUDA_CHECK( cudaEventElapsedTime( &ms, ev0_, ev1_ ) );
+    stats.seconds_gpu += ms * 1e-3;
+    stats.kernel_launches = launches_.load();
 }
 
 // ---- serving -------------------------------------------------------------------
@@ -1510,6 +1742,17 @@ void engine_search( const SearchRequest & req, const std::vector<QueryCodes> & q
         const std::vector<uint32_t> & groups, std::vector<std::vector<Hit>> & out, SearchStats & stats ) {
     std::lock_guard<std::mutex> lock( g_engine_mutex );
     Engine::get().search( req, queries, groups, out, stats );
+}
+
+void engine_align_pairs( const SearchRequest & req, const std::vector<QueryCodes> & queries,
+        const std::vector<uint32_t> & units, std::vector<std::vector<Hit>> & out, SearchStats & stats ) {
+    std::lock_guard<std::mutex> lock( g_engine_mutex );
+    Engine::get().align_pairs( req, queries, units, out, stats );
+}
+
+void engine_set_traceback_memory( uint64_t bytes ) {
+    std::lock_guard<std::mutex> lock( g_engine_mutex );
+    Engine::get().set_traceback_budget( bytes );
 }
 
 const HostDb & engine_database() {

@@ -124,6 +124,12 @@ void engine_search( const SearchRequest & req, const std::vector<QueryCodes> & q
         const std::vector<uint32_t> & groups, std::vector<std::vector<Hit>> & out, SearchStats & stats );
 
 // The packed database (re-read through the plugin when stale).
+// Query i against database unit units[i] alone (one hit per pair, none for an
+// empty sequence); the hits carry alignments when req.align_type asks for them.
+void engine_align_pairs( const SearchRequest & req, const std::vector<QueryCodes> & queries,
+        const std::vector<uint32_t> & units, std::vector<std::vector<Hit>> & out, SearchStats & stats );
+// Device memory for the direction words of one traceback wave (0 = automatic).
+void engine_set_traceback_memory( uint64_t bytes );
 const HostDb & engine_database();
 void engine_invalidate_database();
 void engine_shutdown();

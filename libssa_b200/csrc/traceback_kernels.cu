@@ -21,12 +21,13 @@
 // row in global memory.  All arithmetic is exact (int32, with the host
 // guaranteeing the range), matching the reference's int64 code.
 #include "device_common.cuh"
+#include "wavefront.cuh"
 
 #include <climits>
 
 namespace ssa {
 
-constexpr int TB_R = 8;
+constexpr int TB_R = TB_WORD_ROWS;   // query rows per lane (one direction word)
 constexpr int TB_ROWS = 32 * TB_R;
 
 // The 32x32 score table is staged in shared memory as int32 by every CTA,
@@ -53,68 +54,6 @@ __device__ __forceinline__ void load_rows( const uint8_t * a, int64_t first, int
         code[r] = (r < nvalid) ? a[first + step * r] : 0;
 }
 
-
-// The previous pass's boundary row is read by lane 0 one column per step; a
-// warp stages it in shared memory 32 columns ahead so that the read is never
-// a global-memory round trip on the step's critical path.
-struct BoundaryPrefetch {
-    int4 * tile;     // 32 entries of this warp
-    int4 pf;
-    __device__ void start( const int4 * scratch, uint32_t scratch_cols, uint32_t cols, bool active, int lane ) {
-        pf = make_int4( 0, 0, 0, 0 );
-        if( active && (uint32_t) lane < scratch_cols && (uint32_t) lane < cols )
-            pf = scratch[lane];
-    }
-    __device__ void step( const int4 * scratch, uint32_t scratch_cols, uint32_t cols, bool active, uint32_t s,
-            int lane ) {
-        if( active && (s & 31u) == 0 ) {
-            __syncwarp();
-            tile[lane] = pf;
-            __syncwarp();
-            const uint32_t col = s + 32u + (uint32_t) lane;
-            if( col < scratch_cols && col < cols )
-                pf = scratch[col];
-        }
-    }
-    __device__ int4 get( uint32_t s ) const { return tile[s & 31u]; }
-};
-
-// At step s lane k works on stream position s - k, so the warp needs the
-// database residues of positions s - 31 .. s.  They are staged in a 64-entry
-// ring in shared memory, each 32 positions loaded (one per lane) 32 steps
-// before use, so no step waits on a global load.  Position x is database index
-// x, or b_end - x for the reverse pass.
-struct ResidueRing {
-    uint8_t * ring;      // 64 entries of this warp
-    uint8_t pf;          // this lane's residue for the next refill
-    const uint8_t * b;
-    int32_t n;           // positions 0 .. n - 1
-    int32_t rev_end;     // -1: forward, else b_end of the reverse pass
-    __device__ uint8_t fetch( int32_t x ) const {
-        if( x < 0 || x >= n )
-            return 0;
-        return b[rev_end < 0 ? x : rev_end - x];
-    }
-    __device__ void start( int lane ) { pf = fetch( lane ); }
-    __device__ void step( uint32_t s, int lane ) {
-        if( (s & 31u) == 0 ) {
-            __syncwarp();
-            ring[(s + (uint32_t) lane) & 63u] = pf;
-            __syncwarp();
-            pf = fetch( (int32_t) s + 32 + lane );
-        }
-    }
-    __device__ int get( uint32_t s, int lane ) const { return ring[(s - (uint32_t) lane) & 63u]; }
-};
-
-// Hits are handed out one per warp from a global counter, largest first (the
-// host sorts them), so that the longest alignments start first.
-__device__ __forceinline__ uint32_t next_hit( unsigned long long * counter, int lane ) {
-    unsigned long long v = 0;
-    if( lane == 0 )
-        v = atomicAdd( counter, 1ull );
-    return (uint32_t) __shfl_sync( 0xffffffffu, v, 0 );
-}
 
 // ---------------------------------------------------------------------------
 // 1. SW forward region pass (reference: src/algo/align.c:39-82).  The
@@ -555,26 +494,43 @@ __global__ void tb_walk_kernel( TbParams p ) {
     p.ops_len[h] = (uint32_t) n;
 }
 
-// ev (optional): 5 events recorded around the four kernels.
-cudaError_t launch_traceback( const TbParams & p, bool any_sw, int grid, cudaStream_t st, cudaEvent_t * ev ) {
-    if( p.n_hits == 0 )
-        return cudaSuccess;
+// Region phase (Smith-Waterman hits only): forward and reverse passes.  They
+// need no direction memory, so all hits of a search run in one launch each.
+// ev (optional): 3 events recorded around the two kernels.
+cudaError_t launch_tb_regions( const TbParams & p, int grid, cudaStream_t st, cudaEvent_t * ev ) {
     if( ev )
         cudaEventRecord( ev[0], st );
-    if( any_sw )
+    if( p.n_hits ) {
         tb_forward_kernel<<<grid, 256, 0, st>>>( p );
-    if( ev )
-        cudaEventRecord( ev[1], st );
-    if( any_sw )
+        if( ev )
+            cudaEventRecord( ev[1], st );
         tb_reverse_kernel<<<grid, 256, 0, st>>>( p );
+    }
+    else if( ev ) {
+        cudaEventRecord( ev[1], st );
+    }
     if( ev )
         cudaEventRecord( ev[2], st );
-    tb_directions_kernel<<<grid, 256, 0, st>>>( p );
+    return cudaGetLastError();
+}
+
+// Path phase: direction pass and walk of the hits of one wave (the hits whose
+// direction words fit the memory the host set aside).
+// ev (optional): 3 events recorded around the two kernels.
+cudaError_t launch_tb_paths( const TbParams & p, int grid, cudaStream_t st, cudaEvent_t * ev ) {
     if( ev )
-        cudaEventRecord( ev[3], st );
-    tb_walk_kernel<<<(p.n_hits + 127) / 128, 128, 0, st>>>( p );
+        cudaEventRecord( ev[0], st );
+    if( p.n_hits ) {
+        tb_directions_kernel<<<grid, 256, 0, st>>>( p );
+        if( ev )
+            cudaEventRecord( ev[1], st );
+        tb_walk_kernel<<<(p.n_hits + 127) / 128, 128, 0, st>>>( p );
+    }
+    else if( ev ) {
+        cudaEventRecord( ev[1], st );
+    }
     if( ev )
-        cudaEventRecord( ev[4], st );
+        cudaEventRecord( ev[2], st );
     return cudaGetLastError();
 }
 
