@@ -52,6 +52,7 @@ struct PassSink {
 enum ErrorBits : unsigned int {
     ERR_REQUEUE_OVERFLOW = 1u,
     ERR_SCRATCH_OVERFLOW = 2u,
+    ERR_PIPELINE = 4u,            // a stripe pipeline ran past its step bound
 };
 
 
@@ -99,7 +100,7 @@ struct TbParams {
     const TbHit * hits;
     uint32_t n_hits;
     TbRegion * regions;
-    int4 * scratch;             // per warp
+    int4 * scratch;             // per group of warps on one hit
     uint32_t scratch_cols;
     int32_t * last_h;           // per hit: forward pass last-row H (query-indexed)
     int32_t * last_e;           // per hit: forward pass last-row vertical gap
@@ -118,8 +119,9 @@ cudaError_t launch_emul( int algo, int width, const EmulParams & p, int grid, cu
 cudaError_t launch_build_profile32( const uint8_t * qcodes, const uint64_t * qoff, const uint32_t * qlen,
         const uint32_t * qpad, const uint64_t * prof_off, const int64_t * matrix, int width, int32_t * prof,
         uint32_t n_slots, cudaStream_t st );
-cudaError_t launch_tb_regions( const TbParams & p, int grid, cudaStream_t st, cudaEvent_t * ev );
-cudaError_t launch_tb_paths( const TbParams & p, int grid, cudaStream_t st, cudaEvent_t * ev );
+// group: warps per hit, 1 or 4 (scratch: one boundary row per group)
+cudaError_t launch_tb_regions( const TbParams & p, int group, int grid, cudaStream_t st, cudaEvent_t * ev );
+cudaError_t launch_tb_paths( const TbParams & p, int group, int grid, cudaStream_t st, cudaEvent_t * ev );
 
 
 // ---- fast Smith-Waterman entry pass (sw_fast_kernel.cu) --------------------
@@ -205,9 +207,10 @@ cudaError_t launch_build_profile_qp( const uint8_t * qcodes, const uint64_t * qo
         const uint64_t * prof_off, int width, cudaStream_t st );
 
 // ---- long pairs (pair_kernel.cu) ---------------------------------------------
-// One warp scores one (query, database sequence) pair exactly in int32: lane k
-// owns PAIR_R query rows of a stripe of 32 x PAIR_R rows.
+// A group of PAIR_W warps scores one (query, database sequence) pair exactly in
+// int32: lane k of a warp owns PAIR_R query rows of a stripe of 32 x PAIR_R rows.
 constexpr int PAIR_R = 16;
+constexpr int PAIR_W = 4;
 constexpr int PAIR_THREADS = 256;
 
 struct PairScoreParams {
@@ -221,7 +224,7 @@ struct PairScoreParams {
     const int64_t * matrix;       // 32 x 32, [database code][query code]
     int gap_open, gap_extend;
     int32_t * score;              // per pair, in work order
-    int4 * scratch;               // per warp: scratch_cols boundary columns (H, F)
+    int4 * scratch;               // per group of PAIR_W warps: scratch_cols boundary columns (H, F)
     uint32_t scratch_cols;
     unsigned long long * counter;
     unsigned * error_flags;

@@ -314,7 +314,7 @@ public:
             &d_prof_off_, &d_prof_, &d_matrix_, &d_score_, &d_list_a_, &d_list_b_, &d_counts_, &d_scratch_,
             &d_tb_hits_, &d_tb_regions_, &d_tb_last_, &d_tb_last_off_, &d_tb_dirs_, &d_tb_dir_off_, &d_tb_ops_,
             &d_tb_ops_off_, &d_tb_ops_len_, &d_qp_prof_, &d_qp_off_, &d_qp_rows_, &d_qp_slots_, &d_qp_units_,
-            &d_serve_score_, &d_qp_lmax_, &d_pair_slot_, &d_pair_unit_, &d_pair_score_ };
+            &d_serve_score_, &d_qp_lmax_, &d_pair_slot_, &d_pair_unit_, &d_pair_score_, &d_scratch4_ };
         for( DevBuf * b : bufs )
             b->release();
         h_score_.release();
@@ -385,7 +385,7 @@ private:
     cudaEvent_t ev_phase_[6] = {};
     cudaEvent_t ev_tb_[5] = {};   // batch start, entry pass done, cascade done, copies done, traceback
     DevBuf d_qcodes_, d_qoff_, d_qlen_, d_qpad_, d_prof_off_, d_prof_, d_matrix_;
-    DevBuf d_score_, d_list_a_, d_list_b_, d_counts_, d_scratch_;
+    DevBuf d_score_, d_list_a_, d_list_b_, d_counts_, d_scratch_, d_scratch4_;
     DevBuf d_tb_hits_, d_tb_regions_, d_tb_last_, d_tb_last_off_, d_tb_dirs_, d_tb_dir_off_, d_tb_ops_,
             d_tb_ops_off_, d_tb_ops_len_;
     PinnedBuf h_score_;
@@ -957,8 +957,8 @@ void Engine::search( const SearchRequest & req, const std::vector<QueryCodes> & 
         const uint32_t cap = (uint32_t) std::min<uint64_t>( std::max<uint64_t>( n_pairs, 1 ), 0xffffffffull );
         d_list_a_.ensure( (size_t) cap * sizeof(PairTask) );
         d_list_b_.ensure( (size_t) cap * sizeof(PairTask) );
-        d_counts_.ensure( 16 * sizeof(unsigned long long) );
-        CUDA_CHECK( cudaMemsetAsync( d_counts_.p, 0, 16 * sizeof(unsigned long long), stream_ ) );
+        d_counts_.ensure( 32 * sizeof(unsigned long long) );
+        CUDA_CHECK( cudaMemsetAsync( d_counts_.p, 0, 32 * sizeof(unsigned long long), stream_ ) );
         unsigned * cnt = d_counts_.as<unsigned>();   // [0] list a, [1] list b, [2] errors
 
         // ---- passes
@@ -1132,6 +1132,12 @@ void Engine::upload_queries( const QueryCodes * queries, uint32_t nq, bool profi
     prof_width_ = -1;
 }
 
+// Hits whose alignment runs on a group of 4 warps (stripe_pipeline.cuh): at
+// least 4 stripes of query rows and 8M cells; smaller ones run on one warp.
+static bool tb_large( uint32_t rows, uint32_t cols ) {
+    return rows > 3u * 32u * TB_WORD_ROWS && (uint64_t) rows * cols >= ((uint64_t) 1 << 23);
+}
+
 // Largest magnitude of one DP step: a score-table entry or a gap cost.
 static int64_t max_abs_step( const SearchRequest & req ) {
     int64_t m = std::llabs( (int64_t) req.gap_open ) + std::llabs( (int64_t) req.gap_extend );
@@ -1158,13 +1164,17 @@ void Engine::traceback( const SearchRequest & req, std::vector<std::vector<Hit>>
     const uint32_t nh = (uint32_t) hits.size();
     if( nh == 0 )
         return;
-    // largest alignments first: the kernels hand hits out in this order
+    // the hits of the 4-warp class first, each class largest first: the
+    // kernels hand hits out in this order
     {
         std::vector<uint32_t> perm( nh );
         for( uint32_t h = 0; h < nh; h++ )
             perm[h] = h;
         auto work = [&]( uint32_t h ) { return (uint64_t) h_qlen_[hits[h].qslot] * db_.len[hits[h].id]; };
-        std::stable_sort( perm.begin(), perm.end(), [&]( uint32_t a, uint32_t b ) { return work( a ) > work( b ); } );
+        auto large = [&]( uint32_t h ) { return tb_large( h_qlen_[hits[h].qslot], db_.len[hits[h].id] ); };
+        std::stable_sort( perm.begin(), perm.end(), [&]( uint32_t a, uint32_t b ) {
+            return large( a ) != large( b ) ? large( a ) : work( a ) > work( b );
+        } );
         std::vector<TbHit> hs( nh );
         std::vector<std::pair<uint32_t, uint32_t>> ws( nh );
         for( uint32_t h = 0; h < nh; h++ ) {
@@ -1202,12 +1212,50 @@ void Engine::traceback( const SearchRequest & req, std::vector<std::vector<Hit>>
     p.gap_open = req.gap_open;
     p.gap_extend = req.gap_extend;
     p.error_flags = d_counts_.as<unsigned>() + 2;
-    p.hit_counters = d_counts_.as<unsigned long long>() + 12;   // bytes 96..119
     const int grid = sms_ * 2;
     const uint32_t cols = db_.max_len + 4;
-    const bool multi = max_qlen_ > 256;
-    p.scratch = multi ? (int4 *) d_scratch_.ensure( (size_t) grid * 8 * cols * sizeof(int4) ) : nullptr;
-    p.scratch_cols = multi ? cols : 0;
+    constexpr uint32_t stripe_rows = 32 * TB_WORD_ROWS;
+    // boundary rows in global memory: one per warp for the 1-warp class, one
+    // per group for the 4-warp class (8 and 2 per CTA of 256 threads)
+    int4 * scratch1 = max_qlen_ > stripe_rows ? (int4 *) d_scratch_.ensure( (size_t) grid * 8 * cols * sizeof(int4) )
+                                              : nullptr;
+    int4 * scratch4 = max_qlen_ > 4 * stripe_rows
+            ? (int4 *) d_scratch4_.ensure( (size_t) grid * 2 * cols * sizeof(int4) ) : nullptr;
+    unsigned long long * counters = d_counts_.as<unsigned long long>() + 16;   // bytes 128..191
+    // Launches one phase over the hits [0, n) of the current arrays: [0, k) on
+    // groups of 4 warps, [k, n) on single warps, the two classes concurrently.
+    auto launch_split = [&]( bool region_phase, uint32_t n, uint32_t k, cudaEvent_t * ev ) {
+        TbParams p4 = p, p1 = p;
+        p4.n_hits = k;
+        p4.scratch = scratch4;
+        p4.scratch_cols = scratch4 ? cols : 0;
+        p4.hit_counters = counters;
+        p1.n_hits = n - k;
+        p1.scratch = scratch1;
+        p1.scratch_cols = scratch1 ? cols : 0;
+        p1.hit_counters = counters + 4;
+        p1.hits = p.hits + k;
+        p1.regions = p.regions + k;
+        if( p.last_off )
+            p1.last_off = p.last_off + k;
+        if( p.dir_off ) {
+            p1.dir_off = p.dir_off + k;
+            p1.ops_off = p.ops_off + k;
+            p1.ops_len = p.ops_len + k;
+        }
+        CUDA_CHECK( cudaMemsetAsync( counters, 0, 8 * sizeof(unsigned long long), stream_ ) );
+        CUDA_CHECK( cudaEventRecord( ev_ready_, stream_ ) );
+        CUDA_CHECK( cudaStreamWaitEvent( class_stream_[0], ev_ready_, 0 ) );
+        if( k )
+            CUDA_CHECK( region_phase ? launch_tb_regions( p4, 4, grid, stream_, ev )
+                                     : launch_tb_paths( p4, 4, grid, stream_, ev ) );
+        if( n > k )
+            CUDA_CHECK( region_phase ? launch_tb_regions( p1, 1, grid, class_stream_[0], k ? nullptr : ev )
+                                     : launch_tb_paths( p1, 1, grid, class_stream_[0], k ? nullptr : ev ) );
+        CUDA_CHECK( cudaEventRecord( ev_class_[0], class_stream_[0] ) );
+        CUDA_CHECK( cudaStreamWaitEvent( stream_, ev_class_[0], 0 ) );
+        launches_ += (k ? 2 : 0) + (n > k ? 2 : 0);
+    };
     const bool timing = getenv( "SSA_B200_TIMING" ) != nullptr;
     float t_fwd = 0, t_rev = 0, t_dir = 0, t_walk = 0;
     auto check_errors = [&]() {
@@ -1228,14 +1276,15 @@ void Engine::traceback( const SearchRequest & req, std::vector<std::vector<Hit>>
         p.last_h = last;
         p.last_e = last + last_off[nh];
         p.last_off = (const uint64_t *) d_tb_last_off_.ensure( (nh + 1) * sizeof(uint64_t) );
-        CUDA_CHECK( cudaMemsetAsync( p.hit_counters, 0, 3 * sizeof(unsigned long long), stream_ ) );
         CUDA_CHECK( cudaMemcpyAsync( (void *) p.hits, hits.data(), nh * sizeof(TbHit), cudaMemcpyHostToDevice, stream_ ) );
         CUDA_CHECK( cudaMemcpyAsync( p.regions, regions.data(), nh * sizeof(TbRegion), cudaMemcpyHostToDevice,
                 stream_ ) );
         CUDA_CHECK( cudaMemcpyAsync( (void *) p.last_off, last_off.data(), (nh + 1) * sizeof(uint64_t),
                 cudaMemcpyHostToDevice, stream_ ) );
-        CUDA_CHECK( launch_tb_regions( p, grid, stream_, timing ? ev_tb_ : nullptr ) );
-        launches_ += 2;
+        uint32_t k = 0;
+        while( k < nh && tb_large( h_qlen_[hits[k].qslot], db_.len[hits[k].id] ) )
+            k++;
+        launch_split( true, nh, k, timing ? ev_tb_ : nullptr );
         CUDA_CHECK( cudaMemcpyAsync( regions.data(), p.regions, nh * sizeof(TbRegion), cudaMemcpyDeviceToHost,
                 stream_ ) );
         check_errors();
@@ -1249,7 +1298,7 @@ void Engine::traceback( const SearchRequest & req, std::vector<std::vector<Hit>>
 
     // ---- path phase: direction words (2 bits per cell of rows 0..a_end and
     // columns b_begin..b_end) and the walk, in waves whose direction words fit
-    // the traceback memory; the largest hits are spread over the waves
+    // the traceback memory
     std::vector<uint64_t> dir_words( nh, 0 ), ops_bytes( nh, 0 );
     uint64_t total_dir = 0;
     for( uint32_t h = 0; h < nh; h++ ) {
@@ -1263,22 +1312,30 @@ void Engine::traceback( const SearchRequest & req, std::vector<std::vector<Hit>>
         total_dir += dir_words[h] * sizeof(uint16_t);
     }
     const uint64_t budget = traceback_budget();
+    auto region_large = [&]( uint32_t h ) {
+        const TbRegion & rg = regions[h];
+        return rg.status == 0 && tb_large( (uint32_t) rg.a_end + 1, (uint32_t) rg.b_end + 1 );
+    };
+    // waves: consecutive runs of the hits in (4-warp class first, largest
+    // direction matrix first) order, each run as long as its matrices fit
     std::vector<std::vector<uint32_t>> waves;
     {
-        std::vector<uint64_t> load;
-        for( uint32_t h = 0; h < nh; h++ ) {
+        std::vector<uint32_t> order( nh );
+        for( uint32_t h = 0; h < nh; h++ )
+            order[h] = h;
+        std::stable_sort( order.begin(), order.end(), [&]( uint32_t x, uint32_t y ) {
+            const bool lx = region_large( x ), ly = region_large( y );
+            return lx != ly ? lx : dir_words[x] > dir_words[y];
+        } );
+        uint64_t load = 0;
+        for( uint32_t h : order ) {
             const uint64_t need = dir_words[h] * sizeof(uint16_t);
-            int best = -1;
-            for( size_t w = 0; w < waves.size(); w++ )
-                if( load[w] + need <= budget && (best < 0 || load[w] < load[best]) )
-                    best = (int) w;
-            if( best < 0 ) {
+            if( waves.empty() || (load + need > budget && !waves.back().empty()) ) {
                 waves.emplace_back();
-                load.push_back( 0 );
-                best = (int) waves.size() - 1;
+                load = 0;
             }
-            waves[best].push_back( h );
-            load[best] += need;
+            waves.back().push_back( h );
+            load += need;
         }
     }
     for( const std::vector<uint32_t> & wave : waves ) {
@@ -1300,7 +1357,6 @@ void Engine::traceback( const SearchRequest & req, std::vector<std::vector<Hit>>
         p.ops = (char *) d_tb_ops_.ensure( wops[nw] + 16 );
         p.ops_off = (const uint64_t *) d_tb_ops_off_.ensure( (nw + 1) * sizeof(uint64_t) );
         p.ops_len = (uint32_t *) d_tb_ops_len_.ensure( nw * sizeof(uint32_t) );
-        CUDA_CHECK( cudaMemsetAsync( p.hit_counters, 0, 3 * sizeof(unsigned long long), stream_ ) );
         CUDA_CHECK( cudaMemcpyAsync( (void *) p.hits, whits.data(), nw * sizeof(TbHit), cudaMemcpyHostToDevice,
                 stream_ ) );
         CUDA_CHECK( cudaMemcpyAsync( p.regions, wregs.data(), nw * sizeof(TbRegion), cudaMemcpyHostToDevice, stream_ ) );
@@ -1308,8 +1364,10 @@ void Engine::traceback( const SearchRequest & req, std::vector<std::vector<Hit>>
                 cudaMemcpyHostToDevice, stream_ ) );
         CUDA_CHECK( cudaMemcpyAsync( (void *) p.ops_off, wops.data(), (nw + 1) * sizeof(uint64_t),
                 cudaMemcpyHostToDevice, stream_ ) );
-        CUDA_CHECK( launch_tb_paths( p, grid, stream_, timing ? ev_tb_ + 2 : nullptr ) );
-        launches_ += 2;
+        uint32_t k = 0;
+        while( k < nw && region_large( wave[k] ) )
+            k++;
+        launch_split( false, nw, k, timing ? ev_tb_ + 2 : nullptr );
         std::vector<uint32_t> ops_len( nw );
         std::vector<char> ops( wops[nw] + 1 );
         CUDA_CHECK( cudaMemcpyAsync( ops_len.data(), p.ops_len, nw * sizeof(uint32_t), cudaMemcpyDeviceToHost,
@@ -1434,8 +1492,8 @@ void Engine::align_pairs( const SearchRequest & req, const std::vector<QueryCode
     d_matrix_.ensure( 1024 * sizeof(int64_t) );
     CUDA_CHECK( cudaMemcpyAsync( d_matrix_.p, req.matrix, 1024 * sizeof(int64_t), cudaMemcpyHostToDevice, stream_ ) );
     upload_queries( queries.data(), n, false, stats );
-    d_counts_.ensure( 16 * sizeof(unsigned long long) );
-    CUDA_CHECK( cudaMemsetAsync( d_counts_.p, 0, 16 * sizeof(unsigned long long), stream_ ) );
+    d_counts_.ensure( 32 * sizeof(unsigned long long) );
+    CUDA_CHECK( cudaMemsetAsync( d_counts_.p, 0, 32 * sizeof(unsigned long long), stream_ ) );
     const uint32_t nw = (uint32_t) work.size();
     if( nw ) {
         std::vector<uint32_t> hs( nw ), hu( nw );
@@ -1462,7 +1520,7 @@ void Engine::align_pairs( const SearchRequest & req, const std::vector<QueryCode
         const int grid = sms_ * std::max( 1, per_sm );
         if( max_a > (uint32_t) (32 * PAIR_R) ) {
             p.scratch_cols = max_b;
-            p.scratch = (int4 *) d_scratch_.ensure( (size_t) grid * (PAIR_THREADS / 32) * max_b * sizeof(int4) );
+            p.scratch = (int4 *) d_scratch_.ensure( (size_t) grid * (PAIR_THREADS / (32 * PAIR_W)) * max_b * sizeof(int4) );
         }
         CUDA_CHECK( cudaMemcpyAsync( (void *) p.pair_slot, hs.data(), nw * sizeof(uint32_t), cudaMemcpyHostToDevice,
                 stream_ ) );
@@ -1544,7 +1602,7 @@ void Engine::serve_restore( const SearchRequest & req ) {
     d_qpad_.ensure( S * sizeof(uint32_t) );
     d_prof_off_.ensure( S * sizeof(uint64_t) );
     d_prof_.ensure( (size_t) S * 32 * SERVE_MAX_QUERY * sizeof(int32_t) );
-    d_counts_.ensure( 16 * sizeof(unsigned long long) );
+    d_counts_.ensure( 32 * sizeof(unsigned long long) );
     CUDA_CHECK( cudaMemcpyAsync( d_qoff_.p, h_qoff_.data(), S * sizeof(uint64_t), cudaMemcpyHostToDevice, stream_ ) );
     CUDA_CHECK( cudaMemcpyAsync( d_qlen_.p, h_qlen_.data(), S * sizeof(uint32_t), cudaMemcpyHostToDevice, stream_ ) );
     CUDA_CHECK( cudaMemcpyAsync( d_qpad_.p, h_qpad_.data(), S * sizeof(uint32_t), cudaMemcpyHostToDevice, stream_ ) );
@@ -1624,7 +1682,7 @@ void Engine::serve_wave( const SearchRequest & req, const std::vector<uint32_t> 
     const uint32_t cap = (uint32_t) std::min<uint64_t>( std::max<uint64_t>( n_pairs, 1 ), 0xffffffffull );
     d_list_a_.ensure( (size_t) cap * sizeof(PairTask) );
     d_list_b_.ensure( (size_t) cap * sizeof(PairTask) );
-    CUDA_CHECK( cudaMemsetAsync( d_counts_.p, 0, 16 * sizeof(unsigned long long), stream_ ) );
+    CUDA_CHECK( cudaMemsetAsync( d_counts_.p, 0, 32 * sizeof(unsigned long long), stream_ ) );
     unsigned * cnt = d_counts_.as<unsigned>();
     const int entry = req.bit_width;
     CUDA_CHECK( cudaEventRecord( ev_phase_[0], stream_ ) );

@@ -15,13 +15,15 @@
 //      three observable traceback moves, stored here as 2 bits per cell in HBM;
 //   4. the walk from the end cell with the priority I > D > M.
 //
-// Each pass is a warp wavefront: lane k owns query rows [pass*256 + 8k, +8),
+// Each pass is a warp wavefront: lane k owns query rows [stripe*256 + 8k, +8),
 // database columns stream through the warp, the bottom row of a lane goes to
-// the next lane by shuffle and the bottom row of a pass to a per-warp scratch
-// row in global memory.  All arithmetic is exact (int32, with the host
-// guaranteeing the range), matching the reference's int64 code.
+// the next lane by shuffle.  A hit runs on a group of 1 or 4 warps
+// (stripe_pipeline.cuh): stripe i on warp i % W, its bottom row handed to the
+// next stripe through shared memory or the group's boundary row in global
+// memory.  All arithmetic is exact (int32, with the host guaranteeing the
+// range), matching the reference's int64 code.
 #include "device_common.cuh"
-#include "wavefront.cuh"
+#include "stripe_pipeline.cuh"
 
 #include <climits>
 
@@ -55,6 +57,83 @@ __device__ __forceinline__ void load_rows( const uint8_t * a, int64_t first, int
 }
 
 
+// Per-hit setup shared by the passes: the group's warps, its shared state and
+// boundary row in global memory (stripe_pipeline.cuh).
+template <int W>
+struct TbGroup {
+    static constexpr int GROUPS = 256 / (32 * W);
+    int lane, wig, g;
+    PipeShared<W> * sh;
+    GroupBarrier<W> gb;
+    int4 * scratch;
+    uint32_t scratch_cols;
+    __device__ TbGroup( PipeShared<W> * shs, const TbParams & p ) {
+        lane = threadIdx.x & 31;
+        const int warp = threadIdx.x >> 5;
+        g = warp / W;
+        wig = warp % W;
+        sh = &shs[g];
+        gb = GroupBarrier<W>{ 1u + (uint32_t) g };
+        const uint64_t group = (uint64_t) blockIdx.x * GROUPS + g;
+        scratch = p.scratch ? p.scratch + group * p.scratch_cols : nullptr;
+        scratch_cols = p.scratch ? p.scratch_cols : 0;
+    }
+    // the next hit of the counter, the same on every warp of the group
+    __device__ uint32_t take( unsigned long long * counter ) {
+        if( wig == 0 && lane == 0 )
+            sh->item = (uint32_t) atomicAdd( counter, 1ull );
+        gb.sync();
+        return sh->item;
+    }
+    template <class Body>
+    __device__ void link( Body & body, const int32_t * smat, const TbParams & p ) {
+        body.smat = smat;
+        body.lane = lane;
+        body.gO = p.gap_open;
+        body.gE = p.gap_extend;
+        body.gOE = p.gap_open + p.gap_extend;
+        body.error_flags = p.error_flags;
+        body.link.sh = sh;
+        body.link.scratch = scratch;
+        body.link.scratch_cols = scratch_cols;
+        body.link.wig = wig;
+    }
+};
+
+// Fields and the row-above / bottom-row plumbing common to the stripe bodies.
+template <int W>
+struct TbStripeBase {
+    const int32_t * smat;
+    StripeLink<W> link;
+    ResidueRing rr;
+    int lane;
+    int32_t gO, gE, gOE;
+    unsigned * error_flags;
+    int qa[TB_R];
+    int32_t H[TB_R], E[TB_R];
+    int32_t diag, out_h, out_f, row0;
+    int nvalid;
+    // (H, F) above the lane's first row at column c, given the values of the
+    // first stripe's top boundary
+    __device__ void above( uint32_t s, int32_t c, int32_t top_h, int32_t top_f, int32_t & up_h, int32_t & up_f ) const {
+        if( lane == 0 ) {
+            if( link.stripe == 0 ) {
+                up_h = top_h;
+                up_f = top_f;
+            }
+            else {
+                const int2 v = link.above( s, c );
+                up_h = v.x;
+                up_f = v.y;
+            }
+        }
+    }
+    __device__ void put_bottom( int32_t c ) const {
+        if( lane == 31 && !link.put( c, out_h, out_f ) )
+            atomicOr( error_flags, ERR_SCRATCH_OVERFLOW );
+    }
+};
+
 // ---------------------------------------------------------------------------
 // 1. SW forward region pass (reference: src/algo/align.c:39-82).  The
 //    reference iterates database rows outer and query columns inner, scoring
@@ -62,140 +141,166 @@ __device__ __forceinline__ void load_rows( const uint8_t * a, int64_t first, int
 //    database and keeps the query on lanes.  Key of the end cell: largest
 //    value, then smallest database index, then smallest query index.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__( 256 ) tb_forward_kernel( TbParams p ) {
-    __shared__ int4 tiles[8][32];
-    __shared__ uint8_t rings[8][64];
-    __shared__ int32_t smat[1024];
-    stage_matrix( p.matrix, smat, true );
-    const int lane = threadIdx.x & 31;
-    const uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    int4 * scratch = p.scratch + (uint64_t) w * p.scratch_cols;
-    const int gO = p.gap_open, gE = p.gap_extend;
-    const int gOE = gO + gE;
-    for( uint32_t h = next_hit( p.hit_counters + 0, lane ); h < p.n_hits; h = next_hit( p.hit_counters + 0, lane ) ) {
-        const TbHit hit = p.hits[h];
-        if( hit.algo != 0 )
-            continue;
-        const uint32_t A = p.qlen[hit.qslot];
-        const uint32_t B = p.db.lens[hit.id];
-        const uint8_t * a = p.qcodes + p.qoff[hit.qslot];
-        const uint8_t * b = p.db.codes + p.db.offsets[hit.id];
-        int32_t * lh = p.last_h + p.last_off[h];
-        int32_t * le = p.last_e + p.last_off[h];
-        const uint32_t passes = (A + TB_ROWS - 1) / TB_ROWS;
-        // best cell of this lane: value, db index, query index
-        int32_t best_v = 0;
-        int32_t best_i = INT_MAX, best_j = INT_MAX;
-        for( uint32_t pass = 0; pass < passes; pass++ ) {
-            const bool final_pass = (pass + 1 == passes);
-            const int32_t row0 = (int32_t) (pass * TB_ROWS + lane * TB_R);
-            const int nvalid = max( 0, min( TB_R, (int) A - row0 ) );
-            int qa[TB_R];
-            load_rows( a, row0, 1, nvalid, qa );
-            int32_t H[TB_R], E[TB_R];
+template <int W>
+struct ForwardStripe : TbStripeBase<W> {
+    using B_ = TbStripeBase<W>;
+    static constexpr int32_t cand = INT32_MAX;
+    const uint8_t * a;
+    uint32_t A, B;
+    int32_t * lh;
+    int32_t * le;
+    int32_t pv, pi, pj;                       // this stripe's first maximum
+    int32_t best_v, best_i, best_j;           // over the warp's stripes
+
+    __device__ void begin( uint32_t stripe ) {
+        this->link.stripe = stripe;
+        this->link.last = (stripe + 1) * TB_ROWS >= A;
+        this->row0 = (int32_t) (stripe * TB_ROWS) + this->lane * TB_R;
+        this->nvalid = max( 0, min( TB_R, (int) A - this->row0 ) );
+        load_rows( a, this->row0, 1, this->nvalid, this->qa );
+#pragma unroll
+        for( int r = 0; r < TB_R; r++ ) {
+            this->H[r] = 0;                         // HH[j] = 0
+            this->E[r] = this->gO + this->gE;       // max(EE = gapO, HH + gapO) + gapE at row 0
+        }
+        this->diag = 0;
+        this->out_h = 0;
+        this->out_f = 0;
+        pv = 0;
+        pi = INT_MAX;
+        pj = INT_MAX;
+        this->link.start( B, this->lane );
+        this->rr.start( this->lane );
+    }
+
+    __device__ bool chunk( uint32_t ck, int32_t ) {
+        const uint32_t steps = B + 31, s0 = ck * 32;
+        const int lane = this->lane;
+        const int32_t gE = this->gE, gOE = this->gOE;
+        for( uint32_t s = s0; s < s0 + 32 && s < steps; s++ ) {
+            this->link.step( B, s, lane );
+            this->rr.step( s, lane );
+            int32_t up_h = __shfl_up_sync( 0xffffffffu, this->out_h, 1 );
+            int32_t up_f = __shfl_up_sync( 0xffffffffu, this->out_f, 1 );
+            const int32_t c = (int32_t) s - lane;
+            if( c < 0 || c >= (int32_t) B )
+                continue;
+            // f starts at gapO: max(gapO, 0 + gapO) + gapE
+            this->above( s, c, 0, this->gO + gE, up_h, up_f );
+            int32_t f = up_f, hd = this->diag;
+            const int d = this->rr.get( s, lane );
+            // branch-free rows: the row-to-row chain is a 3-way max, an add and
+            // a fused add-max; a lane visits its cells in (column, row) order,
+            // so within a stripe the first maximum wins with a strict compare
+            int32_t e_last[TB_R];
 #pragma unroll
             for( int r = 0; r < TB_R; r++ ) {
-                H[r] = 0;          // HH[j] = 0
-                E[r] = gO + gE;    // max(EE = gapO, HH + gapO) + gapE at row 0
+                const int32_t e_in = this->E[r];
+                const int32_t t = max( hd + mget( this->smat, d, this->qa[r] ), 0 );
+                const int32_t x = __vimax3_s32( t, f, e_in );
+                const bool take = (r < this->nvalid) && x > pv;
+                pv = take ? x : pv;
+                pi = take ? c : pi;
+                pj = take ? this->row0 + r : pj;
+                e_last[r] = e_in;
+                hd = this->H[r];
+                this->H[r] = x;
+                const int32_t y = x + gOE;
+                f = __viaddmax_s32( f, gE, y );
+                this->E[r] = __viaddmax_s32( e_in, gE, y );
             }
-            int32_t diag = 0;
-            int32_t out_h = 0, out_f = 0;
-            int32_t pv = 0, pi = INT_MAX, pj = INT_MAX;     // this pass's first maximum
-            BoundaryPrefetch bp{ tiles[threadIdx.x >> 5] };
-            bp.start( scratch, p.scratch_cols, B, pass > 0, lane );
-            ResidueRing rr{ rings[threadIdx.x >> 5], 0, b, (int32_t) B, -1 };
-            rr.start( lane );
-            for( uint32_t s = 0; s < B + 31; s++ ) {
-                bp.step( scratch, p.scratch_cols, B, pass > 0, s, lane );
-                rr.step( s, lane );
-                int32_t up_h = __shfl_up_sync( 0xffffffffu, out_h, 1 );
-                int32_t up_f = __shfl_up_sync( 0xffffffffu, out_f, 1 );
-                const int32_t c = (int32_t) s - lane;
-                if( c < 0 || c >= (int32_t) B )
-                    continue;
-                if( lane == 0 ) {
-                    if( pass == 0 ) {
-                        up_h = 0;
-                        up_f = gO + gE;   // f starts at gapO: max(gapO, 0 + gapO) + gapE
-                    }
-                    else {
-                        const int4 v = bp.get( s );
-                        up_h = v.x;
-                        up_f = v.y;
-                    }
-                }
-                int32_t f = up_f, hd = diag;
-                const int d = rr.get( s, lane );
-                // branch-free rows: the row-to-row chain is a 3-way max, an
-                // add and a fused add-max; a lane visits its cells in (column,
-                // row) order, so within a pass the first maximum wins with a
-                // strict compare
-                int32_t e_last[TB_R];
+            if( c == (int32_t) B - 1 ) {
 #pragma unroll
-                for( int r = 0; r < TB_R; r++ ) {
-                    const int32_t e_in = E[r];
-                    const int32_t t = max( hd + mget( smat, d, qa[r] ), 0 );
-                    const int32_t x = __vimax3_s32( t, f, e_in );
-                    const bool take = (r < nvalid) && x > pv;
-                    pv = take ? x : pv;
-                    pi = take ? c : pi;
-                    pj = take ? row0 + r : pj;
-                    e_last[r] = e_in;
-                    hd = H[r];
-                    H[r] = x;
-                    const int32_t y = x + gOE;
-                    f = __viaddmax_s32( f, gE, y );
-                    E[r] = __viaddmax_s32( e_in, gE, y );
-                }
-                if( c == (int32_t) B - 1 ) {
-#pragma unroll
-                    for( int r = 0; r < TB_R; r++ )
-                        if( r < nvalid ) {
-                            lh[row0 + r] = H[r];
-                            le[row0 + r] = e_last[r];
-                        }
-                }
-                diag = up_h;
-                out_h = H[TB_R - 1];
-                out_f = f;
-                if( lane == 31 && !final_pass ) {
-                    if( (uint32_t) c < p.scratch_cols )
-                        scratch[c] = make_int4( out_h, out_f, 0, 0 );
-                    else
-                        atomicOr( p.error_flags, ERR_SCRATCH_OVERFLOW );
+                for( int r = 0; r < TB_R; r++ )
+                    if( r < this->nvalid ) {
+                        lh[this->row0 + r] = this->H[r];
+                        le[this->row0 + r] = e_last[r];
+                    }
+            }
+            this->diag = up_h;
+            this->out_h = this->H[TB_R - 1];
+            this->out_f = f;
+            this->put_bottom( c );
+        }
+        return s0 + 32 < steps;
+    }
+
+    // this stripe's first maximum against the earlier stripes' (value desc,
+    // database index asc, query index asc)
+    __device__ void end() {
+        if( pv > best_v || (pv == best_v && pv > 0 && (pi < best_i || (pi == best_i && pj < best_j))) ) {
+            best_v = pv;
+            best_i = pi;
+            best_j = pj;
+        }
+    }
+};
+
+template <int W>
+__global__ void __launch_bounds__( 256 ) tb_forward_kernel( TbParams p ) {
+    __shared__ PipeShared<W> shs[TbGroup<W>::GROUPS];
+    __shared__ int32_t smat[1024];
+    stage_matrix( p.matrix, smat, true );
+    TbGroup<W> grp( shs, p );
+    for( ;; ) {
+        const uint32_t h = grp.take( p.hit_counters + 0 );
+        if( h >= p.n_hits )
+            break;
+        const TbHit hit = p.hits[h];
+        if( hit.algo == 0 ) {
+            ForwardStripe<W> body;
+            grp.link( body, smat, p );
+            body.A = p.qlen[hit.qslot];
+            body.B = p.db.lens[hit.id];
+            body.a = p.qcodes + p.qoff[hit.qslot];
+            body.lh = p.last_h + p.last_off[h];
+            body.le = p.last_e + p.last_off[h];
+            body.best_v = 0;
+            body.best_i = INT_MAX;
+            body.best_j = INT_MAX;
+            body.rr = ResidueRing{ grp.sh->residues[grp.wig], 0, p.db.codes + p.db.offsets[hit.id], (int32_t) body.B,
+                                   -1 };
+            run_stripes<W>( body, *grp.sh, grp.gb, grp.wig, grp.lane, (body.A + TB_ROWS - 1) / TB_ROWS, body.B,
+                    p.error_flags );
+            // the best key over the warp, then over the group
+            int32_t bv = body.best_v, bi = body.best_i, bj = body.best_j;
+            for( int o = 16; o > 0; o >>= 1 ) {
+                const int32_t v = __shfl_xor_sync( 0xffffffffu, bv, o );
+                const int32_t i = __shfl_xor_sync( 0xffffffffu, bi, o );
+                const int32_t j = __shfl_xor_sync( 0xffffffffu, bj, o );
+                if( v > bv || (v == bv && (i < bi || (i == bi && j < bj))) ) {
+                    bv = v;
+                    bi = i;
+                    bj = j;
                 }
             }
-            // this pass's first maximum against the earlier passes' (value desc,
-            // database index asc, query index asc)
-            if( pv > best_v || (pv == best_v && pv > 0 && (pi < best_i || (pi == best_i && pj < best_j))) ) {
-                best_v = pv;
-                best_i = pi;
-                best_j = pj;
+            if( grp.lane == 0 ) {
+                grp.sh->red[grp.wig][0] = bv;
+                grp.sh->red[grp.wig][1] = bi;
+                grp.sh->red[grp.wig][2] = bj;
             }
-            __syncwarp();
-        }
-        // reduce the best key over the warp
-        for( int o = 16; o > 0; o >>= 1 ) {
-            int32_t v = __shfl_xor_sync( 0xffffffffu, best_v, o );
-            int32_t bi = __shfl_xor_sync( 0xffffffffu, best_i, o );
-            int32_t bj = __shfl_xor_sync( 0xffffffffu, best_j, o );
-            if( v > best_v || (v == best_v && (bi < best_i || (bi == best_i && bj < best_j))) ) {
-                best_v = v;
-                best_i = bi;
-                best_j = bj;
+            grp.gb.sync();
+            if( grp.wig == 0 && grp.lane == 0 ) {
+                for( int k = 1; k < W; k++ ) {
+                    const int32_t v = grp.sh->red[k][0], i = grp.sh->red[k][1], j = grp.sh->red[k][2];
+                    if( v > bv || (v == bv && (i < bi || (i == bi && j < bj))) ) {
+                        bv = v;
+                        bi = i;
+                        bj = j;
+                    }
+                }
+                TbRegion rg;
+                rg.fwd_score = bv;
+                rg.a_end = bj;
+                rg.b_end = bi;
+                rg.a_begin = 0;
+                rg.b_begin = 0;
+                rg.status = (bv > 0) ? 0 : 1;
+                p.regions[h] = rg;
             }
         }
-        if( lane == 0 ) {
-            TbRegion rg;
-            rg.fwd_score = best_v;
-            rg.a_end = best_j;
-            rg.b_end = best_i;
-            rg.a_begin = 0;
-            rg.b_begin = 0;
-            rg.status = (best_v > 0) ? 0 : 1;
-            p.regions[h] = rg;
-        }
-        __syncwarp();
+        // every warp is past this hit's shared state before the next hit
+        grp.gb.sync();
     }
 }
 
@@ -205,141 +310,156 @@ __global__ void __launch_bounds__( 256 ) tb_forward_kernel( TbParams p ) {
 //    i' = b_end - i.  The boundary row before column 0 is the reference's
 //    work row: -1 for query indices <= b_end, the forward pass's last row
 //    above that.  The begin cell is the first cell in (i' asc, j' asc) order
-//    whose value reaches the forward score.
+//    whose value reaches the forward score; columns past the first column
+//    holding a candidate cannot change it, so that column is the group's
+//    limit.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__( 256 ) tb_reverse_kernel( TbParams p ) {
-    __shared__ int4 tiles[8][32];
-    __shared__ uint8_t rings[8][64];
-    __shared__ int32_t smat[1024];
-    stage_matrix( p.matrix, smat, true );
-    const int lane = threadIdx.x & 31;
-    const uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    int4 * scratch = p.scratch + (uint64_t) w * p.scratch_cols;
-    const int gO = p.gap_open, gE = p.gap_extend;
-    const int gOE = gO + gE;
-    for( uint32_t h = next_hit( p.hit_counters + 1, lane ); h < p.n_hits; h = next_hit( p.hit_counters + 1, lane ) ) {
-        const TbHit hit = p.hits[h];
-        if( hit.algo != 0 )
-            continue;
-        TbRegion rg = p.regions[h];
-        if( rg.status != 0 )
-            continue;
-        const int32_t score = rg.fwd_score;
-        const int32_t a_end = rg.a_end, b_end = rg.b_end;
-        const uint32_t A = (uint32_t) a_end + 1;     // rows j' = 0..a_end
-        const uint32_t B = (uint32_t) b_end + 1;     // cols i' = 0..b_end
-        const uint8_t * a = p.qcodes + p.qoff[hit.qslot];
-        const uint8_t * b = p.db.codes + p.db.offsets[hit.id];
-        const int32_t * lh = p.last_h + p.last_off[h];
-        const int32_t * le = p.last_e + p.last_off[h];
-        const uint32_t passes = (A + TB_ROWS - 1) / TB_ROWS;
-        int32_t hit_i = INT_MAX, hit_j = INT_MAX;   // first (i', j') reaching the score
-        for( uint32_t pass = 0; pass < passes; pass++ ) {
-            const bool final_pass = (pass + 1 == passes);
-            const int32_t row0 = (int32_t) (pass * TB_ROWS + lane * TB_R);
-            const int nvalid = max( 0, min( TB_R, (int) A - row0 ) );
-            int qa[TB_R];
-            load_rows( a, (int64_t) a_end - row0, -1, nvalid, qa );
-            int32_t H[TB_R], E[TB_R];
+template <int W>
+struct ReverseStripe : TbStripeBase<W> {
+    const uint8_t * a;
+    uint32_t A, B;
+    int32_t score, a_end, b_end;
+    const int32_t * lh;
+    const int32_t * le;
+    int32_t hit_i, hit_j;          // the lane's first (i', j') reaching the score, over its stripes
+    int32_t cand;                  // = hit_i, read by run_stripes after each chunk
+
+    __device__ void begin( uint32_t stripe ) {
+        const int lane = this->lane;
+        this->link.stripe = stripe;
+        this->link.last = (stripe + 1) * TB_ROWS >= A;
+        this->row0 = (int32_t) (stripe * TB_ROWS) + lane * TB_R;
+        const int32_t row0 = this->row0;
+        this->nvalid = max( 0, min( TB_R, (int) A - row0 ) );
+        load_rows( a, (int64_t) a_end - row0, -1, this->nvalid, this->qa );
+#pragma unroll
+        for( int r = 0; r < TB_R; r++ ) {
+            const int32_t j = a_end - (row0 + r);     // query index
+            int32_t hh = -1, ee = -1;
+            if( r < this->nvalid && j > b_end ) {
+                hh = lh[j];
+                ee = le[j];
+            }
+            this->H[r] = hh;                                // HH(b_end + 1, j)
+            this->E[r] = max( ee, hh + this->gO ) + this->gE;   // EE(b_end, j)
+        }
+        // diagonal of the lane's first row at column 0: HH(b_end+1, j+1), or 0
+        // for the end cell itself
+        const int32_t jprev = a_end - (row0 - 1);
+        this->diag = (row0 == 0) ? 0 : ((jprev > b_end) ? lh[jprev] : -1);
+        this->out_h = 0;
+        this->out_f = 0;
+        this->link.start( B, lane );
+        this->rr.start( lane );
+    }
+
+    __device__ bool chunk( uint32_t ck, int32_t lim ) {
+        // steps up to the limit column on lane 31
+        const uint32_t cols = (lim == INT32_MAX) ? B : min( B, (uint32_t) lim + 1u );
+        const uint32_t steps = cols + 31, s0 = ck * 32;
+        const int lane = this->lane;
+        const int32_t gO = this->gO, gE = this->gE, gOE = this->gOE;
+        for( uint32_t s = s0; s < s0 + 32 && s < steps; s++ ) {
+            this->link.step( B, s, lane );
+            this->rr.step( s, lane );
+            int32_t up_h = __shfl_up_sync( 0xffffffffu, this->out_h, 1 );
+            int32_t up_f = __shfl_up_sync( 0xffffffffu, this->out_f, 1 );
+            const int32_t c = (int32_t) s - lane;
+            if( c < 0 || c >= (int32_t) B )
+                continue;
+            // h starts at -1 per row; f = max(-1, h + gapO) + gapE
+            this->above( s, c, -1, max( -1, -1 + gO ) + gE, up_h, up_f );
+            const int d = this->rr.get( s, lane );          // database index b_end - c
+            int32_t f = up_f, hd = this->diag;               // stripe 0 lane 0: 0 at c == 0, then -1
 #pragma unroll
             for( int r = 0; r < TB_R; r++ ) {
-                const int32_t j = a_end - (row0 + r);     // query index
-                int32_t hh = -1, ee = -1;
-                if( r < nvalid && j > b_end ) {
-                    hh = lh[j];
-                    ee = le[j];
+                const int32_t e_in = this->E[r];
+                const int32_t x = __vimax3_s32( hd + mget( this->smat, d, this->qa[r] ), f, e_in );
+                const bool take = (r < this->nvalid) && x >= score &&
+                        (c < hit_i || (c == hit_i && this->row0 + r < hit_j));
+                hit_i = take ? c : hit_i;
+                hit_j = take ? this->row0 + r : hit_j;
+                hd = this->H[r];
+                this->H[r] = x;
+                const int32_t y = x + gOE;
+                f = __viaddmax_s32( f, gE, y );
+                this->E[r] = __viaddmax_s32( e_in, gE, y );
+            }
+            this->diag = up_h;
+            this->out_h = this->H[TB_R - 1];
+            this->out_f = f;
+            this->put_bottom( c );
+        }
+        cand = hit_i;
+        return s0 + 32 < steps;
+    }
+
+    __device__ void end() {}
+};
+
+template <int W>
+__global__ void __launch_bounds__( 256 ) tb_reverse_kernel( TbParams p ) {
+    __shared__ PipeShared<W> shs[TbGroup<W>::GROUPS];
+    __shared__ int32_t smat[1024];
+    stage_matrix( p.matrix, smat, true );
+    TbGroup<W> grp( shs, p );
+    for( ;; ) {
+        const uint32_t h = grp.take( p.hit_counters + 1 );
+        if( h >= p.n_hits )
+            break;
+        const TbHit hit = p.hits[h];
+        TbRegion rg = p.regions[h];
+        if( hit.algo == 0 && rg.status == 0 ) {
+            ReverseStripe<W> body;
+            grp.link( body, smat, p );
+            body.score = rg.fwd_score;
+            body.a_end = rg.a_end;
+            body.b_end = rg.b_end;
+            body.A = (uint32_t) rg.a_end + 1;     // rows j' = 0..a_end
+            body.B = (uint32_t) rg.b_end + 1;     // cols i' = 0..b_end
+            body.a = p.qcodes + p.qoff[hit.qslot];
+            body.lh = p.last_h + p.last_off[h];
+            body.le = p.last_e + p.last_off[h];
+            body.hit_i = INT_MAX;
+            body.hit_j = INT_MAX;
+            body.cand = INT_MAX;
+            body.rr = ResidueRing{ grp.sh->residues[grp.wig], 0, p.db.codes + p.db.offsets[hit.id], (int32_t) body.B,
+                                   rg.b_end };
+            run_stripes<W>( body, *grp.sh, grp.gb, grp.wig, grp.lane, (body.A + TB_ROWS - 1) / TB_ROWS, body.B,
+                    p.error_flags );
+            int32_t bi = body.hit_i, bj = body.hit_j;
+            for( int o = 16; o > 0; o >>= 1 ) {
+                const int32_t i = __shfl_xor_sync( 0xffffffffu, bi, o );
+                const int32_t j = __shfl_xor_sync( 0xffffffffu, bj, o );
+                if( i < bi || (i == bi && j < bj) ) {
+                    bi = i;
+                    bj = j;
                 }
-                H[r] = hh;                                // HH(b_end + 1, j)
-                E[r] = max( ee, hh + gO ) + gE;           // EE(b_end, j)
             }
-            // diagonal of the lane's first row at column 0: HH(b_end+1, j+1),
-            // or 0 for the end cell itself
-            int32_t diag;
-            {
-                const int32_t jprev = a_end - (row0 - 1);
-                if( row0 == 0 )
-                    diag = 0;
-                else
-                    diag = (jprev > b_end) ? lh[jprev] : -1;
+            if( grp.lane == 0 ) {
+                grp.sh->red[grp.wig][0] = bi;
+                grp.sh->red[grp.wig][1] = bj;
             }
-            int32_t out_h = 0, out_f = 0;
-            // columns past the first one holding a begin-cell candidate cannot
-            // change the result: stop once every lane has passed it
-            int32_t limit = __reduce_min_sync( 0xffffffffu, hit_i );
-            BoundaryPrefetch bp{ tiles[threadIdx.x >> 5] };
-            bp.start( scratch, p.scratch_cols, B, pass > 0, lane );
-            ResidueRing rr{ rings[threadIdx.x >> 5], 0, b, (int32_t) B, b_end };
-            rr.start( lane );
-            for( uint32_t s = 0; s < B + 31; s++ ) {
-                if( (s & 7) == 0 )
-                    limit = __reduce_min_sync( 0xffffffffu, hit_i );
-                if( limit != INT_MAX && (int64_t) s > (int64_t) limit + 31 )
-                    break;
-                bp.step( scratch, p.scratch_cols, B, pass > 0, s, lane );
-                rr.step( s, lane );
-                int32_t up_h = __shfl_up_sync( 0xffffffffu, out_h, 1 );
-                int32_t up_f = __shfl_up_sync( 0xffffffffu, out_f, 1 );
-                const int32_t c = (int32_t) s - lane;
-                if( c < 0 || c >= (int32_t) B )
-                    continue;
-                if( lane == 0 ) {
-                    if( pass == 0 ) {
-                        up_h = -1;                        // h starts at -1 per row
-                        up_f = max( -1, -1 + gO ) + gE;   // f = max(-1, h + gapO) + gapE
+            grp.gb.sync();
+            if( grp.wig == 0 && grp.lane == 0 ) {
+                for( int k = 1; k < W; k++ ) {
+                    const int32_t i = grp.sh->red[k][0], j = grp.sh->red[k][1];
+                    if( i < bi || (i == bi && j < bj) ) {
+                        bi = i;
+                        bj = j;
                     }
-                    else {
-                        const int4 v = bp.get( s );
-                        up_h = v.x;
-                        up_f = v.y;
-                    }
                 }
-                const int d = rr.get( s, lane );          // database index b_end - c
-                int32_t f = up_f, hd = diag;              // lane 0 / pass 0: 0 at c == 0, then -1
-#pragma unroll
-                for( int r = 0; r < TB_R; r++ ) {
-                    const int32_t e_in = E[r];
-                    const int32_t x = __vimax3_s32( hd + mget( smat, d, qa[r] ), f, e_in );
-                    const bool take = (r < nvalid) && x >= score &&
-                            (c < hit_i || (c == hit_i && row0 + r < hit_j));
-                    hit_i = take ? c : hit_i;
-                    hit_j = take ? row0 + r : hit_j;
-                    hd = H[r];
-                    H[r] = x;
-                    const int32_t y = x + gOE;
-                    f = __viaddmax_s32( f, gE, y );
-                    E[r] = __viaddmax_s32( e_in, gE, y );
+                if( bi == INT_MAX ) {
+                    rg.status = 2;
                 }
-                diag = up_h;
-                out_h = H[TB_R - 1];
-                out_f = f;
-                if( lane == 31 && !final_pass ) {
-                    if( (uint32_t) c < p.scratch_cols )
-                        scratch[c] = make_int4( out_h, out_f, 0, 0 );
-                    else
-                        atomicOr( p.error_flags, ERR_SCRATCH_OVERFLOW );
+                else {
+                    rg.b_begin = rg.b_end - bi;
+                    rg.a_begin = rg.a_end - bj;
                 }
-            }
-            __syncwarp();
-        }
-        for( int o = 16; o > 0; o >>= 1 ) {
-            int32_t bi = __shfl_xor_sync( 0xffffffffu, hit_i, o );
-            int32_t bj = __shfl_xor_sync( 0xffffffffu, hit_j, o );
-            if( bi < hit_i || (bi == hit_i && bj < hit_j) ) {
-                hit_i = bi;
-                hit_j = bj;
+                p.regions[h] = rg;
             }
         }
-        if( lane == 0 ) {
-            if( hit_i == INT_MAX ) {
-                rg.status = 2;
-            }
-            else {
-                rg.b_begin = b_end - hit_i;
-                rg.a_begin = a_end - hit_j;
-            }
-            p.regions[h] = rg;
-        }
-        __syncwarp();
+        grp.gb.sync();
     }
 }
 
@@ -350,104 +470,114 @@ __global__ void __launch_bounds__( 256 ) tb_reverse_kernel( TbParams p ) {
 //    Stored for columns [b_begin, b_end] and all query rows of the lane, one
 //    16-bit word (8 rows x 2 bits) per lane and column.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__( 256 ) tb_directions_kernel( TbParams p ) {
-    __shared__ int4 tiles[8][32];
-    __shared__ uint8_t rings[8][64];
-    __shared__ int32_t smat[1024];
-    stage_matrix( p.matrix, smat, false );
-    const int lane = threadIdx.x & 31;
-    const uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    int4 * scratch = p.scratch + (uint64_t) w * p.scratch_cols;
-    const int gO = p.gap_open, gE = p.gap_extend;
-    const int gOE = gO + gE;
-    for( uint32_t h = next_hit( p.hit_counters + 2, lane ); h < p.n_hits; h = next_hit( p.hit_counters + 2, lane ) ) {
-        const TbHit hit = p.hits[h];
-        const TbRegion rg = p.regions[h];
-        if( rg.status != 0 )
-            continue;
-        const bool nw = hit.algo == 1;
-        const uint32_t A = (uint32_t) rg.a_end + 1;   // rows 0..a_end suffice
-        const uint32_t B = (uint32_t) rg.b_end + 1;   // columns 0..b_end
-        const uint32_t words = (A + TB_R - 1) / TB_R;
-        const uint8_t * a = p.qcodes + p.qoff[hit.qslot];
-        const uint8_t * b = p.db.codes + p.db.offsets[hit.id];
-        uint16_t * dir = p.dirs + p.dir_off[h];
-        const uint32_t passes = (A + TB_ROWS - 1) / TB_ROWS;
-        for( uint32_t pass = 0; pass < passes; pass++ ) {
-            const bool final_pass = (pass + 1 == passes);
-            const int32_t row0 = (int32_t) (pass * TB_ROWS + lane * TB_R);
-            const int nvalid = max( 0, min( TB_R, (int) A - row0 ) );
-            int qa[TB_R];
-            load_rows( a, row0, 1, nvalid, qa );
-            int32_t H[TB_R], E[TB_R];
+template <int W>
+struct DirectionStripe : TbStripeBase<W> {
+    static constexpr int32_t cand = INT32_MAX;
+    const uint8_t * a;
+    uint32_t A, B, words;
+    bool nw;
+    int32_t b_begin;
+    uint16_t * dir;
+
+    __device__ void begin( uint32_t stripe ) {
+        const int32_t gO = this->gO, gE = this->gE;
+        this->link.stripe = stripe;
+        this->link.last = (stripe + 1) * TB_ROWS >= A;
+        this->row0 = (int32_t) (stripe * TB_ROWS) + this->lane * TB_R;
+        const int32_t row0 = this->row0;
+        this->nvalid = max( 0, min( TB_R, (int) A - row0 ) );
+        load_rows( a, row0, 1, this->nvalid, this->qa );
+#pragma unroll
+        for( int r = 0; r < TB_R; r++ ) {
+            const int32_t i = row0 + r;
+            this->H[r] = nw ? gO + (i + 1) * gE : 0;
+            this->E[r] = nw ? 2 * gO + (i + 2) * gE : 0;
+        }
+        this->diag = nw ? ((row0 == 0) ? 0 : gO + row0 * gE) : 0;
+        this->out_h = 0;
+        this->out_f = 0;
+        this->link.start( B, this->lane );
+        this->rr.start( this->lane );
+    }
+
+    __device__ bool chunk( uint32_t ck, int32_t ) {
+        const uint32_t steps = B + 31, s0 = ck * 32;
+        const int lane = this->lane;
+        const int32_t gO = this->gO, gE = this->gE, gOE = this->gOE;
+        const int32_t row0 = this->row0;
+        for( uint32_t s = s0; s < s0 + 32 && s < steps; s++ ) {
+            this->link.step( B, s, lane );
+            this->rr.step( s, lane );
+            int32_t up_h = __shfl_up_sync( 0xffffffffu, this->out_h, 1 );
+            int32_t up_f = __shfl_up_sync( 0xffffffffu, this->out_f, 1 );
+            const int32_t j = (int32_t) s - lane;     // database index
+            if( j < 0 || j >= (int32_t) B )
+                continue;
+            // H(-1, j) is the next column's row-0 diagonal
+            this->above( s, j, nw ? gO + (j + 1) * gE : 0, nw ? 2 * gO + (j + 2) * gE : 0, up_h, up_f );
+            const int d = this->rr.get( s, lane );
+            int32_t f = up_f, hd = this->diag;
+            uint32_t code = 0;
+            // flags as in the reference (strict compares in its order),
+            // computed beside a branch-free row-to-row chain
 #pragma unroll
             for( int r = 0; r < TB_R; r++ ) {
-                const int32_t i = row0 + r;
-                H[r] = nw ? gO + (i + 1) * gE : 0;
-                E[r] = nw ? 2 * gO + (i + 2) * gE : 0;
+                const int32_t e = this->E[r];
+                const int32_t x0 = hd + mget( this->smat, d, this->qa[r] );
+                const bool up = f > x0;                      // UP
+                const bool left = e > max( x0, f );          // LEFT
+                const int32_t x = __vimax3_s32( nw ? x0 : max( x0, 0 ), f, e );
+                hd = this->H[r];
+                this->H[r] = x;
+                const int32_t y = x + gOE;
+                const bool ext_up = f + gE > y;              // EXT_UP
+                const bool ext_left = e + gE > y;            // EXT_LEFT
+                f = __viaddmax_s32( f, gE, y );
+                this->E[r] = __viaddmax_s32( e, gE, y );
+                const uint32_t op = (left || ext_left) ? 2u : ((up || ext_up) ? 1u : 0u);
+                code |= (r < this->nvalid) ? op << (2 * r) : 0u;
             }
-            int32_t diag = nw ? ((row0 == 0) ? 0 : gO + row0 * gE) : 0;
-            int32_t out_h = 0, out_f = 0;
-            BoundaryPrefetch bp{ tiles[threadIdx.x >> 5] };
-            bp.start( scratch, p.scratch_cols, B, pass > 0, lane );
-            ResidueRing rr{ rings[threadIdx.x >> 5], 0, b, (int32_t) B, -1 };
-            rr.start( lane );
-            for( uint32_t s = 0; s < B + 31; s++ ) {
-                bp.step( scratch, p.scratch_cols, B, pass > 0, s, lane );
-                rr.step( s, lane );
-                int32_t up_h = __shfl_up_sync( 0xffffffffu, out_h, 1 );
-                int32_t up_f = __shfl_up_sync( 0xffffffffu, out_f, 1 );
-                const int32_t j = (int32_t) s - lane;     // database index
-                if( j < 0 || j >= (int32_t) B )
-                    continue;
-                if( lane == 0 ) {
-                    if( pass == 0 ) {
-                        // H(-1, j) is the next column's row-0 diagonal
-                        up_h = nw ? gO + (j + 1) * gE : 0;
-                        up_f = nw ? 2 * gO + (j + 2) * gE : 0;
-                    }
-                    else {
-                        const int4 v = bp.get( s );
-                        up_h = v.x;
-                        up_f = v.y;
-                    }
-                }
-                const int d = rr.get( s, lane );
-                int32_t f = up_f, hd = diag;
-                uint32_t code = 0;
-                // flags as in the reference (strict compares in its order),
-                // computed beside a branch-free row-to-row chain
-#pragma unroll
-                for( int r = 0; r < TB_R; r++ ) {
-                    const int32_t e = E[r];
-                    const int32_t x0 = hd + mget( smat, d, qa[r] );
-                    const bool up = f > x0;                      // UP
-                    const bool left = e > max( x0, f );          // LEFT
-                    const int32_t x = __vimax3_s32( nw ? x0 : max( x0, 0 ), f, e );
-                    hd = H[r];
-                    H[r] = x;
-                    const int32_t y = x + gOE;
-                    const bool ext_up = f + gE > y;              // EXT_UP
-                    const bool ext_left = e + gE > y;            // EXT_LEFT
-                    f = __viaddmax_s32( f, gE, y );
-                    E[r] = __viaddmax_s32( e, gE, y );
-                    const uint32_t op = (left || ext_left) ? 2u : ((up || ext_up) ? 1u : 0u);
-                    code |= (r < nvalid) ? op << (2 * r) : 0u;
-                }
-                diag = up_h;
-                out_h = H[TB_R - 1];
-                out_f = f;
-                if( j >= rg.b_begin && (uint32_t) (row0 / TB_R) < words )
-                    dir[(uint64_t) (j - rg.b_begin) * words + row0 / TB_R] = (uint16_t) code;
-                if( lane == 31 && !final_pass ) {
-                    if( (uint32_t) j < p.scratch_cols )
-                        scratch[j] = make_int4( out_h, out_f, 0, 0 );
-                    else
-                        atomicOr( p.error_flags, ERR_SCRATCH_OVERFLOW );
-                }
-            }
-            __syncwarp();
+            this->diag = up_h;
+            this->out_h = this->H[TB_R - 1];
+            this->out_f = f;
+            if( j >= b_begin && (uint32_t) (row0 / TB_R) < words )
+                dir[(uint64_t) (j - b_begin) * words + row0 / TB_R] = (uint16_t) code;
+            this->put_bottom( j );
         }
+        return s0 + 32 < steps;
+    }
+
+    __device__ void end() {}
+};
+
+template <int W>
+__global__ void __launch_bounds__( 256 ) tb_directions_kernel( TbParams p ) {
+    __shared__ PipeShared<W> shs[TbGroup<W>::GROUPS];
+    __shared__ int32_t smat[1024];
+    stage_matrix( p.matrix, smat, false );
+    TbGroup<W> grp( shs, p );
+    for( ;; ) {
+        const uint32_t h = grp.take( p.hit_counters + 2 );
+        if( h >= p.n_hits )
+            break;
+        const TbHit hit = p.hits[h];
+        const TbRegion rg = p.regions[h];
+        if( rg.status == 0 ) {
+            DirectionStripe<W> body;
+            grp.link( body, smat, p );
+            body.nw = hit.algo == 1;
+            body.A = (uint32_t) rg.a_end + 1;   // rows 0..a_end suffice
+            body.B = (uint32_t) rg.b_end + 1;   // columns 0..b_end
+            body.words = (body.A + TB_R - 1) / TB_R;
+            body.b_begin = rg.b_begin;
+            body.a = p.qcodes + p.qoff[hit.qslot];
+            body.dir = p.dirs + p.dir_off[h];
+            body.rr = ResidueRing{ grp.sh->residues[grp.wig], 0, p.db.codes + p.db.offsets[hit.id], (int32_t) body.B,
+                                   -1 };
+            run_stripes<W>( body, *grp.sh, grp.gb, grp.wig, grp.lane, (body.A + TB_ROWS - 1) / TB_ROWS, body.B,
+                    p.error_flags );
+        }
+        grp.gb.sync();
     }
 }
 
@@ -496,15 +626,22 @@ __global__ void tb_walk_kernel( TbParams p ) {
 
 // Region phase (Smith-Waterman hits only): forward and reverse passes.  They
 // need no direction memory, so all hits of a search run in one launch each.
-// ev (optional): 3 events recorded around the two kernels.
-cudaError_t launch_tb_regions( const TbParams & p, int grid, cudaStream_t st, cudaEvent_t * ev ) {
+// group: warps per hit (1 or 4).  ev (optional): 3 events recorded around the
+// two kernels.
+cudaError_t launch_tb_regions( const TbParams & p, int group, int grid, cudaStream_t st, cudaEvent_t * ev ) {
     if( ev )
         cudaEventRecord( ev[0], st );
     if( p.n_hits ) {
-        tb_forward_kernel<<<grid, 256, 0, st>>>( p );
+        if( group == 4 )
+            tb_forward_kernel<4><<<grid, 256, 0, st>>>( p );
+        else
+            tb_forward_kernel<1><<<grid, 256, 0, st>>>( p );
         if( ev )
             cudaEventRecord( ev[1], st );
-        tb_reverse_kernel<<<grid, 256, 0, st>>>( p );
+        if( group == 4 )
+            tb_reverse_kernel<4><<<grid, 256, 0, st>>>( p );
+        else
+            tb_reverse_kernel<1><<<grid, 256, 0, st>>>( p );
     }
     else if( ev ) {
         cudaEventRecord( ev[1], st );
@@ -515,13 +652,16 @@ cudaError_t launch_tb_regions( const TbParams & p, int grid, cudaStream_t st, cu
 }
 
 // Path phase: direction pass and walk of the hits of one wave (the hits whose
-// direction words fit the memory the host set aside).
-// ev (optional): 3 events recorded around the two kernels.
-cudaError_t launch_tb_paths( const TbParams & p, int grid, cudaStream_t st, cudaEvent_t * ev ) {
+// direction words fit the memory the host set aside).  ev (optional): 3 events
+// recorded around the two kernels.
+cudaError_t launch_tb_paths( const TbParams & p, int group, int grid, cudaStream_t st, cudaEvent_t * ev ) {
     if( ev )
         cudaEventRecord( ev[0], st );
     if( p.n_hits ) {
-        tb_directions_kernel<<<grid, 256, 0, st>>>( p );
+        if( group == 4 )
+            tb_directions_kernel<4><<<grid, 256, 0, st>>>( p );
+        else
+            tb_directions_kernel<1><<<grid, 256, 0, st>>>( p );
         if( ev )
             cudaEventRecord( ev[1], st );
         tb_walk_kernel<<<(p.n_hits + 127) / 128, 128, 0, st>>>( p );

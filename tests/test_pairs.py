@@ -74,6 +74,19 @@ def test_pairs_match_oracle(built_library, algo, width, align):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("algo", ["sw", "nw"])
+def test_pairs_on_warp_groups_match_oracle(built_library, algo):
+    """Pairs of 2,500-4,000 residues: the traceback runs them on groups of 4
+    warps (more than 8M cells, up to 16 stripes of 256 query rows, so the
+    boundary rows travel through shared memory and the group's global row)."""
+    queries, records, ids = _pairs(23, 8, 2500, 4000)
+    product_setup(1, MATRIX, GAP, 1000, 2, records=records)
+    got = _product(algo, 16, 1, queries, ids)
+    for i, q in enumerate(queries):
+        assert got[i] == _oracle(algo, 16, 1, q, records[ids[i]], ids[i]), i
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("algo", ["sw", "nw"])
 def test_long_pairs_beyond_16_bits(built_library, algo):
     """Config-5-sized pairs: scores above 32767 take the reference's 64-bit path."""
     rng = np.random.default_rng(29)
