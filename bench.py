@@ -218,6 +218,37 @@ def reference_sample(w, n_queries: int, threads: int, repeat: int = 1) -> tuple[
     return cells / secs / 1e9, secs, desc
 
 
+def pairs_reference_sample(pairs, n_pairs: int, threads: int) -> tuple[float, float, str]:
+    """(GCUPS, seconds, description) of the reference on a sample of long pairs:
+    per pair a database of the one partner sequence and sw_align + nw_align
+    with COMPUTE_ALIGNMENT at the 16-bit entry, as a reference caller aligns a
+    pair."""
+    import oracle
+    if not oracle.reference_available():
+        raise RuntimeError("oracle/_ref/ref_run is not built")
+    import numpy as np
+    sizes = np.array([len(a) * len(b) for a, b in pairs])
+    order = np.argsort(sizes)
+    # pairs at the 10th, 30th, ... size percentiles up to the median
+    pick = [int(order[int((0.1 + 0.2 * i) * (len(order) - 1))]) for i in range(n_pairs)]
+    secs, cells = 0.0, 0
+    with tempfile.TemporaryDirectory() as td:
+        for k in pick:
+            a, b = pairs[k]
+            db = os.path.join(td, f"pair{k}.sdb")
+            oracle.write_sdb(db, seqs=[b])
+            for algo in ("sw", "nw"):
+                res = oracle.run_reference(db, [a.decode()], algo=algo, width=16, align=1, hits=1, symtype=1,
+                                           matrix="builtin:blosum62", gap=(-11, -1), chunk=1000, threads=threads,
+                                           simd=2, timing=True)
+                secs += sum(r["seconds"] for r in res)
+                cells += len(a) * len(b)
+    desc = (f"{n_pairs} pairs of the workload ({sorted(int(sizes[k]) for k in pick)} cells), each against a "
+            f"database of its one partner, sw_align and nw_align COMPUTE_ALIGNMENT, 16-bit entry, AVX2, "
+            f"{threads} threads")
+    return cells / secs / 1e9, secs, desc
+
+
 def run_reference_arm(args):
     world, rank, local, pg = dist_setup()
     if rank != 0:
@@ -476,7 +507,7 @@ def run_pairs_arm(args):
     import libssa_b200 as L
     from libssa_b200 import workloads as W
     L.load()
-    pairs = W.long_pairs(seed=5, n_pairs=args.pairs)
+    pairs = W.long_pairs(seed=5, n_pairs=args.pairs, lo=args.pair_lo, hi=args.pair_hi)
     L.set_output_mode(L.OUTPUT_SILENT)
     L.init_symbol_translation(L.AMINOACID, L.FORWARD_STRAND, 1, 1)
     L.init_score_matrix(L.MATRIX_BUILDIN, "blosum62")
@@ -492,8 +523,9 @@ def run_pairs_arm(args):
     for _ in range(args.warmup):
         for algo in algos:
             L.align_pairs(algo, qs, ids, L.BIT_WIDTH_16, L.COMPUTE_ALIGNMENT)
-    dev, wall, score_dev = 0.0, 0.0, 0.0
+    dev, wall = 0.0, 0.0
     per_algo = {0: 0.0, 1: 0.0}
+    h2d = d2h = 0
     for _ in range(args.steps):
         for algo in algos:
             t0 = time.perf_counter()
@@ -501,19 +533,30 @@ def run_pairs_arm(args):
             wall += time.perf_counter() - t0
             st = L.stats()
             dev += st.gpu_seconds
-            score_dev += st.entry_seconds
             per_algo[algo] += st.gpu_seconds
+            h2d += int(st.h2d_bytes)
+            d2h += int(st.d2h_bytes)
     line = {"metric": "GCUPS (long-pair SW and NW alignments with CIGAR, 5k-30k residues per side)",
             "value": round(cells * args.steps / dev / 1e9, 2), "unit": "GCUPS", "n_gpus": 1, "steps": args.steps,
-            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "int32", "data": "synthetic (seeded, BASELINE config 5 shapes)",
-            "config": {"workload": "long_pairs", "pairs": len(pairs), "algorithms": ["sw", "nw"],
-                       "cells_per_step": cells, "bit_width": 16},
-            "e2e": {"value": round(cells * args.steps / wall / 1e9, 2), "unit": "GCUPS"},
+            "warmup": args.warmup, "ms_per_step": round(dev / args.steps * 1e3, 2), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded, BASELINE config 5 shapes)",
+            "config": {"workload": "long_pairs", "pairs": len(pairs), "query_lengths": [args.pair_lo, args.pair_hi],
+                       "algorithms": ["sw", "nw"],
+                       "cells_per_step": cells, "bit_width": 16,
+                       "l2": "inputs and direction matrices far larger than L2"},
+            "e2e": {"value": round(cells * args.steps / wall / 1e9, 2), "unit": "GCUPS",
+                    "h2d_bytes_per_step": h2d // args.steps, "d2h_bytes_per_step": d2h // args.steps},
             "timing": {"device_seconds": round(dev, 4), "wall_seconds": round(wall, 4),
-                       "sw_seconds": round(per_algo[0], 4), "nw_seconds": round(per_algo[1], 4),
-                       "pair_score_seconds": round(score_dev, 4),
-                       "pair_score_gcups": round(cells * args.steps / score_dev / 1e9, 2)}}
+                       "sw_seconds": round(per_algo[0], 4), "nw_seconds": round(per_algo[1], 4)}}
+    if not args.no_cpu_baseline:
+        import multiprocessing
+        threads = multiprocessing.cpu_count()
+        try:
+            g, secs, desc = pairs_reference_sample(pairs, 3, threads)
+            line["cpu_baseline"] = {"value": round(g, 4), "unit": "GCUPS", "cores": threads, "kind": "reference",
+                                    "sample": desc, "seconds": round(secs, 2)}
+        except Exception as e:  # noqa: BLE001
+            line["cpu_baseline"] = {"unavailable": str(e)}
     print(json.dumps(line), flush=True)
     for q in qs:
         L.free_sequence(q)
@@ -554,6 +597,8 @@ def main():
                     help="sw_plain: config 1's 10,000-sequence database with --queries queries of 375")
     ap.add_argument("--queries", type=int, default=None, help="query count for --workload sw_plain")
     ap.add_argument("--pairs", type=int, default=4096, help="pair count for --workload long_pairs")
+    ap.add_argument("--pair-lo", type=int, default=5000, help="shortest query of --workload long_pairs")
+    ap.add_argument("--pair-hi", type=int, default=30000, help="longest query of --workload long_pairs")
     args = ap.parse_args()
     if args.impl == "reference":
         sys.exit(run_reference_arm(args))

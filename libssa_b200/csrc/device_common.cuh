@@ -83,7 +83,7 @@ struct TbHit {
 struct TbRegion {
     int32_t a_begin, a_end;   // query rows
     int32_t b_begin, b_end;   // database columns
-    int32_t fwd_score;
+    int32_t fwd_score;        // SW: forward-pass maximum; NW: H(a_end, b_end) from the direction pass
     int32_t status;           // 0 ok, 1 no positive cell, 2 reverse pass found nothing
 };
 

@@ -349,8 +349,11 @@ private:
             uint32_t seq_hi = UINT32_MAX );
     int32_t * score_sink() { return serving_ ? d_serve_score_.as<int32_t>() : d_score_.as<int32_t>(); }
     void build_profiles( int width, uint32_t n_slots );
+    // scores_from_regions: the hits carry no score yet; take it from the
+    // forward pass (SW, symmetric table) or the direction pass (NW)
     void traceback( const SearchRequest & req, std::vector<std::vector<Hit>> & out,
-            const std::vector<std::pair<uint32_t, uint32_t>> & lists, SearchStats & stats );
+            const std::vector<std::pair<uint32_t, uint32_t>> & lists, SearchStats & stats,
+            bool scores_from_regions = false );
     uint64_t traceback_budget();
     void upload_queries( const QueryCodes * queries, uint32_t nq, bool profiles, SearchStats & stats );
 
@@ -1147,7 +1150,7 @@ static int64_t max_abs_step( const SearchRequest & req ) {
 }
 
 void Engine::traceback( const SearchRequest & req, std::vector<std::vector<Hit>> & out,
-        const std::vector<std::pair<uint32_t, uint32_t>> & lists, SearchStats & stats ) {
+        const std::vector<std::pair<uint32_t, uint32_t>> & lists, SearchStats & stats, bool scores_from_regions ) {
     std::vector<TbHit> hits;
     std::vector<std::pair<uint32_t, uint32_t>> where;   // (list index, hit index)
     for( const auto & l : lists ) {
@@ -1373,7 +1376,15 @@ void Engine::traceback( const SearchRequest & req, std::vector<std::vector<Hit>>
         CUDA_CHECK( cudaMemcpyAsync( ops_len.data(), p.ops_len, nw * sizeof(uint32_t), cudaMemcpyDeviceToHost,
                 stream_ ) );
         CUDA_CHECK( cudaMemcpyAsync( ops.data(), p.ops, wops[nw], cudaMemcpyDeviceToHost, stream_ ) );
+        if( scores_from_regions && req.algo == 1 ) {
+            CUDA_CHECK( cudaMemcpyAsync( wregs.data(), p.regions, nw * sizeof(TbRegion), cudaMemcpyDeviceToHost,
+                    stream_ ) );
+            stats.d2h_bytes += nw * sizeof(TbRegion);
+        }
         check_errors();
+        if( scores_from_regions && req.algo == 1 )
+            for( uint32_t k = 0; k < nw; k++ )
+                regions[wave[k]].fwd_score = wregs[k].fwd_score;
         if( timing ) {
             float a = 0, b = 0;
             CUDA_CHECK( cudaEventElapsedTime( &a, ev_tb_[2], ev_tb_[3] ) );
@@ -1388,6 +1399,8 @@ void Engine::traceback( const SearchRequest & req, std::vector<std::vector<Hit>>
             Hit & hit = out[where[h].first][where[h].second];
             const TbRegion & rg = regions[h];
             hit.has_cigar = true;
+            if( scores_from_regions )
+                hit.score = rg.fwd_score;
             if( rg.status != 0 ) {
                 // no positive cell: the reference leaves the region undefined here
                 hit.q_start = hit.q_end = hit.d_start = hit.d_end = 0;
@@ -1495,7 +1508,25 @@ void Engine::align_pairs( const SearchRequest & req, const std::vector<QueryCode
     d_counts_.ensure( 32 * sizeof(unsigned long long) );
     CUDA_CHECK( cudaMemsetAsync( d_counts_.p, 0, 32 * sizeof(unsigned long long), stream_ ) );
     const uint32_t nw = (uint32_t) work.size();
-    if( nw ) {
+    // With alignments the traceback passes compute the score themselves: the
+    // direction pass ends on cell (A - 1, B - 1) of the same recurrence
+    // (Needleman-Wunsch), the forward region pass finds the same maximum when
+    // the score table is symmetric (Smith-Waterman; it scores [query][db])
+    bool symmetric = true;
+    for( int d = 0; d < 32; d++ )
+        for( int q = 0; q < 32; q++ )
+            symmetric = symmetric && req.matrix[(d << 5) + q] == req.matrix[(q << 5) + d];
+    const bool scores_in_traceback = req.align_type == COMPUTE_ALIGNMENT && (req.algo == 1 || symmetric);
+    if( nw && scores_in_traceback ) {
+        for( uint32_t k = 0; k < nw; k++ ) {
+            const uint32_t i = work[k];
+            Hit h;
+            h.unit = units[i];
+            h.id = units[i] / db.upi;
+            out[i].push_back( h );
+        }
+    }
+    else if( nw ) {
         std::vector<uint32_t> hs( nw ), hu( nw );
         for( uint32_t k = 0; k < nw; k++ ) {
             hs[k] = work[k];
@@ -1561,7 +1592,7 @@ void Engine::align_pairs( const SearchRequest & req, const std::vector<QueryCode
             if( !out[i].empty() )
                 lists.emplace_back( i, i );
         const auto t0 = std::chrono::steady_clock::now();
-        traceback( req, out, lists, stats );
+        traceback( req, out, lists, stats, scores_in_traceback );
         stats.kernel_seconds += std::chrono::duration<double>( std::chrono::steady_clock::now() - t0 ).count();
     }
     CUDA_CHECK( cudaEventRecord( ev1_, stream_ ) );

@@ -478,6 +478,7 @@ struct DirectionStripe : TbStripeBase<W> {
     bool nw;
     int32_t b_begin;
     uint16_t * dir;
+    int32_t * corner;              // Needleman-Wunsch: receives H(A - 1, B - 1)
 
     __device__ void begin( uint32_t stripe ) {
         const int32_t gO = this->gO, gE = this->gE;
@@ -542,6 +543,14 @@ struct DirectionStripe : TbStripeBase<W> {
             this->out_f = f;
             if( j >= b_begin && (uint32_t) (row0 / TB_R) < words )
                 dir[(uint64_t) (j - b_begin) * words + row0 / TB_R] = (uint16_t) code;
+            if( nw && j == (int32_t) B - 1 ) {
+                // the global score: the last cell of the full matrix
+                const int32_t rl = (int32_t) A - 1 - row0;
+#pragma unroll
+                for( int r = 0; r < TB_R; r++ )
+                    if( r == rl )
+                        *corner = this->H[r];
+            }
             this->put_bottom( j );
         }
         return s0 + 32 < steps;
@@ -572,6 +581,7 @@ __global__ void __launch_bounds__( 256 ) tb_directions_kernel( TbParams p ) {
             body.b_begin = rg.b_begin;
             body.a = p.qcodes + p.qoff[hit.qslot];
             body.dir = p.dirs + p.dir_off[h];
+            body.corner = &p.regions[h].fwd_score;
             body.rr = ResidueRing{ grp.sh->residues[grp.wig], 0, p.db.codes + p.db.offsets[hit.id], (int32_t) body.B,
                                    -1 };
             run_stripes<W>( body, *grp.sh, grp.gb, grp.wig, grp.lane, (body.A + TB_ROWS - 1) / TB_ROWS, body.B,

@@ -106,6 +106,38 @@ def test_long_pairs_beyond_16_bits(built_library, algo):
             assert want[0][1] > 32767
 
 
+def _asymmetric_table() -> str:
+    """A score table with M[x][y] != M[y][x]: the region passes score
+    [query][db] and the search [db][query], so the forward pass's maximum is
+    not the score and the pair keeps its separate score pass."""
+    aa = "ARNDCQEGHILKMFPSTWYV"
+    lines = ["   " + "  ".join(aa)]
+    for i, x in enumerate(aa):
+        row = [5 if i == j else ((i * 7 + j * 3) % 9) - 6 for j in range(20)]
+        lines.append(x + " " + " ".join(f"{v:2d}" for v in row))
+    return "\n".join(lines) + "\n"
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("algo", ["sw", "nw"])
+def test_pairs_asymmetric_table(built_library, algo):
+    import libssa_b200 as L
+    text = _asymmetric_table()
+    queries, records, ids = _pairs(31, 10, 100, 2000)
+    product_setup(1, MATRIX, GAP, 1000, 2, records=records)
+    L.init_score_matrix(L.READ_FROM_STRING, text)
+    try:
+        got = _product(algo, 16, 1, queries, ids)
+    finally:
+        L.init_score_matrix(L.MATRIX_BUILDIN, "blosum62")
+    cfg = oracle.SearchConfig(algo=algo, bit_width=16, align_type=1, hitcount=1, gap_open=GAP[0], gap_extend=GAP[1],
+                              matrix=oracle.parse_matrix(text))
+    for i, q in enumerate(queries):
+        hits, _ = oracle.search(cfg, oracle.map_codes(q.decode(), False, True),
+                                [oracle.map_codes(records[ids[i]].decode(), False, False)])
+        assert got[i] == [(ids[i], h.score, h.cigar, h.q_start, h.q_end, h.d_start, h.d_end) for h in hits], i
+
+
 @pytest.mark.gpu
 def test_pairs_in_memory_waves(built_library):
     import libssa_b200 as L
