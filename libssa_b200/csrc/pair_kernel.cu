@@ -76,14 +76,13 @@ struct PairStripe {
         const uint32_t steps = B + 31;
         const uint32_t s0 = ck * 32;
         const int32_t rl = (int32_t) A - 1 - row0;    // Needleman-Wunsch: row A - 1 on this lane
-        for( uint32_t s = s0; s < s0 + 32 && s < steps; s++ ) {
-            link.step( B, s, lane );
-            rr.step( s, lane );
+        // one wavefront step; edge: some lane may be on a column outside 0..B-1
+        auto column = [&]( const uint32_t s, const bool edge ) {
             int32_t up_h = __shfl_up_sync( 0xffffffffu, out_h, 1 );
             int32_t up_f = __shfl_up_sync( 0xffffffffu, out_f, 1 );
             const int32_t c = (int32_t) s - lane;
-            if( c < 0 || c >= (int32_t) B )
-                continue;
+            if( edge && (c < 0 || c >= (int32_t) B) )
+                return;
             if( lane == 0 ) {
                 if( link.stripe == 0 ) {
                     // the reference's row before the first: H(-1, c) (the next
@@ -128,6 +127,18 @@ struct PairStripe {
                     if( r == rl )
                         best = H[r];
             }
+        };
+        // the residue ring and the boundary prefetch refill at the first step of a chunk
+        link.step( B, s0, lane );
+        rr.step( s0, lane );
+        const uint32_t s1 = min( s0 + 32, steps );
+        if( s0 >= 31 && s1 <= B ) {
+            for( uint32_t s = s0; s < s1; s++ )
+                column( s, false );
+        }
+        else {
+            for( uint32_t s = s0; s < s1; s++ )
+                column( s, true );
         }
         return s0 + 32 < steps;
     }

@@ -177,14 +177,13 @@ struct ForwardStripe : TbStripeBase<W> {
         const uint32_t steps = B + 31, s0 = ck * 32;
         const int lane = this->lane;
         const int32_t gE = this->gE, gOE = this->gOE;
-        for( uint32_t s = s0; s < s0 + 32 && s < steps; s++ ) {
-            this->link.step( B, s, lane );
-            this->rr.step( s, lane );
+        // one wavefront step; edge: some lane may be on a column outside 0..B-1
+        auto column = [&]( const uint32_t s, const bool edge ) {
             int32_t up_h = __shfl_up_sync( 0xffffffffu, this->out_h, 1 );
             int32_t up_f = __shfl_up_sync( 0xffffffffu, this->out_f, 1 );
             const int32_t c = (int32_t) s - lane;
-            if( c < 0 || c >= (int32_t) B )
-                continue;
+            if( edge && (c < 0 || c >= (int32_t) B) )
+                return;
             // f starts at gapO: max(gapO, 0 + gapO) + gapE
             this->above( s, c, 0, this->gO + gE, up_h, up_f );
             int32_t f = up_f, hd = this->diag;
@@ -221,6 +220,18 @@ struct ForwardStripe : TbStripeBase<W> {
             this->out_h = this->H[TB_R - 1];
             this->out_f = f;
             this->put_bottom( c );
+        };
+        // the residue ring and the boundary prefetch refill at the first step of a chunk
+        this->link.step( B, s0, lane );
+        this->rr.step( s0, lane );
+        const uint32_t s1 = min( s0 + 32, steps );
+        if( s0 >= 31 && s1 <= B ) {
+            for( uint32_t s = s0; s < s1; s++ )
+                column( s, false );
+        }
+        else {
+            for( uint32_t s = s0; s < s1; s++ )
+                column( s, true );
         }
         return s0 + 32 < steps;
     }
@@ -321,8 +332,9 @@ struct ReverseStripe : TbStripeBase<W> {
     int32_t score, a_end, b_end;
     const int32_t * lh;
     const int32_t * le;
-    int32_t hit_i, hit_j;          // the lane's first (i', j') reaching the score, over its stripes
-    int32_t cand;                  // = hit_i, read by run_stripes after each chunk
+    int32_t hit_i, hit_j;          // the lane's first (i', j') reaching the score, over its finished stripes
+    int32_t s_i, s_j;              // the same in the current stripe
+    int32_t cand;                  // the lane's first column so far, read by run_stripes after each chunk
 
     __device__ void begin( uint32_t stripe ) {
         const int lane = this->lane;
@@ -347,6 +359,8 @@ struct ReverseStripe : TbStripeBase<W> {
         // for the end cell itself
         const int32_t jprev = a_end - (row0 - 1);
         this->diag = (row0 == 0) ? 0 : ((jprev > b_end) ? lh[jprev] : -1);
+        s_i = INT_MAX;
+        s_j = INT_MAX;
         this->out_h = 0;
         this->out_f = 0;
         this->link.start( B, lane );
@@ -359,14 +373,13 @@ struct ReverseStripe : TbStripeBase<W> {
         const uint32_t steps = cols + 31, s0 = ck * 32;
         const int lane = this->lane;
         const int32_t gO = this->gO, gE = this->gE, gOE = this->gOE;
-        for( uint32_t s = s0; s < s0 + 32 && s < steps; s++ ) {
-            this->link.step( B, s, lane );
-            this->rr.step( s, lane );
+        // one wavefront step; edge: some lane may be on a column outside 0..B-1
+        auto column = [&]( const uint32_t s, const bool edge ) {
             int32_t up_h = __shfl_up_sync( 0xffffffffu, this->out_h, 1 );
             int32_t up_f = __shfl_up_sync( 0xffffffffu, this->out_f, 1 );
             const int32_t c = (int32_t) s - lane;
-            if( c < 0 || c >= (int32_t) B )
-                continue;
+            if( edge && (c < 0 || c >= (int32_t) B) )
+                return;
             // h starts at -1 per row; f = max(-1, h + gapO) + gapE
             this->above( s, c, -1, max( -1, -1 + gO ) + gE, up_h, up_f );
             const int d = this->rr.get( s, lane );          // database index b_end - c
@@ -375,10 +388,11 @@ struct ReverseStripe : TbStripeBase<W> {
             for( int r = 0; r < TB_R; r++ ) {
                 const int32_t e_in = this->E[r];
                 const int32_t x = __vimax3_s32( hd + mget( this->smat, d, this->qa[r] ), f, e_in );
-                const bool take = (r < this->nvalid) && x >= score &&
-                        (c < hit_i || (c == hit_i && this->row0 + r < hit_j));
-                hit_i = take ? c : hit_i;
-                hit_j = take ? this->row0 + r : hit_j;
+                // the lane visits a stripe's cells in (column, row) order: its
+                // first candidate in the stripe is the stripe's best on the lane
+                const bool take = (r < this->nvalid) && x >= score && s_i == INT_MAX;
+                s_i = take ? c : s_i;
+                s_j = take ? this->row0 + r : s_j;
                 hd = this->H[r];
                 this->H[r] = x;
                 const int32_t y = x + gOE;
@@ -389,12 +403,30 @@ struct ReverseStripe : TbStripeBase<W> {
             this->out_h = this->H[TB_R - 1];
             this->out_f = f;
             this->put_bottom( c );
+        };
+        // the residue ring and the boundary prefetch refill at the first step of a chunk
+        this->link.step( B, s0, lane );
+        this->rr.step( s0, lane );
+        const uint32_t s1 = min( s0 + 32, steps );
+        if( s0 >= 31 && s1 <= B ) {
+            for( uint32_t s = s0; s < s1; s++ )
+                column( s, false );
         }
-        cand = hit_i;
+        else {
+            for( uint32_t s = s0; s < s1; s++ )
+                column( s, true );
+        }
+        cand = min( hit_i, s_i );
         return s0 + 32 < steps;
     }
 
-    __device__ void end() {}
+    // this stripe's first candidate against the earlier stripes' ((i', j') asc)
+    __device__ void end() {
+        if( s_i < hit_i || (s_i == hit_i && s_j < hit_j) ) {
+            hit_i = s_i;
+            hit_j = s_j;
+        }
+    }
 };
 
 template <int W>
@@ -506,14 +538,13 @@ struct DirectionStripe : TbStripeBase<W> {
         const int lane = this->lane;
         const int32_t gO = this->gO, gE = this->gE, gOE = this->gOE;
         const int32_t row0 = this->row0;
-        for( uint32_t s = s0; s < s0 + 32 && s < steps; s++ ) {
-            this->link.step( B, s, lane );
-            this->rr.step( s, lane );
+        // one wavefront step; edge: some lane may be on a column outside 0..B-1
+        auto column = [&]( const uint32_t s, const bool edge ) {
             int32_t up_h = __shfl_up_sync( 0xffffffffu, this->out_h, 1 );
             int32_t up_f = __shfl_up_sync( 0xffffffffu, this->out_f, 1 );
             const int32_t j = (int32_t) s - lane;     // database index
-            if( j < 0 || j >= (int32_t) B )
-                continue;
+            if( edge && (j < 0 || j >= (int32_t) B) )
+                return;
             // H(-1, j) is the next column's row-0 diagonal
             this->above( s, j, nw ? gO + (j + 1) * gE : 0, nw ? 2 * gO + (j + 2) * gE : 0, up_h, up_f );
             const int d = this->rr.get( s, lane );
@@ -525,18 +556,20 @@ struct DirectionStripe : TbStripeBase<W> {
             for( int r = 0; r < TB_R; r++ ) {
                 const int32_t e = this->E[r];
                 const int32_t x0 = hd + mget( this->smat, d, this->qa[r] );
-                const bool up = f > x0;                      // UP
-                const bool left = e > max( x0, f );          // LEFT
-                const int32_t x = __vimax3_s32( nw ? x0 : max( x0, 0 ), f, e );
+                // each max also yields the negation of one strict flag
+                bool no_up, no_left, no_ext_up, no_ext_left;
+                const int32_t m1 = __vibmax_s32( x0, f, &no_up );       // UP: f > x0
+                const int32_t xr = __vibmax_s32( m1, e, &no_left );     // LEFT: e > max(x0, f)
+                const int32_t x = nw ? xr : max( xr, 0 );
                 hd = this->H[r];
                 this->H[r] = x;
                 const int32_t y = x + gOE;
-                const bool ext_up = f + gE > y;              // EXT_UP
-                const bool ext_left = e + gE > y;            // EXT_LEFT
-                f = __viaddmax_s32( f, gE, y );
-                this->E[r] = __viaddmax_s32( e, gE, y );
-                const uint32_t op = (left || ext_left) ? 2u : ((up || ext_up) ? 1u : 0u);
-                code |= (r < this->nvalid) ? op << (2 * r) : 0u;
+                f = __vibmax_s32( y, f + gE, &no_ext_up );               // EXT_UP: f + gapE > y
+                this->E[r] = __vibmax_s32( y, e + gE, &no_ext_left );    // EXT_LEFT: e + gapE > y
+                // rows past the query's end get codes too; the walk never reads them
+                const bool ins = !(no_left && no_ext_left);
+                const bool del = !(no_up && no_ext_up);
+                code |= (ins ? 2u : (del ? 1u : 0u)) << (2 * r);
             }
             this->diag = up_h;
             this->out_h = this->H[TB_R - 1];
@@ -552,6 +585,18 @@ struct DirectionStripe : TbStripeBase<W> {
                         *corner = this->H[r];
             }
             this->put_bottom( j );
+        };
+        // the residue ring and the boundary prefetch refill at the first step of a chunk
+        this->link.step( B, s0, lane );
+        this->rr.step( s0, lane );
+        const uint32_t s1 = min( s0 + 32, steps );
+        if( s0 >= 31 && s1 <= B ) {
+            for( uint32_t s = s0; s < s1; s++ )
+                column( s, false );
+        }
+        else {
+            for( uint32_t s = s0; s < s1; s++ )
+                column( s, true );
         }
         return s0 + 32 < steps;
     }
