@@ -296,6 +296,8 @@ def run_ours(args):
     L.set_chunk_size(1000)
     L.set_simd_compute_mode(L.COMPUTE_ON_AVX2)
     L.load_db_memory(flat=w.db_flat, offsets=w.db_offsets)
+    if args.db_memory:
+        L.set_db_memory(args.db_memory)     # below the packed size: the database is streamed
     qs = [L.init_sequence_fasta(L.READ_FROM_STRING, q.decode()) for q in w.queries]
     cells = sum(len(q) for q in w.queries) * int(w.db_offsets[-1])
 
@@ -346,7 +348,8 @@ def run_ours(args):
                    "matrix": "blosum62", "gap": [-11, -1], "bit_width": 8, "hits": 10,
                    "align_type": "COMPUTE_ALIGNMENT", "scale": args.scale,
                    "l2": "inputs larger than L2 (database codes %.2f GB)" % (int(w.db_offsets[-1]) / 1e9),
-                   "parallelism": f"{world} x independent query batch vs full database"},
+                   "parallelism": f"{world} x independent query batch vs full database",
+                   "db_streamed": bool(L.db_streamed())},
         "e2e": {"value": round(e2e, 2), "unit": "GCUPS", "h2d_bytes_per_step": int(statistics.median(h2d)),
                 "d2h_bytes_per_step": int(statistics.median(d2h))},
         "roofline": {"bound": "alu", "achieved": round(achieved, 3), "peak": round(peak, 3),
@@ -596,6 +599,8 @@ def main():
     ap.add_argument("--workload", default="sw_batched", choices=["sw_batched", "sw_plain", "sw_served", "nw_nucleotide", "long_pairs"],
                     help="sw_plain: config 1's 10,000-sequence database with --queries queries of 375")
     ap.add_argument("--queries", type=int, default=None, help="query count for --workload sw_plain")
+    ap.add_argument("--db-memory", type=int, default=0,
+                    help="device memory for the database in bytes (0 = automatic; smaller streams it)")
     ap.add_argument("--pairs", type=int, default=4096, help="pair count for --workload long_pairs")
     ap.add_argument("--pair-lo", type=int, default=5000, help="shortest query of --workload long_pairs")
     ap.add_argument("--pair-hi", type=int, default=30000, help="longest query of --workload long_pairs")

@@ -55,6 +55,18 @@ int ssa_align_pairs( int algorithm, p_query * queries, const size_t * db_ids, si
  * several waves.  0 (the default) = the free device memory less a reserve. */
 void ssa_b200_set_traceback_memory( size_t bytes );
 
+/* Device memory (bytes) for the packed database.  A database that needs more
+ * is streamed: its sequences, in segments of the length order, take turns on
+ * the device during each search (each segment's entry pass and overflow
+ * cascade run while it is resident), and the hits' sequences are gathered for
+ * the traceback; results are the same.  The server (ssa_server_start) needs a
+ * resident database.  0 (the default) = 40% of the device memory.  Takes
+ * effect at the next search. */
+void ssa_b200_set_db_memory( size_t bytes );
+
+/* 1 if the current database is streamed, else 0 (packs it first if needed). */
+int ssa_b200_db_streamed( void );
+
 /* Counters of the last search call. */
 typedef struct {
     uint64_t overflow_8_to_16;       /* sequences re-aligned at 16 bit */

@@ -38,7 +38,8 @@ EXPORTED = [
     "free_sequence", "sw_align", "nw_align", "free_alignment", "ssa_exit", "ssa_align_batch", "ssa_get_stats",
     "ssa_query_length", "ssa_db_refresh", "ssa_b200_int_peak", "ssa_b200_score64_noalloc",
     "ssa_server_start", "ssa_server_submit", "ssa_server_wait", "ssa_server_get_stats", "ssa_server_stop",
-    "ssa_b200_translation_table", "ssa_align_pairs", "ssa_b200_set_traceback_memory",
+    "ssa_b200_translation_table", "ssa_align_pairs", "ssa_b200_set_traceback_memory", "ssa_b200_set_db_memory",
+    "ssa_b200_db_streamed",
 ]
 
 # allocation-free scoring (include/libssa_b200.h)
@@ -119,6 +120,8 @@ def load():
                                     ctypes.c_size_t, ctypes.c_int, ctypes.c_int, ctypes.POINTER(P_LIST)]
     lib.ssa_align_pairs.restype = ctypes.c_int
     lib.ssa_b200_set_traceback_memory.argtypes = [ctypes.c_size_t]
+    lib.ssa_b200_set_db_memory.argtypes = [ctypes.c_size_t]
+    lib.ssa_b200_db_streamed.restype = ctypes.c_int
     lib.ssa_get_stats.argtypes = [ctypes.POINTER(Stats)]
     lib.ssa_db_refresh.argtypes = []
     lib.ssa_b200_int_peak.argtypes = [ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
@@ -295,6 +298,15 @@ def align_pairs(algorithm: int, queries: list, db_ids: list[int], bit_width: int
         out.append(_read_list(res[i]))
         lib.free_alignment(res[i])
     return out
+
+
+def set_db_memory(nbytes: int) -> None:
+    """Device memory for the packed database (0 = automatic); a larger database is streamed."""
+    load().ssa_b200_set_db_memory(nbytes)
+
+
+def db_streamed() -> bool:
+    return bool(load().ssa_b200_db_streamed())
 
 
 def set_traceback_memory(nbytes: int) -> None:

@@ -913,6 +913,14 @@ void ssa_b200_set_traceback_memory( size_t bytes ) {
     engine_set_traceback_memory( (uint64_t) bytes );
 }
 
+void ssa_b200_set_db_memory( size_t bytes ) {
+    engine_set_db_memory( (uint64_t) bytes );
+}
+
+int ssa_b200_db_streamed( void ) {
+    return engine_streaming() ? 1 : 0;
+}
+
 void ssa_get_stats( ssa_stats_t * out ) {
     if( !out )
         return;
@@ -959,6 +967,9 @@ ssa_server * ssa_server_start( int algorithm, size_t hitcount, int bit_width, in
         fatal( "Nucleotide sequences can only be aligned using constant scores." );
     if( !(c.symtype == AMINOACID || (c.symtype == NUCLEOTIDE && c.strands == FORWARD_STRAND)) )
         fatal( "The server runs protein and forward-strand nucleotide searches only." );
+    if( engine_streaming() )
+        fatal( "The server keeps the database resident in device memory; this database is larger than the "
+                "database memory budget (ssa_b200_set_db_memory)." );
     ssa_server * sv = new ssa_server();
     ServerImpl & s = sv->impl;
     s.req = make_request( algorithm == SSA_SMITH_WATERMAN ? 0 : 1, hitcount, bit_width, align_type );

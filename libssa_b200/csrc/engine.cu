@@ -28,6 +28,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
+#include <unordered_map>
 #include <thread>
 #include <tuple>
 
@@ -119,6 +120,8 @@ public:
         CUDA_CHECK( cudaEventCreateWithFlags( &ev_ready_, cudaEventDisableTiming ) );
         for( auto & e : ev_phase_ )
             CUDA_CHECK( cudaEventCreate( &e ) );
+        for( auto & e : ev_seg_ )
+            CUDA_CHECK( cudaEventCreate( &e ) );
         for( auto & e : ev_tb_ )
             CUDA_CHECK( cudaEventCreate( &e ) );
         for( int i = 0; i < 4; i++ ) {
@@ -158,7 +161,6 @@ public:
         if( cfg.symtype == TRANS_DB || cfg.symtype == TRANS_BOTH )
             fatal( "Searches of a translated database (symbol type %d) are not supported by the B200 build.",
                     cfg.symtype );
-        uint64_t total = 0;
         std::vector<p_seqinfo> infos( n_rec );
         for( size_t id = 0; id < n_rec; id++ ) {
             p_seqinfo info = ssa_db_get_sequence( id );
@@ -167,13 +169,69 @@ public:
             infos[id] = info;
             if( info->seqlen > (size_t) INT32_MAX / 2 )
                 fatal( "Database sequence %zu is too long (%zu residues).", id, info->seqlen );
-            for( uint32_t k = 0; k < upi; k++ ) {
-                const size_t u = id * upi + k;
-                db.len[u] = (uint32_t) info->seqlen;
-                db.off[u] = total;
-                total += (info->seqlen + 15) & ~(uint64_t) 15;
-            }
+            for( uint32_t k = 0; k < upi; k++ )
+                db.len[id * upi + k] = (uint32_t) info->seqlen;
             db.max_len = std::max( db.max_len, (uint32_t) info->seqlen );
+            db.residues += (uint64_t) info->seqlen * upi;
+        }
+        db.nonempty_before.assign( (size_t) n + 1, 0 );
+        for( uint32_t id = 0; id < db.n_ids; id++ ) {
+            db.nonempty_before[id + 1] = db.nonempty_before[id] + (db.len[id] ? 1 : 0);
+            if( db.len[id] )
+                db.order_desc.push_back( id );
+        }
+        std::stable_sort( db.order_desc.begin(), db.order_desc.end(),
+                [&]( uint32_t a, uint32_t b ) { return db.len[a] > db.len[b]; } );
+        auto padded = [&]( uint32_t id ) { return ((uint64_t) db.len[id] + 15) & ~(uint64_t) 15; };
+
+        // Resident layout: every ID in ID order, plus the interleaved pairs of
+        // the single-query pass.  Streaming layout (the resident one does not
+        // fit the database memory): segments of consecutive IDs in length
+        // order, each a contiguous block that is copied to the device when its
+        // turn comes; the device offsets are relative to the block.
+        init_device();
+        uint64_t codes_bytes = 0;
+        for( uint32_t id = 0; id < db.n_ids; id++ )
+            codes_bytes += padded( id );
+        const uint64_t resident_bytes = 2 * codes_bytes + (uint64_t) n * (8 + 4 + 4) + 64;
+        const uint64_t budget = db_budget();
+        streaming_ = resident_bytes > budget;
+        seg_lo_.clear();
+        seg_hi_.clear();
+        seg_off_.clear();
+        seg_bytes_.clear();
+        std::vector<uint64_t> dev_off( n, 0 );
+        uint64_t total = 0;
+        if( !streaming_ ) {
+            for( uint32_t id = 0; id < db.n_ids; id++ ) {
+                db.off[id] = total;
+                dev_off[id] = total;
+                total += padded( id );
+            }
+        }
+        else {
+            const uint64_t seg_cap = std::max<uint64_t>( 1, budget / 2 );
+            uint64_t in_seg = 0;
+            for( uint32_t pos = 0; pos < (uint32_t) db.order_desc.size(); pos++ ) {
+                const uint32_t id = db.order_desc[pos];
+                if( seg_lo_.empty() || (in_seg > 0 && in_seg + padded( id ) > seg_cap) ) {
+                    if( !seg_lo_.empty() ) {
+                        seg_hi_.push_back( pos );
+                        seg_bytes_.push_back( in_seg );
+                    }
+                    seg_lo_.push_back( pos );
+                    seg_off_.push_back( total );
+                    in_seg = 0;
+                }
+                db.off[id] = total;
+                dev_off[id] = in_seg;
+                total += padded( id );
+                in_seg += padded( id );
+            }
+            if( !seg_lo_.empty() ) {
+                seg_hi_.push_back( (uint32_t) db.order_desc.size() );
+                seg_bytes_.push_back( in_seg );
+            }
         }
         db.codes.assign( total + 16, 0 );
         uint64_t unknown = 0;
@@ -181,6 +239,8 @@ public:
             // unknown symbols become code 0 (reference: src/util/util_sequence.c:298-318)
             const char * s = infos[id]->seq;
             const size_t L = infos[id]->seqlen;
+            if( L == 0 )
+                continue;
             uint8_t * o = db.codes.data() + db.off[id * upi];
             for( size_t k = 0; k < L; k++ ) {
                 int m = nt ? map_nt16( (unsigned char) s[k] ) : map_aa( (unsigned char) s[k] );
@@ -196,22 +256,41 @@ public:
                 for( size_t k = 0; k < L; k++ )
                     rc[k] = nt_complement( o[L - 1 - k] );
             }
-            db.residues += (uint64_t) L * upi;
         }
         if( unknown )
             print_warning( "%llu unknown symbols found and set to zero", (unsigned long long) unknown );
-        db.nonempty_before.assign( (size_t) n + 1, 0 );
-        for( uint32_t id = 0; id < db.n_ids; id++ ) {
-            db.nonempty_before[id + 1] = db.nonempty_before[id] + (db.len[id] ? 1 : 0);
-            if( db.len[id] )
-                db.order_desc.push_back( id );
-        }
-        std::stable_sort( db.order_desc.begin(), db.order_desc.end(),
-                [&]( uint32_t a, uint32_t b ) { return db.len[a] > db.len[b]; } );
         db.symtype = cfg.symtype;
         db.strands = cfg.strands;
         db.generation = ++generation_;
         db.mean_len = db.order_desc.empty() ? 0.0 : (double) db.residues / (double) db.order_desc.size();
+
+        d_off_.ensure( sizeof(uint64_t) * std::max<size_t>( 1, n ) );
+        d_len_.ensure( sizeof(uint32_t) * std::max<size_t>( 1, n ) );
+        d_order_.ensure( sizeof(uint32_t) * std::max<size_t>( 1, db.order_desc.size() ) );
+        if( n ) {
+            CUDA_CHECK( cudaMemcpy( d_off_.p, dev_off.data(), sizeof(uint64_t) * n, cudaMemcpyHostToDevice ) );
+            CUDA_CHECK( cudaMemcpy( d_len_.p, db.len.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice ) );
+        }
+        if( !db.order_desc.empty() )
+            CUDA_CHECK( cudaMemcpy( d_order_.p, db.order_desc.data(), sizeof(uint32_t) * db.order_desc.size(),
+                    cudaMemcpyHostToDevice ) );
+        resident_seg_ = -1;
+        if( streaming_ ) {
+            DevBuf * big[] = { &d_codes_, &d_pair_res_, &d_pair_off_, &d_pair_cols_, &d_pair_ids_ };
+            for( DevBuf * b : big )
+                b->release();
+            uint64_t max_seg = 0;
+            for( uint64_t b : seg_bytes_ )
+                max_seg = std::max( max_seg, b );
+            for( DevBuf & b : d_seg_ )
+                b.ensure( max_seg + 64 );
+            db_ = std::move( db );
+            db_stale_ = false;
+            ranks_.clear();
+            return;
+        }
+        for( DevBuf & b : d_seg_ )
+            b.release();
 
         // pairs of consecutive sequences in length order share the 16x2 lanes
         // of the fast Smith-Waterman pass; columns past a sequence's last
@@ -242,20 +321,8 @@ public:
                     out[2 * j + half] = 0;   // the reference's pad inside the last block
             }
         }
-
-        init_device();
         d_codes_.ensure( db.codes.size() );
-        d_off_.ensure( sizeof(uint64_t) * std::max<size_t>( 1, n ) );
-        d_len_.ensure( sizeof(uint32_t) * std::max<size_t>( 1, n ) );
-        d_order_.ensure( sizeof(uint32_t) * std::max<size_t>( 1, db.order_desc.size() ) );
         CUDA_CHECK( cudaMemcpy( d_codes_.p, db.codes.data(), db.codes.size(), cudaMemcpyHostToDevice ) );
-        if( n ) {
-            CUDA_CHECK( cudaMemcpy( d_off_.p, db.off.data(), sizeof(uint64_t) * n, cudaMemcpyHostToDevice ) );
-            CUDA_CHECK( cudaMemcpy( d_len_.p, db.len.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice ) );
-        }
-        if( !db.order_desc.empty() )
-            CUDA_CHECK( cudaMemcpy( d_order_.p, db.order_desc.data(), sizeof(uint32_t) * db.order_desc.size(),
-                    cudaMemcpyHostToDevice ) );
         {
             std::vector<uint2> ids( std::max<size_t>( 1, n_pairs ) );
             for( size_t pi = 0; pi < n_pairs; pi++ )
@@ -279,7 +346,7 @@ public:
 
     DbView db_view() const {
         DbView v;
-        v.codes = d_codes_.as<uint8_t>();
+        v.codes = streaming_ ? d_seg_[resident_seg_ & 1].as<uint8_t>() : d_codes_.as<uint8_t>();
         v.offsets = d_off_.as<uint64_t>();
         v.lens = d_len_.as<uint32_t>();
         v.n_ids = db_.n_ids;
@@ -306,6 +373,67 @@ public:
     void align_pairs( const SearchRequest & req, const std::vector<QueryCodes> & queries,
             const std::vector<uint32_t> & units, std::vector<std::vector<Hit>> & out, SearchStats & stats );
     void set_traceback_budget( uint64_t bytes ) { tb_budget_ = bytes; }
+    void set_db_budget( uint64_t bytes ) {
+        db_budget_ = bytes;
+        db_stale_ = true;
+    }
+    bool streaming() const { return streaming_; }
+
+    // Device memory for the database: the setting of ssa_b200_set_db_memory,
+    // else 40% of the device memory (scores, re-queue lists, profiles and
+    // traceback matrices take the rest).
+    uint64_t db_budget() {
+        if( db_budget_ )
+            return db_budget_;
+        size_t free_b = 0, total_b = 0;
+        CUDA_CHECK( cudaMemGetInfo( &free_b, &total_b ) );
+        return (uint64_t) total_b / 5 * 2;
+    }
+
+    // Segment s of a streamed database on the device (the other buffer keeps
+    // the previous one); a no-op when it is there already.
+    void make_resident( uint32_t sg, SearchStats & stats ) {
+        if( !streaming_ || resident_seg_ == (int) sg )
+            return;
+        const uint64_t bytes = seg_bytes_[sg];
+        uint8_t * stage = (uint8_t *) h_stage_.ensure( std::max<uint64_t>( bytes, 16 ) );
+        // the staging buffer is reused: the previous copy must have finished
+        CUDA_CHECK( cudaStreamSynchronize( stream_ ) );
+        memcpy( stage, db_.codes.data() + seg_off_[sg], bytes );
+        CUDA_CHECK( cudaMemcpyAsync( d_seg_[sg & 1].p, stage, bytes, cudaMemcpyHostToDevice, stream_ ) );
+        resident_seg_ = (int) sg;
+        stats.h2d_bytes += bytes;
+    }
+
+    // A device view of the given database IDs alone (in that order, view ID k =
+    // ids[k]), for passes over a few sequences of a streamed database.
+    DbView gather_view( const std::vector<uint32_t> & ids, SearchStats & stats ) {
+        std::vector<uint64_t> off( ids.size() + 1, 0 );
+        std::vector<uint32_t> len( std::max<size_t>( 1, ids.size() ), 0 );
+        for( size_t k = 0; k < ids.size(); k++ ) {
+            len[k] = db_.len[ids[k]];
+            off[k + 1] = off[k] + (((uint64_t) len[k] + 15) & ~(uint64_t) 15);
+        }
+        std::vector<uint8_t> codes( off[ids.size()] + 64, 0 );
+        for( size_t k = 0; k < ids.size(); k++ )
+            memcpy( codes.data() + off[k], db_.codes.data() + db_.off[ids[k]], len[k] );
+        d_gather_codes_.ensure( codes.size() );
+        d_gather_off_.ensure( off.size() * sizeof(uint64_t) );
+        d_gather_len_.ensure( len.size() * sizeof(uint32_t) );
+        CUDA_CHECK( cudaMemcpyAsync( d_gather_codes_.p, codes.data(), codes.size(), cudaMemcpyHostToDevice, stream_ ) );
+        CUDA_CHECK( cudaMemcpyAsync( d_gather_off_.p, off.data(), off.size() * sizeof(uint64_t),
+                cudaMemcpyHostToDevice, stream_ ) );
+        CUDA_CHECK( cudaMemcpyAsync( d_gather_len_.p, len.data(), len.size() * sizeof(uint32_t),
+                cudaMemcpyHostToDevice, stream_ ) );
+        CUDA_CHECK( cudaStreamSynchronize( stream_ ) );   // the host vectors go out of scope
+        stats.h2d_bytes += codes.size() + off.size() * sizeof(uint64_t) + len.size() * sizeof(uint32_t);
+        DbView v;
+        v.codes = d_gather_codes_.as<uint8_t>();
+        v.offsets = d_gather_off_.as<uint64_t>();
+        v.lens = d_gather_len_.as<uint32_t>();
+        v.n_ids = (uint32_t) ids.size();
+        return v;
+    }
 
     void shutdown() {
         DevBuf * bufs[] = { &d_codes_, &d_off_, &d_len_, &d_order_, &d_pair_res_, &d_pair_off_, &d_pair_cols_,
@@ -314,10 +442,14 @@ public:
             &d_prof_off_, &d_prof_, &d_matrix_, &d_score_, &d_list_a_, &d_list_b_, &d_counts_, &d_scratch_,
             &d_tb_hits_, &d_tb_regions_, &d_tb_last_, &d_tb_last_off_, &d_tb_dirs_, &d_tb_dir_off_, &d_tb_ops_,
             &d_tb_ops_off_, &d_tb_ops_len_, &d_qp_prof_, &d_qp_off_, &d_qp_rows_, &d_qp_slots_, &d_qp_units_,
-            &d_serve_score_, &d_qp_lmax_, &d_pair_slot_, &d_pair_unit_, &d_pair_score_, &d_scratch4_ };
+            &d_serve_score_, &d_qp_lmax_, &d_pair_slot_, &d_pair_unit_, &d_pair_score_, &d_scratch4_,
+            &d_seg_[0], &d_seg_[1], &d_gather_codes_, &d_gather_off_, &d_gather_len_ };
         for( DevBuf * b : bufs )
             b->release();
         h_score_.release();
+        h_stage_.release();
+        resident_seg_ = -1;
+        streaming_ = false;
         db_ = HostDb();
         db_stale_ = true;
         ranks_.clear();
@@ -386,6 +518,7 @@ private:
     cudaEvent_t ev_cls_t_[8] = {};   // per class start / end, timed (SSA_B200_TIMING)
     cudaEvent_t ev_ready_ = nullptr;
     cudaEvent_t ev_phase_[6] = {};
+    cudaEvent_t ev_seg_[2] = {};     // around one segment's entry pass
     cudaEvent_t ev_tb_[5] = {};   // batch start, entry pass done, cascade done, copies done, traceback
     DevBuf d_qcodes_, d_qoff_, d_qlen_, d_qpad_, d_prof_off_, d_prof_, d_matrix_;
     DevBuf d_score_, d_list_a_, d_list_b_, d_counts_, d_scratch_, d_scratch4_;
@@ -394,6 +527,16 @@ private:
     PinnedBuf h_score_;
     DevBuf d_pair_slot_, d_pair_unit_, d_pair_score_;
     uint64_t tb_budget_ = 0;         // traceback direction memory per wave (0 = automatic)
+    // streaming: the database does not fit its device memory budget; segments
+    // of consecutive positions of the length order take turns on the device
+    uint64_t db_budget_ = 0;         // database device memory (0 = automatic)
+    bool streaming_ = false;
+    std::vector<uint32_t> seg_lo_, seg_hi_;     // per segment: positions in order_desc
+    std::vector<uint64_t> seg_off_, seg_bytes_; // per segment: block in db_.codes
+    DevBuf d_seg_[2];
+    int resident_seg_ = -1;
+    PinnedBuf h_stage_;
+    DevBuf d_gather_codes_, d_gather_off_, d_gather_len_;
 
     // per-batch query layout
     std::vector<uint64_t> h_qoff_;
@@ -831,7 +974,7 @@ void Engine::run_qpair_entry( const SearchRequest & req, uint32_t nq, PairTask *
         CUDA_CHECK( cudaStreamWaitEvent( class_stream_[ri], ev_ready_, 0 ) );
         unsigned long long * unit_counter = d_counts_.as<unsigned long long>() + 8 + ri;   // bytes 64..95
         CUDA_CHECK( cudaMemsetAsync( unit_counter, 0, sizeof(unsigned long long), class_stream_[ri] ) );
-        p.db = DbView{ d_codes_.as<uint8_t>(), d_off_.as<uint64_t>(), d_len_.as<uint32_t>(), db_.n_ids };
+        p.db = db_view();
         p.order = d_order_.as<uint32_t>() + lo;
         p.prof = d_qp_prof_.as<uint32_t>();
         p.prof_off = d_qp_off_.as<uint64_t>();
@@ -969,41 +1112,66 @@ void Engine::search( const SearchRequest & req, const std::vector<QueryCodes> & 
         CUDA_CHECK( cudaEventRecord( ev_phase_[0], stream_ ) );
         const int entry = req.bit_width;
         std::vector<PairTask> list_entry, list_16;   // host copies for the replay
-        unsigned n_a = 0, n_b = 0;
-        if( (fast_eligible( req ) && nq >= 2 && !getenv( "SSA_B200_NO_QPAIR" )) || nw_fast_eligible( req ) )
-            run_qpair_entry( req, nq, d_list_a_.as<PairTask>(), cnt + 0, cap );
-        else if( fast_eligible( req ) )
-            run_fast_entry( req, nq, d_list_a_.as<PairTask>(), cnt + 0, cap );
-        else
-            run_pass( req.algo, entry, req, nq, nullptr, n_pairs, true, d_list_a_.as<PairTask>(), cnt + 0, cap );
-        CUDA_CHECK( cudaEventRecord( ev_phase_[1], stream_ ) );
-        if( entry != 64 ) {
-            CUDA_CHECK( cudaMemcpyAsync( &n_a, cnt + 0, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_ ) );
-            CUDA_CHECK( cudaStreamSynchronize( stream_ ) );
-            n_a = std::min( n_a, cap );
-            if( n_a ) {
-                const int w2 = (entry == 8) ? 16 : 64;
-                PairTask * nx = (w2 == 16) ? d_list_b_.as<PairTask>() : nullptr;
-                run_pass( req.algo, w2, req, nq, d_list_a_.as<PairTask>(), n_a, false, nx, cnt + 1, cap );
-                if( w2 == 16 ) {
-                    CUDA_CHECK( cudaMemcpyAsync( &n_b, cnt + 1, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_ ) );
-                    CUDA_CHECK( cudaStreamSynchronize( stream_ ) );
-                    n_b = std::min( n_b, cap );
-                    if( n_b )
-                        run_pass( req.algo, 64, req, nq, d_list_b_.as<PairTask>(), n_b, false, nullptr, cnt + 3, 0 );
-                }
-                list_entry.resize( n_a );
-                CUDA_CHECK( cudaMemcpyAsync( list_entry.data(), d_list_a_.p, n_a * sizeof(PairTask),
-                        cudaMemcpyDeviceToHost, stream_ ) );
-                if( n_b ) {
-                    list_16.resize( n_b );
-                    CUDA_CHECK( cudaMemcpyAsync( list_16.data(), d_list_b_.p, n_b * sizeof(PairTask),
-                            cudaMemcpyDeviceToHost, stream_ ) );
-                }
+        uint64_t n_a = 0, n_b = 0;
+        float entry_ms = 0;     // the entry passes of all segments
+        // a resident database is one segment; a streamed one runs the entry pass
+        // and the cascade of each segment while it is on the device
+        const uint32_t n_seg = streaming_ ? (uint32_t) seg_lo_.size() : 1;
+        for( uint32_t sg = 0; sg < n_seg; sg++ ) {
+            const uint32_t lo = streaming_ ? seg_lo_[sg] : 0;
+            const uint32_t hi = streaming_ ? seg_hi_[sg] : (uint32_t) n_ne;
+            if( streaming_ ) {
+                make_resident( sg, stats );
+                CUDA_CHECK( cudaMemsetAsync( cnt, 0, 2 * sizeof(unsigned), stream_ ) );
             }
+            const uint64_t seg_pairs = (uint64_t) nq * (hi - lo);
+            CUDA_CHECK( cudaEventRecord( ev_seg_[0], stream_ ) );
+            if( (fast_eligible( req ) && (nq >= 2 || streaming_) && !getenv( "SSA_B200_NO_QPAIR" )) ||
+                    nw_fast_eligible( req ) )
+                run_qpair_entry( req, nq, d_list_a_.as<PairTask>(), cnt + 0, cap, nullptr, lo, hi );
+            else if( fast_eligible( req ) )
+                run_fast_entry( req, nq, d_list_a_.as<PairTask>(), cnt + 0, cap );
+            else
+                run_pass( req.algo, entry, req, nq, nullptr, seg_pairs, true, d_list_a_.as<PairTask>(), cnt + 0, cap,
+                        nullptr, 0, lo );
+            CUDA_CHECK( cudaEventRecord( ev_seg_[1], stream_ ) );
+            CUDA_CHECK( cudaEventSynchronize( ev_seg_[1] ) );
+            float seg_ms = 0;
+            CUDA_CHECK( cudaEventElapsedTime( &seg_ms, ev_seg_[0], ev_seg_[1] ) );
+            entry_ms += seg_ms;
+            if( entry == 64 )
+                continue;
+            unsigned sa = 0, sb = 0;
+            CUDA_CHECK( cudaMemcpyAsync( &sa, cnt + 0, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_ ) );
+            CUDA_CHECK( cudaStreamSynchronize( stream_ ) );
+            sa = std::min( sa, cap );
+            if( sa == 0 )
+                continue;
+            const int w2 = (entry == 8) ? 16 : 64;
+            PairTask * nx = (w2 == 16) ? d_list_b_.as<PairTask>() : nullptr;
+            run_pass( req.algo, w2, req, nq, d_list_a_.as<PairTask>(), sa, false, nx, cnt + 1, cap );
+            if( w2 == 16 ) {
+                CUDA_CHECK( cudaMemcpyAsync( &sb, cnt + 1, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_ ) );
+                CUDA_CHECK( cudaStreamSynchronize( stream_ ) );
+                sb = std::min( sb, cap );
+                if( sb )
+                    run_pass( req.algo, 64, req, nq, d_list_b_.as<PairTask>(), sb, false, nullptr, cnt + 3, 0 );
+            }
+            list_entry.resize( n_a + sa );
+            CUDA_CHECK( cudaMemcpyAsync( list_entry.data() + n_a, d_list_a_.p, sa * sizeof(PairTask),
+                    cudaMemcpyDeviceToHost, stream_ ) );
+            if( sb ) {
+                list_16.resize( n_b + sb );
+                CUDA_CHECK( cudaMemcpyAsync( list_16.data() + n_b, d_list_b_.p, sb * sizeof(PairTask),
+                        cudaMemcpyDeviceToHost, stream_ ) );
+            }
+            n_a += sa;
+            n_b += sb;
+            if( streaming_ )
+                CUDA_CHECK( cudaStreamSynchronize( stream_ ) );   // the lists are reused by the next segment
         }
         CUDA_CHECK( cudaEventRecord( ev_phase_[2], stream_ ) );
-        stats.d2h_bytes += score_bytes + ((uint64_t) n_a + n_b) * sizeof(PairTask);
+        stats.d2h_bytes += score_bytes + (n_a + n_b) * sizeof(PairTask);
         int32_t * hs = (int32_t *) h_score_.ensure( std::max<size_t>( score_bytes, 4 ) );
         if( score_bytes )
             CUDA_CHECK( cudaMemcpyAsync( hs, d_score_.p, score_bytes, cudaMemcpyDeviceToHost, stream_ ) );
@@ -1074,17 +1242,22 @@ void Engine::search( const SearchRequest & req, const std::vector<QueryCodes> & 
         {
             CUDA_CHECK( cudaEventSynchronize( ev_phase_[5] ) );
             float ms[5];
-            for( int i = 0; i < 3; i++ )
-                CUDA_CHECK( cudaEventElapsedTime( &ms[i], ev_phase_[i], ev_phase_[i + 1] ) );
+            // [0] entry passes, [1] cascades (and segment copies), [2] result copies, [3] traceback
+            float passes = 0;
+            CUDA_CHECK( cudaEventElapsedTime( &passes, ev_phase_[0], ev_phase_[2] ) );
+            ms[0] = entry_ms;
+            ms[1] = std::max( 0.0f, passes - entry_ms );
+            CUDA_CHECK( cudaEventElapsedTime( &ms[2], ev_phase_[2], ev_phase_[3] ) );
             CUDA_CHECK( cudaEventElapsedTime( &ms[3], ev_phase_[4], ev_phase_[5] ) );
             const double rep = std::chrono::duration<double, std::milli>( t_replay1 - t_replay0 ).count();
             stats.entry_seconds += ms[0] * 1e-3;
             stats.kernel_seconds += (ms[0] + ms[1] + ms[3]) * 1e-3;
             if( timing )
             fprintf( stderr,
-                    "[ssa timing] queries %u pairs %llu: entry %.3f ms, cascade %.3f ms (%u+%u re-queued), "
+                    "[ssa timing] queries %u pairs %llu: entry %.3f ms, cascade %.3f ms (%llu+%llu re-queued), "
                     "copies %.3f ms, replay %.3f ms, traceback %.3f ms\n",
-                    nq, (unsigned long long) n_pairs, ms[0], ms[1], n_a, n_b, ms[2], rep, ms[3] );
+                    nq, (unsigned long long) n_pairs, ms[0], ms[1], (unsigned long long) n_a,
+                    (unsigned long long) n_b, ms[2], rep, ms[3] );
         }
         g0 = g1;
     }
@@ -1207,7 +1380,25 @@ void Engine::traceback( const SearchRequest & req, std::vector<std::vector<Hit>>
         last_off[h + 1] = last_off[h] + A;
     }
     TbParams p{};
-    p.db = db_view();
+    // the hits as the device sees them: with a streamed database their
+    // sequences are gathered into a view of their own and renumbered
+    std::vector<TbHit> dev_hits = hits;
+    if( streaming_ ) {
+        std::vector<uint32_t> ids;
+        std::unordered_map<uint32_t, uint32_t> index;
+        for( TbHit & t : dev_hits ) {
+            auto it = index.find( t.id );
+            if( it == index.end() ) {
+                it = index.emplace( t.id, (uint32_t) ids.size() ).first;
+                ids.push_back( t.id );
+            }
+            t.id = it->second;
+        }
+        p.db = gather_view( ids, stats );
+    }
+    else {
+        p.db = db_view();
+    }
     p.qcodes = d_qcodes_.as<uint8_t>();
     p.qoff = d_qoff_.as<uint64_t>();
     p.qlen = d_qlen_.as<uint32_t>();
@@ -1279,7 +1470,8 @@ void Engine::traceback( const SearchRequest & req, std::vector<std::vector<Hit>>
         p.last_h = last;
         p.last_e = last + last_off[nh];
         p.last_off = (const uint64_t *) d_tb_last_off_.ensure( (nh + 1) * sizeof(uint64_t) );
-        CUDA_CHECK( cudaMemcpyAsync( (void *) p.hits, hits.data(), nh * sizeof(TbHit), cudaMemcpyHostToDevice, stream_ ) );
+        CUDA_CHECK( cudaMemcpyAsync( (void *) p.hits, dev_hits.data(), nh * sizeof(TbHit), cudaMemcpyHostToDevice,
+                stream_ ) );
         CUDA_CHECK( cudaMemcpyAsync( p.regions, regions.data(), nh * sizeof(TbRegion), cudaMemcpyHostToDevice,
                 stream_ ) );
         CUDA_CHECK( cudaMemcpyAsync( (void *) p.last_off, last_off.data(), (nh + 1) * sizeof(uint64_t),
@@ -1347,7 +1539,7 @@ void Engine::traceback( const SearchRequest & req, std::vector<std::vector<Hit>>
         std::vector<TbRegion> wregs( nw );
         std::vector<uint64_t> wdir( nw + 1, 0 ), wops( nw + 1, 0 );
         for( uint32_t k = 0; k < nw; k++ ) {
-            whits[k] = hits[wave[k]];
+            whits[k] = dev_hits[wave[k]];
             wregs[k] = regions[wave[k]];
             wdir[k + 1] = wdir[k] + dir_words[wave[k]];
             wops[k + 1] = wops[k] + ops_bytes[wave[k]];
@@ -1533,7 +1725,23 @@ void Engine::align_pairs( const SearchRequest & req, const std::vector<QueryCode
             hu[k] = units[work[k]];
         }
         PairScoreParams p{};
-        p.db = db_view();
+        if( streaming_ ) {
+            // the pairs' sequences gathered into a view of their own
+            std::vector<uint32_t> ids;
+            std::unordered_map<uint32_t, uint32_t> index;
+            for( uint32_t & u : hu ) {
+                auto it = index.find( u );
+                if( it == index.end() ) {
+                    it = index.emplace( u, (uint32_t) ids.size() ).first;
+                    ids.push_back( u );
+                }
+                u = it->second;
+            }
+            p.db = gather_view( ids, stats );
+        }
+        else {
+            p.db = db_view();
+        }
         p.qcodes = d_qcodes_.as<uint8_t>();
         p.qoff = d_qoff_.as<uint64_t>();
         p.qlen = d_qlen_.as<uint32_t>();
@@ -1842,6 +2050,18 @@ void engine_align_pairs( const SearchRequest & req, const std::vector<QueryCodes
 void engine_set_traceback_memory( uint64_t bytes ) {
     std::lock_guard<std::mutex> lock( g_engine_mutex );
     Engine::get().set_traceback_budget( bytes );
+}
+
+void engine_set_db_memory( uint64_t bytes ) {
+    std::lock_guard<std::mutex> lock( g_engine_mutex );
+    Engine::get().set_db_budget( bytes );
+}
+
+bool engine_streaming() {
+    std::lock_guard<std::mutex> lock( g_engine_mutex );
+    Engine & e = Engine::get();
+    e.database();
+    return e.streaming();
 }
 
 const HostDb & engine_database() {

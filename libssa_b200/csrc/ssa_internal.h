@@ -130,6 +130,11 @@ void engine_align_pairs( const SearchRequest & req, const std::vector<QueryCodes
         const std::vector<uint32_t> & units, std::vector<std::vector<Hit>> & out, SearchStats & stats );
 // Device memory for the direction words of one traceback wave (0 = automatic).
 void engine_set_traceback_memory( uint64_t bytes );
+// Device memory for the database (0 = automatic); a database that does not fit
+// is streamed through the device in segments.
+void engine_set_db_memory( uint64_t bytes );
+// Whether the current database is streamed (packs it first if needed).
+bool engine_streaming();
 const HostDb & engine_database();
 void engine_invalidate_database();
 void engine_shutdown();
