@@ -119,7 +119,7 @@ cudaError_t launch_emul( int algo, int width, const EmulParams & p, int grid, cu
 cudaError_t launch_build_profile32( const uint8_t * qcodes, const uint64_t * qoff, const uint32_t * qlen,
         const uint32_t * qpad, const uint64_t * prof_off, const int64_t * matrix, int width, int32_t * prof,
         uint32_t n_slots, cudaStream_t st );
-// group: warps per hit, 1 or 4 (scratch: one boundary row per group)
+// group: warps per hit, 1, 2 or 4 (scratch: one boundary row per group)
 cudaError_t launch_tb_regions( const TbParams & p, int group, int grid, cudaStream_t st, cudaEvent_t * ev );
 cudaError_t launch_tb_paths( const TbParams & p, int group, int grid, cudaStream_t st, cudaEvent_t * ev );
 

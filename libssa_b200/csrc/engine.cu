@@ -442,7 +442,7 @@ public:
             &d_prof_off_, &d_prof_, &d_matrix_, &d_score_, &d_list_a_, &d_list_b_, &d_counts_, &d_scratch_,
             &d_tb_hits_, &d_tb_regions_, &d_tb_last_, &d_tb_last_off_, &d_tb_dirs_, &d_tb_dir_off_, &d_tb_ops_,
             &d_tb_ops_off_, &d_tb_ops_len_, &d_qp_prof_, &d_qp_off_, &d_qp_rows_, &d_qp_slots_, &d_qp_units_,
-            &d_serve_score_, &d_qp_lmax_, &d_pair_slot_, &d_pair_unit_, &d_pair_score_, &d_scratch4_,
+            &d_serve_score_, &d_qp_lmax_, &d_pair_slot_, &d_pair_unit_, &d_pair_score_, &d_scratch2_, &d_scratch4_,
             &d_seg_[0], &d_seg_[1], &d_gather_codes_, &d_gather_off_, &d_gather_len_ };
         for( DevBuf * b : bufs )
             b->release();
@@ -521,7 +521,7 @@ private:
     cudaEvent_t ev_seg_[2] = {};     // around one segment's entry pass
     cudaEvent_t ev_tb_[5] = {};   // batch start, entry pass done, cascade done, copies done, traceback
     DevBuf d_qcodes_, d_qoff_, d_qlen_, d_qpad_, d_prof_off_, d_prof_, d_matrix_;
-    DevBuf d_score_, d_list_a_, d_list_b_, d_counts_, d_scratch_, d_scratch4_;
+    DevBuf d_score_, d_list_a_, d_list_b_, d_counts_, d_scratch_, d_scratch2_, d_scratch4_;
     DevBuf d_tb_hits_, d_tb_regions_, d_tb_last_, d_tb_last_off_, d_tb_dirs_, d_tb_dir_off_, d_tb_ops_,
             d_tb_ops_off_, d_tb_ops_len_;
     PinnedBuf h_score_;
@@ -636,7 +636,10 @@ constexpr uint32_t FAST_MAX_PASS_ROWS = 512; // G x R: 16 KiB profile slice per 
 
 // Threads per group G, rows per thread R and passes P for a query of Q rows:
 // the smallest estimated issue cost per database column, counting the
-// wavefront fill (G - 1 steps per pass) and a per-step overhead.
+// wavefront fill (G - 1 steps per pass) and a per-step overhead.  (A model
+// that also bounds small databases by the longest sequence's latency picked
+// G = 32 for a 375-row query against 10,000 sequences, which measured slower
+// than this choice, G = 8, R = 24, P = 2.)
 static FastShape choose_shape( uint32_t Q, double mean_len ) {
     FastShape best{ 0, 0, 0 };
     double best_cost = 1e300;
@@ -1308,10 +1311,14 @@ void Engine::upload_queries( const QueryCodes * queries, uint32_t nq, bool profi
     prof_width_ = -1;
 }
 
-// Hits whose alignment runs on a group of 4 warps (stripe_pipeline.cuh): at
-// least 4 stripes of query rows and 8M cells; smaller ones run on one warp.
-static bool tb_large( uint32_t rows, uint32_t cols ) {
-    return rows > 3u * 32u * TB_WORD_ROWS && (uint64_t) rows * cols >= ((uint64_t) 1 << 23);
+// Warps per hit in the traceback passes (stripe_pipeline.cuh): 4 for at least
+// 4 stripes of query rows and 8M cells, 2 for at least 2 stripes (they run
+// side by side instead of one after the other), else 1.
+static int tb_group( uint32_t rows, uint32_t cols ) {
+    const uint32_t stripes = (rows + 32u * TB_WORD_ROWS - 1) / (32u * TB_WORD_ROWS);
+    if( stripes >= 4 && (uint64_t) rows * cols >= ((uint64_t) 1 << 23) )
+        return 4;
+    return stripes >= 2 ? 2 : 1;
 }
 
 // Largest magnitude of one DP step: a score-table entry or a gap cost.
@@ -1340,16 +1347,16 @@ void Engine::traceback( const SearchRequest & req, std::vector<std::vector<Hit>>
     const uint32_t nh = (uint32_t) hits.size();
     if( nh == 0 )
         return;
-    // the hits of the 4-warp class first, each class largest first: the
+    // the hits by warps per hit (4, 2, 1), each class largest first: the
     // kernels hand hits out in this order
     {
         std::vector<uint32_t> perm( nh );
         for( uint32_t h = 0; h < nh; h++ )
             perm[h] = h;
         auto work = [&]( uint32_t h ) { return (uint64_t) h_qlen_[hits[h].qslot] * db_.len[hits[h].id]; };
-        auto large = [&]( uint32_t h ) { return tb_large( h_qlen_[hits[h].qslot], db_.len[hits[h].id] ); };
+        auto group = [&]( uint32_t h ) { return tb_group( h_qlen_[hits[h].qslot], db_.len[hits[h].id] ); };
         std::stable_sort( perm.begin(), perm.end(), [&]( uint32_t a, uint32_t b ) {
-            return large( a ) != large( b ) ? large( a ) : work( a ) > work( b );
+            return group( a ) != group( b ) ? group( a ) > group( b ) : work( a ) > work( b );
         } );
         std::vector<TbHit> hs( nh );
         std::vector<std::pair<uint32_t, uint32_t>> ws( nh );
@@ -1409,46 +1416,65 @@ void Engine::traceback( const SearchRequest & req, std::vector<std::vector<Hit>>
     const int grid = sms_ * 2;
     const uint32_t cols = db_.max_len + 4;
     constexpr uint32_t stripe_rows = 32 * TB_WORD_ROWS;
-    // boundary rows in global memory: one per warp for the 1-warp class, one
-    // per group for the 4-warp class (8 and 2 per CTA of 256 threads)
+    // boundary rows in global memory: one per group of warps (8, 4 and 2
+    // groups per CTA of 256 threads for groups of 1, 2 and 4)
     int4 * scratch1 = max_qlen_ > stripe_rows ? (int4 *) d_scratch_.ensure( (size_t) grid * 8 * cols * sizeof(int4) )
                                               : nullptr;
+    int4 * scratch2 = max_qlen_ > 2 * stripe_rows
+            ? (int4 *) d_scratch2_.ensure( (size_t) grid * 4 * cols * sizeof(int4) ) : nullptr;
     int4 * scratch4 = max_qlen_ > 4 * stripe_rows
             ? (int4 *) d_scratch4_.ensure( (size_t) grid * 2 * cols * sizeof(int4) ) : nullptr;
-    unsigned long long * counters = d_counts_.as<unsigned long long>() + 16;   // bytes 128..191
-    // Launches one phase over the hits [0, n) of the current arrays: [0, k) on
-    // groups of 4 warps, [k, n) on single warps, the two classes concurrently.
-    auto launch_split = [&]( bool region_phase, uint32_t n, uint32_t k, cudaEvent_t * ev ) {
-        TbParams p4 = p, p1 = p;
-        p4.n_hits = k;
-        p4.scratch = scratch4;
-        p4.scratch_cols = scratch4 ? cols : 0;
-        p4.hit_counters = counters;
-        p1.n_hits = n - k;
-        p1.scratch = scratch1;
-        p1.scratch_cols = scratch1 ? cols : 0;
-        p1.hit_counters = counters + 4;
-        p1.hits = p.hits + k;
-        p1.regions = p.regions + k;
-        if( p.last_off )
-            p1.last_off = p.last_off + k;
-        if( p.dir_off ) {
-            p1.dir_off = p.dir_off + k;
-            p1.ops_off = p.ops_off + k;
-            p1.ops_len = p.ops_len + k;
-        }
-        CUDA_CHECK( cudaMemsetAsync( counters, 0, 8 * sizeof(unsigned long long), stream_ ) );
+    unsigned long long * counters = d_counts_.as<unsigned long long>() + 16;   // bytes 128..223
+    // Launches one phase over the hits [0, n) of the current arrays: [0, k4) on
+    // groups of 4 warps, [k4, k2) on groups of 2, [k2, n) on single warps, the
+    // three classes concurrently on three streams.
+    auto launch_split = [&]( bool region_phase, uint32_t n, uint32_t k4, uint32_t k2, cudaEvent_t * ev ) {
+        const uint32_t lo[3] = { 0, k4, k2 }, hi[3] = { k4, k2, n };
+        const int group[3] = { 4, 2, 1 };
+        int4 * scratch[3] = { scratch4, scratch2, scratch1 };
+        cudaStream_t st[3] = { stream_, class_stream_[0], class_stream_[1] };
+        CUDA_CHECK( cudaMemsetAsync( counters, 0, 12 * sizeof(unsigned long long), stream_ ) );
         CUDA_CHECK( cudaEventRecord( ev_ready_, stream_ ) );
-        CUDA_CHECK( cudaStreamWaitEvent( class_stream_[0], ev_ready_, 0 ) );
-        if( k )
-            CUDA_CHECK( region_phase ? launch_tb_regions( p4, 4, grid, stream_, ev )
-                                     : launch_tb_paths( p4, 4, grid, stream_, ev ) );
-        if( n > k )
-            CUDA_CHECK( region_phase ? launch_tb_regions( p1, 1, grid, class_stream_[0], k ? nullptr : ev )
-                                     : launch_tb_paths( p1, 1, grid, class_stream_[0], k ? nullptr : ev ) );
-        CUDA_CHECK( cudaEventRecord( ev_class_[0], class_stream_[0] ) );
-        CUDA_CHECK( cudaStreamWaitEvent( stream_, ev_class_[0], 0 ) );
-        launches_ += (k ? 2 : 0) + (n > k ? 2 : 0);
+        bool timed = false;
+        for( int c = 0; c < 3; c++ ) {
+            if( hi[c] <= lo[c] )
+                continue;
+            TbParams q = p;
+            q.n_hits = hi[c] - lo[c];
+            q.scratch = scratch[c];
+            q.scratch_cols = scratch[c] ? cols : 0;
+            q.hit_counters = counters + 4 * c;
+            q.hits = p.hits + lo[c];
+            q.regions = p.regions + lo[c];
+            if( p.last_off )
+                q.last_off = p.last_off + lo[c];
+            if( p.dir_off ) {
+                q.dir_off = p.dir_off + lo[c];
+                q.ops_off = p.ops_off + lo[c];
+                q.ops_len = p.ops_len + lo[c];
+            }
+            if( c > 0 )
+                CUDA_CHECK( cudaStreamWaitEvent( st[c], ev_ready_, 0 ) );
+            // events around the first class that runs (the largest hits)
+            cudaEvent_t * e = timed ? nullptr : ev;
+            timed = timed || ev != nullptr;
+            CUDA_CHECK( region_phase ? launch_tb_regions( q, group[c], grid, st[c], e )
+                                     : launch_tb_paths( q, group[c], grid, st[c], e ) );
+            if( c > 0 ) {
+                CUDA_CHECK( cudaEventRecord( ev_class_[c], st[c] ) );
+                CUDA_CHECK( cudaStreamWaitEvent( stream_, ev_class_[c], 0 ) );
+            }
+            launches_ += 2;
+        }
+    };
+    // class bounds of hits sorted by warps per hit
+    auto class_bounds = [&]( uint32_t n, auto group_of, uint32_t & k4, uint32_t & k2 ) {
+        k4 = 0;
+        while( k4 < n && group_of( k4 ) == 4 )
+            k4++;
+        k2 = k4;
+        while( k2 < n && group_of( k2 ) == 2 )
+            k2++;
     };
     const bool timing = getenv( "SSA_B200_TIMING" ) != nullptr;
     float t_fwd = 0, t_rev = 0, t_dir = 0, t_walk = 0;
@@ -1476,10 +1502,10 @@ void Engine::traceback( const SearchRequest & req, std::vector<std::vector<Hit>>
                 stream_ ) );
         CUDA_CHECK( cudaMemcpyAsync( (void *) p.last_off, last_off.data(), (nh + 1) * sizeof(uint64_t),
                 cudaMemcpyHostToDevice, stream_ ) );
-        uint32_t k = 0;
-        while( k < nh && tb_large( h_qlen_[hits[k].qslot], db_.len[hits[k].id] ) )
-            k++;
-        launch_split( true, nh, k, timing ? ev_tb_ : nullptr );
+        uint32_t k4, k2;
+        class_bounds( nh, [&]( uint32_t h ) { return tb_group( h_qlen_[hits[h].qslot], db_.len[hits[h].id] ); }, k4,
+                k2 );
+        launch_split( true, nh, k4, k2, timing ? ev_tb_ : nullptr );
         CUDA_CHECK( cudaMemcpyAsync( regions.data(), p.regions, nh * sizeof(TbRegion), cudaMemcpyDeviceToHost,
                 stream_ ) );
         check_errors();
@@ -1507,20 +1533,21 @@ void Engine::traceback( const SearchRequest & req, std::vector<std::vector<Hit>>
         total_dir += dir_words[h] * sizeof(uint16_t);
     }
     const uint64_t budget = traceback_budget();
-    auto region_large = [&]( uint32_t h ) {
+    auto region_group = [&]( uint32_t h ) {
         const TbRegion & rg = regions[h];
-        return rg.status == 0 && tb_large( (uint32_t) rg.a_end + 1, (uint32_t) rg.b_end + 1 );
+        return rg.status == 0 ? tb_group( (uint32_t) rg.a_end + 1, (uint32_t) rg.b_end + 1 ) : 1;
     };
-    // waves: consecutive runs of the hits in (4-warp class first, largest
-    // direction matrix first) order, each run as long as its matrices fit
+    // waves: consecutive runs of the hits in (more warps per hit first,
+    // largest direction matrix first) order, each run as long as its matrices
+    // fit
     std::vector<std::vector<uint32_t>> waves;
     {
         std::vector<uint32_t> order( nh );
         for( uint32_t h = 0; h < nh; h++ )
             order[h] = h;
         std::stable_sort( order.begin(), order.end(), [&]( uint32_t x, uint32_t y ) {
-            const bool lx = region_large( x ), ly = region_large( y );
-            return lx != ly ? lx : dir_words[x] > dir_words[y];
+            const int gx = region_group( x ), gy = region_group( y );
+            return gx != gy ? gx > gy : dir_words[x] > dir_words[y];
         } );
         uint64_t load = 0;
         for( uint32_t h : order ) {
@@ -1559,10 +1586,9 @@ void Engine::traceback( const SearchRequest & req, std::vector<std::vector<Hit>>
                 cudaMemcpyHostToDevice, stream_ ) );
         CUDA_CHECK( cudaMemcpyAsync( (void *) p.ops_off, wops.data(), (nw + 1) * sizeof(uint64_t),
                 cudaMemcpyHostToDevice, stream_ ) );
-        uint32_t k = 0;
-        while( k < nw && region_large( wave[k] ) )
-            k++;
-        launch_split( false, nw, k, timing ? ev_tb_ + 2 : nullptr );
+        uint32_t k4, k2;
+        class_bounds( nw, [&]( uint32_t k ) { return region_group( wave[k] ); }, k4, k2 );
+        launch_split( false, nw, k4, k2, timing ? ev_tb_ + 2 : nullptr );
         std::vector<uint32_t> ops_len( nw );
         std::vector<char> ops( wops[nw] + 1 );
         CUDA_CHECK( cudaMemcpyAsync( ops_len.data(), p.ops_len, nw * sizeof(uint32_t), cudaMemcpyDeviceToHost,

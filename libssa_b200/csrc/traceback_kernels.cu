@@ -681,20 +681,24 @@ __global__ void tb_walk_kernel( TbParams p ) {
 
 // Region phase (Smith-Waterman hits only): forward and reverse passes.  They
 // need no direction memory, so all hits of a search run in one launch each.
-// group: warps per hit (1 or 4).  ev (optional): 3 events recorded around the
-// two kernels.
+// group: warps per hit (1, 2 or 4).  ev (optional): 3 events recorded around
+// the two kernels.
 cudaError_t launch_tb_regions( const TbParams & p, int group, int grid, cudaStream_t st, cudaEvent_t * ev ) {
     if( ev )
         cudaEventRecord( ev[0], st );
     if( p.n_hits ) {
         if( group == 4 )
             tb_forward_kernel<4><<<grid, 256, 0, st>>>( p );
+        else if( group == 2 )
+            tb_forward_kernel<2><<<grid, 256, 0, st>>>( p );
         else
             tb_forward_kernel<1><<<grid, 256, 0, st>>>( p );
         if( ev )
             cudaEventRecord( ev[1], st );
         if( group == 4 )
             tb_reverse_kernel<4><<<grid, 256, 0, st>>>( p );
+        else if( group == 2 )
+            tb_reverse_kernel<2><<<grid, 256, 0, st>>>( p );
         else
             tb_reverse_kernel<1><<<grid, 256, 0, st>>>( p );
     }
@@ -715,6 +719,8 @@ cudaError_t launch_tb_paths( const TbParams & p, int group, int grid, cudaStream
     if( p.n_hits ) {
         if( group == 4 )
             tb_directions_kernel<4><<<grid, 256, 0, st>>>( p );
+        else if( group == 2 )
+            tb_directions_kernel<2><<<grid, 256, 0, st>>>( p );
         else
             tb_directions_kernel<1><<<grid, 256, 0, st>>>( p );
         if( ev )
