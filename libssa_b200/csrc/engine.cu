@@ -960,8 +960,14 @@ void Engine::run_qpair_entry( const SearchRequest & req, uint32_t nq, PairTask *
     uint64_t seg_residues = 0;
     for( uint32_t i = lo; i < hi; i++ )
         seg_residues += db_.len[db_.order_desc[i]];
-    size_t class_first = 0;
-    for( int ri = 0; ri < 4; ri++ ) {
+    // classes launched heaviest first (most rows per thread: the longest
+    // queries), so that the last class to finish is the lightest
+    size_t class_start[4] = { 0, 0, 0, 0 };
+    for( int ri = 1; ri < 4; ri++ )
+        class_start[ri] = class_start[ri - 1] + by_r[ri - 1].size();
+    for( int k = 0; k < 4; k++ ) {
+        const int ri = 3 - k;
+        const size_t class_first = class_start[ri];
         const std::vector<uint32_t> & cls = by_r[ri];
         if( cls.empty() )
             continue;
@@ -1018,7 +1024,6 @@ void Engine::run_qpair_entry( const SearchRequest & req, uint32_t nq, PairTask *
             CUDA_CHECK( cudaEventRecord( ev_cls_t_[2 * ri + 1], class_stream_[ri] ) );
         CUDA_CHECK( cudaEventRecord( ev_class_[ri], class_stream_[ri] ) );
         CUDA_CHECK( cudaStreamWaitEvent( stream_, ev_class_[ri], 0 ) );
-        class_first += cls.size();
     }
     if( timing ) {
         for( int ri = 0; ri < 4; ri++ ) {
