@@ -84,6 +84,9 @@ struct TbRegion {
     int32_t a_begin, a_end;   // query rows
     int32_t b_begin, b_end;   // database columns
     int32_t fwd_score;        // SW: forward-pass maximum; NW: H(a_end, b_end) from the direction pass
+    // layout of the hit's direction words: words per column (query rows / 8,
+    // rounded up) and the first database column stored
+    int32_t dir_words, dir_col0;
     int32_t status;           // 0 ok, 1 no positive cell, 2 reverse pass found nothing
 };
 
@@ -122,6 +125,7 @@ cudaError_t launch_build_profile32( const uint8_t * qcodes, const uint64_t * qof
 // group: warps per hit, 1, 2 or 4 (scratch: one boundary row per group)
 cudaError_t launch_tb_regions( const TbParams & p, int group, int grid, cudaStream_t st, cudaEvent_t * ev );
 cudaError_t launch_tb_paths( const TbParams & p, int group, int grid, cudaStream_t st, cudaEvent_t * ev );
+cudaError_t launch_tb_fused( const TbParams & p, int group, int grid, cudaStream_t st, cudaEvent_t * ev );
 
 
 // ---- fast Smith-Waterman entry pass (sw_fast_kernel.cu) --------------------

@@ -1433,7 +1433,8 @@ void Engine::traceback( const SearchRequest & req, std::vector<std::vector<Hit>>
     // Launches one phase over the hits [0, n) of the current arrays: [0, k4) on
     // groups of 4 warps, [k4, k2) on groups of 2, [k2, n) on single warps, the
     // three classes concurrently on three streams.
-    auto launch_split = [&]( bool region_phase, uint32_t n, uint32_t k4, uint32_t k2, cudaEvent_t * ev ) {
+    enum { TB_REGIONS, TB_PATHS, TB_FUSED };
+    auto launch_split = [&]( int phase, uint32_t n, uint32_t k4, uint32_t k2, cudaEvent_t * ev ) {
         const uint32_t lo[3] = { 0, k4, k2 }, hi[3] = { k4, k2, n };
         const int group[3] = { 4, 2, 1 };
         int4 * scratch[3] = { scratch4, scratch2, scratch1 };
@@ -1463,13 +1464,14 @@ void Engine::traceback( const SearchRequest & req, std::vector<std::vector<Hit>>
             // events around the first class that runs (the largest hits)
             cudaEvent_t * e = timed ? nullptr : ev;
             timed = timed || ev != nullptr;
-            CUDA_CHECK( region_phase ? launch_tb_regions( q, group[c], grid, st[c], e )
-                                     : launch_tb_paths( q, group[c], grid, st[c], e ) );
+            CUDA_CHECK( phase == TB_REGIONS ? launch_tb_regions( q, group[c], grid, st[c], e )
+                        : phase == TB_PATHS ? launch_tb_paths( q, group[c], grid, st[c], e )
+                                            : launch_tb_fused( q, group[c], grid, st[c], e ) );
             if( c > 0 ) {
                 CUDA_CHECK( cudaEventRecord( ev_class_[c], st[c] ) );
                 CUDA_CHECK( cudaStreamWaitEvent( stream_, ev_class_[c], 0 ) );
             }
-            launches_ += 2;
+            launches_ += (phase == TB_FUSED) ? 3 : 2;
         }
     };
     // class bounds of hits sorted by warps per hit
@@ -1492,8 +1494,27 @@ void Engine::traceback( const SearchRequest & req, std::vector<std::vector<Hit>>
             fatal( "Internal error in the GPU traceback (flags 0x%x).", err );
     };
 
+    // Smith-Waterman with a symmetric score table: the forward region pass and
+    // the direction pass run as one sweep per hit (tb_fwddir_kernel), then the
+    // reverse pass and the walk, wave by wave.  It needs every hit's last
+    // database column past the initial E terms: (B - 1) x gapE < gapO + gapE
+    // with B >= 2, and initial E and F values that are not above zero (gapO <= 0).
+    bool fused = req.algo == 0 && req.gap_extend < 0 && req.gap_open <= 0;
+    for( int d = 0; d < 32 && fused; d++ )
+        for( int q = 0; q < 32 && fused; q++ )
+            fused = req.matrix[(d << 5) + q] == req.matrix[(q << 5) + d];
+    for( uint32_t h = 0; h < nh && fused; h++ )
+        fused = db_.len[hits[h].id] >= 2 &&
+                ((int64_t) db_.len[hits[h].id] - 1) * req.gap_extend < (int64_t) req.gap_open + req.gap_extend;
+    int32_t * last_all = nullptr;
+    if( fused ) {
+        last_all = (int32_t *) d_tb_last_.ensure( 2 * last_off[nh] * sizeof(int32_t) + 16 );
+        p.last_h = last_all;
+        p.last_e = last_all + last_off[nh];
+    }
+
     // ---- region phase (Smith-Waterman): end cell and begin cell of every hit
-    if( req.algo == 0 ) {
+    if( req.algo == 0 && !fused ) {
         p.hits = (const TbHit *) d_tb_hits_.ensure( nh * sizeof(TbHit) );
         p.n_hits = nh;
         p.regions = (TbRegion *) d_tb_regions_.ensure( nh * sizeof(TbRegion) );
@@ -1510,7 +1531,7 @@ void Engine::traceback( const SearchRequest & req, std::vector<std::vector<Hit>>
         uint32_t k4, k2;
         class_bounds( nh, [&]( uint32_t h ) { return tb_group( h_qlen_[hits[h].qslot], db_.len[hits[h].id] ); }, k4,
                 k2 );
-        launch_split( true, nh, k4, k2, timing ? ev_tb_ : nullptr );
+        launch_split( TB_REGIONS, nh, k4, k2, timing ? ev_tb_ : nullptr );
         CUDA_CHECK( cudaMemcpyAsync( regions.data(), p.regions, nh * sizeof(TbRegion), cudaMemcpyDeviceToHost,
                 stream_ ) );
         check_errors();
@@ -1528,17 +1549,32 @@ void Engine::traceback( const SearchRequest & req, std::vector<std::vector<Hit>>
     std::vector<uint64_t> dir_words( nh, 0 ), ops_bytes( nh, 0 );
     uint64_t total_dir = 0;
     for( uint32_t h = 0; h < nh; h++ ) {
-        const TbRegion & rg = regions[h];
+        TbRegion & rg = regions[h];
+        if( fused ) {
+            // the whole matrix: every query row and database column
+            const uint32_t A = h_qlen_[hits[h].qslot], B = db_.len[hits[h].id];
+            rg.dir_words = (int32_t) ((A + TB_WORD_ROWS - 1) / TB_WORD_ROWS);
+            rg.dir_col0 = 0;
+            dir_words[h] = (uint64_t) B * (uint64_t) rg.dir_words;
+            ops_bytes[h] = (uint64_t) A + B + 1;
+            total_dir += dir_words[h] * sizeof(uint16_t);
+            continue;
+        }
         if( rg.status == 2 )
             fatal( "Internal error in align function." );   // reference: src/algo/align.c:131
         if( rg.status != 0 )
             continue;
-        dir_words[h] = (uint64_t) (rg.b_end - rg.b_begin + 1) * (uint64_t) ((rg.a_end + TB_WORD_ROWS) / TB_WORD_ROWS);
+        // rows 0..a_end and columns b_begin..b_end
+        rg.dir_words = (rg.a_end + TB_WORD_ROWS) / TB_WORD_ROWS;
+        rg.dir_col0 = rg.b_begin;
+        dir_words[h] = (uint64_t) (rg.b_end - rg.b_begin + 1) * (uint64_t) rg.dir_words;
         ops_bytes[h] = (uint64_t) (rg.a_end - rg.a_begin + 1) + (uint64_t) (rg.b_end - rg.b_begin + 1) + 1;
         total_dir += dir_words[h] * sizeof(uint16_t);
     }
     const uint64_t budget = traceback_budget();
     auto region_group = [&]( uint32_t h ) {
+        if( fused )
+            return tb_group( h_qlen_[hits[h].qslot], db_.len[hits[h].id] );
         const TbRegion & rg = regions[h];
         return rg.status == 0 ? tb_group( (uint32_t) rg.a_end + 1, (uint32_t) rg.b_end + 1 ) : 1;
     };
@@ -1569,12 +1605,21 @@ void Engine::traceback( const SearchRequest & req, std::vector<std::vector<Hit>>
         const uint32_t nw = (uint32_t) wave.size();
         std::vector<TbHit> whits( nw );
         std::vector<TbRegion> wregs( nw );
-        std::vector<uint64_t> wdir( nw + 1, 0 ), wops( nw + 1, 0 );
+        std::vector<uint64_t> wdir( nw + 1, 0 ), wops( nw + 1, 0 ), wlast( nw, 0 );
         for( uint32_t k = 0; k < nw; k++ ) {
             whits[k] = dev_hits[wave[k]];
             wregs[k] = regions[wave[k]];
             wdir[k + 1] = wdir[k] + dir_words[wave[k]];
             wops[k + 1] = wops[k] + ops_bytes[wave[k]];
+            wlast[k] = last_off[wave[k]];
+        }
+        if( fused ) {
+            // the fused pass writes each hit's last column into its slice of
+            // the last-row arrays of all hits
+            p.last_off = (const uint64_t *) d_tb_last_off_.ensure( std::max<uint32_t>( 1, nw ) * sizeof(uint64_t) );
+            CUDA_CHECK( cudaMemcpyAsync( (void *) p.last_off, wlast.data(), nw * sizeof(uint64_t),
+                    cudaMemcpyHostToDevice, stream_ ) );
+            stats.h2d_bytes += nw * sizeof(uint64_t);
         }
         p.hits = (const TbHit *) d_tb_hits_.ensure( nw * sizeof(TbHit) );
         p.n_hits = nw;
@@ -1593,21 +1638,30 @@ void Engine::traceback( const SearchRequest & req, std::vector<std::vector<Hit>>
                 cudaMemcpyHostToDevice, stream_ ) );
         uint32_t k4, k2;
         class_bounds( nw, [&]( uint32_t k ) { return region_group( wave[k] ); }, k4, k2 );
-        launch_split( false, nw, k4, k2, timing ? ev_tb_ + 2 : nullptr );
+        launch_split( fused ? TB_FUSED : TB_PATHS, nw, k4, k2, timing ? ev_tb_ + 2 : nullptr );
         std::vector<uint32_t> ops_len( nw );
         std::vector<char> ops( wops[nw] + 1 );
         CUDA_CHECK( cudaMemcpyAsync( ops_len.data(), p.ops_len, nw * sizeof(uint32_t), cudaMemcpyDeviceToHost,
                 stream_ ) );
         CUDA_CHECK( cudaMemcpyAsync( ops.data(), p.ops, wops[nw], cudaMemcpyDeviceToHost, stream_ ) );
-        if( scores_from_regions && req.algo == 1 ) {
+        if( fused || (scores_from_regions && req.algo == 1) ) {
             CUDA_CHECK( cudaMemcpyAsync( wregs.data(), p.regions, nw * sizeof(TbRegion), cudaMemcpyDeviceToHost,
                     stream_ ) );
             stats.d2h_bytes += nw * sizeof(TbRegion);
         }
         check_errors();
-        if( scores_from_regions && req.algo == 1 )
+        if( fused ) {
+            // the regions the fused and reverse passes found
+            for( uint32_t k = 0; k < nw; k++ ) {
+                if( wregs[k].status == 2 )
+                    fatal( "Internal error in align function." );   // reference: src/algo/align.c:131
+                regions[wave[k]] = wregs[k];
+            }
+        }
+        else if( scores_from_regions && req.algo == 1 ) {
             for( uint32_t k = 0; k < nw; k++ )
                 regions[wave[k]].fwd_score = wregs[k].fwd_score;
+        }
         if( timing ) {
             float a = 0, b = 0;
             CUDA_CHECK( cudaEventElapsedTime( &a, ev_tb_[2], ev_tb_[3] ) );
@@ -1668,9 +1722,14 @@ void Engine::traceback( const SearchRequest & req, std::vector<std::vector<Hit>>
                 max_b = (uint32_t) B;
             }
         }
-        fprintf( stderr, "[ssa timing] traceback %u hits: forward %.3f ms, reverse %.3f ms, directions %.3f ms, "
-                "walk %.3f ms in %zu wave(s) (%.3f GB of directions); largest hit %u x %u\n", nh, t_fwd, t_rev,
-                t_dir, t_walk, waves.size(), total_dir * 1e-9, max_a, max_b );
+        if( fused )
+            fprintf( stderr, "[ssa timing] traceback %u hits: forward with directions %.3f ms, reverse and walk "
+                    "%.3f ms in %zu wave(s) (%.3f GB of directions); largest hit %u x %u\n", nh, t_dir, t_walk,
+                    waves.size(), total_dir * 1e-9, max_a, max_b );
+        else
+            fprintf( stderr, "[ssa timing] traceback %u hits: forward %.3f ms, reverse %.3f ms, directions %.3f ms, "
+                    "walk %.3f ms in %zu wave(s) (%.3f GB of directions); largest hit %u x %u\n", nh, t_fwd, t_rev,
+                    t_dir, t_walk, waves.size(), total_dir * 1e-9, max_a, max_b );
     }
 }
 

@@ -637,6 +637,205 @@ __global__ void __launch_bounds__( 256 ) tb_directions_kernel( TbParams p ) {
 }
 
 // ---------------------------------------------------------------------------
+// 1 + 3 fused (Smith-Waterman, symmetric score table): the forward region pass
+//    and the direction pass in one sweep of the whole matrix.  The direction
+//    pass's recurrence (reference: src/algo/cigar.c:125-200) and the forward
+//    pass's (src/algo/align.c:39-82) give every cell the same H: they differ
+//    only in the E and F values that enter the first column and row, which are
+//    never above zero and so never reach a Smith-Waterman cell.  With a
+//    symmetric table the two orientations score alike.  So this pass computes
+//    the direction words with the direction pass's values, the end cell (first
+//    maximum, database index then query index) from H, and the last column's H
+//    and E for the reverse pass.  That E is the forward pass's: at the last
+//    column the E chain from earlier cells is at least gapO + gapE (H >= 0),
+//    and the host runs this pass only where (B - 1) x gapE < gapO + gapE, so
+//    neither pass's initial term can be the maximum there.  Directions are
+//    stored for every column and every query row.
+// ---------------------------------------------------------------------------
+template <int W>
+struct FwdDirStripe : TbStripeBase<W> {
+    static constexpr int32_t cand = INT32_MAX;
+    const uint8_t * a;
+    uint32_t A, B, words;
+    uint16_t * dir;
+    int32_t * lh;
+    int32_t * le;
+    int32_t pv, pi, pj;                       // this stripe's first maximum
+    int32_t best_v, best_i, best_j;           // over the warp's stripes
+
+    __device__ void begin( uint32_t stripe ) {
+        this->link.stripe = stripe;
+        this->link.last = (stripe + 1) * TB_ROWS >= A;
+        this->row0 = (int32_t) (stripe * TB_ROWS) + this->lane * TB_R;
+        this->nvalid = max( 0, min( TB_R, (int) A - this->row0 ) );
+        load_rows( a, this->row0, 1, this->nvalid, this->qa );
+#pragma unroll
+        for( int r = 0; r < TB_R; r++ ) {
+            this->H[r] = 0;
+            this->E[r] = 0;
+        }
+        this->diag = 0;
+        this->out_h = 0;
+        this->out_f = 0;
+        pv = 0;
+        pi = INT_MAX;
+        pj = INT_MAX;
+        this->link.start( B, this->lane );
+        this->rr.start( this->lane );
+    }
+
+    __device__ bool chunk( uint32_t ck, int32_t ) {
+        const uint32_t steps = B + 31, s0 = ck * 32;
+        const int lane = this->lane;
+        const int32_t gE = this->gE, gOE = this->gOE;
+        const int32_t row0 = this->row0;
+        // one wavefront step; edge: some lane may be on a column outside 0..B-1
+        auto column = [&]( const uint32_t s, const bool edge ) {
+            int32_t up_h = __shfl_up_sync( 0xffffffffu, this->out_h, 1 );
+            int32_t up_f = __shfl_up_sync( 0xffffffffu, this->out_f, 1 );
+            const int32_t j = (int32_t) s - lane;     // database index
+            if( edge && (j < 0 || j >= (int32_t) B) )
+                return;
+            this->above( s, j, 0, 0, up_h, up_f );
+            const int d = this->rr.get( s, lane );
+            int32_t f = up_f, hd = this->diag;
+            uint32_t code = 0;
+            int32_t e_last[TB_R];
+#pragma unroll
+            for( int r = 0; r < TB_R; r++ ) {
+                const int32_t e = this->E[r];
+                const int32_t x0 = hd + mget( this->smat, d, this->qa[r] );
+                bool no_up, no_left, no_ext_up, no_ext_left;
+                const int32_t m1 = __vibmax_s32( x0, f, &no_up );       // UP: f > x0
+                const int32_t xr = __vibmax_s32( m1, e, &no_left );     // LEFT: e > max(x0, f)
+                const int32_t x = max( xr, 0 );
+                // the lane visits its cells in (column, row) order: within a
+                // stripe the first maximum wins with a strict compare
+                const bool take = (r < this->nvalid) && x > pv;
+                pv = take ? x : pv;
+                pi = take ? j : pi;
+                pj = take ? row0 + r : pj;
+                e_last[r] = e;
+                hd = this->H[r];
+                this->H[r] = x;
+                const int32_t y = x + gOE;
+                f = __vibmax_s32( y, f + gE, &no_ext_up );               // EXT_UP: f + gapE > y
+                this->E[r] = __vibmax_s32( y, e + gE, &no_ext_left );    // EXT_LEFT: e + gapE > y
+                // rows past the query's end get codes too; the walk never reads them
+                const bool ins = !(no_left && no_ext_left);
+                const bool del = !(no_up && no_ext_up);
+                code |= (ins ? 2u : (del ? 1u : 0u)) << (2 * r);
+            }
+            if( (uint32_t) (row0 / TB_R) < words )
+                dir[(uint64_t) j * words + row0 / TB_R] = (uint16_t) code;
+            if( j == (int32_t) B - 1 ) {
+#pragma unroll
+                for( int r = 0; r < TB_R; r++ )
+                    if( r < this->nvalid ) {
+                        lh[row0 + r] = this->H[r];
+                        le[row0 + r] = e_last[r];
+                    }
+            }
+            this->diag = up_h;
+            this->out_h = this->H[TB_R - 1];
+            this->out_f = f;
+            this->put_bottom( j );
+        };
+        // the residue ring and the boundary prefetch refill at the first step of a chunk
+        this->link.step( B, s0, lane );
+        this->rr.step( s0, lane );
+        const uint32_t s1 = min( s0 + 32, steps );
+        if( s0 >= 31 && s1 <= B ) {
+            for( uint32_t s = s0; s < s1; s++ )
+                column( s, false );
+        }
+        else {
+            for( uint32_t s = s0; s < s1; s++ )
+                column( s, true );
+        }
+        return s0 + 32 < steps;
+    }
+
+    // this stripe's first maximum against the earlier stripes' (value desc,
+    // database index asc, query index asc)
+    __device__ void end() {
+        if( pv > best_v || (pv == best_v && pv > 0 && (pi < best_i || (pi == best_i && pj < best_j))) ) {
+            best_v = pv;
+            best_i = pi;
+            best_j = pj;
+        }
+    }
+};
+
+template <int W>
+__global__ void __launch_bounds__( 256 ) tb_fwddir_kernel( TbParams p ) {
+    __shared__ PipeShared<W> shs[TbGroup<W>::GROUPS];
+    __shared__ int32_t smat[1024];
+    stage_matrix( p.matrix, smat, false );
+    TbGroup<W> grp( shs, p );
+    for( ;; ) {
+        const uint32_t h = grp.take( p.hit_counters + 0 );
+        if( h >= p.n_hits )
+            break;
+        const TbHit hit = p.hits[h];
+        FwdDirStripe<W> body;
+        grp.link( body, smat, p );
+        body.A = p.qlen[hit.qslot];
+        body.B = p.db.lens[hit.id];
+        body.words = (body.A + TB_R - 1) / TB_R;
+        body.a = p.qcodes + p.qoff[hit.qslot];
+        body.dir = p.dirs + p.dir_off[h];
+        body.lh = p.last_h + p.last_off[h];
+        body.le = p.last_e + p.last_off[h];
+        body.best_v = 0;
+        body.best_i = INT_MAX;
+        body.best_j = INT_MAX;
+        body.rr = ResidueRing{ grp.sh->residues[grp.wig], 0, p.db.codes + p.db.offsets[hit.id], (int32_t) body.B, -1 };
+        run_stripes<W>( body, *grp.sh, grp.gb, grp.wig, grp.lane, (body.A + TB_ROWS - 1) / TB_ROWS, body.B,
+                p.error_flags );
+        // the best key over the warp, then over the group
+        int32_t bv = body.best_v, bi = body.best_i, bj = body.best_j;
+        for( int o = 16; o > 0; o >>= 1 ) {
+            const int32_t v = __shfl_xor_sync( 0xffffffffu, bv, o );
+            const int32_t i = __shfl_xor_sync( 0xffffffffu, bi, o );
+            const int32_t j = __shfl_xor_sync( 0xffffffffu, bj, o );
+            if( v > bv || (v == bv && (i < bi || (i == bi && j < bj))) ) {
+                bv = v;
+                bi = i;
+                bj = j;
+            }
+        }
+        if( grp.lane == 0 ) {
+            grp.sh->red[grp.wig][0] = bv;
+            grp.sh->red[grp.wig][1] = bi;
+            grp.sh->red[grp.wig][2] = bj;
+        }
+        grp.gb.sync();
+        if( grp.wig == 0 && grp.lane == 0 ) {
+            for( int k = 1; k < W; k++ ) {
+                const int32_t v = grp.sh->red[k][0], i = grp.sh->red[k][1], j = grp.sh->red[k][2];
+                if( v > bv || (v == bv && (i < bi || (i == bi && j < bj))) ) {
+                    bv = v;
+                    bi = i;
+                    bj = j;
+                }
+            }
+            // the host set the direction layout of the region; keep it
+            TbRegion rg = p.regions[h];
+            rg.fwd_score = bv;
+            rg.a_end = bj;
+            rg.b_end = bi;
+            rg.a_begin = 0;
+            rg.b_begin = 0;
+            rg.status = (bv > 0) ? 0 : 1;
+            p.regions[h] = rg;
+        }
+        // every warp is past this hit's shared state before the next hit
+        grp.gb.sync();
+    }
+}
+
+// ---------------------------------------------------------------------------
 // 4. Walk (reference: src/algo/cigar.c:300-334): one thread per hit writes the
 //    moves in traceback order (end to begin); the host run-length encodes.
 // ---------------------------------------------------------------------------
@@ -649,14 +848,14 @@ __global__ void tb_walk_kernel( TbParams p ) {
         p.ops_len[h] = 0;
         return;
     }
-    const uint32_t words = ((uint32_t) rg.a_end + 1 + TB_R - 1) / TB_R;
+    const uint32_t words = (uint32_t) rg.dir_words;
     const uint16_t * dir = p.dirs + p.dir_off[h];
     char * out = p.ops + p.ops_off[h];
     const uint64_t cap = p.ops_off[h + 1] - p.ops_off[h];
     int64_t i = rg.a_end, j = rg.b_end;
     uint64_t n = 0;
     while( i >= rg.a_begin && j >= rg.b_begin && i >= 0 && j >= 0 ) {
-        const uint32_t word = dir[(uint64_t) (j - rg.b_begin) * words + (uint64_t) (i / TB_R)];
+        const uint32_t word = dir[(uint64_t) (j - rg.dir_col0) * words + (uint64_t) (i / TB_R)];
         const uint32_t op = (word >> (2 * (i % TB_R))) & 3u;
         char ch;
         if( op == 2u ) {
@@ -701,6 +900,42 @@ cudaError_t launch_tb_regions( const TbParams & p, int group, int grid, cudaStre
             tb_reverse_kernel<2><<<grid, 256, 0, st>>>( p );
         else
             tb_reverse_kernel<1><<<grid, 256, 0, st>>>( p );
+    }
+    else if( ev ) {
+        cudaEventRecord( ev[1], st );
+    }
+    if( ev )
+        cudaEventRecord( ev[2], st );
+    return cudaGetLastError();
+}
+
+// Fused Smith-Waterman traceback of the hits of one wave: the forward region
+// pass with the direction words (symmetric score table), the reverse pass and
+// the walk.  ev (optional): 3 events, before and after the fused pass and after
+// the walk.
+cudaError_t launch_tb_fused( const TbParams & p, int group, int grid, cudaStream_t st, cudaEvent_t * ev ) {
+    if( ev )
+        cudaEventRecord( ev[0], st );
+    if( p.n_hits ) {
+        if( group == 4 ) {
+            tb_fwddir_kernel<4><<<grid, 256, 0, st>>>( p );
+            if( ev )
+                cudaEventRecord( ev[1], st );
+            tb_reverse_kernel<4><<<grid, 256, 0, st>>>( p );
+        }
+        else if( group == 2 ) {
+            tb_fwddir_kernel<2><<<grid, 256, 0, st>>>( p );
+            if( ev )
+                cudaEventRecord( ev[1], st );
+            tb_reverse_kernel<2><<<grid, 256, 0, st>>>( p );
+        }
+        else {
+            tb_fwddir_kernel<1><<<grid, 256, 0, st>>>( p );
+            if( ev )
+                cudaEventRecord( ev[1], st );
+            tb_reverse_kernel<1><<<grid, 256, 0, st>>>( p );
+        }
+        tb_walk_kernel<<<(p.n_hits + 127) / 128, 128, 0, st>>>( p );
     }
     else if( ev ) {
         cudaEventRecord( ev[1], st );
