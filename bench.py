@@ -19,7 +19,7 @@ Metric: GCUPS = sum over queries of query length x database residues / time.
   half), 9 integer operations per cell;
 * ``cpu_baseline``: the reference libssa (built from its sources into
   oracle/_ref) on the host cores, on a sample of the same workload;
-* ``served``: config 4, 64 requests arriving as a Poisson process (50/s) into
+* ``served``: 64 requests arriving as a Poisson process (50/s) into
   the request loop (``ssa_server_*``) over a resident 1,000,000-sequence
   database: GCUPS over first arrival to last result, p50/p99 latency.
   ``--workload sw_served`` prints that leg alone as its own line.
@@ -155,7 +155,7 @@ def barrier(pg):
 def make_workload(scale: float, query_seed: int, kind: str = "sw_batched", n_queries: int | None = None):
     from libssa_b200 import workloads as W
     if kind == "sw_plain":
-        # config 1's database (10,000 sequences) and n_queries queries of 375
+        # a 10,000-sequence database and n_queries queries of 375
         import numpy as np
         w = W.sw_plain(seed=1, scale=scale)
         rng = np.random.default_rng(2000 + query_seed)
@@ -345,7 +345,8 @@ def run_ours(args):
         "metric": metric, "value": round(value, 2), "unit": "GCUPS", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(1e3 * t_dev / args.steps, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int16x2 (8-bit lane semantics), int32",
-        "data": "synthetic (seeded, BASELINE config %d shapes)" % (1 if plain else 3),
+        "data": ("synthetic (seeded: queries of 375 vs 10,000 gamma-length sequences)" if plain else
+                 "synthetic (seeded: 1,024 lognormal-length queries vs 500,000 gamma-length sequences)"),
         "config": {"workload": args.workload, "queries_per_gpu": len(w.queries), "db_sequences": w.n_db,
                    "db_residues": int(w.db_offsets[-1]), "cells_per_step_per_gpu": cells,
                    "matrix": "blosum62", "gap": [-11, -1], "bit_width": 8, "hits": 10,
@@ -407,7 +408,7 @@ def run_ours(args):
 # served: Poisson arrivals into the request loop (ssa_server_*)
 # --------------------------------------------------------------------------
 def served_leg(args, L) -> dict:
-    """Config 4: a resident 1,000,000-sequence database, queries arriving as a
+    """A resident 1,000,000-sequence database, queries arriving as a
     Poisson process into the server; GCUPS over the wall time from the first
     arrival to the last completion, and the submit-to-result latencies."""
     import numpy as np
@@ -463,7 +464,7 @@ def served_leg(args, L) -> dict:
 
 
 def run_nw_arm(args):
-    """Config 2: 64 nucleotide queries vs 200,000 sequences, Needleman-Wunsch,
+    """64 nucleotide queries vs 200,000 sequences, Needleman-Wunsch,
     16-bit entry, constant scores 2/-3, gaps 5/2, top 20 with CIGAR; one step is
     one batched search (ssa_align_batch)."""
     import libssa_b200 as L
@@ -491,7 +492,7 @@ def run_nw_arm(args):
     line = {"metric": "GCUPS (batched NW nucleotide search, 64 queries vs 200k sequences, top 20 with CIGAR)",
             "value": round(cells * args.steps / dev / 1e9, 2), "unit": "GCUPS", "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "int16 lanes (16-bit entry), int32", "data": "synthetic (seeded, BASELINE config 2 shapes)",
+            "dtype": "int16 lanes (16-bit entry), int32", "data": "synthetic (seeded: 64 nucleotide queries of 150-600 vs 200,000 sequences of 100-1,500)",
             "config": {"workload": "nw_nucleotide", "queries": len(qs), "db_sequences": w.n_db,
                        "db_residues": int(w.db_offsets[-1]), "cells_per_step": cells, "scale": args.scale},
             "e2e": {"value": round(cells * args.steps / wall / 1e9, 2), "unit": "GCUPS"},
@@ -505,7 +506,7 @@ def run_nw_arm(args):
 
 
 def run_pairs_arm(args):
-    """Config 5: long pairs, each a query of 5,000-30,000 residues and a mutated
+    """Long pairs, each a query of 5,000-30,000 residues and a mutated
     copy of it (85-99% identity, 1% indel events of length 1-20), BLOSUM62, gaps
     11/1, 16-bit entry, full CIGAR.  One step aligns every pair with
     Smith-Waterman and with Needleman-Wunsch through ssa_align_pairs (query i
@@ -545,7 +546,7 @@ def run_pairs_arm(args):
     line = {"metric": "GCUPS (long-pair SW and NW alignments with CIGAR, 5k-30k residues per side)",
             "value": round(cells * args.steps / dev / 1e9, 2), "unit": "GCUPS", "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(dev / args.steps * 1e3, 2), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded, BASELINE config 5 shapes)",
+            "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded: 4,096 query / mutated-copy pairs of 5,000-30,000 residues)",
             "config": {"workload": "long_pairs", "pairs": len(pairs), "query_lengths": [args.pair_lo, args.pair_hi],
                        "algorithms": ["sw", "nw"],
                        "cells_per_step": cells, "bit_width": 16,
@@ -576,7 +577,7 @@ def run_served_arm(args):
     line = {"metric": "GCUPS (served SW search, 1,000,000 resident sequences, Poisson arrivals, top 10 with CIGAR)",
             "value": res["value"], "unit": "GCUPS", "n_gpus": 1, "steps": 1, "warmup": 0,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "int16x2 (8-bit lane semantics), int32", "data": "synthetic (seeded, BASELINE config 4 shapes)",
+            "dtype": "int16x2 (8-bit lane semantics), int32", "data": "synthetic (seeded: 1,000,000 resident sequences, Poisson arrivals)",
             **{k: v for k, v in res.items() if k not in ("value", "unit")}}
     print(json.dumps(line), flush=True)
     return 0
@@ -594,13 +595,13 @@ def main():
     ap.add_argument("--plain-queries", type=int, default=16,
                     help="queries timed through the plain one-query-per-call path (0 = skip)")
     ap.add_argument("--served-queries", type=int, default=64,
-                    help="requests of the served leg (config 4 database; 0 = skip)")
+                    help="requests of the served leg (1,000,000-sequence database; 0 = skip)")
     ap.add_argument("--served-rate", type=float, default=50.0, help="Poisson arrival rate of the served leg, 1/s")
     ap.add_argument("--served-slots", type=int, default=64, help="resident query slots of the server")
     ap.add_argument("--served-segments", type=int, default=8, help="database segments per scan turn")
     ap.add_argument("--served-scale", type=float, default=1.0, help="served database scale (1.0 = 1M sequences)")
     ap.add_argument("--workload", default="sw_batched", choices=["sw_batched", "sw_plain", "sw_served", "nw_nucleotide", "long_pairs"],
-                    help="sw_plain: config 1's 10,000-sequence database with --queries queries of 375")
+                    help="sw_plain: a 10,000-sequence database with --queries queries of 375")
     ap.add_argument("--queries", type=int, default=None, help="query count for --workload sw_plain")
     ap.add_argument("--db-memory", type=int, default=0,
                     help="device memory for the database in bytes (0 = automatic; smaller streams it)")

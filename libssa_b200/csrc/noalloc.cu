@@ -15,7 +15,7 @@
 // library's BIT_WIDTH_64 searches (emul_kernel.cu at width 64).
 //
 // Where its memory comes from: the file-scope __device__ arrays below, sized
-// for the SSA_B200_NOALLOC_* limits of libssa_b200.h.  The driver reserves
+// for the SSA_B200_NOALLOC_* limits of libssa_b200.h.  The CUDA driver reserves
 // them when this file's module is loaded onto a device.  The first call on
 // each device (with that device current) loads the module and looks up the
 // arrays' addresses with cudaGetSymbolAddress; a caller should make that first

@@ -1,6 +1,6 @@
-"""Test-only checkers for the libssa B200 build.
+"""The test-only oracle of the libssa B200 build.
 
-TEST INFRASTRUCTURE ONLY.  Two checkers live here and only ``tests/``,
+TEST INFRASTRUCTURE ONLY.  Two programs live here and only ``tests/``,
 ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline leg may use them:
 
 * ``liboracle.so`` -- ``ssa_oracle.c``, a plain-C restatement of the reference

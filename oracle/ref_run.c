@@ -2,7 +2,7 @@
  * ref_run.c -- command-line driver around the reference libssa, built from
  * the reference's own sources by oracle/Makefile into oracle/_ref/ref_run.
  *
- * TEST INFRASTRUCTURE ONLY.  This program is the checker's ground truth: it
+ * TEST INFRASTRUCTURE ONLY.  This program is the oracle's ground truth: it
  * runs the unmodified CPU libssa through its public API (reference:
  * src/libssa.h:122-263) and prints what it returns.  Tests, the golden-fixture
  * generator and bench.py's CPU-baseline leg execute it; the product never
@@ -22,7 +22,7 @@
  *   --gap O,E           --chunk C           --threads T     --simd M
  *   --max-queries N     --repeat R          --time
  *
- * For every query record of the FASTA file the driver calls
+ * For every query record of the FASTA file ref_run calls
  * init_sequence_fasta(READ_FROM_STRING, seq), sw_align/nw_align and writes one
  * JSON object per line to OUT.json with the hits (score, ID, CIGAR,
  * coordinates), the 8->16 and 16->64 overflow counts the library reports, and

@@ -722,8 +722,8 @@ int oracle_search( const oracle_config * cfg, const uint8_t * query, uint64_t ql
             chunk.lens[chunk.n] = len;
             chunk.n++;
         }
-        /* a chunk without non-empty sequences ends the search: the drivers
-         * loop while( chunk->fill_pointer ) (search_8.c:652, search_16.c:785,
+        /* a chunk without non-empty sequences ends the search: the reference's
+         * search functions loop while( chunk->fill_pointer ) (search_8.c:652, search_16.c:785,
          * search_64.c:963), so later chunks are never read */
         if( chunk.n == 0 )
             break;

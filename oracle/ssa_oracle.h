@@ -1,7 +1,7 @@
 /*
  * ssa_oracle.h -- CPU restatement of the libssa database-search path.
  *
- * TEST INFRASTRUCTURE ONLY: the checker the CUDA build is compared against.
+ * TEST INFRASTRUCTURE ONLY: the oracle the CUDA build is compared against.
  * Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg load
  * it.  It is itself pinned against the reference binary built from the
  * reference's sources (oracle/_ref/ref_run) and the reference's known-answer

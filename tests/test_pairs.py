@@ -88,7 +88,7 @@ def test_pairs_on_warp_groups_match_oracle(built_library, algo):
 @pytest.mark.gpu
 @pytest.mark.parametrize("algo", ["sw", "nw"])
 def test_long_pairs_beyond_16_bits(built_library, algo):
-    """Config-5-sized pairs: scores above 32767 take the reference's 64-bit path."""
+    """Pairs of 9,000 and 14,000 residues: scores above 32767 take the reference's 64-bit path."""
     rng = np.random.default_rng(29)
     queries, records = [], []
     for n in (9000, 14000):
