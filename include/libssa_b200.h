@@ -105,7 +105,7 @@ int ssa_b200_translation_table( int code, uint8_t * out );
 
 /*
  * Database plugin extension implemented by libsdb_b200 (the plugin that ships
- * with this build): installs count records from memory, record i being
+ * with this library): installs count records from memory, record i being
  * residues[offsets[i] .. offsets[i+1]).  The data is copied.  Returns 0.
  */
 int ssa_db_b200_load_memory( size_t count, const char * residues, const uint64_t * offsets );
