@@ -199,3 +199,24 @@ def test_pairs_refuse_truncating_settings(built_library):
     finally:
         L.free_sequence(q)
         L.init_gap_penalties(-11, -1)
+
+
+def test_pairs_refuse_two_strand_setups(built_library):
+    """A pair is one query sequence against one database sequence; setups that
+    search several strands or frames per query are refused before any device
+    work."""
+    import libssa_b200 as L
+    L.set_output_mode(L.OUTPUT_SILENT)
+    L.init_symbol_translation(L.NUCLEOTIDE, L.BOTH_STRANDS, 1, 1)
+    L.init_constant_scores(2, -3)
+    L.init_gap_penalties(-5, -2)
+    L.load_db_memory([b"ACGTACGTAC"])
+    q = L.init_sequence_fasta(L.READ_FROM_STRING, "ACGTA")
+    try:
+        with pytest.raises(ValueError):
+            L.align_pairs(L.SSA_NEEDLEMAN_WUNSCH, [q], [0], L.BIT_WIDTH_16, L.COMPUTE_SCORE)
+    finally:
+        L.free_sequence(q)
+        L.init_symbol_translation(L.AMINOACID, L.FORWARD_STRAND, 1, 1)
+        L.init_score_matrix(L.MATRIX_BUILDIN, "blosum62")
+        L.init_gap_penalties(-11, -1)
