@@ -1711,6 +1711,10 @@ void Engine::traceback( const SearchRequest & req, std::vector<std::vector<Hit>>
             hit.cigar = std::move( cig );
         }
     }
+    // a very large direction buffer (long pairs) is not kept for later calls,
+    // whose scores, lists and database segments need the device memory
+    if( d_tb_dirs_.bytes > ((uint64_t) 8 << 30) )
+        d_tb_dirs_.release();
     if( timing ) {
         uint64_t max_cells = 0;
         uint32_t max_a = 0, max_b = 0;
