@@ -31,10 +31,13 @@ AA_SYMBOLS = "-ABCDEFGHIKLMNPQRSTVWXYZU*OJ"
 NT_SYMBOLS = "-ACMGRSVTWYHKDBN"
 
 
-def build(reference_root: str = "/root/reference") -> None:
-    """Builds liboracle.so, and ref_run when the reference sources exist."""
+def build(reference_root: str | None = None) -> None:
+    """Builds liboracle.so, and ref_run when the reference sources are given
+    (``reference_root``, else the ``SSA_REFERENCE_ROOT`` environment variable)
+    and present."""
     subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
-    if os.path.isdir(os.path.join(reference_root, "src")):
+    reference_root = reference_root or os.environ.get("SSA_REFERENCE_ROOT")
+    if reference_root and os.path.isdir(os.path.join(reference_root, "src")):
         subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={reference_root}"], check=True)
 
 

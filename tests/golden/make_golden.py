@@ -1,6 +1,6 @@
 """Generates the golden fixtures under tests/golden/ from the reference itself.
 
-    python tests/golden/make_golden.py [--reference /root/reference]
+    python tests/golden/make_golden.py --reference REFERENCE_ROOT
 
 Needs the reference sources (to build oracle/_ref/ref_run and to copy the FASTA
 fixtures of its own test suite).  Writes:
@@ -16,6 +16,8 @@ fixtures of its own test suite).  Writes:
 * ``abi_layout.json`` -- sizes, field offsets and constants of the
   reference's libssa.h / libssa_extern_db.h as its compiler sees them
   (tests/c_client/abi_layout.c built against the reference's headers);
+* ``wide_cases.json`` and ``data/wide_scores.txt`` -- score-only searches
+  with a score-matrix file whose 64-bit values leave the int32 range;
 * ``cases.json``    -- seeded synthetic search cases (inputs stored inline, or
   regenerated from libssa_b200.workloads with the stored seed and checked by
   hash) with the reference's complete answer: hit IDs, scores, CIGARs,
@@ -251,13 +253,88 @@ def write_abi_layout(reference: str) -> None:
         json.dump(layout, f, indent=1)
 
 
+WIDE_MATRIX = "wide_scores.txt"
+WIDE_SCALE = 100_000_007
+
+
+def write_wide_matrix(data: str) -> None:
+    """A score-matrix file in the reference's text format with BLOSUM62's
+    entries times 100,000,007: 64-bit scores far outside the int32 range, and
+    8/16-bit truncations that scramble the table (the reference's lanes use
+    them as they come, src/matrices.c:351-380)."""
+    with open(os.path.join(HERE, "matrices.json")) as f:
+        b62 = json.load(f)["blosum62"]
+    sym = "ARNDCQEGHILKMFPSTWYVBZX*"
+    aa = "-ABCDEFGHIKLMNPQRSTVWXYZU*OJ"
+    with open(os.path.join(data, WIDE_MATRIX), "w") as f:
+        f.write("# BLOSUM62 x %d\n" % WIDE_SCALE)
+        f.write("   " + "  ".join(sym) + "\n")
+        for a in sym:
+            row = [b62[(aa.index(a) << 5) + aa.index(b)] * WIDE_SCALE for b in sym]
+            f.write(a + " " + " ".join(str(v) for v in row) + "\n")
+
+
+def wide_cases() -> list[tuple[dict, list[bytes], list[bytes]]]:
+    """Score-only searches whose 64-bit values leave the int32 range: the
+    64-bit entry and the 8->16->64 / 16->64 cascades, SW and NW."""
+    rng = np.random.default_rng(4242)
+    out = []
+    for algo, width, chunk in (("sw", 64, 1000), ("nw", 64, 37), ("sw", 8, 50), ("nw", 16, 1000), ("sw", 16, 13)):
+        q = W.random_residues(rng, int(rng.integers(150, 420)), W.AA20)
+        recs = []
+        for i in range(int(rng.integers(90, 160))):
+            r = rng.random()
+            if r < 0.15:
+                recs.append(W.mutate(rng, q, W.AA20, 0.05, 0.02, (1, 4)))
+            elif r < 0.18:
+                recs.append(np.zeros(0, np.uint8))
+            else:
+                recs.append(W.random_residues(rng, int(rng.integers(1, 700)), W.AA20))
+        case = {"name": f"wide_{algo}_{width}", "algo": algo, "width": width, "align": 0, "hits": 12, "symtype": 1,
+                "matrix": "file:" + WIDE_MATRIX, "gap": [-11, -1], "chunk": chunk, "simd": 2}
+        out.append((case, [q.tobytes()], [r.tobytes() for r in recs]))
+    return out
+
+
+def write_wide_cases() -> None:
+    import tempfile
+    data = os.path.join(HERE, "data")
+    write_wide_matrix(data)
+    res_all = []
+    with tempfile.TemporaryDirectory() as tmp:
+        for case, queries, records in wide_cases():
+            db = os.path.join(tmp, "db.sdb")
+            oracle.write_sdb(db, seqs=records)
+            res = oracle.run_reference(db, [q.decode() for q in queries], algo=case["algo"], width=case["width"],
+                                       align=case["align"], hits=case["hits"], symtype=case["symtype"],
+                                       matrix="file:" + os.path.join(data, WIDE_MATRIX), gap=tuple(case["gap"]),
+                                       chunk=case["chunk"], simd=case["simd"])
+            case = dict(case)
+            case["queries"] = [q.decode() for q in queries]
+            case["records"] = [r.decode() for r in records]
+            case["expected"] = [{"ovf8": r["ovf8"], "ovf16": r["ovf16"],
+                                 "hits": [[h["id"], h["score"], h["cigar"], h["q_start"], h["q_end"], h["d_start"],
+                                           h["d_end"]] for h in r["hits"]]} for r in res]
+            res_all.append(case)
+            print(case["name"], "records", len(records), "top", case["expected"][0]["hits"][:2])
+    with open(os.path.join(HERE, "wide_cases.json"), "w") as f:
+        json.dump(res_all, f, indent=0)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("SSA_REFERENCE_ROOT"), required="SSA_REFERENCE_ROOT" not in os.environ,
+                    help="root of the reference source tree (default: $SSA_REFERENCE_ROOT)")
     ap.add_argument("--abi-only", action="store_true", help="only regenerate abi_layout.json")
     ap.add_argument("--frames-only", action="store_true",
                     help="only regenerate frame_cases.json and genetic_codes.json")
+    ap.add_argument("--wide-only", action="store_true",
+                    help="only regenerate wide_cases.json (and its matrix file)")
     args = ap.parse_args()
+    if args.wide_only:
+        oracle.build(args.reference)
+        write_wide_cases()
+        return
     write_abi_layout(args.reference)
     if args.abi_only:
         return
@@ -296,6 +373,7 @@ def main() -> None:
             print(case["name"], "queries", len(queries), "records", len(records))
     with open(os.path.join(HERE, "cases.json"), "w") as f:
         json.dump(out, f, indent=0)
+    write_wide_cases()
 
 
 if __name__ == "__main__":
