@@ -2,6 +2,7 @@
 // sm_100a kernels of the libssa B200 build.
 #pragma once
 
+#include <climits>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -35,6 +36,9 @@ struct QueryView {
     const uint32_t * qlen;        // per slot
     const uint32_t * qpad;        // per slot, rows of the profile
     uint32_t n_slots;
+    // the same table with exact int64 entries (same offsets), for the 64-bit
+    // pass in int64 arithmetic; nullptr otherwise
+    const int64_t * prof64 = nullptr;
 };
 
 // Result sink of a pass.  score[slot * n_ids + id] receives the pass's score.
@@ -47,7 +51,13 @@ struct PassSink {
     unsigned int * next_count;
     uint32_t next_cap;
     unsigned int * error_flags;   // bit 0: next[] overflow
+    // the 64-bit pass in int64 arithmetic writes its scores here (same index)
+    // and SCORE_IN_WIDE into score[]
+    int64_t * score64 = nullptr;
 };
+
+// score[] marker of a pair whose exact score is in PassSink::score64
+constexpr int32_t SCORE_IN_WIDE = INT32_MIN;
 
 enum ErrorBits : unsigned int {
     ERR_REQUEUE_OVERFLOW = 1u,
@@ -118,10 +128,19 @@ struct TbParams {
 };
 
 // Kernel launchers.
-cudaError_t launch_emul( int algo, int width, const EmulParams & p, int grid, cudaStream_t st );
+// wide: the 64-bit pass in int64 arithmetic (p.qv.prof64, p.sink.score64,
+// scratch of 32 bytes per column); otherwise int32
+cudaError_t launch_emul( int algo, int width, const EmulParams & p, int grid, cudaStream_t st, bool wide = false );
 cudaError_t launch_build_profile32( const uint8_t * qcodes, const uint64_t * qoff, const uint32_t * qlen,
         const uint32_t * qpad, const uint64_t * prof_off, const int64_t * matrix, int width, int32_t * prof,
         uint32_t n_slots, cudaStream_t st );
+// loads the int32 64-bit lane kernels and the int32 profile builder onto the
+// current device (no launch)
+cudaError_t preload_emul64();
+// exact int64 entries, layout of launch_build_profile32
+cudaError_t launch_build_profile64( const uint8_t * qcodes, const uint64_t * qoff, const uint32_t * qlen,
+        const uint32_t * qpad, const uint64_t * prof_off, const int64_t * matrix, int64_t * prof, uint32_t n_slots,
+        cudaStream_t st );
 // group: warps per hit, 1, 2 or 4 (scratch: one boundary row per group)
 cudaError_t launch_tb_regions( const TbParams & p, int group, int grid, cudaStream_t st, cudaEvent_t * ev );
 cudaError_t launch_tb_paths( const TbParams & p, int group, int grid, cudaStream_t st, cudaEvent_t * ev );

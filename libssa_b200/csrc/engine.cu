@@ -34,6 +34,8 @@
 
 namespace ssa {
 
+static_assert( REPLAY_SCORE_IN_WIDE == SCORE_IN_WIDE, "one marker for scores held in int64" );
+
 #define CUDA_CHECK( expr ) \
     do { \
         cudaError_t e_ = (expr); \
@@ -443,10 +445,11 @@ public:
             &d_tb_hits_, &d_tb_regions_, &d_tb_last_, &d_tb_last_off_, &d_tb_dirs_, &d_tb_dir_off_, &d_tb_ops_,
             &d_tb_ops_off_, &d_tb_ops_len_, &d_qp_prof_, &d_qp_off_, &d_qp_rows_, &d_qp_slots_, &d_qp_units_,
             &d_serve_score_, &d_qp_lmax_, &d_pair_slot_, &d_pair_unit_, &d_pair_score_, &d_scratch2_, &d_scratch4_,
-            &d_seg_[0], &d_seg_[1], &d_gather_codes_, &d_gather_off_, &d_gather_len_ };
+            &d_seg_[0], &d_seg_[1], &d_gather_codes_, &d_gather_off_, &d_gather_len_, &d_prof64_, &d_score64_ };
         for( DevBuf * b : bufs )
             b->release();
         h_score_.release();
+        h_score64_.release();
         h_stage_.release();
         resident_seg_ = -1;
         streaming_ = false;
@@ -525,6 +528,11 @@ private:
     DevBuf d_tb_hits_, d_tb_regions_, d_tb_last_, d_tb_last_off_, d_tb_dirs_, d_tb_dir_off_, d_tb_ops_,
             d_tb_ops_off_, d_tb_ops_len_;
     PinnedBuf h_score_;
+    // the 64-bit pass in int64 arithmetic (wide_): exact profiles and scores
+    DevBuf d_prof64_, d_score64_;
+    PinnedBuf h_score64_;
+    bool wide_ = false;
+    int prof64_width_ = -1;
     DevBuf d_pair_slot_, d_pair_unit_, d_pair_score_;
     uint64_t tb_budget_ = 0;         // traceback direction memory per wave (0 = automatic)
     // streaming: the database does not fit its device memory budget; segments
@@ -550,7 +558,24 @@ private:
 };
 
 void Engine::build_profiles( int width, uint32_t n_slots ) {
-    if( prof_width_ == width && prof_slots_ == n_slots )
+    if( wide_ && width == 64 ) {
+        // exact int64 table (same offsets as the int32 one, twice the bytes)
+        if( prof_width_ == 64 && prof64_width_ == 64 && prof_slots_ == n_slots )
+            return;
+        uint64_t elems = 0;
+        for( uint32_t s = 0; s < n_slots && s < h_prof_off_.size(); s++ )
+            elems = std::max<uint64_t>( elems, h_prof_off_[s] + 32ull * h_qpad_[s] );
+        d_prof64_.ensure( std::max<uint64_t>( elems, 1 ) * sizeof(int64_t) );
+        CUDA_CHECK( launch_build_profile64( d_qcodes_.as<uint8_t>(), d_qoff_.as<uint64_t>(), d_qlen_.as<uint32_t>(),
+                d_qpad_.as<uint32_t>(), d_prof_off_.as<uint64_t>(), d_matrix_.as<int64_t>(), d_prof64_.as<int64_t>(),
+                n_slots, stream_ ) );
+        launches_++;
+        prof_width_ = 64;
+        prof64_width_ = 64;
+        prof_slots_ = n_slots;
+        return;
+    }
+    if( prof_width_ == width && prof_slots_ == n_slots && prof64_width_ != 64 )
         return;
     launch_build_profile32( d_qcodes_.as<uint8_t>(), d_qoff_.as<uint64_t>(), d_qlen_.as<uint32_t>(),
             d_qpad_.as<uint32_t>(), d_prof_off_.as<uint64_t>(), d_matrix_.as<int64_t>(), width,
@@ -558,6 +583,7 @@ void Engine::build_profiles( int width, uint32_t n_slots ) {
     CUDA_CHECK( cudaGetLastError() );
     launches_++;
     prof_width_ = width;
+    prof64_width_ = -1;
     prof_slots_ = n_slots;
 }
 
@@ -590,18 +616,40 @@ void Engine::run_pass( int algo, int width, const SearchRequest & req, uint32_t 
     p.sink.next_count = next_count;
     p.sink.next_cap = next_cap;
     p.sink.error_flags = d_counts_.as<unsigned>() + 2;
+    const bool wide = wide_ && width == 64;
+    if( wide ) {
+        if( serving_ )
+            fatal( "Internal error: int64 scoring is not available to the server." );
+        p.qv.prof64 = d_prof64_.as<int64_t>();
+        p.sink.score64 = d_score64_.as<int64_t>();
+    }
     const int grid = sms_ * 2;
     const uint32_t cols = ((db_.max_len + 3u) & ~3u) + 4;
     if( max_qlen_ > 256 ) {
-        p.scratch = (int4 *) d_scratch_.ensure( (size_t) grid * 8 * cols * sizeof(int4) );
+        // a boundary column is 4 values: 16 bytes in int32, 32 in int64
+        const size_t col_bytes = wide ? 2 * sizeof(int4) : sizeof(int4);
+        p.scratch = (int4 *) d_scratch_.ensure( (size_t) grid * 8 * cols * col_bytes );
         p.scratch_cols = cols;
     }
     else {
         p.scratch = nullptr;
         p.scratch_cols = 0;
     }
-    CUDA_CHECK( launch_emul( algo, width, p, grid, stream_ ) );
+    CUDA_CHECK( launch_emul( algo, width, p, grid, stream_, wide ) );
     launches_++;
+}
+
+// Whether the 64-bit pass needs int64 arithmetic: a DP value is bounded by the
+// number of steps of a path (query rows + columns + a few boundary terms) times
+// the largest magnitude of one step (a score-table entry, or gapO + gapE); at
+// or below the int32 range (with a factor 2 of margin for the sums formed
+// before each max) int32 is exact.
+static bool needs_int64( const SearchRequest & req, uint32_t max_qlen, uint32_t max_dlen ) {
+    int64_t m = std::llabs( (int64_t) req.gap_open ) + std::llabs( (int64_t) req.gap_extend );
+    for( int k = 0; k < 1024; k++ )
+        m = std::max<int64_t>( m, req.matrix[k] == INT64_MIN ? INT64_MAX / 4 : std::llabs( req.matrix[k] ) );
+    const int64_t steps = (int64_t) max_qlen + max_dlen + 8;
+    return m > (int64_t) INT32_MAX / 2 || steps * (m + 1) * 2 > (int64_t) INT32_MAX;
 }
 
 // The 16x2 pass reproduces the 8-bit Smith-Waterman lanes exactly when the
@@ -1077,6 +1125,7 @@ void Engine::search( const SearchRequest & req, const std::vector<QueryCodes> & 
     if( gstart.back() != queries.size() )
         fatal( "Internal error: query groups do not cover the queries." );
     out.assign( groups.size(), {} );
+    stats.query_overflow.assign( groups.size(), { 0, 0 } );
     if( queries.empty() )
         return;
     const uint64_t n_ne = db.order_desc.size();
@@ -1085,8 +1134,16 @@ void Engine::search( const SearchRequest & req, const std::vector<QueryCodes> & 
     d_matrix_.ensure( 1024 * sizeof(int64_t) );
     CUDA_CHECK( cudaMemcpyAsync( d_matrix_.p, req.matrix, 1024 * sizeof(int64_t), cudaMemcpyHostToDevice, stream_ ) );
 
-    // sub-batches bounded by the per-pair result memory
-    const uint64_t pair_budget = (uint64_t) 1 << 28;
+    // the 64-bit pass in int64 arithmetic when the values can leave the int32 range
+    {
+        uint32_t qmax = 0;
+        for( const QueryCodes & q : queries )
+            qmax = std::max( qmax, q.len );
+        wide_ = needs_int64( req, qmax, db.max_len );
+    }
+    // sub-batches bounded by the per-pair result memory (int32 scores, plus
+    // int64 ones in the wide case)
+    const uint64_t pair_budget = (uint64_t) 1 << (wide_ ? 27 : 28);
     const uint64_t per_query = std::max<uint64_t>( 1, std::max<uint64_t>( n_ne, db.n_ids ) );
     const size_t batch = (size_t) std::max<uint64_t>(
             1, std::min<uint64_t>( std::min<uint64_t>( queries.size(), pair_budget / per_query ), 65535 ) );
@@ -1108,6 +1165,8 @@ void Engine::search( const SearchRequest & req, const std::vector<QueryCodes> & 
         const uint64_t n_pairs = (uint64_t) nq * n_ne;
         const size_t score_bytes = (size_t) nq * db.n_ids * sizeof(int32_t);
         d_score_.ensure( std::max<size_t>( score_bytes, 4 ) );
+        if( wide_ )
+            d_score64_.ensure( std::max<size_t>( 2 * score_bytes, 8 ) );
         const uint32_t cap = (uint32_t) std::min<uint64_t>( std::max<uint64_t>( n_pairs, 1 ), 0xffffffffull );
         d_list_a_.ensure( (size_t) cap * sizeof(PairTask) );
         d_list_b_.ensure( (size_t) cap * sizeof(PairTask) );
@@ -1183,6 +1242,12 @@ void Engine::search( const SearchRequest & req, const std::vector<QueryCodes> & 
         int32_t * hs = (int32_t *) h_score_.ensure( std::max<size_t>( score_bytes, 4 ) );
         if( score_bytes )
             CUDA_CHECK( cudaMemcpyAsync( hs, d_score_.p, score_bytes, cudaMemcpyDeviceToHost, stream_ ) );
+        int64_t * hs64 = nullptr;
+        if( wide_ && score_bytes ) {
+            hs64 = (int64_t *) h_score64_.ensure( 2 * score_bytes );
+            CUDA_CHECK( cudaMemcpyAsync( hs64, d_score64_.p, 2 * score_bytes, cudaMemcpyDeviceToHost, stream_ ) );
+            stats.d2h_bytes += 2 * score_bytes;
+        }
         unsigned err = 0;
         CUDA_CHECK( cudaMemcpyAsync( &err, cnt + 2, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_ ) );
         CUDA_CHECK( cudaEventRecord( ev_phase_[3], stream_ ) );
@@ -1193,8 +1258,11 @@ void Engine::search( const SearchRequest & req, const std::vector<QueryCodes> & 
 
         // ---- host replay, one query (group of query sequences) per worker
         std::vector<ReplayQuery> rq( nq );
-        for( uint32_t s = 0; s < nq; s++ )
+        for( uint32_t s = 0; s < nq; s++ ) {
             rq[s].score = hs + (size_t) s * db.n_ids;
+            if( hs64 )
+                rq[s].score64 = hs64 + (size_t) s * db.n_ids;
+        }
         for( const PairTask & t : list_entry )
             rq[t.qslot].ovf_entry.emplace_back( t.id, t.nb_prev );
         for( const PairTask & t : list_16 )
@@ -1233,9 +1301,10 @@ void Engine::search( const SearchRequest & req, const std::vector<QueryCodes> & 
                 for( auto & t : th )
                     t.join();
             }
-            for( const ReplayCounts & c : counts ) {
-                stats.overflow8 += c.overflow8;
-                stats.overflow16 += c.overflow16;
+            for( uint32_t i = 0; i < ng; i++ ) {
+                stats.overflow8 += counts[i].overflow8;
+                stats.overflow16 += counts[i].overflow16;
+                stats.query_overflow[g0 + i] = { counts[i].overflow8, counts[i].overflow16 };
             }
         }
         const auto t_replay1 = std::chrono::steady_clock::now();
@@ -1953,6 +2022,10 @@ void Engine::serve_restore( const SearchRequest & req ) {
 std::vector<uint32_t> Engine::serve_open( const SearchRequest & req, uint32_t slots, uint32_t segments ) {
     init_device();
     const HostDb & db = database();
+    if( needs_int64( req, SERVE_MAX_QUERY, db.max_len ) )
+        fatal( "The server scores in int32: the score table and gap penalties can exceed that range on this "
+               "database; use sw_align/nw_align." );
+    wide_ = false;
     serve_slots_ = slots;
     serve_codes_.assign( slots, {} );
     d_serve_score_.ensure( std::max<size_t>( 4, (size_t) slots * db.n_ids * sizeof(int32_t) ) );
@@ -2002,6 +2075,7 @@ void Engine::serve_wave( const SearchRequest & req, const std::vector<uint32_t> 
     if( !serve_layout_ )
         serve_restore( req );
     serving_ = true;
+    wide_ = false;                 // the server's settings were checked at serve_open
     const uint32_t n_seg = seq_hi - seq_lo;
     max_qlen_ = 0;
     uint64_t seg_res = 0;

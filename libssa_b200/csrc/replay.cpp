@@ -169,7 +169,7 @@ void replay_query( const HostDb & db, const SearchRequest & req, const ReplayQue
             for( uint64_t id = start; id < end; id++ ) {
                 if( db.len[id] == 0 )
                     continue;
-                const int64_t s = rq.score[id];
+                const int64_t s = rq.score_of( id );
                 if( filter && s <= r )
                     continue;
                 cand.emplace_back( req.bit_width == 64 ? (uint32_t) (id - start) : rank_entry[id], (uint32_t) id );
@@ -178,7 +178,7 @@ void replay_query( const HostDb & db, const SearchRequest & req, const ReplayQue
                 continue;
             std::sort( cand.begin(), cand.end() );
             for( auto & c : cand )
-                heap.add( c.second, rq.score[c.second] );
+                heap.add( c.second, rq.score_of( c.second ) );
             continue;
         }
         // the chunk has overflowing sequences: re-run its schedules
@@ -202,7 +202,7 @@ void replay_query( const HostDb & db, const SearchRequest & req, const ReplayQue
             if( ovfE.find( id, b ) )
                 next.push_back( id );
             else
-                heap.add( id, rq.score[id] );
+                heap.add( id, rq.score_of( id ) );
         }
         if( req.bit_width == 8 )
             counts.overflow8 += next.size() - n_entry_before;
@@ -224,15 +224,15 @@ void replay_query( const HostDb & db, const SearchRequest & req, const ReplayQue
                 if( ovf16.find( id, b ) )
                     list64.push_back( id );
                 else
-                    heap.add( id, rq.score[id] );
+                    heap.add( id, rq.score_of( id ) );
             }
             counts.overflow16 += list64.size();
             for( uint32_t id : list64 )
-                heap.add( id, rq.score[id] );
+                heap.add( id, rq.score_of( id ) );
         }
         else {
             for( uint32_t id : next )
-                heap.add( id, rq.score[id] );
+                heap.add( id, rq.score_of( id ) );
         }
     }
 
@@ -285,7 +285,7 @@ void replay_frames( const HostDb & db, const SearchRequest & req, const ReplayQu
         if( req.bit_width == 64 ) {
             for( uint32_t q = 0; q < F; q++ )
                 for( uint32_t u : units )
-                    heap.add( u, rq[q].score[u], q );
+                    heap.add( u, rq[q].score_of( u ), q );
             continue;
         }
         ovf_chunk.clear();
@@ -302,7 +302,7 @@ void replay_frames( const HostDb & db, const SearchRequest & req, const ReplayQu
                 if( ovfE[q].find( u, b ) )
                     ovf_chunk.push_back( u );
                 else
-                    heap.add( u, rq[q].score[u], q );
+                    heap.add( u, rq[q].score_of( u ), q );
             }
         }
         if( ovf_chunk.empty() )
@@ -324,19 +324,19 @@ void replay_frames( const HostDb & db, const SearchRequest & req, const ReplayQu
                     if( ovfE[q].find( u, b8 ) && ovf16[q].find( u, b16 ) )
                         list64.push_back( u );
                     else
-                        heap.add( u, rq[q].score[u], q );
+                        heap.add( u, rq[q].score_of( u ), q );
                 }
             }
             counts.overflow16 += list64.size();
             for( uint32_t q = 0; q < F; q++ )
                 for( uint32_t u : list64 )
-                    heap.add( u, rq[q].score[u], q );
+                    heap.add( u, rq[q].score_of( u ), q );
         }
         else {
             counts.overflow16 += ovf_chunk.size();
             for( uint32_t q = 0; q < F; q++ )
                 for( uint32_t u : ovf_chunk )
-                    heap.add( u, rq[q].score[u], q );
+                    heap.add( u, rq[q].score_of( u ), q );
         }
     }
     // score, then database ID, both descending; entries equal in both keep

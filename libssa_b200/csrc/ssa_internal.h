@@ -1,6 +1,7 @@
 // ssa_internal.h -- internal interfaces of the libssa B200 library.
 #pragma once
 
+#include <climits>
 #include <cstdint>
 #include <cstddef>
 #include <string>
@@ -91,6 +92,8 @@ struct Hit {
 struct SearchStats {
     uint64_t overflow8 = 0;     // sequences re-aligned at 16 bit
     uint64_t overflow16 = 0;    // sequences re-aligned at 64 bit
+    // the same per query (per entry of the call's query list)
+    std::vector<std::pair<uint64_t, uint64_t>> query_overflow;
     uint64_t cells = 0;         // query length x database residues, summed
     uint64_t kernel_launches = 0;
     double seconds_gpu = 0;
@@ -141,10 +144,20 @@ void engine_shutdown();
 uint64_t engine_kernel_launches();
 
 // ---- host replay of the CPU lane schedule and min-heap (replay.cpp) ----------
+// score[] marker of a pair whose exact score is in ReplayQuery::score64 (the
+// 64-bit pass ran in int64 arithmetic)
+constexpr int32_t REPLAY_SCORE_IN_WIDE = INT32_MIN;
+
 struct ReplayQuery {
     const int32_t * score = nullptr;                // per ID, final score
+    const int64_t * score64 = nullptr;              // per ID, where score[] holds the marker
     std::vector<std::pair<uint32_t, int32_t>> ovf_entry;   // (id, blocks) not reported by the entry pass
     std::vector<std::pair<uint32_t, int32_t>> ovf16;       // (id, blocks) not reported by the 16-bit pass
+
+    int64_t score_of( uint32_t id ) const {
+        const int32_t s = score[id];
+        return (s == REPLAY_SCORE_IN_WIDE && score64) ? score64[id] : (int64_t) s;
+    }
 };
 
 // ---- serving (engine.cu): resident query slots, waves over database segments --

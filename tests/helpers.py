@@ -53,13 +53,24 @@ def golden_cases() -> list[dict]:
         return json.load(f)
 
 
+def wide_cases() -> list[dict]:
+    """Score-only searches with a matrix file whose 64-bit values leave the
+    int32 range (make_golden.py write_wide_cases)."""
+    with open(os.path.join(GOLDEN, "wide_cases.json")) as f:
+        return json.load(f)
+
+
 def matrix_table(spec) -> np.ndarray:
-    """spec: ("const", match, mismatch) | ("builtin", name) | "const:M,X" | "builtin:name"."""
+    """spec: ("const", match, mismatch) | ("builtin", name) | ("file", name under golden/data) |
+    "const:M,X" | "builtin:name" | "file:name"."""
     if isinstance(spec, str):
         kind, arg = spec.split(":", 1)
         spec = ("const", *map(int, arg.split(","))) if kind == "const" else (kind, arg)
     if spec[0] == "const":
         return oracle.constant_matrix(spec[1], spec[2])
+    if spec[0] == "file":
+        with open(os.path.join(DATA, spec[1])) as f:
+            return oracle.parse_matrix(f.read())
     return np.array(golden_matrices()[spec[1]], dtype=np.int64)
 
 
@@ -119,6 +130,8 @@ def product_setup(symtype, matrix, gap, chunk, simd, records: list[bytes] | None
         matrix = ("const", *map(int, arg.split(","))) if kind == "const" else (kind, arg)
     if matrix[0] == "const":
         L.init_constant_scores(matrix[1], matrix[2])
+    elif matrix[0] == "file":
+        L.init_score_matrix(L.READ_FROM_FILE, os.path.join(DATA, matrix[1]))
     else:
         L.init_score_matrix(L.MATRIX_BUILDIN, matrix[1])
     L.init_gap_penalties(gap[0], gap[1])

@@ -10,8 +10,8 @@ import os
 import numpy as np
 import pytest
 
-from helpers import DATA, case_inputs, first_fasta_sequence, golden_cases, oracle_search, product_search, \
-    product_setup, read_fasta
+from helpers import DATA, ROOT, case_inputs, first_fasta_sequence, golden_cases, oracle_search, product_search, \
+    product_setup, read_fasta, wide_cases
 from kats import KATS, matches
 from libssa_b200 import workloads as W
 
@@ -46,6 +46,51 @@ def test_golden_reference_runs(built_library, case):
         exp = case["expected"][qi]
         assert [list(r) for r in res[qi]] == exp["hits"], (case["name"], qi)
         assert list(ovf[qi]) == [exp["ovf8"], exp["ovf16"]], (case["name"], qi)
+
+
+@pytest.mark.parametrize("case", wide_cases(), ids=[c["name"] for c in wide_cases()])
+@pytest.mark.parametrize("batch", [False, True], ids=["single", "batch"])
+def test_wide_value_reference_runs(built_library, case, batch):
+    """Scores far outside the int32 range (a matrix file of BLOSUM62 times
+    100,000,007): the 64-bit pass runs in int64 and matches the reference's
+    full_sw / full_nw (src/algo/64/smith_waterman_63.c:32-98,
+    needleman_wunsch_64.c:32-98), at the 64-bit entry and at the end of the
+    8/16-bit cascades."""
+    queries = [q.encode() for q in case["queries"]]
+    records = [r.encode() for r in case["records"]]
+    product_setup(case["symtype"], case["matrix"], tuple(case["gap"]), case["chunk"], case["simd"], records=records)
+    res, ovf = product_search(case["algo"], case["width"], case["align"], case["hits"], queries + queries[:1] * batch,
+                              batch=batch)
+    exp = case["expected"][0]
+    for r in res:
+        assert [list(x) for x in r] == exp["hits"], case["name"]
+    if ovf is not None:
+        assert list(ovf[0]) == [exp["ovf8"], exp["ovf16"]], case["name"]
+
+
+def test_alignment_beyond_int32_is_refused(built_library, tmp_path):
+    """The traceback kernels compute in int32: an alignment whose values could
+    leave that range ends in fatal() with a message (exit status 1, as the
+    reference's errors do), never with a wrapped result."""
+    import subprocess
+    import sys
+    case = [c for c in wide_cases() if c["name"] == "wide_sw_64"][0]
+    script = f"""
+import sys
+sys.path.insert(0, {ROOT!r}); sys.path.insert(0, {os.path.join(ROOT, "tests")!r})
+import libssa_b200 as L
+from helpers import product_setup, product_search
+L.load()
+case_q = {case["queries"][0]!r}
+recs = {case["records"][:20]!r}
+product_setup(1, "file:wide_scores.txt", (-11, -1), 1000, 2, records=[r.encode() for r in recs])
+product_search("sw", 64, 1, 5, [case_q.encode()])
+print("returned")
+"""
+    r = subprocess.run([sys.executable, "-c", script], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 1, (r.returncode, r.stdout, r.stderr)
+    assert "exceeds the supported score range" in r.stderr
+    assert "returned" not in r.stdout
 
 
 def test_batched_equals_single(built_library):

@@ -8,7 +8,7 @@ import pytest
 
 import oracle
 from helpers import DATA, case_inputs, first_fasta_sequence, golden_cases, golden_matrices, matrix_table, \
-    oracle_search, read_fasta
+    oracle_search, read_fasta, wide_cases
 from kats import KATS, matches
 
 
@@ -99,3 +99,32 @@ def test_oracle_against_fresh_reference_runs(tmp_path):
         assert [list(r) for r in res] == [[h["id"], h["score"], h["cigar"], h["q_start"], h["q_end"], h["d_start"],
                                            h["d_end"]] for h in ref["hits"]]
         assert (ref["ovf8"], ref["ovf16"]) == ovf
+
+
+@pytest.mark.parametrize("case", wide_cases(), ids=[c["name"] for c in wide_cases()])
+def test_oracle_matches_wide_value_reference_runs(case):
+    """64-bit scores far outside the int32 range (a matrix file of BLOSUM62
+    times 100,000,007), at the 64-bit entry and through the 8/16-bit cascades
+    whose lanes use the truncated table."""
+    queries = [q.encode() for q in case["queries"]]
+    records = [r.encode() for r in case["records"]]
+    for qi, q in enumerate(queries):
+        res, ovf = oracle_search(case["algo"], case["width"], case["align"], case["hits"], case["symtype"],
+                                 case["matrix"], case["gap"], case["chunk"], case["simd"], q, records)
+        exp = case["expected"][qi]
+        assert [list(r) for r in res] == exp["hits"]
+        assert [exp["ovf8"], exp["ovf16"]] == list(ovf)
+        assert max(h[1] for h in exp["hits"]) > 2 ** 31
+
+
+def test_wide_matrix_file_parses_like_the_reference():
+    """The oracle's parser reads the large entries as the reference does
+    (int64, unset cells -1)."""
+    m = matrix_table("file:wide_scores.txt")
+    b62 = np.array(golden_matrices()["blosum62"], dtype=np.int64)
+    aa = "-ABCDEFGHIKLMNPQRSTVWXYZU*OJ"
+    listed = [aa.index(c) for c in "ARNDCQEGHILKMFPSTWYVBZX*"]
+    for a in range(32):
+        for b in range(32):
+            want = b62[(a << 5) + b] * 100_000_007 if a in listed and b in listed else -1
+            assert m[(a << 5) + b] == want, (a, b)
