@@ -82,6 +82,13 @@ typedef struct {
 
 void ssa_get_stats( ssa_stats_t * out );
 
+/* The overflow counters of ssa_get_stats per query of the last search call
+ * (sw_align/nw_align: one query; ssa_align_batch: queries[i] at index i), as
+ * the reference reports them for each sw_align/nw_align call
+ * (src/algo/manager.c:156-159).  Writes min(n, count) entries of each non-NULL
+ * array and returns count, the number of queries of that call. */
+size_t ssa_b200_query_overflows( uint64_t * overflow_8_to_16, uint64_t * overflow_16_to_64, size_t n );
+
 /* Measured integer ALU-pipe ceiling of the current device: the rate of the
  * fused packed 16x2 add-max instruction, in operations per second (an add and
  * a max in each 16-bit half of each thread: 4 per instruction and thread),
@@ -159,9 +166,12 @@ void ssa_server_stop( ssa_server * server );
  * allocate their buffers per call (src/algo/searcher.c:43,160).
  *
  * Scores one query against count database sequences that the caller already
- * holds in device memory, with the exact 64-bit recurrences of a BIT_WIDTH_64
- * search (same scores as sw_align/nw_align at BIT_WIDTH_64), writing
- * d_scores[i] for sequence i.  Uses the global matrix and gap penalties.
+ * holds in device memory, as a BIT_WIDTH_64 search scores them (same scores as
+ * sw_align/nw_align at BIT_WIDTH_64), writing d_scores[i] for sequence i.
+ * Uses the global matrix and gap penalties.  Within the limits below (and
+ * score-table entries within int16, else SSA_B200_NOALLOC_EINVAL) every value
+ * of the recurrence stays below 2^29 in magnitude, so the int32 arithmetic
+ * and int32 scores are exact.
  * Residues are the library's codes: index into "-ABCDEFGHIKLMNPQRSTVWXYZU*OJ"
  * for amino acids, into "-ACMGRSVTWYHKDBN" for nucleotides; sequence i is
  * d_db_codes[d_db_offsets[i] .. + d_db_lengths[i]).  A sequence of length 0
@@ -171,8 +181,10 @@ void ssa_server_stop( ssa_server * server );
  * their own pool, or that cannot take cudaFree's device-wide synchronisation
  * on a latency-bound path.  Its working buffers are fixed-size device arrays
  * of the library (about 9.6 MiB per device), set up by the first call on each
- * device -- make that first call, with the device current, before the phase
- * that must not allocate and before any stream capture.  Sizes beyond the
+ * device, which also loads every kernel the call uses -- make that first call,
+ * with the device current, before the phase that must not allocate and before
+ * any stream capture.  Calls must be made in the device's primary context
+ * (the one the CUDA runtime API uses).  Sizes beyond the
  * limits below are rejected with SSA_B200_NOALLOC_ETOOBIG; max_seq_len is the
  * caller's bound on the database lengths.  The call runs on `stream` (a
  * cudaStream_t; NULL = default stream) and returns when the scores are

@@ -9,20 +9,31 @@
 // device, stalling every stream).  The regular search path sizes its device
 // buffers to each request and grows them with cudaMalloc/cudaFree.
 //
-// What it computes: the exact 64-bit Smith-Waterman or Needleman-Wunsch score
-// of one query against every sequence of a database the caller already holds
-// in device memory -- the same recurrences, kernel and results as the
-// library's BIT_WIDTH_64 searches (emul_kernel.cu at width 64).
+// What it computes: the Smith-Waterman or Needleman-Wunsch score of one query
+// against every sequence of a database the caller already holds in device
+// memory, as a BIT_WIDTH_64 search scores it (the library's 64-bit lane
+// kernel, emul_kernel.cu at width 64).  Within this entry point's limits --
+// query and sequences of at most 4096 residues, score-table entries within
+// int16 (other tables are rejected), int8 gap penalties -- no value of the
+// recurrence exceeds (4096 + 4096 + 8) x (32767 + 256) < 2^29 in magnitude,
+// so int32 arithmetic and int32 scores give the 64-bit results exactly.
 //
 // Where its memory comes from: the file-scope __device__ arrays below, sized
 // for the SSA_B200_NOALLOC_* limits of libssa_b200.h.  The CUDA driver reserves
 // them when this file's module is loaded onto a device.  The first call on
-// each device (with that device current) loads the module and looks up the
-// arrays' addresses with cudaGetSymbolAddress; a caller should make that first
-// call before it enters its no-allocation phase (and before any stream
-// capture).  Every later call only launches kernels and reads back one status
-// word.  What must start at zero on every call (the work counter, the error
-// word, the re-queue counter) is cleared by the call's first kernel.
+// each device (with that device current) loads the module, looks up the
+// arrays' addresses with cudaGetSymbolAddress and loads every kernel a call
+// launches (CUDA loads modules lazily by default, and a load can allocate); a
+// caller should make that first call before it enters its no-allocation phase
+// (and before any stream capture).  Every later call only launches kernels
+// and reads back one status word.  What must start at zero on every call (the
+// work counter, the error word, the re-queue counter) is cleared by the call's
+// first kernel.
+//
+// The addresses are looked up once per device ordinal in the device's primary
+// context, the one the CUDA runtime uses: calls must be made with that context
+// current (a context created through the driver API has its own copies of the
+// arrays at other addresses).
 //
 // The arrays are shared by all calls on a device: two calls in flight on the
 // same device at the same time (from two host threads, or on two streams)
@@ -119,6 +130,13 @@ static int na_setup( int dev, NoAllocDevice ** out ) {
                 cudaGetSymbolAddress( &a[3], na_matrix ) != cudaSuccess ||
                 cudaGetSymbolAddress( &a[4], na_state ) != cudaSuccess )
             return na_error( SSA_B200_NOALLOC_ECUDA, cudaGetErrorString( cudaGetLastError() ) );
+        // load every kernel a call launches now, not at its first launch
+        cudaFuncAttributes fa;
+        cudaError_t e = cudaFuncGetAttributes( &fa, noalloc_prepare_kernel );
+        if( e == cudaSuccess )
+            e = preload_emul64();
+        if( e != cudaSuccess )
+            return na_error( SSA_B200_NOALLOC_ECUDA, cudaGetErrorString( e ) );
         d.scratch = (int4 *) a[0];
         d.profile = (int32_t *) a[1];
         d.order = (uint32_t *) a[2];

@@ -50,17 +50,24 @@ def _device_db(torch, records: list[bytes]):
             int(lens.max()))
 
 
-def _noalloc(torch, algo: str, query: bytes, db, n: int) -> np.ndarray:
+def _noalloc_rc(torch, algo: str, query: bytes, db, n: int, max_len: int | None = None):
     import libssa_b200 as L
     import oracle
-    d_codes, d_offs, d_lens, max_len = db
+    d_codes, d_offs, d_lens, longest = db
     qc = torch.from_numpy(oracle.map_codes(query.decode(), False, True)).to("cuda:0")
     out = torch.full((n,), -7, dtype=torch.int32, device="cuda:0")
     rc = L.score64_noalloc(L.SSA_SMITH_WATERMAN if algo == "sw" else L.SSA_NEEDLEMAN_WUNSCH, qc.data_ptr(),
-                           qc.numel(), d_codes.data_ptr(), d_offs.data_ptr(), d_lens.data_ptr(), n, max_len,
-                           out.data_ptr(), torch.cuda.current_stream().cuda_stream)
+                           qc.numel(), d_codes.data_ptr(), d_offs.data_ptr(), d_lens.data_ptr(), n,
+                           longest if max_len is None else max_len, out.data_ptr(),
+                           torch.cuda.current_stream().cuda_stream)
+    return rc, out.cpu().numpy()
+
+
+def _noalloc(torch, algo: str, query: bytes, db, n: int) -> np.ndarray:
+    import libssa_b200 as L
+    rc, out = _noalloc_rc(torch, algo, query, db, n)
     assert rc == L.NOALLOC_OK
-    return out.cpu().numpy()
+    return out
 
 
 @pytest.mark.parametrize("algo", ["sw", "nw"])
@@ -94,3 +101,72 @@ def test_noalloc_rejects_sizes_beyond_limits(built_library):
     assert L.score64_noalloc(sw, p, 10, p, p, p, 1, L.NOALLOC_MAX_SEQ_LEN + 1, p) == L.NOALLOC_ETOOBIG
     assert L.score64_noalloc(sw, p, 10, p, p, p, L.NOALLOC_MAX_SEQS + 1, 10, p) == L.NOALLOC_ETOOBIG
     assert L.score64_noalloc(7, p, 10, p, p, p, 1, 10, p) == L.NOALLOC_EINVAL
+
+
+def test_noalloc_sequence_longer_than_its_bound(built_library):
+    """A caller that passes max_seq_len 4096 but holds a longer sequence gets
+    SSA_B200_NOALLOC_ESEQLEN (the per-warp boundary rows of a multi-pass query
+    hold 4096 columns), and every other sequence's score is still right."""
+    torch = pytest.importorskip("torch")
+    import libssa_b200 as L
+    records = _records(13, 60, 900)
+    records[7] = _protein(np.random.default_rng(14), 5000)
+    product_setup(L.AMINOACID, ("builtin", "blosum62"), (-11, -1), 1000, L.COMPUTE_ON_AVX2, records=records)
+    nonempty = [i for i, r in enumerate(records) if r]
+    query = _protein(np.random.default_rng(23), 600)           # three 256-row passes
+    want = _regular_scores("sw", query, len(nonempty))
+    db = _device_db(torch, records)
+    rc, got = _noalloc_rc(torch, "sw", query, db, len(records), max_len=L.NOALLOC_MAX_SEQ_LEN)
+    assert rc == L.NOALLOC_ESEQLEN
+    assert all(int(got[i]) == want[i] for i in nonempty if i != 7)
+
+
+_NO_GROWTH_SCRIPT = r"""
+import sys
+sys.path.insert(0, sys.argv[1]); sys.path.insert(0, sys.argv[2])
+import numpy as np
+import torch
+import libssa_b200 as L
+import test_zz_no_alloc as T
+from helpers import product_setup
+L.load()
+records = T._records(15, 200, 1200)
+product_setup(L.AMINOACID, ("builtin", "blosum62"), (-11, -1), 1000, L.COMPUTE_ON_AVX2)
+db = T._device_db(torch, records)
+d_codes, d_offs, d_lens, longest = db
+qs = [torch.from_numpy(np.frombuffer(T._protein(np.random.default_rng(s), n), np.uint8) % 20 + 1).to("cuda:0")
+      for s, n in ((31, 300), (32, 700))]
+outs = [torch.zeros(len(records), dtype=torch.int32, device="cuda:0") for _ in range(4)]
+stream = torch.cuda.current_stream().cuda_stream
+def call(algo, q, out):
+    rc = L.score64_noalloc(algo, q.data_ptr(), q.numel(), d_codes.data_ptr(), d_offs.data_ptr(), d_lens.data_ptr(),
+                           len(records), longest, out.data_ptr(), stream)
+    assert rc == L.NOALLOC_OK, rc
+torch.cuda.synchronize()
+call(L.SSA_SMITH_WATERMAN, qs[0], outs[0])          # set-up call: Smith-Waterman only
+torch.cuda.synchronize()
+free0 = torch.cuda.mem_get_info()[0]
+for k in range(3):
+    call(L.SSA_SMITH_WATERMAN, qs[k % 2], outs[1])
+    call(L.SSA_NEEDLEMAN_WUNSCH, qs[k % 2], outs[2])
+torch.cuda.synchronize()
+free1 = torch.cuda.mem_get_info()[0]
+print("free", free0, free1)
+assert free1 == free0, (free0, free1)
+"""
+
+
+def test_noalloc_calls_after_setup_allocate_nothing(built_library, tmp_path):
+    """In a fresh process: after one Smith-Waterman set-up call, repeated
+    Smith-Waterman and Needleman-Wunsch calls leave the device's free memory
+    unchanged -- the set-up loaded every kernel a call launches, so none is
+    loaded (and allocated for) later."""
+    import os
+    import subprocess
+    import sys
+    here = os.path.dirname(os.path.abspath(__file__))
+    script = tmp_path / "no_growth.py"
+    script.write_text(_NO_GROWTH_SCRIPT)
+    r = subprocess.run([sys.executable, str(script), os.path.dirname(here), here], capture_output=True, text=True,
+                       timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
