@@ -123,6 +123,9 @@ def load():
     lib.ssa_b200_set_db_memory.argtypes = [ctypes.c_size_t]
     lib.ssa_b200_db_streamed.restype = ctypes.c_int
     lib.ssa_get_stats.argtypes = [ctypes.POINTER(Stats)]
+    lib.ssa_b200_query_overflows.restype = ctypes.c_size_t
+    lib.ssa_b200_query_overflows.argtypes = [ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64),
+                                             ctypes.c_size_t]
     lib.ssa_db_refresh.argtypes = []
     lib.ssa_b200_int_peak.argtypes = [ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
     lib.ssa_b200_int_peak.restype = ctypes.c_int
@@ -318,6 +321,16 @@ def stats() -> Stats:
     s = Stats()
     load().ssa_get_stats(ctypes.byref(s))
     return s
+
+
+def query_overflows() -> list[tuple[int, int]]:
+    """(8->16, 16->64) overflow counters of each query of the last search call."""
+    lib = load()
+    n = lib.ssa_b200_query_overflows(None, None, 0)
+    a = (ctypes.c_uint64 * max(1, n))()
+    b = (ctypes.c_uint64 * max(1, n))()
+    lib.ssa_b200_query_overflows(a, b, n)
+    return [(int(a[i]), int(b[i])) for i in range(n)]
 
 
 def int_peak() -> tuple[float, float]:

@@ -935,6 +935,18 @@ void ssa_get_stats( ssa_stats_t * out ) {
     out->d2h_bytes = g_last_stats.d2h_bytes;
 }
 
+size_t ssa_b200_query_overflows( uint64_t * overflow_8_to_16, uint64_t * overflow_16_to_64, size_t n ) {
+    const auto & q = g_last_stats.query_overflow;
+    const size_t m = std::min( n, q.size() );
+    for( size_t i = 0; i < m; i++ ) {
+        if( overflow_8_to_16 )
+            overflow_8_to_16[i] = q[i].first;
+        if( overflow_16_to_64 )
+            overflow_16_to_64[i] = q[i].second;
+    }
+    return q.size();
+}
+
 void ssa_db_refresh( void ) {
     engine_invalidate_database();
 }

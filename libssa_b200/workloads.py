@@ -155,9 +155,11 @@ def sw_batched(seed: int = 3, scale: float = 1.0, n_queries: int = 1024, n_db: i
     records_lens = np.zeros(n, dtype=np.int64)
     bulk = random_residues(rng, int(lens[~is_copy].sum()), AA20)
     pos = 0
+    copy_src = {}                  # record -> index of the query it copies
     for i in range(n):
         if is_copy[i]:
-            src = queries[int(rng.integers(0, nq))]
+            copy_src[i] = int(rng.integers(0, nq))
+            src = queries[copy_src[i]]
             target = int(rng.integers(8000, 35001))
             tiled = np.tile(src, target // len(src) + 1)[:target]
             rec = mutate(rng, tiled, AA20, 0.02, 0.0, (1, 1))
@@ -168,7 +170,7 @@ def sw_batched(seed: int = 3, scale: float = 1.0, n_queries: int = 1024, n_db: i
         records_lens[i] = len(rec)
     flat, offsets = _pack(flat_parts)
     return Workload("sw_batched", "sw", 8, 10, 1, 1, "builtin:blosum62", (-11, -1), [q.tobytes() for q in queries],
-                    flat, offsets, {"seed": seed, "scale": scale, "long_copies": int(is_copy.sum())})
+                    flat, offsets, {"seed": seed, "scale": scale, "long_copies": int(is_copy.sum()), "copy_src": copy_src})
 
 
 def sw_served_db(seed: int = 4, scale: float = 1.0) -> Workload:
