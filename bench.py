@@ -14,15 +14,24 @@ Metric: GCUPS = sum over queries of query length x database residues / time.
   traceback; CUDA events on the library's streams), database resident in HBM;
 * ``e2e``: wall time of the public C-ABI call with host buffers (query upload,
   result download, host schedule/heap replay and list building included);
+* ``parity``: the last timed step's lists of a 64-query sample (IDs, scores,
+  order, CIGARs, coordinates, overflow counters) against the reference's own
+  answers at 1 thread (tests/golden/scale_sw_batched.json);
 * ``roofline``: the entry-pass kernel against the measured integer ALU-pipe
   ceiling of the same device (fused 16x2 add-max: an add and a max per 16-bit
   half), 9 integer operations per cell;
 * ``cpu_baseline``: the reference libssa (built from its sources into
-  oracle/_ref) on the host cores, on a sample of the same workload;
-* ``served``: 64 requests arriving as a Poisson process (50/s) into
-  the request loop (``ssa_server_*``) over a resident 1,000,000-sequence
-  database: GCUPS over first arrival to last result, p50/p99 latency.
-  ``--workload sw_served`` prints that leg alone as its own line.
+  oracle/_ref) on the host cores, all threads on a 16-query length-stratified
+  sample and 1 thread on 4 of them, against the full database;
+* ``plain_gpu``: the same queries one ``sw_align`` call each (16-query sample);
+* ``config1`` / ``config2`` / ``config5``: 1 x 375 vs 10,000 sequences
+  (sw_align), 64 nucleotide queries vs 200,000 (NW, batched), 4,096 long
+  pairs (SW and NW with CIGARs), each with its parity check;
+* ``served``: the 200-request stream of the served workload at Poisson rates
+  50-2,000/s into the request loop (``ssa_server_*``) over a resident
+  1,000,000-sequence database: GCUPS, p50/p99 latency, admission counts and
+  parity against the reference per rate.  ``--workload sw_served`` prints
+  that leg alone as its own line.
 
 With N > 1 (torchrun) every rank searches its own seeded 1,024-query batch
 against the full database (weak scaling, no collective on the data path);
@@ -191,31 +200,96 @@ def load_traffic() -> float | None:
 
 
 # --------------------------------------------------------------------------
+# parity of timed outputs against the reference's golden runs
+# --------------------------------------------------------------------------
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+
+
+def golden(name: str) -> dict | None:
+    try:
+        with open(os.path.join(GOLDEN, f"scale_{name}.json")) as f:
+            return json.load(f)
+    except OSError:
+        return None
+
+
+def hit_rows(hits) -> list[list]:
+    return [[h.id, h.score, h.cigar, h.q_start, h.q_end, h.d_start, h.d_end] for h in hits]
+
+
+def parity(name: str, lists: dict, overflows: dict | None = None) -> dict:
+    """Compares {query index: hit list} (and {index: (ovf8, ovf16)}) with the
+    reference's answers stored in tests/golden/scale_<name>.json."""
+    g = golden(name)
+    if g is None:
+        return {"sample": 0, "mismatches": None, "source": f"tests/golden/scale_{name}.json missing"}
+    bad = []
+    for i in g["sample"]:
+        exp = g["results"][str(i)]
+        if i not in lists or hit_rows(lists[i]) != exp["hits"]:
+            bad.append(i)
+        elif overflows is not None and list(overflows[i]) != exp["ovf"]:
+            bad.append(i)
+    return {"sample": len(g["sample"]), "mismatches": len(bad), "mismatched": bad[:8],
+            "checked": "IDs, scores, order, CIGARs, coordinates" + (", overflow counters" if overflows else ""),
+            "source": f"tests/golden/scale_{name}.json (the reference's sw_align/nw_align, 1 thread, AVX2)"}
+
+
+# --------------------------------------------------------------------------
 # CPU baseline: the reference built from its sources (oracle/_ref/ref_run)
 # --------------------------------------------------------------------------
-def reference_sample(w, n_queries: int, threads: int, repeat: int = 1) -> tuple[float, float, str]:
-    """(GCUPS, seconds, description) of the reference on a query sample."""
+def stratified(lengths, n: int) -> list[int]:
+    """n indices at evenly spaced length quantiles."""
+    import numpy as np
+    order = np.argsort(np.asarray(lengths), kind="stable")
+    return [int(order[int((i + 0.5) * len(order) / n)]) for i in range(n)]
+
+
+def reference_run(w, pick: list[int], threads: int, db_path: str | None = None) -> tuple[int, float]:
+    """(cells, seconds of the align calls) of the reference on queries `pick`
+    against the full database of workload w."""
     import oracle
     if not oracle.reference_available():
         raise RuntimeError("oracle/_ref/ref_run is not built")
     import numpy as np
-    lens = np.array([len(q) for q in w.queries])
-    # a representative sample: queries at evenly spaced length quantiles
-    order = np.argsort(lens)
-    pick = [int(order[int((i + 0.5) * len(order) / n_queries)]) for i in range(n_queries)]
     qs = [w.queries[i].decode() for i in pick]
+    with tempfile.TemporaryDirectory() as td:
+        db = db_path
+        if db is None:
+            db = os.path.join(td, "db.sdb")
+            oracle.write_sdb(db, flat=w.db_flat, lengths=np.diff(w.db_offsets))
+        res = oracle.run_reference(db, qs, algo="sw", width=8, align=1, hits=10, symtype=1,
+                                   matrix="builtin:blosum62", gap=(-11, -1), chunk=1000, threads=threads, simd=2,
+                                   timing=True)
+    return sum(len(q) for q in qs) * int(w.db_offsets[-1]), sum(r["seconds"] for r in res)
+
+
+REF_POOL = 16          # length-stratified queries the reference is timed on
+REF_PER_STEP = 4       # of them per step of the reference arm, in rotation
+
+
+def cpu_baselines(w) -> dict:
+    """The reference on this host: all threads on the 16-query pool, 1 thread
+    on 4 of its queries (every 4th length quantile)."""
+    import oracle
+    import numpy as np
+    threads = os.cpu_count() or 1
+    pool = stratified([len(q) for q in w.queries], REF_POOL)
     with tempfile.TemporaryDirectory() as td:
         db = os.path.join(td, "db.sdb")
         oracle.write_sdb(db, flat=w.db_flat, lengths=np.diff(w.db_offsets))
-        res = oracle.run_reference(db, qs, algo="sw", width=8, align=1, hits=10, symtype=1,
-                                   matrix="builtin:blosum62", gap=(-11, -1), chunk=1000, threads=threads, simd=2,
-                                   timing=True, repeat=repeat)
-    residues = int(w.db_offsets[-1])
-    secs = sum(r["seconds"] for r in res)
-    cells = sum(len(q) for q in qs) * residues
-    desc = (f"{n_queries} queries (lengths {sorted(len(q) for q in qs)}) of the workload vs the full "
-            f"{w.n_db}-sequence database, sw_align COMPUTE_ALIGNMENT, 8-bit entry, AVX2, {threads} threads")
-    return cells / secs / 1e9, secs, desc
+        cells, secs = reference_run(w, pool, threads, db)
+        one = pool[1::4]
+        cells1, secs1 = reference_run(w, one, 1, db)
+    lens = sorted(len(w.queries[i]) for i in pool)
+    return {"value": round(cells / secs / 1e9, 3), "unit": "GCUPS", "cores": threads, "kind": "reference",
+            "sample": f"{REF_POOL} length-stratified queries (lengths {lens}) vs the full {w.n_db}-sequence database, "
+                      f"sw_align COMPUTE_ALIGNMENT, 8-bit entry, AVX2, {threads} threads; cells / summed call time",
+            "seconds": round(secs, 2),
+            "one_thread": {"value": round(cells1 / secs1 / 1e9, 3), "unit": "GCUPS", "cores": 1,
+                           "sample": f"{len(one)} of those queries (lengths "
+                                     f"{sorted(len(w.queries[i]) for i in one)}), 1 thread",
+                           "seconds": round(secs1, 2)}}
 
 
 def pairs_reference_sample(pairs, n_pairs: int, threads: int) -> tuple[float, float, str]:
@@ -250,22 +324,41 @@ def pairs_reference_sample(pairs, n_pairs: int, threads: int) -> tuple[float, fl
 
 
 def run_reference_arm(args):
+    """The reference's own CPU path on this host's cores: every step runs 4
+    queries of a 16-query length-stratified pool (in rotation, so the timed
+    steps cover the whole pool) against the full database; the value is all
+    timed steps' cells over their summed align-call time."""
+    import oracle
+    import numpy as np
     world, rank, local, pg = dist_setup()
     if rank != 0:
         return 0
     w = make_workload(args.scale, 3)
     threads = os.cpu_count() or 1
-    vals = []
-    desc = ""
-    for i in range(args.warmup + args.steps):
-        g, secs, desc = reference_sample(w, args.ref_queries, threads)
-        if i >= args.warmup:
-            vals.append((g, secs))
-    value = statistics.median(v[0] for v in vals)
+    pool = stratified([len(q) for q in w.queries], REF_POOL)
+    cells_t, secs_t, step_s = 0, 0.0, []
+    covered = set()
+    with tempfile.TemporaryDirectory() as td:
+        db = os.path.join(td, "db.sdb")
+        oracle.write_sdb(db, flat=w.db_flat, lengths=np.diff(w.db_offsets))
+        for i in range(args.warmup + args.steps):
+            k0 = (i * REF_PER_STEP) % REF_POOL
+            pick = pool[k0:k0 + REF_PER_STEP]
+            cells, secs = reference_run(w, pick, threads, db)
+            if i >= args.warmup:
+                cells_t += cells
+                secs_t += secs
+                step_s.append(secs)
+                covered.update(pick)
+    value = cells_t / secs_t / 1e9
+    desc = (f"{len(covered)} of a {REF_POOL}-query length-stratified pool (lengths "
+            f"{sorted(len(w.queries[i]) for i in pool)}), {REF_PER_STEP} per step in rotation, vs the full "
+            f"{w.n_db}-sequence database, sw_align COMPUTE_ALIGNMENT, 8-bit entry, AVX2, {threads} threads; "
+            "cells over summed call time")
     line = {
         "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": "GCUPS", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": round(1e3 * statistics.median(v[1] for v in vals), 3), "higher_is_better": True,
+        "ms_per_step": round(1e3 * statistics.median(step_s), 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int8/int16/int64", "data": "synthetic (seeded)",
         "config": {"workload": "sw_batched", "queries": len(w.queries), "db_sequences": w.n_db,
                    "db_residues": int(w.db_offsets[-1]), "scale": args.scale},
@@ -280,6 +373,19 @@ def run_reference_arm(args):
 # --------------------------------------------------------------------------
 # the B200 arm
 # --------------------------------------------------------------------------
+def set_search(L, matrix: str = "blosum62", gap=(-11, -1), symtype=None):
+    L.set_output_mode(L.OUTPUT_SILENT)
+    L.init_symbol_translation(L.AMINOACID if symtype is None else symtype, L.FORWARD_STRAND, 1, 1)
+    if matrix.startswith("const:"):
+        L.init_constant_scores(*map(int, matrix[6:].split(",")))
+    else:
+        L.init_score_matrix(L.MATRIX_BUILDIN, matrix)
+    L.init_gap_penalties(*gap)
+    L.set_chunk_size(1000)
+    L.set_simd_compute_mode(L.COMPUTE_ON_AVX2)
+    L.set_thread_count(1)
+
+
 def run_ours(args):
     world, rank, local, pg = dist_setup()
     os.environ["SSA_B200_DEVICE"] = str(local)
@@ -289,12 +395,7 @@ def run_ours(args):
         build.build()
     L.load()
     w = rank_workload(args, rank)
-    L.set_output_mode(L.OUTPUT_SILENT)
-    L.init_symbol_translation(L.AMINOACID, L.FORWARD_STRAND, 1, 1)
-    L.init_score_matrix(L.MATRIX_BUILDIN, "blosum62")
-    L.init_gap_penalties(-11, -1)
-    L.set_chunk_size(1000)
-    L.set_simd_compute_mode(L.COMPUTE_ON_AVX2)
+    set_search(L)
     L.load_db_memory(flat=w.db_flat, offsets=w.db_offsets)
     if args.db_memory:
         L.set_db_memory(args.db_memory)     # below the packed size: the database is streamed
@@ -312,9 +413,10 @@ def run_ours(args):
     sampler = ClockSampler(local)
     sampler.start()
     wall, dev, entry, h2d, d2h = [], [], [], [], []
+    lists = None
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        step()
+        lists = step()
         wall.append(time.perf_counter() - t0)
         st = L.stats()
         dev.append(st.kernel_seconds)
@@ -323,6 +425,7 @@ def run_ours(args):
         d2h.append(st.d2h_bytes)
     clocks = sampler.stop()
     launches = L.stats().kernel_launches_total - launches0
+    ovf = L.query_overflows()
     barrier(pg)
     t_wall = reduce_max(pg, sum(wall))
     t_dev = reduce_max(pg, sum(dev))
@@ -372,60 +475,170 @@ def run_ours(args):
         "timing": {"device_seconds": round(t_dev, 4), "wall_seconds": round(t_wall, 4),
                    "entry_seconds_median": round(t_entry, 4)},
     }
+    if not plain and args.scale == 1.0 and rank == 0 and lists is not None:
+        line["parity"] = parity("sw_batched", dict(enumerate(lists)), dict(enumerate(ovf)))
     if args.plain_queries > 0:
         # the plain one-query-per-call path on a length-stratified query sample
-        import numpy as np
-        lens = np.array([len(q) for q in w.queries])
-        order = np.argsort(lens)
-        pick = [int(order[int((i + 0.5) * len(order) / args.plain_queries)]) for i in range(args.plain_queries)]
+        pick = stratified([len(q) for q in w.queries], args.plain_queries)
         sample = [qs[i] for i in pick]
         L.sw_align(sample[0], 10, L.BIT_WIDTH_8, L.COMPUTE_ALIGNMENT)
-        t0 = time.perf_counter()
+        t_plain, d_plain = 0.0, 0.0
         for q in sample:
+            t0 = time.perf_counter()
             L.sw_align(q, 10, L.BIT_WIDTH_8, L.COMPUTE_ALIGNMENT)
-        t_plain = time.perf_counter() - t0
+            t_plain += time.perf_counter() - t0
+            d_plain += L.stats().kernel_seconds
         cells_plain = sum(len(w.queries[i]) for i in pick) * int(w.db_offsets[-1])
-        line["plain_gpu"] = {"value": round(cells_plain / t_plain / 1e9, 2), "unit": "GCUPS",
+        plain_e2e = cells_plain / t_plain / 1e9
+        line["plain_gpu"] = {"value": round(plain_e2e, 2), "unit": "GCUPS",
+                             "device": round(cells_plain / d_plain / 1e9, 2),
+                             "batched_over_plain": {"e2e": round(e2e / plain_e2e, 2),
+                                                    "device": round(value / (cells_plain / d_plain / 1e9), 2)},
                              "sample": f"{args.plain_queries} length-stratified queries, one sw_align call each "
-                                       "(COMPUTE_ALIGNMENT), wall time"}
+                                       "(COMPUTE_ALIGNMENT); value: wall time of the calls (like e2e), device: "
+                                       "device time of their kernels (like value)"}
+    for q in qs:
+        L.free_sequence(q)
     if world == 1 and not args.no_cpu_baseline:
         try:
-            g, secs, desc = reference_sample(w, args.ref_queries, os.cpu_count() or 1)
-            line["cpu_baseline"] = {"value": round(g, 3), "unit": "GCUPS", "cores": os.cpu_count() or 1,
-                                    "kind": "reference", "sample": desc}
+            line["cpu_baseline"] = cpu_baselines(w)
         except Exception as e:  # noqa: BLE001
             line["cpu_baseline"] = {"value": None, "unit": "GCUPS", "cores": os.cpu_count() or 1,
                                     "kind": "reference", "sample": f"unavailable: {e}"}
-    for q in qs:
-        L.free_sequence(q)
-    if world == 1 and args.served_queries > 0:
-        line["served"] = served_leg(args, L)
+    if world == 1 and not plain and args.scale == 1.0 and not args.no_legs:
+        del w
+        line["config1"] = config1_leg(L)
+        line["config2"] = config2_leg(L)
+        line["config5"] = config5_leg(L, args)
+    if world == 1 and args.served_requests > 0:
+        line["served"] = served_sweep(args, L)
     print(json.dumps(line), flush=True)
     return 0
 
 
 # --------------------------------------------------------------------------
+# the other configurations, measured in the same run
+# --------------------------------------------------------------------------
+def config1_leg(L) -> dict:
+    """1 query of 375 residues vs 10,000 sequences through sw_align (8-bit
+    entry, top 10 with CIGAR): per-call wall and device time over 20 calls."""
+    from libssa_b200 import workloads as W
+    w = W.sw_plain(seed=1)
+    set_search(L)
+    L.load_db_memory(flat=w.db_flat, offsets=w.db_offsets)
+    q = L.init_sequence_fasta(L.READ_FROM_STRING, w.queries[0].decode())
+    for _ in range(3):
+        hits = L.sw_align(q, 10, L.BIT_WIDTH_8, L.COMPUTE_ALIGNMENT)
+    wall, dev, entry = [], [], []
+    for _ in range(20):
+        t0 = time.perf_counter()
+        hits = L.sw_align(q, 10, L.BIT_WIDTH_8, L.COMPUTE_ALIGNMENT)
+        wall.append(time.perf_counter() - t0)
+        st = L.stats()
+        dev.append(st.kernel_seconds)
+        entry.append(st.entry_seconds)
+    ovf = L.query_overflows()[0]
+    L.free_sequence(q)
+    cells = w.cells()
+    # golden: the reference's answer on this exact input (tests/golden/cases.json, sw_plain_full)
+    par = {"sample": 1, "mismatches": None}
+    try:
+        with open(os.path.join(GOLDEN, "cases.json")) as f:
+            case = [c for c in json.load(f) if c["name"] == "sw_plain_full"][0]
+        exp = case["expected"][0]
+        ok = hit_rows(hits) == exp["hits"] and list(ovf) == [exp["ovf8"], exp["ovf16"]]
+        par = {"sample": 1, "mismatches": 0 if ok else 1, "source": "tests/golden/cases.json sw_plain_full"}
+    except (OSError, IndexError, KeyError):
+        pass
+    return {"metric": "GCUPS (plain SW, 1 query of 375 vs 10,000 sequences, top 10 with CIGAR)",
+            "value": round(cells / statistics.median(dev) / 1e9, 2), "unit": "GCUPS",
+            "e2e": round(cells / statistics.median(wall) / 1e9, 2),
+            "ms_per_call": {"wall_median": round(1e3 * statistics.median(wall), 3),
+                            "device_median": round(1e3 * statistics.median(dev), 3),
+                            "entry_median": round(1e3 * statistics.median(entry), 3)},
+            "calls": 20, "parity": par,
+            "timing": "value: device time of the call's kernels (median of 20 calls); e2e: wall time of sw_align"}
+
+
+def config2_leg(L) -> dict:
+    """64 nucleotide queries vs 200,000 sequences, Needleman-Wunsch, 16-bit
+    entry, constant scores 2/-3, gaps 5/2, top 20 with CIGAR, one batched call
+    per step."""
+    from libssa_b200 import workloads as W
+    w = W.nw_nucleotide(seed=2)
+    set_search(L, "const:2,-3", (-5, -2), symtype=L.NUCLEOTIDE)
+    L.load_db_memory(flat=w.db_flat, offsets=w.db_offsets)
+    qs = [L.init_sequence_fasta(L.READ_FROM_STRING, q.decode()) for q in w.queries]
+    cells = w.cells()
+    L.align_batch(L.SSA_NEEDLEMAN_WUNSCH, qs, 20, L.BIT_WIDTH_16, L.COMPUTE_ALIGNMENT)
+    dev, wall = 0.0, 0.0
+    steps = 3
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        lists = L.align_batch(L.SSA_NEEDLEMAN_WUNSCH, qs, 20, L.BIT_WIDTH_16, L.COMPUTE_ALIGNMENT)
+        wall += time.perf_counter() - t0
+        dev += L.stats().kernel_seconds
+    ovf = L.query_overflows()
+    for q in qs:
+        L.free_sequence(q)
+    return {"metric": "GCUPS (batched NW nucleotide search, 64 queries vs 200,000 sequences, top 20 with CIGAR)",
+            "value": round(cells * steps / dev / 1e9, 2), "unit": "GCUPS",
+            "e2e": round(cells * steps / wall / 1e9, 2), "steps": steps,
+            "ms_per_step": round(1e3 * dev / steps, 2), "cells_per_step": cells,
+            "parity": parity("nw_nucleotide", dict(enumerate(lists)), dict(enumerate(ovf)))}
+
+
+def config5_leg(L, args) -> dict:
+    """4,096 long pairs (5,000-30,000 residues, a query and its mutated copy),
+    SW and NW with CIGARs through ssa_align_pairs, one timed step after one
+    warm-up."""
+    from libssa_b200 import workloads as W
+    pairs = W.long_pairs(seed=5)
+    set_search(L, gap=(-11, -1))
+    L.load_db_memory([b for _, b in pairs])
+    qs = [L.init_sequence_fasta(L.READ_FROM_STRING, a.decode()) for a, _ in pairs]
+    ids = list(range(len(pairs)))
+    cells = 2 * sum(len(a) * len(b) for a, b in pairs)
+    algos = (L.SSA_SMITH_WATERMAN, L.SSA_NEEDLEMAN_WUNSCH)
+    for algo in algos:
+        L.align_pairs(algo, qs, ids, L.BIT_WIDTH_16, L.COMPUTE_ALIGNMENT)
+    dev, wall = 0.0, 0.0
+    out = {}
+    for algo in algos:
+        t0 = time.perf_counter()
+        out[algo] = L.align_pairs(algo, qs, ids, L.BIT_WIDTH_16, L.COMPUTE_ALIGNMENT)
+        wall += time.perf_counter() - t0
+        dev += L.stats().gpu_seconds
+    for q in qs:
+        L.free_sequence(q)
+    g = golden("long_pairs")
+    par = {"sample": 0, "mismatches": None}
+    if g is not None:
+        bad = []
+        for k in g["sample"]:
+            for algo, name in ((algos[0], "sw"), (algos[1], "nw")):
+                got = [[0] + r[1:] for r in hit_rows(out[algo][k])]   # the reference's one-sequence database: ID 0
+                if got != g["results"][str(k)][name]:
+                    bad.append((k, name))
+        par = {"sample": len(g["sample"]), "mismatches": len(bad), "mismatched": bad[:8],
+               "source": "tests/golden/scale_long_pairs.json (the reference, one-sequence databases, 1 thread)"}
+    return {"metric": "GCUPS (4,096 long-pair SW and NW alignments with CIGAR, 5k-30k residues per side)",
+            "value": round(cells / dev / 1e9, 2), "unit": "GCUPS", "e2e": round(cells / wall / 1e9, 2),
+            "ms_per_step": round(1e3 * dev, 1), "cells_per_step": cells, "parity": par}
+
+
+# --------------------------------------------------------------------------
 # served: Poisson arrivals into the request loop (ssa_server_*)
 # --------------------------------------------------------------------------
-def served_leg(args, L) -> dict:
-    """A resident 1,000,000-sequence database, queries arriving as a
-    Poisson process into the server; GCUPS over the wall time from the first
-    arrival to the last completion, and the submit-to-result latencies."""
+SERVED_RATES = (50, 100, 200, 500, 1000, 2000)
+
+
+def served_once(L, texts, qs, residues, rate: float, seed: int, slots: int, segments: int) -> tuple[dict, list]:
+    """One Poisson stream of the queries `qs` at `rate`/s into a fresh server."""
     import numpy as np
     from libssa_b200 import workloads as W
-    w = W.sw_served_db(seed=4, scale=args.served_scale)
-    L.set_output_mode(L.OUTPUT_SILENT)
-    L.init_symbol_translation(L.AMINOACID, L.FORWARD_STRAND, 1, 1)
-    L.init_score_matrix(L.MATRIX_BUILDIN, "blosum62")
-    L.init_gap_penalties(-11, -1)
-    L.set_chunk_size(1000)
-    L.set_simd_compute_mode(L.COMPUTE_ON_AVX2)
-    L.load_db_memory(flat=w.db_flat, offsets=w.db_offsets)
-    texts = [q.decode() for q in W.served_queries(seed=40, n=args.served_queries)]
-    arrivals = W.poisson_arrivals(seed=41, rate=args.served_rate, n=len(texts))
-    qs = [L.init_sequence_fasta(L.READ_FROM_STRING, t) for t in texts]
-    server = L.Server(L.SSA_SMITH_WATERMAN, 10, L.BIT_WIDTH_8, L.COMPUTE_ALIGNMENT, slots=args.served_slots,
-                      segments=args.served_segments)
+    arrivals = W.poisson_arrivals(seed=seed, rate=rate, n=len(qs))
+    server = L.Server(L.SSA_SMITH_WATERMAN, 10, L.BIT_WIDTH_8, L.COMPUTE_ALIGNMENT, slots=slots, segments=segments)
     tickets = [None] * len(qs)
     t0 = time.perf_counter()
 
@@ -439,123 +652,121 @@ def served_leg(args, L) -> dict:
     th = threading.Thread(target=client)
     th.start()
     th.join()
-    lat = []
+    lat, results = [], []
     for t in tickets:
-        _, latency = server.wait(t)
+        hits, latency = server.wait(t)
         lat.append(latency)
+        results.append(hits)
     wall = time.perf_counter() - t0
     st = server.stats()
     server.stop()
-    for q in qs:
-        L.free_sequence(q)
-    residues = int(w.db_offsets[-1])
     cells = sum(len(t) for t in texts) * residues
     lat_ms = np.array(lat) * 1e3
-    return {"value": round(cells / wall / 1e9, 2), "unit": "GCUPS",
-            "latency_ms": {"p50": round(float(np.percentile(lat_ms, 50)), 1),
-                           "p99": round(float(np.percentile(lat_ms, 99)), 1),
-                           "max": round(float(lat_ms.max()), 1)},
+    return ({"rate_qps": rate, "value": round(cells / wall / 1e9, 2), "unit": "GCUPS",
+             "latency_ms": {"p50": round(float(np.percentile(lat_ms, 50)), 1),
+                            "p99": round(float(np.percentile(lat_ms, 99)), 1),
+                            "max": round(float(lat_ms.max()), 1)},
+             "requests": len(qs), "queued": int(st.queued), "admitted_at_once": len(qs) - int(st.queued),
+             "max_waiting": int(st.max_pending), "max_slots_used": int(st.max_occupied),
+             "mean_slots_used": round(st.slot_waves / max(1, st.waves), 1), "waves": int(st.waves),
+             "device_seconds": round(st.device_seconds, 3), "wall_seconds": round(wall, 3)}, results)
+
+
+def served_sweep(args, L) -> dict:
+    """A resident 1,000,000-sequence database; the 200-request stream of the
+    served workload arrives as a Poisson process at each rate into a fresh
+    server.  GCUPS over the wall time from the first arrival to the last
+    result, submit-to-result latency, admission counts, and every result
+    against the reference's answer for that request."""
+    from libssa_b200 import workloads as W
+    w = W.sw_served_db(seed=4, scale=args.served_scale)
+    set_search(L)
+    L.load_db_memory(flat=w.db_flat, offsets=w.db_offsets)
+    g = golden("sw_served") if args.served_scale == 1.0 else None
+    n = g["gen"]["queries"] if g else args.served_requests
+    texts = [q.decode() for q in W.served_queries(seed=40, n=n)][:args.served_requests]
+    qs = [L.init_sequence_fasta(L.READ_FROM_STRING, t) for t in texts]
+    residues = int(w.db_offsets[-1])
+    rates = [args.served_rate] if args.served_rate else list(SERVED_RATES)
+    per_rate = []
+    for k, rate in enumerate(rates):
+        res, results = served_once(L, texts, qs, residues, rate, 41 + k, args.served_slots, args.served_segments)
+        if g is not None:
+            res["parity"] = parity("sw_served", {i: results[i] for i in range(len(results))})
+        per_rate.append(res)
+    for q in qs:
+        L.free_sequence(q)
+    return {"per_rate": per_rate, "unit": "GCUPS",
             "config": {"workload": "sw_served", "db_sequences": w.n_db, "db_residues": residues,
-                       "queries": len(texts), "arrival_rate_qps": args.served_rate, "slots": args.served_slots,
-                       "segments": int(st.segments), "waves": int(st.waves), "hits": 10,
-                       "align_type": "COMPUTE_ALIGNMENT"},
-            "device_seconds": round(st.device_seconds, 3), "wall_seconds": round(wall, 3),
+                       "requests_per_rate": len(qs), "slots": args.served_slots, "segments": args.served_segments,
+                       "hits": 10, "align_type": "COMPUTE_ALIGNMENT",
+                       "queries": "the served stream's first requests (query seed 40), lognormal(300, 0.8) lengths"},
             "timing": "wall time from the first arrival to the last completion; latency = submit to result"}
 
 
 def run_nw_arm(args):
-    """64 nucleotide queries vs 200,000 sequences, Needleman-Wunsch,
-    16-bit entry, constant scores 2/-3, gaps 5/2, top 20 with CIGAR; one step is
-    one batched search (ssa_align_batch)."""
     import libssa_b200 as L
-    from libssa_b200 import workloads as W
     L.load()
-    w = W.nw_nucleotide(seed=2, scale=args.scale, n_queries=64)
-    L.set_output_mode(L.OUTPUT_SILENT)
-    L.init_symbol_translation(L.NUCLEOTIDE, L.FORWARD_STRAND, 1, 1)
-    L.init_constant_scores(2, -3)
-    L.init_gap_penalties(-5, -2)
-    L.set_chunk_size(1000)
-    L.set_simd_compute_mode(L.COMPUTE_ON_AVX2)
-    L.load_db_memory(flat=w.db_flat, offsets=w.db_offsets)
-    qs = [L.init_sequence_fasta(L.READ_FROM_STRING, q.decode()) for q in w.queries]
-    cells = sum(len(q) for q in w.queries) * int(w.db_offsets[-1])
-    for _ in range(args.warmup):
-        L.align_batch(L.SSA_NEEDLEMAN_WUNSCH, qs, 20, L.BIT_WIDTH_16, L.COMPUTE_ALIGNMENT)
-    dev, wall = 0.0, 0.0
-    for _ in range(args.steps):
-        t0 = time.perf_counter()
-        L.align_batch(L.SSA_NEEDLEMAN_WUNSCH, qs, 20, L.BIT_WIDTH_16, L.COMPUTE_ALIGNMENT)
-        wall += time.perf_counter() - t0
-        dev += L.stats().kernel_seconds
-    st = L.stats()
-    line = {"metric": "GCUPS (batched NW nucleotide search, 64 queries vs 200k sequences, top 20 with CIGAR)",
-            "value": round(cells * args.steps / dev / 1e9, 2), "unit": "GCUPS", "n_gpus": 1, "steps": args.steps,
-            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "int16 lanes (16-bit entry), int32", "data": "synthetic (seeded: 64 nucleotide queries of 150-600 vs 200,000 sequences of 100-1,500)",
-            "config": {"workload": "nw_nucleotide", "queries": len(qs), "db_sequences": w.n_db,
-                       "db_residues": int(w.db_offsets[-1]), "cells_per_step": cells, "scale": args.scale},
-            "e2e": {"value": round(cells * args.steps / wall / 1e9, 2), "unit": "GCUPS"},
-            "timing": {"device_seconds": round(dev, 4), "wall_seconds": round(wall, 4),
-                       "entry_seconds_last": round(st.entry_seconds, 4),
-                       "overflow_16_to_64_last": int(st.overflow_16_to_64)}}
+    leg = config2_leg(L)
+    line = {"metric": leg["metric"], "value": leg["value"], "unit": "GCUPS", "n_gpus": 1, "steps": leg["steps"],
+            "warmup": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "int16 lanes (16-bit entry), int32",
+            "data": "synthetic (seeded: 64 nucleotide queries of 150-600 vs 200,000 sequences of 100-1,500)",
+            "config": {"workload": "nw_nucleotide", "cells_per_step": leg["cells_per_step"]},
+            "e2e": {"value": leg["e2e"], "unit": "GCUPS"}, "parity": leg["parity"]}
     print(json.dumps(line), flush=True)
-    for q in qs:
-        L.free_sequence(q)
     return 0
 
 
 def run_pairs_arm(args):
     """Long pairs, each a query of 5,000-30,000 residues and a mutated
     copy of it (85-99% identity, 1% indel events of length 1-20), BLOSUM62, gaps
-    11/1, 16-bit entry, full CIGAR.  One step aligns every pair with
-    Smith-Waterman and with Needleman-Wunsch through ssa_align_pairs (query i
-    against database sequence i alone)."""
+    11/1, 16-bit entry.  One step aligns every pair with Smith-Waterman and with
+    Needleman-Wunsch through ssa_align_pairs (query i against database sequence
+    i alone); --pair-align score times the score-only calls."""
     import libssa_b200 as L
     from libssa_b200 import workloads as W
     L.load()
     pairs = W.long_pairs(seed=5, n_pairs=args.pairs, lo=args.pair_lo, hi=args.pair_hi)
-    L.set_output_mode(L.OUTPUT_SILENT)
-    L.init_symbol_translation(L.AMINOACID, L.FORWARD_STRAND, 1, 1)
-    L.init_score_matrix(L.MATRIX_BUILDIN, "blosum62")
-    L.init_gap_penalties(-11, -1)
-    L.set_chunk_size(1000)
-    L.set_simd_compute_mode(L.COMPUTE_ON_AVX2)
+    set_search(L)
     L.load_db_memory([b for _, b in pairs])
     qs = [L.init_sequence_fasta(L.READ_FROM_STRING, a.decode()) for a, _ in pairs]
     ids = list(range(len(pairs)))
     cells_one = sum(len(a) * len(b) for a, b in pairs)
     cells = 2 * cells_one
+    align = L.COMPUTE_SCORE if args.pair_align == "score" else L.COMPUTE_ALIGNMENT
     algos = (L.SSA_SMITH_WATERMAN, L.SSA_NEEDLEMAN_WUNSCH)
     for _ in range(args.warmup):
         for algo in algos:
-            L.align_pairs(algo, qs, ids, L.BIT_WIDTH_16, L.COMPUTE_ALIGNMENT)
+            L.align_pairs(algo, qs, ids, L.BIT_WIDTH_16, align)
     dev, wall = 0.0, 0.0
     per_algo = {0: 0.0, 1: 0.0}
     h2d = d2h = 0
     for _ in range(args.steps):
         for algo in algos:
             t0 = time.perf_counter()
-            L.align_pairs(algo, qs, ids, L.BIT_WIDTH_16, L.COMPUTE_ALIGNMENT)
+            L.align_pairs(algo, qs, ids, L.BIT_WIDTH_16, align)
             wall += time.perf_counter() - t0
             st = L.stats()
             dev += st.gpu_seconds
             per_algo[algo] += st.gpu_seconds
             h2d += int(st.h2d_bytes)
             d2h += int(st.d2h_bytes)
-    line = {"metric": "GCUPS (long-pair SW and NW alignments with CIGAR, 5k-30k residues per side)",
+    line = {"metric": "GCUPS (long-pair SW and NW alignments" + (" with CIGAR" if align else ", scores only") +
+                      ", 5k-30k residues per side)",
             "value": round(cells * args.steps / dev / 1e9, 2), "unit": "GCUPS", "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(dev / args.steps * 1e3, 2), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded: 4,096 query / mutated-copy pairs of 5,000-30,000 residues)",
+            "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+            "data": "synthetic (seeded: query / mutated-copy pairs of 5,000-30,000 residues)",
             "config": {"workload": "long_pairs", "pairs": len(pairs), "query_lengths": [args.pair_lo, args.pair_hi],
-                       "algorithms": ["sw", "nw"],
+                       "algorithms": ["sw", "nw"], "align": args.pair_align,
                        "cells_per_step": cells, "bit_width": 16,
                        "l2": "inputs and direction matrices far larger than L2"},
             "e2e": {"value": round(cells * args.steps / wall / 1e9, 2), "unit": "GCUPS",
                     "h2d_bytes_per_step": h2d // args.steps, "d2h_bytes_per_step": d2h // args.steps},
             "timing": {"device_seconds": round(dev, 4), "wall_seconds": round(wall, 4),
                        "sw_seconds": round(per_algo[0], 4), "nw_seconds": round(per_algo[1], 4)}}
-    if not args.no_cpu_baseline:
+    if not args.no_cpu_baseline and align:
         import multiprocessing
         threads = multiprocessing.cpu_count()
         try:
@@ -573,12 +784,13 @@ def run_pairs_arm(args):
 def run_served_arm(args):
     import libssa_b200 as L
     L.load()
-    res = served_leg(args, L)
+    res = served_sweep(args, L)
+    best = max(res["per_rate"], key=lambda r: r["value"])
     line = {"metric": "GCUPS (served SW search, 1,000,000 resident sequences, Poisson arrivals, top 10 with CIGAR)",
-            "value": res["value"], "unit": "GCUPS", "n_gpus": 1, "steps": 1, "warmup": 0,
+            "value": best["value"], "unit": "GCUPS", "n_gpus": 1, "steps": 1, "warmup": 0,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "int16x2 (8-bit lane semantics), int32", "data": "synthetic (seeded: 1,000,000 resident sequences, Poisson arrivals)",
-            **{k: v for k, v in res.items() if k not in ("value", "unit")}}
+            "dtype": "int16x2 (8-bit lane semantics), int32",
+            "data": "synthetic (seeded: 1,000,000 resident sequences, Poisson arrivals)", **res}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -590,13 +802,14 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--scale", type=float, default=1.0, help="database and query count scale (1.0 = full)")
-    ap.add_argument("--ref-queries", type=int, default=4, help="queries in the reference CPU sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-legs", action="store_true", help="skip the config-1, -2 and -5 legs")
     ap.add_argument("--plain-queries", type=int, default=16,
                     help="queries timed through the plain one-query-per-call path (0 = skip)")
-    ap.add_argument("--served-queries", type=int, default=64,
-                    help="requests of the served leg (1,000,000-sequence database; 0 = skip)")
-    ap.add_argument("--served-rate", type=float, default=50.0, help="Poisson arrival rate of the served leg, 1/s")
+    ap.add_argument("--served-requests", type=int, default=200,
+                    help="requests per arrival rate of the served leg (1,000,000-sequence database; 0 = skip)")
+    ap.add_argument("--served-rate", type=float, default=0.0,
+                    help="one Poisson arrival rate for the served leg, 1/s (0 = the sweep 50-2,000/s)")
     ap.add_argument("--served-slots", type=int, default=64, help="resident query slots of the server")
     ap.add_argument("--served-segments", type=int, default=8, help="database segments per scan turn")
     ap.add_argument("--served-scale", type=float, default=1.0, help="served database scale (1.0 = 1M sequences)")
@@ -608,6 +821,8 @@ def main():
     ap.add_argument("--pairs", type=int, default=4096, help="pair count for --workload long_pairs")
     ap.add_argument("--pair-lo", type=int, default=5000, help="shortest query of --workload long_pairs")
     ap.add_argument("--pair-hi", type=int, default=30000, help="longest query of --workload long_pairs")
+    ap.add_argument("--pair-align", default="alignment", choices=["alignment", "score"],
+                    help="--workload long_pairs: COMPUTE_ALIGNMENT or COMPUTE_SCORE")
     args = ap.parse_args()
     if args.impl == "reference":
         sys.exit(run_reference_arm(args))

@@ -96,6 +96,14 @@ size_t ssa_b200_query_overflows( uint64_t * overflow_8_to_16, uint64_t * overflo
  * search kernels' integer-pipe roofline.  Returns 0 on success. */
 int ssa_b200_int_peak( double * lane_ops_per_second, double * instructions_per_clock_per_sm );
 
+/* Issue rate of one packed-integer intrinsic on the current device, in warp
+ * intrinsics per clock per SM (eight interleaved dependent chains on every SM):
+ * op 0 __viaddmax_s16x2, 1 __vmaxs2, 2 __vimax3_s16x2, 3 __vaddss2,
+ * 4 __vsubss2, 5 __vaddss4, 6 __vmaxs4, 7 __vsubus4, 8 __vaddus4, 9 __vmaxu4,
+ * 10 __vadd4, 11 __vsub4.  The measurement behind the choice of 16x2 lanes
+ * over 8x4 ones.  Returns 0, or -1 for an unknown op or a CUDA error. */
+int ssa_b200_simd_rate( int op, double * per_clock_per_sm );
+
 /* Marks the packed copy of the database stale, so the next search reads it
  * again through the plugin.  init_db() does this itself; call it after
  * loading a database into the plugin by other means. */
@@ -147,6 +155,10 @@ typedef struct {
     double busy_seconds;         /* wall time of the loop's waves and completions */
     double device_seconds;       /* device time of the waves' entry passes and cascades */
     uint32_t slots, segments;
+    uint64_t queued;             /* requests not admitted at the first wave after their submit */
+    uint64_t slot_waves;         /* occupied slots summed over waves (mean occupancy = slot_waves / waves) */
+    uint32_t max_pending;        /* most requests waiting for admission after an admission point */
+    uint32_t max_occupied;       /* most slots occupied in one wave */
 } ssa_server_stats_t;
 
 ssa_server * ssa_server_start( int algorithm, size_t hitcount, int bit_width, int align_type, size_t slots,

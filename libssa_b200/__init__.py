@@ -128,6 +128,7 @@ def load():
                                              ctypes.c_size_t]
     lib.ssa_db_refresh.argtypes = []
     lib.ssa_b200_int_peak.argtypes = [ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
+    lib.ssa_b200_simd_rate.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
     lib.ssa_b200_int_peak.restype = ctypes.c_int
     lib.ssa_query_length.argtypes = [ctypes.c_void_p]
     lib.ssa_query_length.restype = ctypes.c_size_t
@@ -323,6 +324,22 @@ def stats() -> Stats:
     return s
 
 
+SIMD_PROBE_OPS = ["__viaddmax_s16x2", "__vmaxs2", "__vimax3_s16x2", "__vaddss2", "__vsubss2", "__vaddss4",
+                  "__vmaxs4", "__vsubus4", "__vaddus4", "__vmaxu4", "__vadd4", "__vsub4"]
+
+
+def simd_rates() -> dict[str, float]:
+    """Warp intrinsics per clock per SM of each probed packed-integer intrinsic."""
+    lib = load()
+    out = {}
+    for op, name in enumerate(SIMD_PROBE_OPS):
+        v = ctypes.c_double(0)
+        if lib.ssa_b200_simd_rate(op, ctypes.byref(v)) != 0:
+            raise RuntimeError(f"probe of {name} failed")
+        out[name] = v.value
+    return out
+
+
 def query_overflows() -> list[tuple[int, int]]:
     """(8->16, 16->64) overflow counters of each query of the last search call."""
     lib = load()
@@ -354,7 +371,8 @@ def score64_noalloc(algorithm: int, d_query: int, query_len: int, d_codes: int, 
 class ServerStats(ctypes.Structure):
     _fields_ = [("submitted", ctypes.c_uint64), ("completed", ctypes.c_uint64), ("waves", ctypes.c_uint64),
                 ("cells", ctypes.c_uint64), ("busy_seconds", ctypes.c_double), ("device_seconds", ctypes.c_double),
-                ("slots", ctypes.c_uint32), ("segments", ctypes.c_uint32)]
+                ("slots", ctypes.c_uint32), ("segments", ctypes.c_uint32), ("queued", ctypes.c_uint64),
+                ("slot_waves", ctypes.c_uint64), ("max_pending", ctypes.c_uint32), ("max_occupied", ctypes.c_uint32)]
 
 
 SERVE_MAX_QUERY = 8192

@@ -580,6 +580,7 @@ struct ServeTicket {
     int slot = -1;
     uint32_t waves = 0;
     bool done = false;
+    bool waited = false;       // left waiting at an admission point (no free slot or memory)
     std::chrono::steady_clock::time_point t_submit, t_done;
     ReplayQuery lists;
     p_alignment_list result = nullptr;
@@ -606,6 +607,8 @@ struct ServerImpl {
     std::thread loop_thread;
     // statistics
     uint64_t submitted = 0, completed = 0, waves = 0, cells = 0;
+    uint64_t queued = 0, slot_waves = 0;
+    uint32_t max_pending = 0, max_occupied = 0;
     double busy_seconds = 0, device_seconds = 0;
 
     void loop();
@@ -634,6 +637,16 @@ void ServerImpl::loop() {
                 mem_in_use += t->mem;
                 admitted.push_back( t );
             }
+            // requests this admission point could not take wait for a later wave
+            for( ServeTicket * t : pending ) {
+                if( !t->waited ) {
+                    t->waited = true;
+                    queued++;
+                }
+            }
+            max_pending = std::max<uint32_t>( max_pending, (uint32_t) pending.size() );
+            max_occupied = std::max( max_occupied, occupied );
+            slot_waves += occupied;
         }
         const auto t0 = std::chrono::steady_clock::now();
         for( ServeTicket * t : admitted )
@@ -1065,6 +1078,10 @@ void ssa_server_get_stats( ssa_server * sv, ssa_server_stats_t * out ) {
     out->device_seconds = s.device_seconds;
     out->slots = s.slots;
     out->segments = (uint32_t) s.seg.size() - 1;
+    out->queued = s.queued;
+    out->slot_waves = s.slot_waves;
+    out->max_pending = s.max_pending;
+    out->max_occupied = s.max_occupied;
 }
 
 void ssa_server_stop( ssa_server * sv ) {

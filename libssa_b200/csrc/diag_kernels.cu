@@ -40,9 +40,100 @@ __global__ void __launch_bounds__( 256 ) int_peak_kernel( unsigned * sink, unsig
         sink[blockIdx.x] = r;
 }
 
+// Issue-rate probe of one SIMD-video / DPX intrinsic: eight interleaved chains
+// x_i = op(x_i, x_{i+1}) (three-operand forms also read x_{i+2}), so nothing
+// folds.  Timing the launch gives intrinsics per clock per SM; ncu's
+// instruction counters of the same launch give instructions per intrinsic.
+// OP: 0 __viaddmax_s16x2, 1 __vmaxs2, 2 __vimax3_s16x2, 3 __vaddss2,
+//     4 __vsubss2, 5 __vaddss4, 6 __vmaxs4, 7 __vsubus4, 8 __vaddus4,
+//     9 __vmaxu4, 10 __vadd4, 11 __vsub4.
+template <int OP>
+__device__ __forceinline__ unsigned probe_op( unsigned a, unsigned b, unsigned c ) {
+    if constexpr( OP == 0 ) return __viaddmax_s16x2( a, b, c );
+    else if constexpr( OP == 1 ) return __vmaxs2( a, b );
+    else if constexpr( OP == 2 ) return __vimax3_s16x2( a, b, c );
+    else if constexpr( OP == 3 ) return __vaddss2( a, b );
+    else if constexpr( OP == 4 ) return __vsubss2( a, b );
+    else if constexpr( OP == 5 ) return __vaddss4( a, b );
+    else if constexpr( OP == 6 ) return __vmaxs4( a, b );
+    else if constexpr( OP == 7 ) return __vsubus4( a, b );
+    else if constexpr( OP == 8 ) return __vaddus4( a, b );
+    else if constexpr( OP == 9 ) return __vmaxu4( a, b );
+    else if constexpr( OP == 10 ) return __vadd4( a, b );
+    else return __vsub4( a, b );
+}
+
+constexpr int PROBE_OPS = 12;
+constexpr int PROBE_ITERS = 1024;
+
+template <int OP>
+__global__ void __launch_bounds__( 256 ) simd_probe_kernel( unsigned * sink, unsigned seed ) {
+    unsigned x[PEAK_CHAINS];
+#pragma unroll
+    for( int i = 0; i < PEAK_CHAINS; i++ )
+        x[i] = (threadIdx.x * (i + 3)) ^ (seed * 0x9e3779b9u);
+    for( int it = 0; it < PROBE_ITERS; it++ ) {
+#pragma unroll
+        for( int i = 0; i < PEAK_CHAINS; i++ )
+            x[i] = probe_op<OP>( x[i], x[(i + 1) % PEAK_CHAINS], x[(i + 2) % PEAK_CHAINS] );
+    }
+    unsigned r = 0;
+#pragma unroll
+    for( int i = 0; i < PEAK_CHAINS; i++ )
+        r ^= x[i];
+    if( r == 0x9e3779b9u )
+        sink[blockIdx.x] = r;
+}
+
+template <int OP>
+static void launch_probe( int blocks, unsigned * sink, unsigned seed ) {
+    simd_probe_kernel<OP><<<blocks, 256>>>( sink, seed );
+}
+
+typedef void (*ProbeLaunch)( int, unsigned *, unsigned );
+static const ProbeLaunch probe_launch[PROBE_OPS] = {
+    launch_probe<0>, launch_probe<1>, launch_probe<2>, launch_probe<3>, launch_probe<4>, launch_probe<5>,
+    launch_probe<6>, launch_probe<7>, launch_probe<8>, launch_probe<9>, launch_probe<10>, launch_probe<11> };
+
 }  // namespace ssa
 
 #pragma GCC visibility push( default )
+extern "C" int ssa_b200_simd_rate( int op, double * per_clock_per_sm ) {
+    using namespace ssa;
+    if( op < 0 || op >= PROBE_OPS || !per_clock_per_sm )
+        return -1;
+    int dev = 0;
+    cudaDeviceProp prop;
+    if( cudaGetDevice( &dev ) != cudaSuccess || cudaGetDeviceProperties( &prop, dev ) != cudaSuccess )
+        return -1;
+    const int blocks = prop.multiProcessorCount * 8;
+    unsigned * sink = nullptr;
+    if( cudaMalloc( &sink, blocks * sizeof(unsigned) ) != cudaSuccess )
+        return -1;
+    cudaEvent_t a, b;
+    cudaEventCreate( &a );
+    cudaEventCreate( &b );
+    probe_launch[op]( blocks, sink, 1 );
+    cudaEventRecord( a );
+    const int reps = 5;
+    for( int r = 0; r < reps; r++ )
+        probe_launch[op]( blocks, sink, 2 + r );
+    cudaEventRecord( b );
+    cudaEventSynchronize( b );
+    float ms = 0;
+    cudaEventElapsedTime( &ms, a, b );
+    cudaEventDestroy( a );
+    cudaEventDestroy( b );
+    cudaFree( sink );
+    if( cudaGetLastError() != cudaSuccess || ms <= 0 )
+        return -1;
+    int clk_khz = 0;
+    cudaDeviceGetAttribute( &clk_khz, cudaDevAttrClockRate, dev );
+    const double intrinsics = (double) reps * blocks * (256.0 / 32.0) * PROBE_ITERS * PEAK_CHAINS;
+    *per_clock_per_sm = intrinsics / (ms * 1e-3) / prop.multiProcessorCount / (clk_khz * 1e3);
+    return 0;
+}
+
 extern "C" int ssa_b200_int_peak( double * lane_ops_per_second, double * instructions_per_clock_per_sm ) {
     using namespace ssa;
     int dev = 0;
