@@ -104,6 +104,19 @@ int ssa_b200_int_peak( double * lane_ops_per_second, double * instructions_per_c
  * over 8x4 ones.  Returns 0, or -1 for an unknown op or a CUDA error. */
 int ssa_b200_simd_rate( int op, double * per_clock_per_sm );
 
+/*
+ * Entry-pass shape table.  The entry kernels pick their tile shape (rows per
+ * thread and resident CTAs per SM of the query-pair kernel; threads per
+ * sequence and rows per thread of the single-query kernel) per query from
+ * measured costs per shape and database bucket, written by libssa_b200/tune.py
+ * into libssa_b200/tuning/b200.tune (SSA_B200_TUNING=<path> reads another
+ * file, SSA_B200_TUNING=builtin the built-in costs).  This writes, as
+ * NUL-terminated JSON, where the table came from (file, version, device) and
+ * the shapes the last search call ran with; returns the length needed
+ * including the NUL.  The reference has a fixed tile instead
+ * (src/algo/8/search_8_util.h:25-27). */
+size_t ssa_b200_tuning_report( char * buf, size_t n );
+
 /* Marks the packed copy of the database stale, so the next search reads it
  * again through the plugin.  init_db() does this itself; call it after
  * loading a database into the plugin by other means. */

@@ -129,6 +129,8 @@ def load():
     lib.ssa_db_refresh.argtypes = []
     lib.ssa_b200_int_peak.argtypes = [ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
     lib.ssa_b200_simd_rate.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+    lib.ssa_b200_tuning_report.restype = ctypes.c_size_t
+    lib.ssa_b200_tuning_report.argtypes = [ctypes.c_char_p, ctypes.c_size_t]
     lib.ssa_b200_int_peak.restype = ctypes.c_int
     lib.ssa_query_length.argtypes = [ctypes.c_void_p]
     lib.ssa_query_length.restype = ctypes.c_size_t
@@ -338,6 +340,16 @@ def simd_rates() -> dict[str, float]:
             raise RuntimeError(f"probe of {name} failed")
         out[name] = v.value
     return out
+
+
+def tuning_report() -> dict:
+    """Origin of the entry-pass shape table and the shapes of the last search call."""
+    import json
+    lib = load()
+    n = lib.ssa_b200_tuning_report(None, 0)
+    buf = ctypes.create_string_buffer(n)
+    lib.ssa_b200_tuning_report(buf, n)
+    return json.loads(buf.value.decode())
 
 
 def query_overflows() -> list[tuple[int, int]]:

@@ -33,7 +33,7 @@ CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-fvisibility=hidden", "-Wall", "-I" 
 
 CU_SOURCES = ["engine.cu", "emul_kernel.cu", "traceback_kernels.cu", "diag_kernels.cu", "sw_fast_kernel.cu",
               "noalloc.cu", "sw_qpair_kernel.cu", "pair_kernel.cu"]
-CPP_SOURCES = ["api.cpp", "replay.cpp"]
+CPP_SOURCES = ["api.cpp", "replay.cpp", "tuning.cpp"]
 HEADERS = ["device_common.cuh", "wavefront.cuh", "stripe_pipeline.cuh", "ssa_internal.h", "builtin_matrices.inc"]
 
 LIB = os.path.join(OUT, "libssa.so")

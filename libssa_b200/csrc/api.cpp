@@ -948,6 +948,16 @@ void ssa_get_stats( ssa_stats_t * out ) {
     out->d2h_bytes = g_last_stats.d2h_bytes;
 }
 
+size_t ssa_b200_tuning_report( char * buf, size_t n ) {
+    const std::string r = tuning_report();
+    if( buf && n ) {
+        const size_t m = std::min( n - 1, r.size() );
+        memcpy( buf, r.data(), m );
+        buf[m] = 0;
+    }
+    return r.size() + 1;
+}
+
 size_t ssa_b200_query_overflows( uint64_t * overflow_8_to_16, uint64_t * overflow_16_to_64, size_t n ) {
     const auto & q = g_last_stats.query_overflow;
     const size_t m = std::min( n, q.size() );

@@ -27,6 +27,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <unordered_map>
 #include <thread>
@@ -528,6 +529,18 @@ private:
     DevBuf d_tb_hits_, d_tb_regions_, d_tb_last_, d_tb_last_off_, d_tb_dirs_, d_tb_dir_off_, d_tb_ops_,
             d_tb_ops_off_, d_tb_ops_len_;
     PinnedBuf h_score_;
+public:
+    // entry-pass shapes of the last search call: kernel, (R, CTAs per SM) for
+    // the query-pair kernel or (G, R) for the single-query one, queries or
+    // query pairs, database bucket
+    struct ShapeUse {
+        const char * kernel;
+        int a, b;
+        uint32_t n;
+        int bucket;
+    };
+    std::vector<ShapeUse> last_shapes_;
+private:
     // the 64-bit pass in int64 arithmetic (wide_): exact profiles and scores
     DevBuf d_prof64_, d_score64_;
     PinnedBuf h_score64_;
@@ -688,18 +701,30 @@ constexpr uint32_t FAST_MAX_PASS_ROWS = 512; // G x R: 16 KiB profile slice per 
 // that also bounds small databases by the longest sequence's latency picked
 // G = 32 for a 375-row query against 10,000 sequences, which measured slower
 // than this choice, G = 8, R = 24, P = 2.)
-static FastShape choose_shape( uint32_t Q, double mean_len ) {
+// With a measured shape table for the database's bucket (tuning.cpp) the cost
+// of a shape is passes x its measured cost per pass and column.
+static FastShape choose_shape( uint32_t Q, double mean_len, int bucket ) {
     FastShape best{ 0, 0, 0 };
     double best_cost = 1e300;
     const int Gs[] = { 8, 16, 32 };
     const int Rs[] = { 8, 16, 24, 32 };
-    for( int G : Gs ) {
-        for( int R : Rs ) {
+    const TuningTable & tt = tuning();
+    bool measured = false;
+    for( int gi = 0; gi < 3 && tt.has_fast; gi++ )
+        for( int ri = 0; ri < 4; ri++ )
+            measured |= tt.fast[bucket][gi][ri] > 0;
+    for( int gi = 0; gi < 3; gi++ ) {
+        const int G = Gs[gi];
+        for( int ri = 0; ri < 4; ri++ ) {
+            const int R = Rs[ri];
             const uint32_t per = (uint32_t) (G * R);
             const uint32_t P = (Q + per - 1) / per;
             if( per > FAST_MAX_PASS_ROWS || (uint64_t) P * per > FAST_MAX_ROWS )
                 continue;
-            const double cost = (double) P * G * (mean_len + G - 1) * (8.0 * R + 24.0);
+            if( measured && tt.fast[bucket][gi][ri] <= 0 )
+                continue;
+            const double cost = measured ? (double) P * tt.fast[bucket][gi][ri]
+                                         : (double) P * G * (mean_len + G - 1) * (8.0 * R + 24.0);
             if( cost < best_cost ) {
                 best_cost = cost;
                 best = FastShape{ G, R, (int) P };
@@ -720,8 +745,20 @@ void Engine::run_fast_entry( const SearchRequest & req, uint32_t nq, PairTask * 
     std::vector<uint32_t> rows_of( nq, 0 );
     std::vector<uint32_t> fallback;
     std::vector<std::vector<uint32_t>> by_r( 4 );   // R = 8, 16, 24, 32
+    const int bucket = db_bucket( db_.mean_len, db_.order_desc.size() );
+    // SSA_B200_FAST_SHAPE=G,R pins the shape (tuning)
+    int pin_g = 0, pin_r = 0;
+    if( const char * pin = getenv( "SSA_B200_FAST_SHAPE" ) )
+        if( sscanf( pin, "%d,%d", &pin_g, &pin_r ) != 2 )
+            pin_g = pin_r = 0;
     for( uint32_t s = 0; s < nq; s++ ) {
-        shape[s] = choose_shape( h_qlen_[s], db_.mean_len );
+        shape[s] = choose_shape( h_qlen_[s], db_.mean_len, bucket );
+        if( pin_g && shape[s].G ) {
+            const uint32_t per = (uint32_t) (pin_g * pin_r);
+            const uint32_t P = (h_qlen_[s] + per - 1) / per;
+            if( per <= FAST_MAX_PASS_ROWS && (uint64_t) P * per <= FAST_MAX_ROWS )
+                shape[s] = FastShape{ pin_g, pin_r, (int) P };
+        }
         if( shape[s].G == 0 ) {
             fallback.push_back( s );
             continue;
@@ -806,6 +843,13 @@ void Engine::run_fast_entry( const SearchRequest & req, uint32_t nq, PairTask * 
             multi |= shape[s].P > 1;
             slice_rows = std::max( slice_rows, (uint32_t) (shape[s].G * R) );
         }
+        {
+            std::map<int, uint32_t> by_g;
+            for( uint32_t s : cls )
+                by_g[shape[s].G]++;
+            for( auto & kv : by_g )
+                last_shapes_.push_back( { "sw_fast", kv.first, R, kv.second, bucket } );
+        }
         FastParams p{};
         p.slice_rows = slice_rows;
         int per_sm = 0;
@@ -861,9 +905,21 @@ void Engine::run_fast_entry( const SearchRequest & req, uint32_t nq, PairTask * 
 // queries of 375 residues against 10,000 sequences, each R pinned): R = 16
 // pays for 2-way shared-memory bank conflicts inside a group, R = 28 for a
 // few spilled registers.
-static int choose_qpair_rows( uint32_t Q, uint32_t * passes, int pinned ) {
+// The costs come from the measured shape table (tuning.cpp): per pass and
+// database column of a query pair, for each rows-per-thread R and resident
+// CTAs per SM (4 or 5); the smallest passes x cost wins.  pinned_r / pinned_mb
+// (SSA_B200_QP_R, SSA_B200_QP_MB) force a shape, as the tuner does.
+static int qpair_mb( int bucket, int R, int pinned_mb ) {
+    if( pinned_mb == 4 || pinned_mb == 5 )
+        return pinned_mb;
+    const double * c = tuning().qpair[bucket][R / 4 - 4];
+    if( c[0] > 0 && c[1] > 0 )
+        return c[1] < c[0] ? 5 : 4;
+    return c[1] > 0 ? 5 : 4;
+}
+
+static int choose_qpair_rows( uint32_t Q, uint32_t * passes, int pinned, int bucket, int pinned_mb ) {
     static const int rs[4] = { 16, 20, 24, 28 };
-    static const double cost[4] = { 4.28, 3.77, 4.56, 5.41 };
     int best_r = 0;
     double best_cost = 1e300;
     for( int i = 0; i < 4; i++ ) {
@@ -874,7 +930,10 @@ static int choose_qpair_rows( uint32_t Q, uint32_t * passes, int pinned ) {
         const uint32_t P = std::max<uint32_t>( 1, (Q + per - 1) / per );
         if( (uint64_t) P * per > FAST_MAX_ROWS )
             continue;
-        const double c = (double) P * cost[i];
+        const double unit = tuning().qpair[bucket][i][qpair_mb( bucket, R, pinned_mb ) - 4];
+        if( unit <= 0 && !pinned )
+            continue;                   // not measured
+        const double c = (double) P * (unit > 0 ? unit : 1.0);
         if( c < best_cost ) {
             best_cost = c;
             best_r = R;
@@ -882,7 +941,11 @@ static int choose_qpair_rows( uint32_t Q, uint32_t * passes, int pinned ) {
         }
     }
     if( best_r == 0 && pinned )         // the pinned R does not fit this query
-        return choose_qpair_rows( Q, passes, 0 );
+        return choose_qpair_rows( Q, passes, 0, bucket, pinned_mb );
+    if( best_r == 0 ) {                 // an empty table: 20 rows per thread
+        best_r = 20;
+        *passes = std::max<uint32_t>( 1, (Q + QP_G * 20 - 1) / (QP_G * 20) );
+    }
     return best_r;
 }
 
@@ -907,9 +970,16 @@ void Engine::run_qpair_entry( const SearchRequest & req, uint32_t nq, PairTask *
     }
     std::stable_sort( fit.begin(), fit.end(), [&]( uint32_t a, uint32_t b ) { return h_qlen_[a] > h_qlen_[b]; } );
     const uint32_t n_qp = (uint32_t) ((fit.size() + 1) / 2);
-    // SSA_B200_QP_R=16|20|24|28 pins R (tuning)
+    // SSA_B200_QP_R=16|20|24|28 and SSA_B200_QP_MB=4|5 pin the shape (tuning)
     const char * pin = getenv( "SSA_B200_QP_R" );
     const int pinned_r = pin ? atoi( pin ) : 0;
+    const char * pin_mb = getenv( "SSA_B200_QP_MB" );
+    const int pinned_mb = pin_mb ? atoi( pin_mb ) : 0;
+    // the database bucket of the shape table: these sequences' mean length and count
+    uint64_t seq_res = 0;
+    for( uint32_t i = lo; i < hi; i++ )
+        seq_res += db_.len[db_.order_desc[i]];
+    const int bucket = db_bucket( (double) seq_res / std::max<uint32_t>( 1, n_seq ), n_seq );
     std::vector<uint32_t> qp_slots( 2 * std::max<uint32_t>( 1, n_qp ), 0xffffffffu );
     std::vector<uint32_t> qp_rows( std::max<uint32_t>( 1, n_qp ), 0 );
     std::vector<uint64_t> qp_off( std::max<uint32_t>( 1, n_qp ), 0 );
@@ -920,7 +990,7 @@ void Engine::run_qpair_entry( const SearchRequest & req, uint32_t nq, PairTask *
         if( 2 * i + 1 < fit.size() )
             qp_slots[2 * i + 1] = fit[2 * i + 1];
         uint32_t P = 1;
-        const int R = choose_qpair_rows( h_qlen_[fit[2 * i]], &P, pinned_r );
+        const int R = choose_qpair_rows( h_qlen_[fit[2 * i]], &P, pinned_r, bucket, pinned_mb );
         qp_rows[i] = P * (uint32_t) (QP_G * R);
         by_r[R / 4 - 4].push_back( i );
     }
@@ -1020,13 +1090,15 @@ void Engine::run_qpair_entry( const SearchRequest & req, uint32_t nq, PairTask *
         if( cls.empty() )
             continue;
         const int R = 4 * (ri + 4);
+        const int mb = nw ? 4 : qpair_mb( bucket, R, pinned_mb );
         bool multi = false;
         for( uint32_t i : cls )
             multi |= qp_rows[i] > (uint32_t) (QP_G * R);
+        last_shapes_.push_back( { nw ? "nw_qpair" : "sw_qpair", R, mb, (uint32_t) cls.size(), bucket } );
         QPairParams p{};
         int per_sm = 0;
         CUDA_CHECK( nw ? launch_nw_qpair( R, p, 0, class_stream_[ri], &per_sm )
-                       : launch_sw_qpair( R, p, 0, class_stream_[ri], &per_sm ) );
+                       : launch_sw_qpair( R, mb, p, 0, class_stream_[ri], &per_sm ) );
         const int grid = sms_ * std::max( 1, per_sm );
         CUDA_CHECK( cudaStreamWaitEvent( class_stream_[ri], ev_ready_, 0 ) );
         unsigned long long * unit_counter = d_counts_.as<unsigned long long>() + 8 + ri;   // bytes 64..95
@@ -1066,7 +1138,7 @@ void Engine::run_qpair_entry( const SearchRequest & req, uint32_t nq, PairTask *
         if( timing )
             CUDA_CHECK( cudaEventRecord( ev_cls_t_[2 * ri], class_stream_[ri] ) );
         CUDA_CHECK( nw ? launch_nw_qpair( R, p, grid, class_stream_[ri], nullptr )
-                       : launch_sw_qpair( R, p, grid, class_stream_[ri], nullptr ) );
+                       : launch_sw_qpair( R, mb, p, grid, class_stream_[ri], nullptr ) );
         launches_++;
         if( timing )
             CUDA_CHECK( cudaEventRecord( ev_cls_t_[2 * ri + 1], class_stream_[ri] ) );
@@ -1126,6 +1198,7 @@ void Engine::search( const SearchRequest & req, const std::vector<QueryCodes> & 
         fatal( "Internal error: query groups do not cover the queries." );
     out.assign( groups.size(), {} );
     stats.query_overflow.assign( groups.size(), { 0, 0 } );
+    last_shapes_.clear();
     if( queries.empty() )
         return;
     const uint64_t n_ne = db.order_desc.size();
@@ -2277,6 +2350,32 @@ void engine_serve_finish( const SearchRequest & req, const std::vector<uint32_t>
         std::vector<ReplayQuery> & rq, std::vector<std::vector<Hit>> & out, SearchStats & stats ) {
     std::lock_guard<std::mutex> lock( g_engine_mutex );
     Engine::get().serve_finish( req, done, rq, out, stats );
+}
+
+std::string tuning_report() {
+    const TuningTable & t = tuning();
+    std::string out = "{\"source\": \"";
+    for( char c : t.source )
+        if( c != '"' && c != '\\' )
+            out += c;
+    out += "\", \"version\": " + std::to_string( t.version ) + ", \"device\": \"";
+    for( char c : t.device )
+        if( c != '"' && c != '\\' )
+            out += c;
+    out += "\", \"last_call\": [";
+    std::lock_guard<std::mutex> lock( g_engine_mutex );
+    bool first = true;
+    for( const auto & u : Engine::get().last_shapes_ ) {
+        char buf[160];
+        const bool qp = strcmp( u.kernel, "sw_fast" ) != 0;
+        snprintf( buf, sizeof buf, "%s{\"kernel\": \"%s\", \"%s\": %d, \"%s\": %d, \"%s\": %u, \"bucket\": %d}",
+                first ? "" : ", ", u.kernel, qp ? "R" : "G", u.a, qp ? "ctas_per_sm" : "R", u.b,
+                qp ? "query_pairs" : "queries", u.n, u.bucket );
+        out += buf;
+        first = false;
+    }
+    out += "]}";
+    return out;
 }
 
 uint64_t engine_kernel_launches() {

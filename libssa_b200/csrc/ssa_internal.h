@@ -143,6 +143,27 @@ void engine_invalidate_database();
 void engine_shutdown();
 uint64_t engine_kernel_launches();
 
+// ---- measured entry-pass shape costs (tuning.cpp, libssa_b200/tune.py) ---------
+constexpr int TUNE_BUCKETS = 6;   // database mean length <250 / <1000 / longer, x fewer / more than 50,000 sequences
+
+struct TuningTable {
+    int version = 0;
+    std::string device;
+    std::string source = "built-in";
+    // query-pair kernel: cost per (query pair, pass, database column) by
+    // [bucket][R / 4 - 4][resident CTAs per SM - 4]; 0 = not measured
+    double qpair[TUNE_BUCKETS][4][2] = {};
+    // single-query kernel: cost per (pass, database column) by
+    // [bucket][G = 8, 16, 32][R / 8 - 1]; 0 = not measured
+    double fast[TUNE_BUCKETS][3][4] = {};
+    bool has_fast = false;
+};
+
+const TuningTable & tuning();
+int db_bucket( double mean_len, uint64_t n_seqs );
+// JSON of the table's origin and the shapes the last search call used
+std::string tuning_report();
+
 // ---- host replay of the CPU lane schedule and min-heap (replay.cpp) ----------
 // score[] marker of a pair whose exact score is in ReplayQuery::score64 (the
 // 64-bit pass ran in int64 arithmetic)

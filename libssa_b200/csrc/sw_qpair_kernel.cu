@@ -44,8 +44,10 @@ constexpr uint32_t QP_BIAS2 = (QP_BIAS << 16) | QP_BIAS;
 constexpr uint32_t QP_CROSS_ADD = ((0x8000u - (QP_BIAS + 255u)) << 16) | (0x8000u - (QP_BIAS + 255u));
 constexpr int QP_THREADS = QP_THREADS_PER_CTA;
 
-template <int R>
-__global__ void __launch_bounds__( QP_THREADS, 4 ) sw_qpair_kernel( QPairParams p ) {
+// MB: resident CTAs per SM the register allocation is bounded for (4: up to
+// 128 registers a thread, 5: up to 102); chosen per class by the tuning table.
+template <int R, int MB>
+__global__ void __launch_bounds__( QP_THREADS, MB ) sw_qpair_kernel( QPairParams p ) {
     constexpr int G = QP_G;
     constexpr uint32_t GR = (uint32_t) (G * R);
     extern __shared__ __align__( 16 ) uint32_t qsm[];
@@ -260,32 +262,34 @@ __global__ void __launch_bounds__( QP_THREADS, 4 ) sw_qpair_kernel( QPairParams 
 }
 
 // grid == 0: report the resident CTAs per SM in *blocks_per_sm without launching.
-template <int R>
+template <int R, int MB>
 static cudaError_t launch_qp_one( const QPairParams & p, int grid, cudaStream_t st, int * blocks_per_sm ) {
     const size_t smem = (size_t) (QP_THREADS / 32) * QP_CODES * QP_G * R * sizeof(uint32_t);
-    cudaError_t e = cudaFuncSetAttribute( sw_qpair_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t e = cudaFuncSetAttribute( sw_qpair_kernel<R, MB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
             (int) smem );
     if( e != cudaSuccess )
         return e;
     if( grid == 0 )
-        return cudaOccupancyMaxActiveBlocksPerMultiprocessor( blocks_per_sm, sw_qpair_kernel<R>, QP_THREADS, smem );
-    sw_qpair_kernel<R><<<grid, QP_THREADS, smem, st>>>( p );
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor( blocks_per_sm, sw_qpair_kernel<R, MB>, QP_THREADS,
+                smem );
+    sw_qpair_kernel<R, MB><<<grid, QP_THREADS, smem, st>>>( p );
     return cudaGetLastError();
 }
 
-cudaError_t launch_sw_qpair( int R, const QPairParams & p, int grid, cudaStream_t st, int * blocks_per_sm ) {
+cudaError_t launch_sw_qpair( int R, int mb, const QPairParams & p, int grid, cudaStream_t st, int * blocks_per_sm ) {
+#define SSA_QP_CASE( RR ) \
+    case RR: \
+        return mb == 5 ? launch_qp_one<RR, 5>( p, grid, st, blocks_per_sm ) \
+                       : launch_qp_one<RR, 4>( p, grid, st, blocks_per_sm );
     switch( R ) {
-    case 16:
-        return launch_qp_one<16>( p, grid, st, blocks_per_sm );
-    case 20:
-        return launch_qp_one<20>( p, grid, st, blocks_per_sm );
-    case 24:
-        return launch_qp_one<24>( p, grid, st, blocks_per_sm );
-    case 28:
-        return launch_qp_one<28>( p, grid, st, blocks_per_sm );
+    SSA_QP_CASE( 16 )
+    SSA_QP_CASE( 20 )
+    SSA_QP_CASE( 24 )
+    SSA_QP_CASE( 28 )
     default:
         return cudaErrorInvalidValue;
     }
+#undef SSA_QP_CASE
 }
 
 // ---------------------------------------------------------------------------

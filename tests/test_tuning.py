@@ -1,0 +1,54 @@
+"""The entry-pass shape table (libssa_b200/csrc/tuning.cpp, written by
+libssa_b200/tune.py): the library reads the committed table next to its build,
+another file named by SSA_B200_TUNING, or its built-in costs, and reports
+which.  CPU only: reading the table touches no device."""
+import json
+import os
+import subprocess
+import sys
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+_REPORT = "import json, libssa_b200 as L; L.load(); print(json.dumps(L.tuning_report()))"
+
+
+def _report(env_value: str | None) -> dict:
+    env = dict(os.environ)
+    env.pop("SSA_B200_TUNING", None)
+    if env_value is not None:
+        env["SSA_B200_TUNING"] = env_value
+    out = subprocess.run([sys.executable, "-c", _REPORT], cwd=ROOT, env=env, capture_output=True, text=True,
+                         check=True).stdout
+    return json.loads(out.strip().splitlines()[-1])
+
+
+def test_builtin_table_on_request(built_library):
+    r = _report("builtin")
+    assert r["source"] == "built-in"
+    assert r["version"] == 0
+    assert r["last_call"] == []
+
+
+def test_table_file_is_read(built_library, tmp_path):
+    path = tmp_path / "t.tune"
+    path.write_text("# a table\nversion 7\ndevice Test Device 1\nqpair 1 20 5 12.5\nfast 4 8 24 3.0\n")
+    r = _report(str(path))
+    assert r["source"] == str(path)
+    assert r["version"] == 7
+    assert r["device"] == "Test Device 1"
+
+
+def test_committed_table_is_the_default(built_library):
+    committed = os.path.join(ROOT, "libssa_b200", "tuning", "b200.tune")
+    r = _report(None)
+    if os.path.exists(committed):
+        assert os.path.realpath(r["source"]) == os.path.realpath(committed)
+        with open(committed) as f:
+            lines = [ln.split() for ln in f if ln.strip() and not ln.startswith("#")]
+        version = [int(x[1]) for x in lines if x[0] == "version"]
+        assert version and r["version"] == version[0]
+        # every database bucket has a measured cost for every query-pair shape
+        qp = {(int(x[1]), int(x[2]), int(x[3])) for x in lines if x[0] == "qpair"}
+        assert qp == {(b, R, mb) for b in range(6) for R in (16, 20, 24, 28) for mb in (4, 5)}
+    else:
+        assert r["source"] == "built-in"
