@@ -105,6 +105,38 @@ int ssa_b200_int_peak( double * lane_ops_per_second, double * instructions_per_c
 int ssa_b200_simd_rate( int op, double * per_clock_per_sm );
 
 /*
+ * Database-sharded search, for one process per GPU.  No counterpart in the
+ * reference, whose threads split a search by database chunk
+ * (src/algo/manager.c:83-185, chunks from src/db_adapter.c:212-239) inside one
+ * process.  Every process loads the same database through the plugin; each
+ * scores its own contiguous range of records, and one process gathers the
+ * per-record results and replays them.
+ *
+ * ssa_b200_shard_scores: the entry pass and overflow cascade of every query
+ * against records [id_lo, id_hi) only.  For query q and record id the arrays
+ * (n_queries x (id_hi - id_lo), row-major, index q * (id_hi - id_lo) + id -
+ * id_lo) receive the pair's final score, and the number of 4-column blocks the
+ * entry-width lane and the 16-bit lane spent on it where they overflowed
+ * (-1 where the lane reported; empty records: 0, -1, -1).
+ *
+ * ssa_b200_replay_gathered: given those arrays for ALL records (n_queries x
+ * database size, gathered from every range in record order), replays the
+ * reference's lane schedule and top-hit heap per query and, for
+ * COMPUTE_ALIGNMENT, traces the hits back on this process's device.
+ * results[i] is exactly the list sw_align/nw_align returns for queries[i];
+ * with COMPUTE_SCORE it needs no device.
+ *
+ * Both take amino-acid queries, or nucleotide queries on the forward strand,
+ * with the current global settings, and return 0, or -1 (message on stderr)
+ * for other setups or bad arguments.
+ */
+int ssa_b200_shard_scores( int algorithm, p_query * queries, size_t n_queries, int bit_width, size_t id_lo,
+        size_t id_hi, int64_t * scores, int32_t * blocks_entry, int32_t * blocks_16 );
+int ssa_b200_replay_gathered( int algorithm, p_query * queries, size_t n_queries, size_t hitcount, int bit_width,
+        int align_type, const int64_t * scores, const int32_t * blocks_entry, const int32_t * blocks_16,
+        p_alignment_list * results );
+
+/*
  * Entry-pass shape table.  The entry kernels pick their tile shape (rows per
  * thread and resident CTAs per SM of the query-pair kernel; threads per
  * sequence and rows per thread of the single-query kernel) per query from

@@ -129,6 +129,12 @@ def load():
     lib.ssa_db_refresh.argtypes = []
     lib.ssa_b200_int_peak.argtypes = [ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
     lib.ssa_b200_simd_rate.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+    lib.ssa_b200_shard_scores.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p), ctypes.c_size_t,
+                                          ctypes.c_int, ctypes.c_size_t, ctypes.c_size_t, ctypes.c_void_p,
+                                          ctypes.c_void_p, ctypes.c_void_p]
+    lib.ssa_b200_replay_gathered.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p), ctypes.c_size_t,
+                                             ctypes.c_size_t, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                                             ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(P_LIST)]
     lib.ssa_b200_tuning_report.restype = ctypes.c_size_t
     lib.ssa_b200_tuning_report.argtypes = [ctypes.c_char_p, ctypes.c_size_t]
     lib.ssa_b200_int_peak.restype = ctypes.c_int
@@ -339,6 +345,47 @@ def simd_rates() -> dict[str, float]:
         if lib.ssa_b200_simd_rate(op, ctypes.byref(v)) != 0:
             raise RuntimeError(f"probe of {name} failed")
         out[name] = v.value
+    return out
+
+
+def shard_scores(algorithm: int, queries: list, bit_width: int, id_lo: int, id_hi: int):
+    """ssa_b200_shard_scores(): (scores int64, entry-width blocks int32,
+    16-bit blocks int32), each n_queries x (id_hi - id_lo); blocks are -1 where
+    the lane reported."""
+    import numpy as np
+    lib = load()
+    n = len(queries)
+    w = max(0, id_hi - id_lo)
+    sc = np.zeros((n, w), dtype=np.int64)
+    be = np.full((n, w), -1, dtype=np.int32)
+    b16 = np.full((n, w), -1, dtype=np.int32)
+    qarr = (ctypes.c_void_p * max(1, n))(*queries)
+    if lib.ssa_b200_shard_scores(algorithm, qarr, n, bit_width, id_lo, id_hi, sc.ctypes.data, be.ctypes.data,
+                                 b16.ctypes.data) != 0:
+        raise ValueError("ssa_b200_shard_scores refused the settings or range")
+    return sc, be, b16
+
+
+def replay_gathered(algorithm: int, queries: list, hitcount: int, bit_width: int, align_type: int, scores,
+                    blocks_entry, blocks_16) -> list[list[Hit]]:
+    """ssa_b200_replay_gathered(): hit lists from per-record results of the
+    whole database (n_queries x records arrays, as shard_scores returns them
+    per range, concatenated in record order)."""
+    import numpy as np
+    lib = load()
+    n = len(queries)
+    sc = np.ascontiguousarray(scores, dtype=np.int64)
+    be = np.ascontiguousarray(blocks_entry, dtype=np.int32)
+    b16 = np.ascontiguousarray(blocks_16, dtype=np.int32)
+    qarr = (ctypes.c_void_p * max(1, n))(*queries)
+    res = (P_LIST * max(1, n))()
+    if lib.ssa_b200_replay_gathered(algorithm, qarr, n, hitcount, bit_width, align_type, sc.ctypes.data,
+                                    be.ctypes.data, b16.ctypes.data, res) != 0:
+        raise ValueError("ssa_b200_replay_gathered refused the settings")
+    out = []
+    for i in range(n):
+        out.append(_read_list(res[i]))
+        lib.free_alignment(res[i])
     return out
 
 

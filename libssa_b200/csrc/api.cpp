@@ -948,6 +948,107 @@ void ssa_get_stats( ssa_stats_t * out ) {
     out->d2h_bytes = g_last_stats.d2h_bytes;
 }
 
+// ---- database-sharded searches ----------------------------------------------------
+// Shared checks: one query sequence per query (amino acids, or nucleotides on
+// the forward strand) and a database searched on one strand.
+static bool shard_query_codes( p_query * queries, size_t n, std::vector<QueryCodes> & qc, const char * who ) {
+    const Config & c = config();
+    if( c.symtype != AMINOACID && !(c.symtype == NUCLEOTIDE && c.strands == FORWARD_STRAND) ) {
+        print_error( "%s: database-sharded searches take amino-acid or forward-strand nucleotide queries", who );
+        return false;
+    }
+    for( size_t i = 0; i < n; i++ ) {
+        test_configuration( queries[i] );
+        if( queries[i]->symtype != c.symtype )
+            fatal( "Query was read with a different symbol type than the current one." );
+        if( queries[i]->len == 0 )
+            fatal( "Query sequence is empty." );
+        const QueryFrame & f = (*queries[i]->frames)[0];
+        qc.push_back( QueryCodes{ (const uint8_t *) f.seq.data(), (uint32_t) (f.seq.size() - 1) } );
+    }
+    return true;
+}
+
+int ssa_b200_shard_scores( int algorithm, p_query * queries, size_t n_queries, int bit_width, size_t id_lo,
+        size_t id_hi, int64_t * scores, int32_t * blocks_entry, int32_t * blocks_16 ) {
+    if( algorithm != SSA_SMITH_WATERMAN && algorithm != SSA_NEEDLEMAN_WUNSCH ) {
+        print_error( "ssa_b200_shard_scores: unknown algorithm %d", algorithm );
+        return -1;
+    }
+    if( id_lo > id_hi || id_hi > UINT32_MAX ) {
+        print_error( "ssa_b200_shard_scores: bad record range [%zu, %zu)", id_lo, id_hi );
+        return -1;
+    }
+    if( n_queries && id_hi > id_lo && (!queries || !scores || !blocks_entry || !blocks_16) ) {
+        print_error( "ssa_b200_shard_scores: null array" );
+        return -1;
+    }
+    std::vector<QueryCodes> qc;
+    if( !shard_query_codes( queries, n_queries, qc, "ssa_b200_shard_scores" ) )
+        return -1;
+    SearchRequest req = make_request( algorithm == SSA_SMITH_WATERMAN ? 0 : 1, 1, bit_width, COMPUTE_SCORE );
+    SearchStats st;
+    engine_shard_scores( req, qc, (uint32_t) id_lo, (uint32_t) id_hi, scores, blocks_entry, blocks_16, st );
+    g_last_stats = st;
+    return 0;
+}
+
+int ssa_b200_replay_gathered( int algorithm, p_query * queries, size_t n_queries, size_t hitcount, int bit_width,
+        int align_type, const int64_t * scores, const int32_t * blocks_entry, const int32_t * blocks_16,
+        p_alignment_list * results ) {
+    if( algorithm != SSA_SMITH_WATERMAN && algorithm != SSA_NEEDLEMAN_WUNSCH ) {
+        print_error( "ssa_b200_replay_gathered: unknown algorithm %d", algorithm );
+        return -1;
+    }
+    if( n_queries && (!queries || !results) ) {
+        print_error( "ssa_b200_replay_gathered: null array" );
+        return -1;
+    }
+    std::vector<QueryCodes> qc;
+    if( !shard_query_codes( queries, n_queries, qc, "ssa_b200_replay_gathered" ) )
+        return -1;
+    SearchRequest req = make_request( algorithm == SSA_SMITH_WATERMAN ? 0 : 1, hitcount, bit_width, align_type );
+    HostDb db;
+    lengths_db( db );
+    const size_t n = db.n_ids;
+    if( n && n_queries && (!scores || !blocks_entry || !blocks_16) ) {
+        print_error( "ssa_b200_replay_gathered: null array" );
+        return -1;
+    }
+    std::vector<uint32_t> rank;
+    if( bit_width != BIT_WIDTH_64 )
+        schedule_ranks( db, req.chunk_size, bit_width == BIT_WIDTH_8 ? req.lanes8 : req.lanes16, rank );
+    std::vector<std::vector<Hit>> hits( n_queries );
+    SearchStats st;
+    st.query_overflow.assign( n_queries, { 0, 0 } );
+    std::vector<int32_t> s32( n );
+    for( size_t q = 0; q < n_queries; q++ ) {
+        const int64_t * row = scores + q * n;
+        ReplayQuery rq;
+        for( size_t id = 0; id < n; id++ ) {
+            const int64_t v = row[id];
+            s32[id] = (v > INT32_MIN && v <= INT32_MAX) ? (int32_t) v : REPLAY_SCORE_IN_WIDE;
+            if( blocks_entry[q * n + id] >= 0 )
+                rq.ovf_entry.emplace_back( (uint32_t) id, blocks_entry[q * n + id] );
+            if( blocks_16[q * n + id] >= 0 )
+                rq.ovf16.emplace_back( (uint32_t) id, blocks_16[q * n + id] );
+        }
+        rq.score = s32.data();
+        rq.score64 = row;
+        ReplayCounts counts;
+        replay_query( db, req, rq, rank.empty() ? nullptr : rank.data(), hits[q], counts );
+        st.overflow8 += counts.overflow8;
+        st.overflow16 += counts.overflow16;
+        st.query_overflow[q] = { counts.overflow8, counts.overflow16 };
+    }
+    if( align_type == COMPUTE_ALIGNMENT )
+        engine_align_hits( req, qc, hits, st );
+    g_last_stats = st;
+    for( size_t i = 0; i < n_queries; i++ )
+        results[i] = make_list( hits[i], queries[i], align_type == COMPUTE_ALIGNMENT );
+    return 0;
+}
+
 size_t ssa_b200_tuning_report( char * buf, size_t n ) {
     const std::string r = tuning_report();
     if( buf && n ) {

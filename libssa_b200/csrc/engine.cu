@@ -375,6 +375,14 @@ public:
     // query i against database unit units[i] alone
     void align_pairs( const SearchRequest & req, const std::vector<QueryCodes> & queries,
             const std::vector<uint32_t> & units, std::vector<std::vector<Hit>> & out, SearchStats & stats );
+    // database-sharded search: entry pass and cascade of every query against
+    // the records [id_lo, id_hi) only; per (query, record) the final score and
+    // the blocks the entry-width and 16-bit lanes spent when they overflowed
+    void shard_scores( const SearchRequest & req, const std::vector<QueryCodes> & queries, uint32_t id_lo,
+            uint32_t id_hi, int64_t * scores, int32_t * blocks_entry, int32_t * blocks_16, SearchStats & stats );
+    // traceback of replayed hit lists (out[q] for query q)
+    void align_hits( const SearchRequest & req, const std::vector<QueryCodes> & queries,
+            std::vector<std::vector<Hit>> & out, SearchStats & stats );
     void set_traceback_budget( uint64_t bytes ) { tb_budget_ = bytes; }
     void set_db_budget( uint64_t bytes ) {
         db_budget_ = bytes;
@@ -2056,6 +2064,167 @@ void Engine::align_pairs( const SearchRequest & req, const std::vector<QueryCode
 // traceback) and freed for the next request.
 constexpr uint32_t SERVE_QSTRIDE = SERVE_MAX_QUERY + 16;
 
+// ---- database-sharded searches (one process per GPU, contiguous record
+// ranges; the per-record results are gathered to one replaying process) ----
+void Engine::shard_scores( const SearchRequest & req, const std::vector<QueryCodes> & queries, uint32_t id_lo,
+        uint32_t id_hi, int64_t * scores, int32_t * blocks_entry, int32_t * blocks_16, SearchStats & stats ) {
+    init_device();
+    const HostDb & db = database();
+    if( db.upi != 1 )
+        fatal( "Database-sharded searches support one database strand." );
+    if( streaming_ )
+        fatal( "Database-sharded searches need the database resident on the device." );
+    serving_ = false;
+    serve_layout_ = false;
+    last_shapes_.clear();
+    id_hi = std::min( id_hi, db.n_ids );
+    id_lo = std::min( id_lo, id_hi );
+    const uint64_t width = id_hi - id_lo;
+    const uint32_t nq_all = (uint32_t) queries.size();
+    for( uint64_t k = 0; k < (uint64_t) nq_all * width; k++ ) {
+        scores[k] = 0;
+        blocks_entry[k] = -1;
+        blocks_16[k] = -1;
+    }
+    if( width == 0 || queries.empty() )
+        return;
+    // this shard's non-empty records, longest first: the entry passes see it as
+    // their whole database
+    std::vector<uint32_t> shard;
+    for( uint32_t id : db.order_desc )
+        if( id >= id_lo && id < id_hi )
+            shard.push_back( id );
+    const uint64_t n_sh = shard.size();
+    {
+        uint32_t qmax = 0;
+        for( const QueryCodes & q : queries )
+            qmax = std::max( qmax, q.len );
+        wide_ = needs_int64( req, qmax, db.max_len );
+    }
+    d_matrix_.ensure( 1024 * sizeof(int64_t) );
+    CUDA_CHECK( cudaMemcpyAsync( d_matrix_.p, req.matrix, 1024 * sizeof(int64_t), cudaMemcpyHostToDevice, stream_ ) );
+    std::vector<uint32_t> full_order;
+    full_order.swap( db_.order_desc );
+    db_.order_desc = shard;
+    if( n_sh )
+        CUDA_CHECK( cudaMemcpyAsync( d_order_.p, shard.data(), n_sh * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                stream_ ) );
+    const uint64_t pair_budget = (uint64_t) 1 << (wide_ ? 27 : 28);
+    const uint32_t batch = (uint32_t) std::max<uint64_t>( 1, std::min<uint64_t>( nq_all,
+            pair_budget / std::max<uint64_t>( 1, db.n_ids ) ) );
+    for( uint32_t b0 = 0; b0 < nq_all && n_sh; b0 += batch ) {
+        const uint32_t nq = std::min( batch, nq_all - b0 );
+        upload_queries( queries.data() + b0, nq, true, stats );
+        for( uint32_t q = 0; q < nq; q++ ) {
+            uint64_t res = 0;
+            for( uint32_t id : shard )
+                res += db.len[id];
+            stats.cells += (uint64_t) h_qlen_[q] * res;
+        }
+        const size_t score_bytes = (size_t) nq * db.n_ids * sizeof(int32_t);
+        d_score_.ensure( std::max<size_t>( score_bytes, 4 ) );
+        if( wide_ )
+            d_score64_.ensure( std::max<size_t>( 2 * score_bytes, 8 ) );
+        const uint32_t cap = (uint32_t) std::min<uint64_t>( std::max<uint64_t>( (uint64_t) nq * n_sh, 1 ),
+                0xffffffffull );
+        d_list_a_.ensure( (size_t) cap * sizeof(PairTask) );
+        d_list_b_.ensure( (size_t) cap * sizeof(PairTask) );
+        d_counts_.ensure( 32 * sizeof(unsigned long long) );
+        CUDA_CHECK( cudaMemsetAsync( d_counts_.p, 0, 32 * sizeof(unsigned long long), stream_ ) );
+        unsigned * cnt = d_counts_.as<unsigned>();
+        const int entry = req.bit_width;
+        CUDA_CHECK( cudaEventRecord( ev_seg_[0], stream_ ) );
+        if( fast_eligible( req ) || nw_fast_eligible( req ) )
+            run_qpair_entry( req, nq, d_list_a_.as<PairTask>(), cnt + 0, cap, nullptr, 0, (uint32_t) n_sh );
+        else
+            run_pass( req.algo, entry, req, nq, nullptr, (uint64_t) nq * n_sh, true, d_list_a_.as<PairTask>(),
+                    cnt + 0, cap );
+        CUDA_CHECK( cudaEventRecord( ev_seg_[1], stream_ ) );
+        std::vector<PairTask> list_entry, list_16;
+        unsigned sa = 0, sb = 0;
+        if( entry != 64 ) {
+            CUDA_CHECK( cudaMemcpyAsync( &sa, cnt + 0, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_ ) );
+            CUDA_CHECK( cudaStreamSynchronize( stream_ ) );
+            sa = std::min( sa, cap );
+            if( sa ) {
+                const int w2 = (entry == 8) ? 16 : 64;
+                PairTask * nx = (w2 == 16) ? d_list_b_.as<PairTask>() : nullptr;
+                run_pass( req.algo, w2, req, nq, d_list_a_.as<PairTask>(), sa, false, nx, cnt + 1, cap );
+                if( w2 == 16 ) {
+                    CUDA_CHECK( cudaMemcpyAsync( &sb, cnt + 1, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_ ) );
+                    CUDA_CHECK( cudaStreamSynchronize( stream_ ) );
+                    sb = std::min( sb, cap );
+                    if( sb )
+                        run_pass( req.algo, 64, req, nq, d_list_b_.as<PairTask>(), sb, false, nullptr, cnt + 3, 0 );
+                }
+                list_entry.resize( sa );
+                CUDA_CHECK( cudaMemcpyAsync( list_entry.data(), d_list_a_.p, sa * sizeof(PairTask),
+                        cudaMemcpyDeviceToHost, stream_ ) );
+                if( sb ) {
+                    list_16.resize( sb );
+                    CUDA_CHECK( cudaMemcpyAsync( list_16.data(), d_list_b_.p, sb * sizeof(PairTask),
+                            cudaMemcpyDeviceToHost, stream_ ) );
+                }
+            }
+        }
+        int32_t * hs = (int32_t *) h_score_.ensure( std::max<size_t>( score_bytes, 4 ) );
+        CUDA_CHECK( cudaMemcpyAsync( hs, d_score_.p, score_bytes, cudaMemcpyDeviceToHost, stream_ ) );
+        int64_t * hs64 = nullptr;
+        if( wide_ ) {
+            hs64 = (int64_t *) h_score64_.ensure( 2 * score_bytes );
+            CUDA_CHECK( cudaMemcpyAsync( hs64, d_score64_.p, 2 * score_bytes, cudaMemcpyDeviceToHost, stream_ ) );
+        }
+        unsigned err = 0;
+        CUDA_CHECK( cudaMemcpyAsync( &err, cnt + 2, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_ ) );
+        CUDA_CHECK( cudaStreamSynchronize( stream_ ) );
+        if( err )
+            fatal( "Internal error in the GPU search (flags 0x%x).", err );
+        float ms = 0;
+        CUDA_CHECK( cudaEventElapsedTime( &ms, ev_seg_[0], ev_seg_[1] ) );
+        stats.entry_seconds += ms * 1e-3;
+        stats.d2h_bytes += score_bytes + (sa + sb) * sizeof(PairTask);
+        for( uint32_t q = 0; q < nq; q++ ) {
+            const uint64_t row = (uint64_t) (b0 + q) * width;
+            ReplayQuery rq;
+            rq.score = hs + (size_t) q * db.n_ids;
+            rq.score64 = hs64 ? hs64 + (size_t) q * db.n_ids : nullptr;
+            for( uint32_t id : shard )
+                scores[row + (id - id_lo)] = rq.score_of( id );
+        }
+        for( const PairTask & t : list_entry )
+            blocks_entry[(uint64_t) (b0 + t.qslot) * width + (t.id - id_lo)] = t.nb_prev;
+        for( const PairTask & t : list_16 )
+            blocks_16[(uint64_t) (b0 + t.qslot) * width + (t.id - id_lo)] = t.nb_prev;
+    }
+    db_.order_desc.swap( full_order );
+    if( !db_.order_desc.empty() )
+        CUDA_CHECK( cudaMemcpyAsync( d_order_.p, db_.order_desc.data(), db_.order_desc.size() * sizeof(uint32_t),
+                cudaMemcpyHostToDevice, stream_ ) );
+    CUDA_CHECK( cudaStreamSynchronize( stream_ ) );
+    stats.kernel_launches = launches_.load();
+}
+
+void Engine::align_hits( const SearchRequest & req, const std::vector<QueryCodes> & queries,
+        std::vector<std::vector<Hit>> & out, SearchStats & stats ) {
+    init_device();
+    database();
+    serving_ = false;
+    serve_layout_ = false;
+    d_matrix_.ensure( 1024 * sizeof(int64_t) );
+    CUDA_CHECK( cudaMemcpyAsync( d_matrix_.p, req.matrix, 1024 * sizeof(int64_t), cudaMemcpyHostToDevice, stream_ ) );
+    const uint32_t nq = (uint32_t) queries.size();
+    const uint32_t batch = 65535;
+    for( uint32_t b0 = 0; b0 < nq; b0 += batch ) {
+        const uint32_t n = std::min( batch, nq - b0 );
+        upload_queries( queries.data() + b0, n, false, stats );
+        std::vector<std::pair<uint32_t, uint32_t>> lists;
+        for( uint32_t q = 0; q < n; q++ )
+            lists.emplace_back( b0 + q, q );
+        traceback( req, out, lists, stats );
+    }
+    CUDA_CHECK( cudaStreamSynchronize( stream_ ) );
+}
+
 void Engine::serve_restore( const SearchRequest & req ) {
     const uint32_t S = serve_slots_;
     d_matrix_.ensure( 1024 * sizeof(int64_t) );
@@ -2350,6 +2519,47 @@ void engine_serve_finish( const SearchRequest & req, const std::vector<uint32_t>
         std::vector<ReplayQuery> & rq, std::vector<std::vector<Hit>> & out, SearchStats & stats ) {
     std::lock_guard<std::mutex> lock( g_engine_mutex );
     Engine::get().serve_finish( req, done, rq, out, stats );
+}
+
+void engine_shard_scores( const SearchRequest & req, const std::vector<QueryCodes> & queries, uint32_t id_lo,
+        uint32_t id_hi, int64_t * scores, int32_t * blocks_entry, int32_t * blocks_16, SearchStats & stats ) {
+    std::lock_guard<std::mutex> lock( g_engine_mutex );
+    Engine::get().shard_scores( req, queries, id_lo, id_hi, scores, blocks_entry, blocks_16, stats );
+}
+
+void engine_align_hits( const SearchRequest & req, const std::vector<QueryCodes> & queries,
+        std::vector<std::vector<Hit>> & out, SearchStats & stats ) {
+    std::lock_guard<std::mutex> lock( g_engine_mutex );
+    Engine::get().align_hits( req, queries, out, stats );
+}
+
+// Host-only: the database's record lengths through the plugin (no device),
+// as the schedule replay needs them.
+void lengths_db( HostDb & db ) {
+    db = HostDb();
+    const size_t n = ssa_db_get_sequence_count();
+    if( n > UINT32_MAX )
+        fatal( "Database has %zu sequences; at most %u are supported.", n, UINT32_MAX );
+    db.n_ids = db.n_records = (uint32_t) n;
+    db.upi = 1;
+    db.len.assign( n, 0 );
+    for( size_t id = 0; id < n; id++ ) {
+        p_seqinfo info = ssa_db_get_sequence( id );
+        if( !info )
+            fatal( "Could not get sequence from DB: %zu", id );
+        db.len[id] = (uint32_t) info->seqlen;
+        db.max_len = std::max( db.max_len, db.len[id] );
+        db.residues += info->seqlen;
+    }
+    db.nonempty_before.assign( n + 1, 0 );
+    for( uint32_t id = 0; id < db.n_ids; id++ ) {
+        db.nonempty_before[id + 1] = db.nonempty_before[id] + (db.len[id] ? 1 : 0);
+        if( db.len[id] )
+            db.order_desc.push_back( id );
+    }
+    std::stable_sort( db.order_desc.begin(), db.order_desc.end(),
+            [&]( uint32_t a, uint32_t b ) { return db.len[a] > db.len[b]; } );
+    db.mean_len = db.order_desc.empty() ? 0.0 : (double) db.residues / (double) db.order_desc.size();
 }
 
 std::string tuning_report() {

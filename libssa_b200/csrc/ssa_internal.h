@@ -143,6 +143,19 @@ void engine_invalidate_database();
 void engine_shutdown();
 uint64_t engine_kernel_launches();
 
+// ---- database-sharded searches ------------------------------------------------
+// Entry pass and cascade of every query against database records [id_lo,
+// id_hi) only: scores[q * (id_hi - id_lo) + id - id_lo] = the pair's final
+// score, blocks_entry / blocks_16 = the blocks the entry-width / 16-bit lane
+// spent where it overflowed, else -1 (empty records: 0, -1, -1).
+void engine_shard_scores( const SearchRequest & req, const std::vector<QueryCodes> & queries, uint32_t id_lo,
+        uint32_t id_hi, int64_t * scores, int32_t * blocks_entry, int32_t * blocks_16, SearchStats & stats );
+// Traceback of replayed hit lists (out[q] belongs to queries[q]).
+void engine_align_hits( const SearchRequest & req, const std::vector<QueryCodes> & queries,
+        std::vector<std::vector<Hit>> & out, SearchStats & stats );
+// The record lengths of the plugin's database (host only, no device).
+void lengths_db( HostDb & db );
+
 // ---- measured entry-pass shape costs (tuning.cpp, libssa_b200/tune.py) ---------
 constexpr int TUNE_BUCKETS = 6;   // database mean length <250 / <1000 / longer, x fewer / more than 50,000 sequences
 
