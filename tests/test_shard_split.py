@@ -199,3 +199,19 @@ def test_device_shards_replayed_equal_plain_search(built_library, seed):
             L.free_sequence(q)
     key = lambda lst: [(h.id, h.score, h.cigar, h.q_start, h.q_end, h.d_start, h.d_end) for h in lst]  # noqa: E731
     assert [key(x) for x in got] == [key(x) for x in want]
+
+
+def test_bench_record_ranges_cover_the_database_in_chunks():
+    """The benchmark's --split db layout: contiguous ranges, together the whole
+    database, cut at multiples of 1,000 records, about equal residues."""
+    sys.path.insert(0, ROOT)
+    import bench
+    rng = np.random.default_rng(3)
+    lens = W.gamma_lengths(rng, 23_456, 350.0, 20, 35_000)
+    for parts in (1, 2, 3, 8):
+        b = bench.record_ranges(lens, parts)
+        assert b[0] == 0 and b[-1] == len(lens) and len(b) == parts + 1
+        assert all(b[i] <= b[i + 1] for i in range(parts))
+        assert all(x % 1000 == 0 for x in b[1:-1])
+        res = [int(lens[b[i]:b[i + 1]].sum()) for i in range(parts)]
+        assert max(res) - min(res) <= 2 * 1000 * 35_000 / 10 + lens.sum() * 0.1
