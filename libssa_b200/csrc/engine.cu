@@ -917,16 +917,37 @@ void Engine::run_fast_entry( const SearchRequest & req, uint32_t nq, PairTask * 
 // database column of a query pair, for each rows-per-thread R and resident
 // CTAs per SM (4 or 5); the smallest passes x cost wins.  pinned_r / pinned_mb
 // (SSA_B200_QP_R, SSA_B200_QP_MB) force a shape, as the tuner does.
-static int qpair_mb( int bucket, int R, int pinned_mb ) {
-    if( pinned_mb == 4 || pinned_mb == 5 )
-        return pinned_mb;
-    const double * c = tuning().qpair[bucket][R / 4 - 4];
-    if( c[0] > 0 && c[1] > 0 )
-        return c[1] < c[0] ? 5 : 4;
-    return c[1] > 0 ? 5 : 4;
+struct QpVariant {
+    int mb;         // resident CTAs per SM
+    int cols;       // columns per step
+    double cost;    // measured cost, 0 = none
+};
+
+// The cheapest measured variant of the query-pair kernel for rows-per-thread
+// R (pinned_mb / pinned_c force one).
+static QpVariant qpair_variant( int bucket, int R, int pinned_mb, int pinned_c ) {
+    QpVariant best{ 4, 2, 0 };
+    for( int mi = 0; mi < 2; mi++ )
+        for( int ci = 0; ci < 2; ci++ ) {
+            const int mb = 4 + mi, cols = 2 + 2 * ci;
+            if( (pinned_mb == 4 || pinned_mb == 5) && mb != pinned_mb )
+                continue;
+            if( (pinned_c == 2 || pinned_c == 4) && cols != pinned_c )
+                continue;
+            const double c = tuning().qpair[bucket][R / 4 - 4][mi][ci];
+            if( c > 0 && (best.cost <= 0 || c < best.cost) )
+                best = QpVariant{ mb, cols, c };
+        }
+    if( best.cost <= 0 ) {
+        if( pinned_mb == 4 || pinned_mb == 5 )
+            best.mb = pinned_mb;
+        if( pinned_c == 2 || pinned_c == 4 )
+            best.cols = pinned_c;
+    }
+    return best;
 }
 
-static int choose_qpair_rows( uint32_t Q, uint32_t * passes, int pinned, int bucket, int pinned_mb ) {
+static int choose_qpair_rows( uint32_t Q, uint32_t * passes, int pinned, int bucket, int pinned_mb, int pinned_c ) {
     static const int rs[4] = { 16, 20, 24, 28 };
     int best_r = 0;
     double best_cost = 1e300;
@@ -938,7 +959,7 @@ static int choose_qpair_rows( uint32_t Q, uint32_t * passes, int pinned, int buc
         const uint32_t P = std::max<uint32_t>( 1, (Q + per - 1) / per );
         if( (uint64_t) P * per > FAST_MAX_ROWS )
             continue;
-        const double unit = tuning().qpair[bucket][i][qpair_mb( bucket, R, pinned_mb ) - 4];
+        const double unit = qpair_variant( bucket, R, pinned_mb, pinned_c ).cost;
         if( unit <= 0 && !pinned )
             continue;                   // not measured
         const double c = (double) P * (unit > 0 ? unit : 1.0);
@@ -949,7 +970,7 @@ static int choose_qpair_rows( uint32_t Q, uint32_t * passes, int pinned, int buc
         }
     }
     if( best_r == 0 && pinned )         // the pinned R does not fit this query
-        return choose_qpair_rows( Q, passes, 0, bucket, pinned_mb );
+        return choose_qpair_rows( Q, passes, 0, bucket, pinned_mb, pinned_c );
     if( best_r == 0 ) {                 // an empty table: 20 rows per thread
         best_r = 20;
         *passes = std::max<uint32_t>( 1, (Q + QP_G * 20 - 1) / (QP_G * 20) );
@@ -983,6 +1004,8 @@ void Engine::run_qpair_entry( const SearchRequest & req, uint32_t nq, PairTask *
     const int pinned_r = pin ? atoi( pin ) : 0;
     const char * pin_mb = getenv( "SSA_B200_QP_MB" );
     const int pinned_mb = pin_mb ? atoi( pin_mb ) : 0;
+    const char * pin_c = getenv( "SSA_B200_QP_C" );      // 2|4 columns per step
+    const int pinned_c = pin_c ? atoi( pin_c ) : 0;
     // the database bucket of the shape table: these sequences' mean length and count
     uint64_t seq_res = 0;
     for( uint32_t i = lo; i < hi; i++ )
@@ -998,7 +1021,7 @@ void Engine::run_qpair_entry( const SearchRequest & req, uint32_t nq, PairTask *
         if( 2 * i + 1 < fit.size() )
             qp_slots[2 * i + 1] = fit[2 * i + 1];
         uint32_t P = 1;
-        const int R = choose_qpair_rows( h_qlen_[fit[2 * i]], &P, pinned_r, bucket, pinned_mb );
+        const int R = choose_qpair_rows( h_qlen_[fit[2 * i]], &P, pinned_r, bucket, pinned_mb, pinned_c );
         qp_rows[i] = P * (uint32_t) (QP_G * R);
         by_r[R / 4 - 4].push_back( i );
     }
@@ -1098,15 +1121,22 @@ void Engine::run_qpair_entry( const SearchRequest & req, uint32_t nq, PairTask *
         if( cls.empty() )
             continue;
         const int R = 4 * (ri + 4);
-        const int mb = nw ? 4 : qpair_mb( bucket, R, pinned_mb );
+        const QpVariant var = nw ? QpVariant{ 4, 2, 0 } : qpair_variant( bucket, R, pinned_mb, pinned_c );
+        const int mb = var.mb;
+        auto launch = [&]( const QPairParams & pp, int grid, int * per ) {
+            if( nw )
+                return launch_nw_qpair( R, pp, grid, class_stream_[ri], per );
+            return var.cols == 4 ? launch_sw_qpair4( R, mb, pp, grid, class_stream_[ri], per )
+                                 : launch_sw_qpair( R, mb, pp, grid, class_stream_[ri], per );
+        };
         bool multi = false;
         for( uint32_t i : cls )
             multi |= qp_rows[i] > (uint32_t) (QP_G * R);
-        last_shapes_.push_back( { nw ? "nw_qpair" : "sw_qpair", R, mb, (uint32_t) cls.size(), bucket } );
+        last_shapes_.push_back( { nw ? "nw_qpair" : (var.cols == 4 ? "sw_qpair4" : "sw_qpair"), R, mb,
+                (uint32_t) cls.size(), bucket } );
         QPairParams p{};
         int per_sm = 0;
-        CUDA_CHECK( nw ? launch_nw_qpair( R, p, 0, class_stream_[ri], &per_sm )
-                       : launch_sw_qpair( R, mb, p, 0, class_stream_[ri], &per_sm ) );
+        CUDA_CHECK( launch( p, 0, &per_sm ) );
         const int grid = sms_ * std::max( 1, per_sm );
         CUDA_CHECK( cudaStreamWaitEvent( class_stream_[ri], ev_ready_, 0 ) );
         unsigned long long * unit_counter = d_counts_.as<unsigned long long>() + 8 + ri;   // bytes 64..95
@@ -1145,8 +1175,7 @@ void Engine::run_qpair_entry( const SearchRequest & req, uint32_t nq, PairTask *
         p.redo_cap = cap;
         if( timing )
             CUDA_CHECK( cudaEventRecord( ev_cls_t_[2 * ri], class_stream_[ri] ) );
-        CUDA_CHECK( nw ? launch_nw_qpair( R, p, grid, class_stream_[ri], nullptr )
-                       : launch_sw_qpair( R, mb, p, grid, class_stream_[ri], nullptr ) );
+        CUDA_CHECK( launch( p, grid, nullptr ) );
         launches_++;
         if( timing )
             CUDA_CHECK( cudaEventRecord( ev_cls_t_[2 * ri + 1], class_stream_[ri] ) );

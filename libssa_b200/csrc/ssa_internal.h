@@ -164,8 +164,9 @@ struct TuningTable {
     std::string device;
     std::string source = "built-in";
     // query-pair kernel: cost per (query pair, pass, database column) by
-    // [bucket][R / 4 - 4][resident CTAs per SM - 4]; 0 = not measured
-    double qpair[TUNE_BUCKETS][4][2] = {};
+    // [bucket][R / 4 - 4][resident CTAs per SM - 4][columns per step 2, 4];
+    // 0 = not measured
+    double qpair[TUNE_BUCKETS][4][2][2] = {};
     // single-query kernel: cost per (pass, database column) by
     // [bucket][G = 8, 16, 32][R / 8 - 1]; 0 = not measured
     double fast[TUNE_BUCKETS][3][4] = {};

@@ -261,6 +261,296 @@ __global__ void __launch_bounds__( QP_THREADS, MB ) sw_qpair_kernel( QPairParams
     }
 }
 
+// ---------------------------------------------------------------------------
+// The same pass, one 4-column block per step: a thread interleaves four
+// columns (cell (r, c + j) in row iteration r + j, j = 0..3), four independent
+// dependency chains instead of two.  The semantics, the group layout, the
+// profile slices and the scheduling are those of sw_qpair_kernel; a step reads
+// one 32-bit word of residues (the block) and crosses the pass boundary as two
+// int4 per block (H and F of the bottom row, four columns).  The running
+// maximum's first crossing of 255 is recorded per block directly.
+//
+// H[r] holds column c - 1 (the previous step's last column) until chain 3
+// overwrites it with column c + 3 (iteration r + 3); chain j reads the
+// diagonal H(r - 1, c + j - 1) from chain j - 1's value two iterations back,
+// and E[r] passes from chain j - 1 (iteration r + j - 1) to chain j.
+// ---------------------------------------------------------------------------
+template <int R, int MB>
+__global__ void __launch_bounds__( QP_THREADS, MB ) sw_qpair4_kernel( QPairParams p ) {
+    constexpr int G = QP_G;
+    constexpr int C = 4;
+    constexpr uint32_t GR = (uint32_t) (G * R);
+    extern __shared__ __align__( 16 ) uint32_t qsm[];
+    const int lane = threadIdx.x & 31;
+    const uint32_t warp_in_cta = threadIdx.x >> 5;
+    const uint32_t warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    uint32_t * slice = qsm + warp_in_cta * (QP_CODES * GR);
+    const int k = lane & (G - 1);
+    const int g = lane / G;
+    const uint32_t GOE32 = (uint32_t) ((int32_t) p.gap_oe * 65536 + (int32_t) p.gap_oe);
+    const uint32_t GE2 = ((uint32_t) (uint16_t) (int16_t) p.gap_e << 16) | (uint16_t) (int16_t) p.gap_e;
+    int4 * scratch = p.scratch + ((uint64_t) warp_global * QP_GPW + (uint32_t) g) * p.scratch_cols;
+    uint64_t loaded_key = ~0ull;
+
+    for( ;; ) {
+        unsigned long long u = 0;
+        if( lane == 0 )
+            u = atomicAdd( p.unit_counter, 1ull );
+        u = __shfl_sync( 0xffffffffu, u, 0 );
+        if( u >= p.n_units )
+            break;
+        const uint32_t qp = p.unit_pairs[u / p.n_chunks];
+        const uint32_t chunk = (uint32_t) (u % p.n_chunks);
+        const uint32_t seq_begin = p.chunk_bounds[chunk], seq_end = p.chunk_bounds[chunk + 1];
+        const uint32_t rows = p.qp_rows[qp];
+        const uint32_t passes = rows / GR;
+        const uint32_t * prof = p.prof + p.prof_off[qp];
+        const uint32_t slot_a = p.qp_slots[2 * qp], slot_b = p.qp_slots[2 * qp + 1];
+
+        for( uint32_t b0 = seq_begin; b0 < seq_end; b0 += (uint32_t) QP_GPW ) {
+            const uint32_t idx = b0 + (uint32_t) g;
+            const bool valid = idx < seq_end;
+            const uint32_t id = valid ? p.order[idx] : 0u;
+            const uint32_t L = valid ? p.db.lens[id] : 0u;
+            const uint32_t nb = (L + 3u) >> 2;                    // 4-column blocks
+            const uint32_t max_nb = __reduce_max_sync( 0xffffffffu, nb );
+            const uint8_t * res = p.db.codes + (valid ? p.db.offsets[id] : 0ull);
+
+            uint32_t best = QP_BIAS2;
+            int cross_a = INT_MAX, cross_b = INT_MAX;
+
+            for( uint32_t pass = 0; pass < passes; pass++ ) {
+                const bool last_pass = (pass + 1 == passes);
+                const uint64_t key = ((uint64_t) qp << 24) | pass;
+                if( key != loaded_key ) {
+                    __syncwarp();
+                    constexpr uint32_t per_code = GR / 4u;
+                    const uint4 * src = reinterpret_cast<const uint4 *>( prof + (size_t) pass * GR );
+                    uint4 * dst = reinterpret_cast<uint4 *>( slice );
+                    for( uint32_t i = (uint32_t) lane; i < QP_CODES * per_code; i += 32u ) {
+                        const uint32_t code = i / per_code, w = i % per_code;
+                        dst[i] = src[(size_t) code * (rows / 4u) + w];
+                    }
+                    loaded_key = key;
+                    __syncwarp();
+                }
+                uint32_t H[R], E[R];
+#pragma unroll
+                for( int r = 0; r < R; r++ ) {
+                    H[r] = QP_BIAS2;
+                    E[r] = QP_BIAS2;
+                }
+                uint32_t diag = QP_BIAS2, smax = QP_BIAS2, seen = 0;
+                uint32_t out_h[C], out_f[C];
+#pragma unroll
+                for( int j = 0; j < C; j++ ) {
+                    out_h[j] = QP_BIAS2;
+                    out_f[j] = QP_BIAS2;
+                }
+                // residues of blocks b .. b + 3, one block fetched ahead every
+                // step; past the last block the reads stay inside the padded
+                // record or the next one (never used)
+                const uint32_t fetch_limit = nb + 3u;
+                auto fetch = [&]( int32_t b ) -> uint32_t {
+                    const uint32_t c = min( (uint32_t) max( b, 0 ), fetch_limit );
+                    return *reinterpret_cast<const uint32_t *>( res + 4u * c );
+                };
+                uint32_t q0 = fetch( -k ), q1 = fetch( 1 - k ), q2 = fetch( 2 - k ), q3 = fetch( 3 - k );
+                // thread 0: the previous pass's bottom row, one block ahead
+                const bool reads_boundary = (k == 0) && pass > 0;
+                int4 bq0 = make_int4( 0, 0, 0, 0 ), bq1 = bq0;
+                if( reads_boundary && nb > 0 ) {
+                    bq0 = scratch[0];
+                    bq1 = scratch[1];
+                }
+                const uint32_t steps = max_nb + (uint32_t) G - 1u;
+                for( uint32_t s = 0; s < steps; s++ ) {
+                    uint32_t up_h[C], up_f[C];
+#pragma unroll
+                    for( int j = 0; j < C; j++ ) {
+                        up_h[j] = __shfl_up_sync( 0xffffffffu, out_h[j], 1, G );
+                        up_f[j] = __shfl_up_sync( 0xffffffffu, out_f[j], 1, G );
+                    }
+                    const int32_t b = (int32_t) s - k;
+                    const uint32_t w = q0;
+                    q0 = q1;
+                    q1 = q2;
+                    q2 = q3;
+                    q3 = fetch( b + 4 );
+                    const int4 bnd0 = bq0, bnd1 = bq1;
+                    if( reads_boundary ) {
+                        const uint32_t nxt = (uint32_t) b + 1u;
+                        if( nxt < nb && 2u * nxt + 1u < p.scratch_cols ) {
+                            bq0 = scratch[2u * nxt];
+                            bq1 = scratch[2u * nxt + 1u];
+                        }
+                    }
+                    if( b < 0 || (uint32_t) b >= nb )
+                        continue;
+                    if( k == 0 ) {
+                        if( pass ) {
+                            up_h[0] = (uint32_t) bnd0.x;
+                            up_f[0] = (uint32_t) bnd0.y;
+                            up_h[1] = (uint32_t) bnd0.z;
+                            up_f[1] = (uint32_t) bnd0.w;
+                            up_h[2] = (uint32_t) bnd1.x;
+                            up_f[2] = (uint32_t) bnd1.y;
+                            up_h[3] = (uint32_t) bnd1.z;
+                            up_f[3] = (uint32_t) bnd1.w;
+                        }
+                        else {
+#pragma unroll
+                            for( int j = 0; j < C; j++ ) {
+                                up_h[j] = QP_BIAS2;
+                                up_f[j] = QP_BIAS2;
+                            }
+                        }
+                    }
+                    const uint32_t * pc[C];
+#pragma unroll
+                    for( int j = 0; j < C; j++ )
+                        pc[j] = slice + ((w >> (8 * j)) & 0xffu) * GR + (uint32_t) (k * R);
+                    uint4 x[C];
+                    uint32_t f[C];
+                    // hv[j][r]: H of chain j (column c + j) at row r; only the
+                    // last two rows of chains 0..2 stay live
+                    uint32_t hv[C][R];
+#pragma unroll
+                    for( int j = 0; j < C; j++ )
+                        f[j] = up_f[j];
+#pragma unroll
+                    for( int it = 0; it < R + C - 1; it++ ) {
+                        uint32_t hnew[C];
+#pragma unroll
+                        for( int j = 0; j < C; j++ ) {
+                            const int r = it - j;
+                            if( r < 0 || r >= R )
+                                continue;
+                            if( (r & 3) == 0 )
+                                x[j] = *reinterpret_cast<const uint4 *>( pc[j] + r );
+                            const uint32_t v = (r & 3) == 0 ? x[j].x : (r & 3) == 1 ? x[j].y
+                                    : (r & 3) == 2 ? x[j].z : x[j].w;
+                            uint32_t hd;
+                            if( r == 0 )
+                                hd = (j == 0) ? diag : up_h[j - 1];
+                            else
+                                hd = (j == 0) ? H[r - 1] : hv[j - 1][r - 1];
+                            const uint32_t t = __vimax3_s16x2( E[r], f[j], QP_BIAS2 );
+                            const uint32_t h = __viaddmax_s16x2( hd, v, t );
+                            const uint32_t hg = h + GOE32;
+                            f[j] = __viaddmax_s16x2( f[j], GE2, hg );
+                            E[r] = __viaddmax_s16x2( E[r], GE2, hg );
+                            hv[j][r] = h;
+                            hnew[j] = h;
+                        }
+                        // the new cells of this iteration into the running maximum
+                        const int j0 = it - (R - 1) > 0 ? it - (R - 1) : 0;
+                        const int j1 = it < C - 1 ? it : C - 1;
+#pragma unroll
+                        for( int j = j0; j <= j1; j += 2 ) {
+                            if( j + 1 <= j1 )
+                                smax = __vimax3_s16x2( smax, hnew[j], hnew[j + 1] );
+                            else
+                                smax = __vmaxs2( smax, hnew[j] );
+                        }
+                        // chain 3 leaves column c + 3 in H
+                        if( it - (C - 1) >= 0 && it - (C - 1) < R )
+                            H[it - (C - 1)] = hnew[C - 1];
+                    }
+                    diag = up_h[C - 1];
+#pragma unroll
+                    for( int j = 0; j < C; j++ ) {
+                        out_h[j] = hv[j][R - 1];
+                        out_f[j] = f[j];
+                    }
+                    // first block at which this thread's maximum reached 255
+                    const uint32_t ge = (smax + QP_CROSS_ADD) & 0x80008000u;
+                    if( ge != seen ) {
+                        if( (ge & 0x8000u) && !(seen & 0x8000u) )
+                            cross_a = min( cross_a, b );
+                        if( (ge & 0x80000000u) && !(seen & 0x80000000u) )
+                            cross_b = min( cross_b, b );
+                        seen = ge;
+                    }
+                    if( k == G - 1 && !last_pass ) {
+                        if( 2u * (uint32_t) b + 1u < p.scratch_cols ) {
+                            scratch[2u * b] = make_int4( (int) out_h[0], (int) out_f[0], (int) out_h[1],
+                                    (int) out_f[1] );
+                            scratch[2u * b + 1u] = make_int4( (int) out_h[2], (int) out_f[2], (int) out_h[3],
+                                    (int) out_f[3] );
+                        }
+                        else {
+                            atomicOr( p.sink.error_flags, ERR_SCRATCH_OVERFLOW );
+                        }
+                    }
+                }
+                best = __vmaxs2( best, smax );
+                __syncwarp();
+            }
+#pragma unroll
+            for( int o = 1; o < G; o <<= 1 ) {
+                best = __vmaxs2( best, __shfl_xor_sync( 0xffffffffu, best, o, G ) );
+                cross_a = min( cross_a, __shfl_xor_sync( 0xffffffffu, cross_a, o, G ) );
+                cross_b = min( cross_b, __shfl_xor_sync( 0xffffffffu, cross_b, o, G ) );
+            }
+            if( valid && k == 0 ) {
+                const uint32_t slots[2] = { slot_a, slot_b };
+                const int cross[2] = { cross_a, cross_b };
+                const uint32_t sv[2] = { best & 0xffffu, best >> 16 };
+#pragma unroll
+                for( int h = 0; h < 2; h++ ) {
+                    if( slots[h] == 0xffffffffu )
+                        continue;
+                    int32_t * dst = p.sink.score + (uint64_t) slots[h] * p.sink.score_stride + id;
+                    if( cross[h] == INT_MAX ) {
+                        *dst = (int32_t) (sv[h] - QP_BIAS);
+                    }
+                    else {
+                        *dst = 255;
+                        unsigned q = atomicAdd( p.sink.next_count, 1u );
+                        if( q < p.sink.next_cap )
+                            p.sink.next[q] = PairTask{ slots[h], id, cross[h] + 1, 0 };
+                        else
+                            atomicOr( p.sink.error_flags, ERR_REQUEUE_OVERFLOW );
+                    }
+                }
+            }
+        }
+    }
+}
+
+// grid == 0: report the resident CTAs per SM in *blocks_per_sm without launching.
+template <int R, int MB>
+static cudaError_t launch_qp4_one( const QPairParams & p, int grid, cudaStream_t st, int * blocks_per_sm ) {
+    const size_t smem = (size_t) (QP_THREADS / 32) * QP_CODES * QP_G * R * sizeof(uint32_t);
+    cudaError_t e = cudaFuncSetAttribute( sw_qpair4_kernel<R, MB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            (int) smem );
+    if( e != cudaSuccess )
+        return e;
+    if( grid == 0 )
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor( blocks_per_sm, sw_qpair4_kernel<R, MB>, QP_THREADS,
+                smem );
+    sw_qpair4_kernel<R, MB><<<grid, QP_THREADS, smem, st>>>( p );
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sw_qpair4( int R, int mb, const QPairParams & p, int grid, cudaStream_t st,
+        int * blocks_per_sm ) {
+#define SSA_QP4_CASE( RR ) \
+    case RR: \
+        return mb == 5 ? launch_qp4_one<RR, 5>( p, grid, st, blocks_per_sm ) \
+                       : launch_qp4_one<RR, 4>( p, grid, st, blocks_per_sm );
+    switch( R ) {
+    SSA_QP4_CASE( 16 )
+    SSA_QP4_CASE( 20 )
+    SSA_QP4_CASE( 24 )
+    SSA_QP4_CASE( 28 )
+    default:
+        return cudaErrorInvalidValue;
+    }
+#undef SSA_QP4_CASE
+}
+
 // grid == 0: report the resident CTAs per SM in *blocks_per_sm without launching.
 template <int R, int MB>
 static cudaError_t launch_qp_one( const QPairParams & p, int grid, cudaStream_t st, int * blocks_per_sm ) {

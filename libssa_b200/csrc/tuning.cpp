@@ -17,6 +17,7 @@
 //   version <n>
 //   device <name ...>
 //   qpair <bucket> <R> <MB> <ps per query pair, pass and database column>
+//   qpair4 <bucket> <R> <MB> <ps ...>       (the kernel with 4 columns per step)
 //   fast <bucket> <G> <R> <ps per pass and database column>
 // Buckets: db_bucket() below.  Missing entries fall back to the built-in
 // costs (measured the same way on a B200 before the tuner existed).
@@ -42,7 +43,7 @@ void builtin( TuningTable & t ) {
     static const double cost[4] = { 4.28, 3.77, 4.56, 5.41 };
     for( int b = 0; b < TUNE_BUCKETS; b++ )
         for( int ri = 0; ri < 4; ri++ )
-            t.qpair[b][ri][0] = cost[ri];
+            t.qpair[b][ri][0][0] = cost[ri];
 }
 
 std::string default_path() {
@@ -90,19 +91,18 @@ void load( TuningTable & t ) {
             while( !t.device.empty() && (t.device.back() == '\n' || t.device.back() == '\r' || t.device.back() == ' ') )
                 t.device.pop_back();
         }
-        else if( !strcmp( key, "qpair" ) ) {
+        else if( !strcmp( key, "qpair" ) || !strcmp( key, "qpair4" ) ) {
+            const int ci = strcmp( key, "qpair4" ) ? 0 : 1;
             int b, R, mb;
             double ps;
             if( sscanf( line, "%*s %d %d %d %lf", &b, &R, &mb, &ps ) == 4 && b >= 0 && b < TUNE_BUCKETS &&
                     R >= 16 && R <= 28 && R % 4 == 0 && (mb == 4 || mb == 5) && ps > 0 ) {
                 if( !any ) {
                     // a measured table replaces the built-in costs entirely
-                    for( int bb = 0; bb < TUNE_BUCKETS; bb++ )
-                        for( int ri = 0; ri < 4; ri++ )
-                            t.qpair[bb][ri][0] = t.qpair[bb][ri][1] = 0;
+                    memset( t.qpair, 0, sizeof t.qpair );
                     any = true;
                 }
-                t.qpair[b][R / 4 - 4][mb - 4] = ps;
+                t.qpair[b][R / 4 - 4][mb - 4][ci] = ps;
             }
         }
         else if( !strcmp( key, "fast" ) ) {

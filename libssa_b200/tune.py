@@ -8,7 +8,9 @@ lanes per vector (src/algo/8/search_8_util.h:25-27, src/algo/8/search_8.c:
 script times every candidate, per database bucket, on seeded synthetic data:
 
 * the query-pair Smith-Waterman kernel (batches): rows per thread
-  R in {16, 20, 24, 28} x resident CTAs per SM in {4, 5}, on 64 queries of
+  R in {16, 20, 24, 28} x resident CTAs per SM in {4, 5} x columns per step
+  in {2, 4} (column-strip width: two or four dependency chains per thread),
+  on 64 queries of
   exactly two passes (2 x 4R rows); cost = entry-pass device time per
   (query pair x pass x database column);
 * the single-query kernel (sw_align): threads per sequence G in {8, 16, 32}
@@ -41,6 +43,7 @@ LENGTHS = [(150.0, 20, 600), (350.0, 20, 5000), (1500.0, 100, 20000)]
 COUNTS = [10_000, 200_000]
 QPAIR_R = (16, 20, 24, 28)
 QPAIR_MB = (4, 5)
+QPAIR_COLS = (2, 4)
 FAST_G = (8, 16, 32)
 FAST_R = (8, 16, 24, 32)
 
@@ -94,15 +97,18 @@ def tune(reps: int = 3, log=print) -> list[str]:
                                             W.random_residues(rng, rows, W.AA20).tobytes().decode())
                       for _ in range(64)]
                 for mb in QPAIR_MB:
-                    os.environ["SSA_B200_QP_R"] = str(R)
-                    os.environ["SSA_B200_QP_MB"] = str(mb)
-                    try:
-                        t = _entry_seconds(L, lambda: L.align_batch(L.SSA_SMITH_WATERMAN, qs, 10, L.BIT_WIDTH_8,
-                                                                    L.COMPUTE_SCORE), reps)
-                    finally:
-                        del os.environ["SSA_B200_QP_R"], os.environ["SSA_B200_QP_MB"]
-                    ps = t / (32 * 2 * cols) * 1e12
-                    lines.append(f"qpair {bucket} {R} {mb} {ps:.4f}")
+                    for c in QPAIR_COLS:
+                        os.environ["SSA_B200_QP_R"] = str(R)
+                        os.environ["SSA_B200_QP_MB"] = str(mb)
+                        os.environ["SSA_B200_QP_C"] = str(c)
+                        try:
+                            t = _entry_seconds(L, lambda: L.align_batch(L.SSA_SMITH_WATERMAN, qs, 10,
+                                                                        L.BIT_WIDTH_8, L.COMPUTE_SCORE), reps)
+                        finally:
+                            for v in ("SSA_B200_QP_R", "SSA_B200_QP_MB", "SSA_B200_QP_C"):
+                                del os.environ[v]
+                        ps = t / (32 * 2 * cols) * 1e12
+                        lines.append(f"{'qpair4' if c == 4 else 'qpair'} {bucket} {R} {mb} {ps:.4f}")
                 for q in qs:
                     L.free_sequence(q)
             # single-query kernel: one query of exactly two passes
@@ -140,6 +146,7 @@ def write(lines: list[str], path: str, version: int) -> None:
     with open(path, "w") as f:
         f.write("# libssa B200 entry-pass shape table, written by python -m libssa_b200.tune\n")
         f.write("# qpair <bucket> <R> <CTAs per SM> <ps per query pair, pass and database column>\n")
+        f.write("# qpair4 <bucket> <R> <CTAs per SM> <ps ...>  (4 columns per step)\n")
         f.write("# fast <bucket> <G> <R> <ps per pass and database column>\n")
         f.write("# bucket = length bucket (mean <250, <1000, longer) + 3 x size bucket (<50,000 sequences, more)\n")
         f.write(f"version {version}\n")

@@ -48,7 +48,8 @@ def test_committed_table_is_the_default(built_library):
         version = [int(x[1]) for x in lines if x[0] == "version"]
         assert version and r["version"] == version[0]
         # every database bucket has a measured cost for every query-pair shape
-        qp = {(int(x[1]), int(x[2]), int(x[3])) for x in lines if x[0] == "qpair"}
-        assert qp == {(b, R, mb) for b in range(6) for R in (16, 20, 24, 28) for mb in (4, 5)}
+        for kind in ("qpair", "qpair4"):
+            qp = {(int(x[1]), int(x[2]), int(x[3])) for x in lines if x[0] == kind}
+            assert qp == {(b, R, mb) for b in range(6) for R in (16, 20, 24, 28) for mb in (4, 5)}, kind
     else:
         assert r["source"] == "built-in"
