@@ -177,6 +177,9 @@ def make_workload(scale: float, query_seed: int, kind: str = "sw_batched", n_que
         rng = np.random.default_rng(1000 + query_seed)
         lens = W.lognormal_lengths(rng, len(w.queries), 300.0, 0.7)
         w.queries = [W.random_residues(rng, int(L), W.AA20).tobytes() for L in lens]
+    if n_queries:
+        # a length-stratified subset of the batch (small profiling cases)
+        w.queries = [w.queries[i] for i in sorted(stratified([len(q) for q in w.queries], n_queries))]
     return w
 
 
@@ -475,7 +478,7 @@ def run_ours(args):
         "timing": {"device_seconds": round(t_dev, 4), "wall_seconds": round(t_wall, 4),
                    "entry_seconds_median": round(t_entry, 4)},
     }
-    if not plain and args.scale == 1.0 and rank == 0 and lists is not None:
+    if not plain and args.scale == 1.0 and not args.queries and rank == 0 and lists is not None:
         line["parity"] = parity("sw_batched", dict(enumerate(lists)), dict(enumerate(ovf)))
     if args.plain_queries > 0:
         # the plain one-query-per-call path on a length-stratified query sample
@@ -505,7 +508,7 @@ def run_ours(args):
         except Exception as e:  # noqa: BLE001
             line["cpu_baseline"] = {"value": None, "unit": "GCUPS", "cores": os.cpu_count() or 1,
                                     "kind": "reference", "sample": f"unavailable: {e}"}
-    if world == 1 and not plain and args.scale == 1.0 and not args.no_legs:
+    if world == 1 and not plain and args.scale == 1.0 and not args.queries and not args.no_legs:
         del w
         line["config1"] = config1_leg(L)
         line["config2"] = config2_leg(L)
@@ -922,7 +925,9 @@ def main():
     ap.add_argument("--served-scale", type=float, default=1.0, help="served database scale (1.0 = 1M sequences)")
     ap.add_argument("--workload", default="sw_batched", choices=["sw_batched", "sw_plain", "sw_served", "nw_nucleotide", "long_pairs"],
                     help="sw_plain: a 10,000-sequence database with --queries queries of 375")
-    ap.add_argument("--queries", type=int, default=None, help="query count for --workload sw_plain")
+    ap.add_argument("--queries", type=int, default=None,
+                    help="query count: --workload sw_plain (queries of 375), or a length-stratified subset of the "
+                         "1,024-query batch")
     ap.add_argument("--db-memory", type=int, default=0,
                     help="device memory for the database in bytes (0 = automatic; smaller streams it)")
     ap.add_argument("--pairs", type=int, default=4096, help="pair count for --workload long_pairs")
