@@ -429,6 +429,7 @@ def run_ours(args):
     clocks = sampler.stop()
     launches = L.stats().kernel_launches_total - launches0
     ovf = L.query_overflows()
+    tuning = L.tuning_report()
     barrier(pg)
     t_wall = reduce_max(pg, sum(wall))
     t_dev = reduce_max(pg, sum(dev))
@@ -477,6 +478,9 @@ def run_ours(args):
         "clocks": clocks,
         "timing": {"device_seconds": round(t_dev, 4), "wall_seconds": round(t_wall, 4),
                    "entry_seconds_median": round(t_entry, 4)},
+        "tuning": {"table": os.path.relpath(tuning["source"], ROOT) if os.path.isabs(tuning["source"])
+                   else tuning["source"], "version": tuning["version"], "device": tuning["device"],
+                   "shapes_last_call": tuning["last_call"]},
     }
     if not plain and args.scale == 1.0 and not args.queries and rank == 0 and lists is not None:
         line["parity"] = parity("sw_batched", dict(enumerate(lists)), dict(enumerate(ovf)))
