@@ -100,7 +100,8 @@ int ssa_b200_int_peak( double * lane_ops_per_second, double * instructions_per_c
  * intrinsics per clock per SM (eight interleaved dependent chains on every SM):
  * op 0 __viaddmax_s16x2, 1 __vmaxs2, 2 __vimax3_s16x2, 3 __vaddss2,
  * 4 __vsubss2, 5 __vaddss4, 6 __vmaxs4, 7 __vsubus4, 8 __vaddus4, 9 __vmaxu4,
- * 10 __vadd4, 11 __vsub4.  The measurement behind the choice of 16x2 lanes
+ * 10 __vadd4, 11 __vsub4, 12 max.f16x2, 13 32-bit integer add.  The
+ * measurement behind the choice of 16x2 lanes
  * over 8x4 ones.  Returns 0, or -1 for an unknown op or a CUDA error. */
 int ssa_b200_simd_rate( int op, double * per_clock_per_sm );
 

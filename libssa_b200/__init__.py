@@ -333,7 +333,7 @@ def stats() -> Stats:
 
 
 SIMD_PROBE_OPS = ["__viaddmax_s16x2", "__vmaxs2", "__vimax3_s16x2", "__vaddss2", "__vsubss2", "__vaddss4",
-                  "__vmaxs4", "__vsubus4", "__vaddus4", "__vmaxu4", "__vadd4", "__vsub4"]
+                  "__vmaxs4", "__vsubus4", "__vaddus4", "__vmaxu4", "__vadd4", "__vsub4", "max.f16x2", "iadd"]
 
 
 def simd_rates() -> dict[str, float]:

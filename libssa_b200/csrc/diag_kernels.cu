@@ -46,7 +46,7 @@ __global__ void __launch_bounds__( 256 ) int_peak_kernel( unsigned * sink, unsig
 // instruction counters of the same launch give instructions per intrinsic.
 // OP: 0 __viaddmax_s16x2, 1 __vmaxs2, 2 __vimax3_s16x2, 3 __vaddss2,
 //     4 __vsubss2, 5 __vaddss4, 6 __vmaxs4, 7 __vsubus4, 8 __vaddus4,
-//     9 __vmaxu4, 10 __vadd4, 11 __vsub4.
+//     9 __vmaxu4, 10 __vadd4, 11 __vsub4, 12 max.f16x2, 13 32-bit integer add.
 template <int OP>
 __device__ __forceinline__ unsigned probe_op( unsigned a, unsigned b, unsigned c ) {
     if constexpr( OP == 0 ) return __viaddmax_s16x2( a, b, c );
@@ -60,10 +60,16 @@ __device__ __forceinline__ unsigned probe_op( unsigned a, unsigned b, unsigned c
     else if constexpr( OP == 8 ) return __vaddus4( a, b );
     else if constexpr( OP == 9 ) return __vmaxu4( a, b );
     else if constexpr( OP == 10 ) return __vadd4( a, b );
-    else return __vsub4( a, b );
+    else if constexpr( OP == 11 ) return __vsub4( a, b );
+    else if constexpr( OP == 12 ) {
+        unsigned r;
+        asm( "max.f16x2 %0, %1, %2;" : "=r"( r ) : "r"( a ), "r"( b ) );
+        return r;
+    }
+    else return a + b;
 }
 
-constexpr int PROBE_OPS = 12;
+constexpr int PROBE_OPS = 14;
 constexpr int PROBE_ITERS = 1024;
 
 template <int OP>
@@ -93,7 +99,8 @@ static void launch_probe( int blocks, unsigned * sink, unsigned seed ) {
 typedef void (*ProbeLaunch)( int, unsigned *, unsigned );
 static const ProbeLaunch probe_launch[PROBE_OPS] = {
     launch_probe<0>, launch_probe<1>, launch_probe<2>, launch_probe<3>, launch_probe<4>, launch_probe<5>,
-    launch_probe<6>, launch_probe<7>, launch_probe<8>, launch_probe<9>, launch_probe<10>, launch_probe<11> };
+    launch_probe<6>, launch_probe<7>, launch_probe<8>, launch_probe<9>, launch_probe<10>, launch_probe<11>,
+    launch_probe<12>, launch_probe<13> };
 
 }  // namespace ssa
 

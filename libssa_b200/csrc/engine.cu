@@ -920,34 +920,46 @@ void Engine::run_fast_entry( const SearchRequest & req, uint32_t nq, PairTask * 
 struct QpVariant {
     int mb;         // resident CTAs per SM
     int cols;       // columns per step
+    bool hmax;      // running maximum in fp16x2 (4 columns, 4 CTAs per SM)
     double cost;    // measured cost, 0 = none
 };
 
 // The cheapest measured variant of the query-pair kernel for rows-per-thread
-// R (pinned_mb / pinned_c force one).
-static QpVariant qpair_variant( int bucket, int R, int pinned_mb, int pinned_c ) {
-    QpVariant best{ 4, 2, 0 };
+// R (pinned_mb / pinned_c / pinned_h force one; pinned_h: 0 or 1, -1 = free).
+static QpVariant qpair_variant( int bucket, int R, int pinned_mb, int pinned_c, int pinned_h ) {
+    QpVariant best{ 4, 2, false, 0 };
     for( int mi = 0; mi < 2; mi++ )
-        for( int ci = 0; ci < 2; ci++ ) {
-            const int mb = 4 + mi, cols = 2 + 2 * ci;
+        for( int vi = 0; vi < 3; vi++ ) {
+            const int mb = 4 + mi, cols = vi ? 4 : 2;
+            const bool hm = vi == 2;
+            if( hm && mb != 4 )
+                continue;
             if( (pinned_mb == 4 || pinned_mb == 5) && mb != pinned_mb )
                 continue;
             if( (pinned_c == 2 || pinned_c == 4) && cols != pinned_c )
                 continue;
-            const double c = tuning().qpair[bucket][R / 4 - 4][mi][ci];
+            if( pinned_h >= 0 && hm != (pinned_h == 1) )
+                continue;
+            const double c = tuning().qpair[bucket][R / 4 - 4][mi][vi];
             if( c > 0 && (best.cost <= 0 || c < best.cost) )
-                best = QpVariant{ mb, cols, c };
+                best = QpVariant{ mb, cols, hm, c };
         }
     if( best.cost <= 0 ) {
         if( pinned_mb == 4 || pinned_mb == 5 )
             best.mb = pinned_mb;
         if( pinned_c == 2 || pinned_c == 4 )
             best.cols = pinned_c;
+        if( pinned_h == 1 ) {
+            best.cols = 4;
+            best.mb = 4;
+            best.hmax = true;
+        }
     }
     return best;
 }
 
-static int choose_qpair_rows( uint32_t Q, uint32_t * passes, int pinned, int bucket, int pinned_mb, int pinned_c ) {
+static int choose_qpair_rows( uint32_t Q, uint32_t * passes, int pinned, int bucket, int pinned_mb, int pinned_c,
+        int pinned_h ) {
     static const int rs[4] = { 16, 20, 24, 28 };
     int best_r = 0;
     double best_cost = 1e300;
@@ -959,7 +971,7 @@ static int choose_qpair_rows( uint32_t Q, uint32_t * passes, int pinned, int buc
         const uint32_t P = std::max<uint32_t>( 1, (Q + per - 1) / per );
         if( (uint64_t) P * per > FAST_MAX_ROWS )
             continue;
-        const double unit = qpair_variant( bucket, R, pinned_mb, pinned_c ).cost;
+        const double unit = qpair_variant( bucket, R, pinned_mb, pinned_c, pinned_h ).cost;
         if( unit <= 0 && !pinned )
             continue;                   // not measured
         const double c = (double) P * (unit > 0 ? unit : 1.0);
@@ -970,7 +982,7 @@ static int choose_qpair_rows( uint32_t Q, uint32_t * passes, int pinned, int buc
         }
     }
     if( best_r == 0 && pinned )         // the pinned R does not fit this query
-        return choose_qpair_rows( Q, passes, 0, bucket, pinned_mb, pinned_c );
+        return choose_qpair_rows( Q, passes, 0, bucket, pinned_mb, pinned_c, pinned_h );
     if( best_r == 0 ) {                 // an empty table: 20 rows per thread
         best_r = 20;
         *passes = std::max<uint32_t>( 1, (Q + QP_G * 20 - 1) / (QP_G * 20) );
@@ -1006,6 +1018,8 @@ void Engine::run_qpair_entry( const SearchRequest & req, uint32_t nq, PairTask *
     const int pinned_mb = pin_mb ? atoi( pin_mb ) : 0;
     const char * pin_c = getenv( "SSA_B200_QP_C" );      // 2|4 columns per step
     const int pinned_c = pin_c ? atoi( pin_c ) : 0;
+    const char * pin_h = getenv( "SSA_B200_QP_HMAX" );   // 0|1 running maximum in fp16x2
+    const int pinned_h = pin_h ? (atoi( pin_h ) ? 1 : 0) : -1;
     // the database bucket of the shape table: these sequences' mean length and count
     uint64_t seq_res = 0;
     for( uint32_t i = lo; i < hi; i++ )
@@ -1021,7 +1035,7 @@ void Engine::run_qpair_entry( const SearchRequest & req, uint32_t nq, PairTask *
         if( 2 * i + 1 < fit.size() )
             qp_slots[2 * i + 1] = fit[2 * i + 1];
         uint32_t P = 1;
-        const int R = choose_qpair_rows( h_qlen_[fit[2 * i]], &P, pinned_r, bucket, pinned_mb, pinned_c );
+        const int R = choose_qpair_rows( h_qlen_[fit[2 * i]], &P, pinned_r, bucket, pinned_mb, pinned_c, pinned_h );
         qp_rows[i] = P * (uint32_t) (QP_G * R);
         by_r[R / 4 - 4].push_back( i );
     }
@@ -1121,18 +1135,19 @@ void Engine::run_qpair_entry( const SearchRequest & req, uint32_t nq, PairTask *
         if( cls.empty() )
             continue;
         const int R = 4 * (ri + 4);
-        const QpVariant var = nw ? QpVariant{ 4, 2, 0 } : qpair_variant( bucket, R, pinned_mb, pinned_c );
+        const QpVariant var = nw ? QpVariant{ 4, 2, false, 0 } : qpair_variant( bucket, R, pinned_mb, pinned_c,
+                pinned_h );
         const int mb = var.mb;
         auto launch = [&]( const QPairParams & pp, int grid, int * per ) {
             if( nw )
                 return launch_nw_qpair( R, pp, grid, class_stream_[ri], per );
-            return var.cols == 4 ? launch_sw_qpair4( R, mb, pp, grid, class_stream_[ri], per )
+            return var.cols == 4 ? launch_sw_qpair4( R, mb, var.hmax, pp, grid, class_stream_[ri], per )
                                  : launch_sw_qpair( R, mb, pp, grid, class_stream_[ri], per );
         };
         bool multi = false;
         for( uint32_t i : cls )
             multi |= qp_rows[i] > (uint32_t) (QP_G * R);
-        last_shapes_.push_back( { nw ? "nw_qpair" : (var.cols == 4 ? "sw_qpair4" : "sw_qpair"), R, mb,
+        last_shapes_.push_back( { nw ? "nw_qpair" : var.hmax ? "sw_qpair4h" : var.cols == 4 ? "sw_qpair4" : "sw_qpair", R, mb,
                 (uint32_t) cls.size(), bucket } );
         QPairParams p{};
         int per_sm = 0;

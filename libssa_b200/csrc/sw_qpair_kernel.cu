@@ -275,7 +275,25 @@ __global__ void __launch_bounds__( QP_THREADS, MB ) sw_qpair_kernel( QPairParams
 // diagonal H(r - 1, c + j - 1) from chain j - 1's value two iterations back,
 // and E[r] passes from chain j - 1 (iteration r + j - 1) to chain j.
 // ---------------------------------------------------------------------------
-template <int R, int MB>
+// The running maximum of H as fp16x2: every H is at least the bias (1024, the
+// fp16 bit pattern of a positive normal number), and positive fp16 values
+// order like their bit patterns, so a half-precision max of the bit patterns
+// is the integer max.  Patterns past 0x7c00 (infinity, NaN) -- scores more
+// than 30,000 above the bias -- are ignored or taken as the largest; a cell
+// only gets there through cells that crossed 255 earlier on its path, whose
+// own crossing is recorded, so the first crossing and every reported score
+// (below 255) are unchanged.  This max issues to another pipe than the
+// integer ALU, which the rest of the recurrence saturates.
+__device__ __forceinline__ uint32_t hmax_bits( uint32_t a, uint32_t b ) {
+    uint32_t r;
+    asm( "max.f16x2 %0, %1, %2;" : "=r"( r ) : "r"( a ), "r"( b ) );
+    return r;
+}
+
+// HM: track the running maximum with hmax_bits (one instruction per cell
+// pair, off the ALU pipe) instead of the 3-way integer max (half an ALU
+// instruction per cell pair).
+template <int R, int MB, bool HM>
 __global__ void __launch_bounds__( QP_THREADS, MB ) sw_qpair4_kernel( QPairParams p ) {
     constexpr int G = QP_G;
     constexpr int C = 4;
@@ -446,12 +464,19 @@ __global__ void __launch_bounds__( QP_THREADS, MB ) sw_qpair4_kernel( QPairParam
                         // the new cells of this iteration into the running maximum
                         const int j0 = it - (R - 1) > 0 ? it - (R - 1) : 0;
                         const int j1 = it < C - 1 ? it : C - 1;
+                        if constexpr( HM ) {
 #pragma unroll
-                        for( int j = j0; j <= j1; j += 2 ) {
-                            if( j + 1 <= j1 )
-                                smax = __vimax3_s16x2( smax, hnew[j], hnew[j + 1] );
-                            else
-                                smax = __vmaxs2( smax, hnew[j] );
+                            for( int j = j0; j <= j1; j++ )
+                                smax = hmax_bits( smax, hnew[j] );
+                        }
+                        else {
+#pragma unroll
+                            for( int j = j0; j <= j1; j += 2 ) {
+                                if( j + 1 <= j1 )
+                                    smax = __vimax3_s16x2( smax, hnew[j], hnew[j + 1] );
+                                else
+                                    smax = __vmaxs2( smax, hnew[j] );
+                            }
                         }
                         // chain 3 leaves column c + 3 in H
                         if( it - (C - 1) >= 0 && it - (C - 1) < R )
@@ -520,26 +545,28 @@ __global__ void __launch_bounds__( QP_THREADS, MB ) sw_qpair4_kernel( QPairParam
 }
 
 // grid == 0: report the resident CTAs per SM in *blocks_per_sm without launching.
-template <int R, int MB>
+template <int R, int MB, bool HM>
 static cudaError_t launch_qp4_one( const QPairParams & p, int grid, cudaStream_t st, int * blocks_per_sm ) {
     const size_t smem = (size_t) (QP_THREADS / 32) * QP_CODES * QP_G * R * sizeof(uint32_t);
-    cudaError_t e = cudaFuncSetAttribute( sw_qpair4_kernel<R, MB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-            (int) smem );
+    cudaError_t e = cudaFuncSetAttribute( sw_qpair4_kernel<R, MB, HM>,
+            cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem );
     if( e != cudaSuccess )
         return e;
     if( grid == 0 )
-        return cudaOccupancyMaxActiveBlocksPerMultiprocessor( blocks_per_sm, sw_qpair4_kernel<R, MB>, QP_THREADS,
-                smem );
-    sw_qpair4_kernel<R, MB><<<grid, QP_THREADS, smem, st>>>( p );
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor( blocks_per_sm, sw_qpair4_kernel<R, MB, HM>,
+                QP_THREADS, smem );
+    sw_qpair4_kernel<R, MB, HM><<<grid, QP_THREADS, smem, st>>>( p );
     return cudaGetLastError();
 }
 
-cudaError_t launch_sw_qpair4( int R, int mb, const QPairParams & p, int grid, cudaStream_t st,
+// hmax: the running maximum in fp16x2 (4 resident CTAs per SM only)
+cudaError_t launch_sw_qpair4( int R, int mb, bool hmax, const QPairParams & p, int grid, cudaStream_t st,
         int * blocks_per_sm ) {
 #define SSA_QP4_CASE( RR ) \
     case RR: \
-        return mb == 5 ? launch_qp4_one<RR, 5>( p, grid, st, blocks_per_sm ) \
-                       : launch_qp4_one<RR, 4>( p, grid, st, blocks_per_sm );
+        return hmax ? launch_qp4_one<RR, 4, true>( p, grid, st, blocks_per_sm ) \
+                    : mb == 5 ? launch_qp4_one<RR, 5, false>( p, grid, st, blocks_per_sm ) \
+                              : launch_qp4_one<RR, 4, false>( p, grid, st, blocks_per_sm );
     switch( R ) {
     SSA_QP4_CASE( 16 )
     SSA_QP4_CASE( 20 )

@@ -10,7 +10,7 @@ script times every candidate, per database bucket, on seeded synthetic data:
 * the query-pair Smith-Waterman kernel (batches): rows per thread
   R in {16, 20, 24, 28} x resident CTAs per SM in {4, 5} x columns per step
   in {2, 4} (column-strip width: two or four dependency chains per thread),
-  on 64 queries of
+  and the 4-column kernel with its running maximum in fp16x2, on 64 queries of
   exactly two passes (2 x 4R rows); cost = entry-pass device time per
   (query pair x pass x database column);
 * the single-query kernel (sw_align): threads per sequence G in {8, 16, 32}
@@ -42,8 +42,8 @@ DEFAULT_OUT = os.path.join(HERE, "tuning", "b200.tune")
 LENGTHS = [(150.0, 20, 600), (350.0, 20, 5000), (1500.0, 100, 20000)]
 COUNTS = [10_000, 200_000]
 QPAIR_R = (16, 20, 24, 28)
-QPAIR_MB = (4, 5)
-QPAIR_COLS = (2, 4)
+# (resident CTAs per SM, columns per step, running maximum in fp16x2)
+QPAIR_VARIANTS = ((4, 2, 0), (5, 2, 0), (4, 4, 0), (5, 4, 0), (4, 4, 1))
 FAST_G = (8, 16, 32)
 FAST_R = (8, 16, 24, 32)
 
@@ -96,19 +96,20 @@ def tune(reps: int = 3, log=print) -> list[str]:
                 qs = [L.init_sequence_fasta(L.READ_FROM_STRING,
                                             W.random_residues(rng, rows, W.AA20).tobytes().decode())
                       for _ in range(64)]
-                for mb in QPAIR_MB:
-                    for c in QPAIR_COLS:
-                        os.environ["SSA_B200_QP_R"] = str(R)
-                        os.environ["SSA_B200_QP_MB"] = str(mb)
-                        os.environ["SSA_B200_QP_C"] = str(c)
-                        try:
-                            t = _entry_seconds(L, lambda: L.align_batch(L.SSA_SMITH_WATERMAN, qs, 10,
-                                                                        L.BIT_WIDTH_8, L.COMPUTE_SCORE), reps)
-                        finally:
-                            for v in ("SSA_B200_QP_R", "SSA_B200_QP_MB", "SSA_B200_QP_C"):
-                                del os.environ[v]
-                        ps = t / (32 * 2 * cols) * 1e12
-                        lines.append(f"{'qpair4' if c == 4 else 'qpair'} {bucket} {R} {mb} {ps:.4f}")
+                for mb, c, hm in QPAIR_VARIANTS:
+                    os.environ["SSA_B200_QP_R"] = str(R)
+                    os.environ["SSA_B200_QP_MB"] = str(mb)
+                    os.environ["SSA_B200_QP_C"] = str(c)
+                    os.environ["SSA_B200_QP_HMAX"] = str(hm)
+                    try:
+                        t = _entry_seconds(L, lambda: L.align_batch(L.SSA_SMITH_WATERMAN, qs, 10,
+                                                                    L.BIT_WIDTH_8, L.COMPUTE_SCORE), reps)
+                    finally:
+                        for v in ("SSA_B200_QP_R", "SSA_B200_QP_MB", "SSA_B200_QP_C", "SSA_B200_QP_HMAX"):
+                            del os.environ[v]
+                    ps = t / (32 * 2 * cols) * 1e12
+                    kind = "qpair4h" if hm else "qpair4" if c == 4 else "qpair"
+                    lines.append(f"{kind} {bucket} {R} {mb} {ps:.4f}")
                 for q in qs:
                     L.free_sequence(q)
             # single-query kernel: one query of exactly two passes
@@ -147,6 +148,7 @@ def write(lines: list[str], path: str, version: int) -> None:
         f.write("# libssa B200 entry-pass shape table, written by python -m libssa_b200.tune\n")
         f.write("# qpair <bucket> <R> <CTAs per SM> <ps per query pair, pass and database column>\n")
         f.write("# qpair4 <bucket> <R> <CTAs per SM> <ps ...>  (4 columns per step)\n")
+        f.write("# qpair4h <bucket> <R> <CTAs per SM> <ps ...>  (4 columns, running maximum in fp16x2)\n")
         f.write("# fast <bucket> <G> <R> <ps per pass and database column>\n")
         f.write("# bucket = length bucket (mean <250, <1000, longer) + 3 x size bucket (<50,000 sequences, more)\n")
         f.write(f"version {version}\n")

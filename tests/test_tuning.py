@@ -51,5 +51,8 @@ def test_committed_table_is_the_default(built_library):
         for kind in ("qpair", "qpair4"):
             qp = {(int(x[1]), int(x[2]), int(x[3])) for x in lines if x[0] == kind}
             assert qp == {(b, R, mb) for b in range(6) for R in (16, 20, 24, 28) for mb in (4, 5)}, kind
+        # the fp16x2-maximum variant exists at 4 CTAs per SM only
+        qp = {(int(x[1]), int(x[2]), int(x[3])) for x in lines if x[0] == "qpair4h"}
+        assert not qp or qp == {(b, R, 4) for b in range(6) for R in (16, 20, 24, 28)}
     else:
         assert r["source"] == "built-in"
