@@ -117,6 +117,7 @@ public:
             fatal( "libssa B200 build needs an sm_100 device, found %s (sm_%d%d).", prop.name, prop.major,
                     prop.minor );
         sms_ = prop.multiProcessorCount;
+        device_memory_ = prop.totalGlobalMem;
         CUDA_CHECK( cudaStreamCreateWithFlags( &stream_, cudaStreamNonBlocking ) );
         CUDA_CHECK( cudaEventCreate( &ev0_ ) );
         CUDA_CHECK( cudaEventCreate( &ev1_ ) );
@@ -504,6 +505,15 @@ private:
     bool ready_ = false;
     int device_ = 0;
     int sms_ = 148;
+    uint64_t device_memory_ = 0;
+    // (query, sequence) pairs of one sub-batch: its int32 scores (4 B) and, at
+    // most, two re-queue lists of 16 B per pair; 2^29 pairs (19 GB) on devices
+    // of 64 GB and more (a 1,024-query batch against 500,000 sequences in one
+    // pass), 2^28 otherwise; halved when the 64-bit pass keeps int64 scores
+    uint64_t pair_budget() const {
+        const int log2 = device_memory_ >= ((uint64_t) 64 << 30) ? 29 : 28;
+        return (uint64_t) 1 << (wide_ ? log2 - 1 : log2);
+    }
     cudaStream_t stream_ = nullptr;
     cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
     HostDb db_;
@@ -1268,7 +1278,7 @@ void Engine::search( const SearchRequest & req, const std::vector<QueryCodes> & 
     }
     // sub-batches bounded by the per-pair result memory (int32 scores, plus
     // int64 ones in the wide case)
-    const uint64_t pair_budget = (uint64_t) 1 << (wide_ ? 27 : 28);
+    const uint64_t pair_budget = this->pair_budget();
     const uint64_t per_query = std::max<uint64_t>( 1, std::max<uint64_t>( n_ne, db.n_ids ) );
     const size_t batch = (size_t) std::max<uint64_t>(
             1, std::min<uint64_t>( std::min<uint64_t>( queries.size(), pair_budget / per_query ), 65535 ) );
@@ -2153,7 +2163,7 @@ void Engine::shard_scores( const SearchRequest & req, const std::vector<QueryCod
     if( n_sh )
         CUDA_CHECK( cudaMemcpyAsync( d_order_.p, shard.data(), n_sh * sizeof(uint32_t), cudaMemcpyHostToDevice,
                 stream_ ) );
-    const uint64_t pair_budget = (uint64_t) 1 << (wide_ ? 27 : 28);
+    const uint64_t pair_budget = this->pair_budget();
     const uint32_t batch = (uint32_t) std::max<uint64_t>( 1, std::min<uint64_t>( nq_all,
             pair_budget / std::max<uint64_t>( 1, db.n_ids ) ) );
     for( uint32_t b0 = 0; b0 < nq_all && n_sh; b0 += batch ) {

@@ -290,6 +290,10 @@ __device__ __forceinline__ uint32_t hmax_bits( uint32_t a, uint32_t b ) {
     return r;
 }
 
+// The 4-column kernel loads database residues with the streaming cache
+// operator (ld.global.cs: evict first): the database passes through L2 once
+// per pass and query pair, and the pass-boundary row of a multi-pass query,
+// written in one pass and read back in the next, should stay there instead.
 // HM: track the running maximum with hmax_bits (one instruction per cell
 // pair, off the ALU pipe) instead of the 3-way integer max (half an ALU
 // instruction per cell pair).
@@ -371,7 +375,7 @@ __global__ void __launch_bounds__( QP_THREADS, MB ) sw_qpair4_kernel( QPairParam
                 const uint32_t fetch_limit = nb + 3u;
                 auto fetch = [&]( int32_t b ) -> uint32_t {
                     const uint32_t c = min( (uint32_t) max( b, 0 ), fetch_limit );
-                    return *reinterpret_cast<const uint32_t *>( res + 4u * c );
+                    return __ldcs( reinterpret_cast<const unsigned int *>( res + 4u * c ) );
                 };
                 uint32_t q0 = fetch( -k ), q1 = fetch( 1 - k ), q2 = fetch( 2 - k ), q3 = fetch( 3 - k );
                 // thread 0: the previous pass's bottom row, one block ahead
