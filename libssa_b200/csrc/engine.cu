@@ -1302,12 +1302,19 @@ void Engine::search( const SearchRequest & req, const std::vector<QueryCodes> & 
         d_score_.ensure( std::max<size_t>( score_bytes, 4 ) );
         if( wide_ )
             d_score64_.ensure( std::max<size_t>( 2 * score_bytes, 8 ) );
-        const uint32_t cap = (uint32_t) std::min<uint64_t>( std::max<uint64_t>( n_pairs, 1 ), 0xffffffffull );
+        // re-queue lists sized for the overflows a search expects (a few per
+        // query): 1/32 of the pairs, at least 4M entries; an entry pass that
+        // re-queues more runs again with lists of its count
+        const uint64_t all_pairs = std::min<uint64_t>( std::max<uint64_t>( n_pairs, 1 ), 0xffffffffull );
+        uint32_t cap = (uint32_t) std::min<uint64_t>( all_pairs, std::max<uint64_t>( (uint64_t) 1 << 22,
+                all_pairs >> 5 ) );
+        if( const char * c0 = getenv( "SSA_B200_REQUEUE_CAP" ) )   // a smaller first size (tests of the regrowth)
+            cap = (uint32_t) std::max<uint64_t>( 1, std::min<uint64_t>( cap, strtoull( c0, nullptr, 10 ) ) );
         d_list_a_.ensure( (size_t) cap * sizeof(PairTask) );
         d_list_b_.ensure( (size_t) cap * sizeof(PairTask) );
         d_counts_.ensure( 32 * sizeof(unsigned long long) );
         CUDA_CHECK( cudaMemsetAsync( d_counts_.p, 0, 32 * sizeof(unsigned long long), stream_ ) );
-        unsigned * cnt = d_counts_.as<unsigned>();   // [0] list a, [1] list b, [2] errors
+        unsigned * cnt = d_counts_.as<unsigned>();   // [0] list a, [1] list b, [2] errors, [5] NW redo
 
         // ---- passes
         const bool timing = getenv( "SSA_B200_TIMING" ) != nullptr;
@@ -1328,14 +1335,32 @@ void Engine::search( const SearchRequest & req, const std::vector<QueryCodes> & 
             }
             const uint64_t seg_pairs = (uint64_t) nq * (hi - lo);
             CUDA_CHECK( cudaEventRecord( ev_seg_[0], stream_ ) );
-            if( (fast_eligible( req ) && (nq >= 2 || streaming_) && !getenv( "SSA_B200_NO_QPAIR" )) ||
-                    nw_fast_eligible( req ) )
-                run_qpair_entry( req, nq, d_list_a_.as<PairTask>(), cnt + 0, cap, nullptr, lo, hi );
-            else if( fast_eligible( req ) )
-                run_fast_entry( req, nq, d_list_a_.as<PairTask>(), cnt + 0, cap );
-            else
-                run_pass( req.algo, entry, req, nq, nullptr, seg_pairs, true, d_list_a_.as<PairTask>(), cnt + 0, cap,
-                        nullptr, 0, lo );
+            auto run_entry = [&]() {
+                if( (fast_eligible( req ) && (nq >= 2 || streaming_) && !getenv( "SSA_B200_NO_QPAIR" )) ||
+                        nw_fast_eligible( req ) )
+                    run_qpair_entry( req, nq, d_list_a_.as<PairTask>(), cnt + 0, cap, nullptr, lo, hi );
+                else if( fast_eligible( req ) )
+                    run_fast_entry( req, nq, d_list_a_.as<PairTask>(), cnt + 0, cap );
+                else
+                    run_pass( req.algo, entry, req, nq, nullptr, seg_pairs, true, d_list_a_.as<PairTask>(), cnt + 0,
+                            cap, nullptr, 0, lo );
+            };
+            run_entry();
+            for( ;; ) {
+                // counts of the entry list and the NW redo list (their atomic
+                // counters count every append, kept or not) and the error flags
+                unsigned c[6] = {};
+                CUDA_CHECK( cudaMemcpyAsync( c, cnt, sizeof c, cudaMemcpyDeviceToHost, stream_ ) );
+                CUDA_CHECK( cudaStreamSynchronize( stream_ ) );
+                const uint64_t need = std::max<uint64_t>( c[0], c[5] );
+                if( need <= cap && !(c[2] & ERR_REQUEUE_OVERFLOW) )
+                    break;
+                cap = (uint32_t) std::min<uint64_t>( all_pairs, std::max<uint64_t>( need, 2ull * cap ) );
+                d_list_a_.ensure( (size_t) cap * sizeof(PairTask) );
+                d_list_b_.ensure( (size_t) cap * sizeof(PairTask) );
+                CUDA_CHECK( cudaMemsetAsync( cnt, 0, 6 * sizeof(unsigned), stream_ ) );
+                run_entry();
+            }
             CUDA_CHECK( cudaEventRecord( ev_seg_[1], stream_ ) );
             CUDA_CHECK( cudaEventSynchronize( ev_seg_[1] ) );
             float seg_ms = 0;

@@ -93,6 +93,25 @@ print("returned")
     assert "returned" not in r.stdout
 
 
+@pytest.mark.parametrize("name", ["sw_batched_small", "mixed_sw_8_2", "mixed_nw_8_2"])
+def test_requeue_lists_grow_when_a_pass_overflows_them(built_library, monkeypatch, name):
+    """The re-queue lists start small (here 2 entries); an entry pass that
+    re-queues more pairs runs again with lists of its count, and the answer is
+    the reference's."""
+    monkeypatch.setenv("SSA_B200_REQUEUE_CAP", "2")
+    case = [c for c in golden_cases() if c["name"] == name][0]
+    queries, records = case_inputs(case)
+    product_setup(case["symtype"], case["matrix"], tuple(case["gap"]), case["chunk"], case["simd"], records=records)
+    for batch in (False, True):
+        res, ovf = product_search(case["algo"], case["width"], case["align"], case["hits"], queries, batch=batch)
+        for qi in range(len(queries)):
+            exp = case["expected"][qi]
+            assert [list(r) for r in res[qi]] == exp["hits"], (name, qi, batch)
+            if ovf is not None:
+                assert list(ovf[qi]) == [exp["ovf8"], exp["ovf16"]], (name, qi)
+    assert any(e["ovf8"] + e["ovf16"] > 2 for e in case["expected"])
+
+
 def test_batched_equals_single(built_library):
     """Each query's result is the same alone and inside a batch."""
     case = [c for c in golden_cases() if c["name"] == "sw_batched_small"][0]
@@ -249,6 +268,21 @@ def _nw_batch_case(seed):
     return dict(queries=[q.tobytes() for q in qs], records=recs, gap=gap, matrix=matrix, symtype=0 if nuc else 1,
                 chunk=int([1000, 33][int(rng.integers(0, 2))]), hits=int(rng.integers(1, 12)),
                 simd=int([2, 1][int(rng.integers(0, 2))]))
+
+
+@pytest.mark.parametrize("seed", [1, 3])
+def test_nw16_redo_list_grows(built_library, monkeypatch, seed):
+    """The NW query-pair pass sends sequences beyond its exact range to a redo
+    list; with lists starting at 2 entries the pass runs again with room for
+    all of them, and the batch still matches the oracle."""
+    monkeypatch.setenv("SSA_B200_REQUEUE_CAP", "2")
+    c = _nw_batch_case(seed)
+    product_setup(c["symtype"], c["matrix"], c["gap"], c["chunk"], c["simd"], records=c["records"])
+    batched, _ = product_search("nw", 16, 1, c["hits"], c["queries"], batch=True)
+    for qi, q in enumerate(c["queries"]):
+        exp, _ = oracle_search("nw", 16, 1, c["hits"], c["symtype"], c["matrix"], c["gap"], c["chunk"], c["simd"],
+                               q, c["records"])
+        assert batched[qi] == exp, (seed, qi, len(q))
 
 
 @pytest.mark.parametrize("seed", range(8))
