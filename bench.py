@@ -191,7 +191,7 @@ def rank_workload(args, rank: int):
 
 def load_traffic() -> float | None:
     """DRAM bytes per cell of the entry pass, from the committed ncu summary."""
-    path = os.path.join(ROOT, "profiles", "sw_qpair_kernel_traffic_scale05.md")
+    path = os.path.join(ROOT, "profiles", "sw_qpair4_kernel_32q.md")
     try:
         with open(path) as f:
             for line in f:
@@ -466,10 +466,11 @@ def run_ours(args):
         "roofline": {"bound": "alu", "achieved": round(achieved, 3), "peak": round(peak, 3),
                      "unit": "Top/s", "frac": round(achieved / peak, 4),
                      "traffic": (round(traffic_per_cell * cells) if traffic_per_cell else None),
-                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the entry-pass launches "
-                                       "at half scale, scaled by cells (profiles/sw_qpair_kernel_traffic_scale05.md)",
-                     "kernel": ("sw_qpair_kernel (entry pass, all rows-per-thread classes)" if len(w.queries) > 1
-                                else "sw_fast_kernel (entry pass)"),
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per cell of an entry-pass "
+                                       "launch on a small case (32 queries vs 250,000 sequences), scaled by cells "
+                                       "(profiles/sw_qpair4_kernel_32q.md)",
+                     "kernel": ("sw_qpair4_kernel / sw_qpair_kernel (entry pass, all rows-per-thread classes)"
+                                if len(w.queries) > 1 else "sw_fast_kernel (entry pass)"),
                      "peak_source": "measured on this device: integer ALU pipe running fused 16x2 add-max "
                                     f"({peak_ipc:.2f} warp-inst/clk/SM, an add and a max per 16-bit half); "
                                     "9 integer ops per cell (4 adds, 5 maxes); neither HBM nor tensor cores "
