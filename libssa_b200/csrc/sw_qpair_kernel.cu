@@ -293,24 +293,7 @@ __device__ __forceinline__ uint32_t hmax_bits( uint32_t a, uint32_t b ) {
 // The 4-column kernel loads database residues with the streaming cache
 // operator (ld.global.cs: evict first): the database passes through L2 once
 // per pass and query pair, and the pass-boundary row of a multi-pass query,
-// written in one pass and read back in the next, should stay there instead:
-// its stores and loads carry an evict-last L2 policy, created at each use so
-// that no register holds it across the step.
-__device__ __forceinline__ int4 ld_boundary( const int4 * a ) {
-    int4 v;
-    asm volatile( "{\n\t.reg .b64 pol;\n\t"
-            "createpolicy.fractional.L2::evict_last.b64 pol, 1.0;\n\t"
-            "ld.global.L2::cache_hint.v4.s32 {%0, %1, %2, %3}, [%4], pol;\n\t}"
-            : "=r"( v.x ), "=r"( v.y ), "=r"( v.z ), "=r"( v.w ) : "l"( a ) : "memory" );
-    return v;
-}
-
-__device__ __forceinline__ void st_boundary( int4 * a, int4 v ) {
-    asm volatile( "{\n\t.reg .b64 pol;\n\t"
-            "createpolicy.fractional.L2::evict_last.b64 pol, 1.0;\n\t"
-            "st.global.L2::cache_hint.v4.s32 [%0], {%1, %2, %3, %4}, pol;\n\t}"
-            :: "l"( a ), "r"( v.x ), "r"( v.y ), "r"( v.z ), "r"( v.w ) : "memory" );
-}
+// written in one pass and read back in the next, should stay there instead.
 // HM: track the running maximum with hmax_bits (one instruction per cell
 // pair, off the ALU pipe) instead of the 3-way integer max (half an ALU
 // instruction per cell pair).
@@ -399,8 +382,8 @@ __global__ void __launch_bounds__( QP_THREADS, MB ) sw_qpair4_kernel( QPairParam
                 const bool reads_boundary = (k == 0) && pass > 0;
                 int4 bq0 = make_int4( 0, 0, 0, 0 ), bq1 = bq0;
                 if( reads_boundary && nb > 0 ) {
-                    bq0 = ld_boundary( scratch );
-                    bq1 = ld_boundary( scratch + 1 );
+                    bq0 = scratch[0];
+                    bq1 = scratch[1];
                 }
                 const uint32_t steps = max_nb + (uint32_t) G - 1u;
                 for( uint32_t s = 0; s < steps; s++ ) {
@@ -420,8 +403,8 @@ __global__ void __launch_bounds__( QP_THREADS, MB ) sw_qpair4_kernel( QPairParam
                     if( reads_boundary ) {
                         const uint32_t nxt = (uint32_t) b + 1u;
                         if( nxt < nb && 2u * nxt + 1u < p.scratch_cols ) {
-                            bq0 = ld_boundary( scratch + 2u * nxt );
-                            bq1 = ld_boundary( scratch + 2u * nxt + 1u );
+                            bq0 = scratch[2u * nxt];
+                            bq1 = scratch[2u * nxt + 1u];
                         }
                     }
                     if( b < 0 || (uint32_t) b >= nb )
@@ -520,10 +503,10 @@ __global__ void __launch_bounds__( QP_THREADS, MB ) sw_qpair4_kernel( QPairParam
                     }
                     if( k == G - 1 && !last_pass ) {
                         if( 2u * (uint32_t) b + 1u < p.scratch_cols ) {
-                            st_boundary( scratch + 2u * b, make_int4( (int) out_h[0], (int) out_f[0],
-                                    (int) out_h[1], (int) out_f[1] ) );
-                            st_boundary( scratch + 2u * b + 1u, make_int4( (int) out_h[2], (int) out_f[2],
-                                    (int) out_h[3], (int) out_f[3] ) );
+                            scratch[2u * b] = make_int4( (int) out_h[0], (int) out_f[0], (int) out_h[1],
+                                    (int) out_f[1] );
+                            scratch[2u * b + 1u] = make_int4( (int) out_h[2], (int) out_f[2], (int) out_h[3],
+                                    (int) out_f[3] );
                         }
                         else {
                             atomicOr( p.sink.error_flags, ERR_SCRATCH_OVERFLOW );
