@@ -224,8 +224,9 @@ struct QPairParams {
 // mb: 4 or 5 resident CTAs per SM (register bound of the instantiation)
 cudaError_t launch_sw_qpair( int R, int mb, const QPairParams & p, int grid, cudaStream_t st, int * blocks_per_sm );
 // the same pass with one 4-column block per step (four dependency chains per
-// thread); hmax: the running maximum in fp16x2 off the ALU pipe (mb 4 only)
-cudaError_t launch_sw_qpair4( int R, int mb, bool hmax, const QPairParams & p, int grid, cudaStream_t st,
+// thread); hmax: the running maximum in fp16x2 off the ALU pipe (mb 4 only);
+// g8: R = 24 rows per pass of 4 threads run as 8 threads of 12 rows
+cudaError_t launch_sw_qpair4( int R, int mb, bool hmax, bool g8, const QPairParams & p, int grid, cudaStream_t st,
         int * blocks_per_sm );
 cudaError_t launch_nw_qpair( int R, const QPairParams & p, int grid, cudaStream_t st, int * blocks_per_sm );
 // width 8: (int8) scores, -128 past a query (Smith-Waterman 8-bit entry);

@@ -814,11 +814,20 @@ void Engine::run_fast_entry( const SearchRequest & req, uint32_t nq, PairTask * 
     }
 
     // work units: ranges of length-sorted pairs holding about equal numbers
-    // of columns (at least 4 pairs), the longest first; every query of a
-    // class gets every range.  A warp takes one unit at a time.
+    // of columns, the longest first; every query of a class gets every range.
+    // A warp takes one unit at a time and runs its pairs 32 / G at a time, so
+    // a unit holds at least one such round for the smallest group of the call
+    // (no idle groups) and, where the columns allow, no more: on a small
+    // database the longest pairs then run side by side in separate warps
+    // instead of one after another in the same warp.
     uint64_t total_cols = 0;
     for( uint32_t c : db_.pair_cols )
         total_cols += c;
+    int g_min = 32;
+    for( uint32_t s = 0; s < nq; s++ )
+        if( shape[s].G )
+            g_min = std::min( g_min, shape[s].G );
+    const uint32_t min_pairs = 32u / (uint32_t) g_min;
     const uint64_t want_units = (uint64_t) sms_ * 16 * 24;   // ~24 units per resident warp
     const uint64_t target = std::max<uint64_t>( 1, total_cols * std::max<size_t>( 1, n_shaped ) / want_units );
     std::vector<uint32_t> bounds{ 0 };
@@ -828,7 +837,7 @@ void Engine::run_fast_entry( const SearchRequest & req, uint32_t nq, PairTask * 
         for( uint32_t pi = 0; pi < n_pairs; pi++ ) {
             acc += db_.pair_cols[pi];
             cnt++;
-            if( acc >= target && cnt >= 4 ) {
+            if( acc >= target && cnt >= min_pairs ) {
                 bounds.push_back( pi + 1 );
                 acc = 0;
                 cnt = 0;
@@ -931,18 +940,20 @@ struct QpVariant {
     int mb;         // resident CTAs per SM
     int cols;       // columns per step
     bool hmax;      // running maximum in fp16x2 (4 columns, 4 CTAs per SM)
+    bool g8;        // 8 threads of 12 rows per sequence (R = 24, 4 columns)
     double cost;    // measured cost, 0 = none
 };
 
 // The cheapest measured variant of the query-pair kernel for rows-per-thread
-// R (pinned_mb / pinned_c / pinned_h force one; pinned_h: 0 or 1, -1 = free).
-static QpVariant qpair_variant( int bucket, int R, int pinned_mb, int pinned_c, int pinned_h ) {
-    QpVariant best{ 4, 2, false, 0 };
+// R (pinned_mb / pinned_c / pinned_h / pinned_g8 force one; pinned_h and
+// pinned_g8: 0 or 1, -1 = free).
+static QpVariant qpair_variant( int bucket, int R, int pinned_mb, int pinned_c, int pinned_h, int pinned_g8 ) {
+    QpVariant best{ 4, 2, false, false, 0 };
     for( int mi = 0; mi < 2; mi++ )
-        for( int vi = 0; vi < 3; vi++ ) {
+        for( int vi = 0; vi < 4; vi++ ) {
             const int mb = 4 + mi, cols = vi ? 4 : 2;
-            const bool hm = vi == 2;
-            if( hm && mb != 4 )
+            const bool hm = vi == 2, g8 = vi == 3;
+            if( (hm && mb != 4) || (g8 && R != 24) )
                 continue;
             if( (pinned_mb == 4 || pinned_mb == 5) && mb != pinned_mb )
                 continue;
@@ -950,9 +961,11 @@ static QpVariant qpair_variant( int bucket, int R, int pinned_mb, int pinned_c, 
                 continue;
             if( pinned_h >= 0 && hm != (pinned_h == 1) )
                 continue;
+            if( pinned_g8 >= 0 && g8 != (pinned_g8 == 1) )
+                continue;
             const double c = tuning().qpair[bucket][R / 4 - 4][mi][vi];
             if( c > 0 && (best.cost <= 0 || c < best.cost) )
-                best = QpVariant{ mb, cols, hm, c };
+                best = QpVariant{ mb, cols, hm, g8, c };
         }
     if( best.cost <= 0 ) {
         if( pinned_mb == 4 || pinned_mb == 5 )
@@ -964,12 +977,16 @@ static QpVariant qpair_variant( int bucket, int R, int pinned_mb, int pinned_c, 
             best.mb = 4;
             best.hmax = true;
         }
+        else if( pinned_g8 == 1 && R == 24 ) {
+            best.cols = 4;
+            best.g8 = true;
+        }
     }
     return best;
 }
 
 static int choose_qpair_rows( uint32_t Q, uint32_t * passes, int pinned, int bucket, int pinned_mb, int pinned_c,
-        int pinned_h ) {
+        int pinned_h, int pinned_g8 ) {
     static const int rs[4] = { 16, 20, 24, 28 };
     int best_r = 0;
     double best_cost = 1e300;
@@ -981,7 +998,7 @@ static int choose_qpair_rows( uint32_t Q, uint32_t * passes, int pinned, int buc
         const uint32_t P = std::max<uint32_t>( 1, (Q + per - 1) / per );
         if( (uint64_t) P * per > FAST_MAX_ROWS )
             continue;
-        const double unit = qpair_variant( bucket, R, pinned_mb, pinned_c, pinned_h ).cost;
+        const double unit = qpair_variant( bucket, R, pinned_mb, pinned_c, pinned_h, pinned_g8 ).cost;
         if( unit <= 0 && !pinned )
             continue;                   // not measured
         const double c = (double) P * (unit > 0 ? unit : 1.0);
@@ -992,7 +1009,7 @@ static int choose_qpair_rows( uint32_t Q, uint32_t * passes, int pinned, int buc
         }
     }
     if( best_r == 0 && pinned )         // the pinned R does not fit this query
-        return choose_qpair_rows( Q, passes, 0, bucket, pinned_mb, pinned_c, pinned_h );
+        return choose_qpair_rows( Q, passes, 0, bucket, pinned_mb, pinned_c, pinned_h, pinned_g8 );
     if( best_r == 0 ) {                 // an empty table: 20 rows per thread
         best_r = 20;
         *passes = std::max<uint32_t>( 1, (Q + QP_G * 20 - 1) / (QP_G * 20) );
@@ -1030,6 +1047,8 @@ void Engine::run_qpair_entry( const SearchRequest & req, uint32_t nq, PairTask *
     const int pinned_c = pin_c ? atoi( pin_c ) : 0;
     const char * pin_h = getenv( "SSA_B200_QP_HMAX" );   // 0|1 running maximum in fp16x2
     const int pinned_h = pin_h ? (atoi( pin_h ) ? 1 : 0) : -1;
+    const char * pin_g8 = getenv( "SSA_B200_QP_G8" );    // 0|1 8 threads per sequence (R = 24)
+    const int pinned_g8 = pin_g8 ? (atoi( pin_g8 ) ? 1 : 0) : -1;
     // the database bucket of the shape table: these sequences' mean length and count
     uint64_t seq_res = 0;
     for( uint32_t i = lo; i < hi; i++ )
@@ -1045,7 +1064,8 @@ void Engine::run_qpair_entry( const SearchRequest & req, uint32_t nq, PairTask *
         if( 2 * i + 1 < fit.size() )
             qp_slots[2 * i + 1] = fit[2 * i + 1];
         uint32_t P = 1;
-        const int R = choose_qpair_rows( h_qlen_[fit[2 * i]], &P, pinned_r, bucket, pinned_mb, pinned_c, pinned_h );
+        const int R = choose_qpair_rows( h_qlen_[fit[2 * i]], &P, pinned_r, bucket, pinned_mb, pinned_c, pinned_h,
+                pinned_g8 );
         qp_rows[i] = P * (uint32_t) (QP_G * R);
         by_r[R / 4 - 4].push_back( i );
     }
@@ -1145,19 +1165,20 @@ void Engine::run_qpair_entry( const SearchRequest & req, uint32_t nq, PairTask *
         if( cls.empty() )
             continue;
         const int R = 4 * (ri + 4);
-        const QpVariant var = nw ? QpVariant{ 4, 2, false, 0 } : qpair_variant( bucket, R, pinned_mb, pinned_c,
-                pinned_h );
+        const QpVariant var = nw ? QpVariant{ 4, 2, false, false, 0 } : qpair_variant( bucket, R, pinned_mb, pinned_c,
+                pinned_h, pinned_g8 );
         const int mb = var.mb;
         auto launch = [&]( const QPairParams & pp, int grid, int * per ) {
             if( nw )
                 return launch_nw_qpair( R, pp, grid, class_stream_[ri], per );
-            return var.cols == 4 ? launch_sw_qpair4( R, mb, var.hmax, pp, grid, class_stream_[ri], per )
+            return var.cols == 4 ? launch_sw_qpair4( R, mb, var.hmax, var.g8, pp, grid, class_stream_[ri], per )
                                  : launch_sw_qpair( R, mb, pp, grid, class_stream_[ri], per );
         };
         bool multi = false;
         for( uint32_t i : cls )
             multi |= qp_rows[i] > (uint32_t) (QP_G * R);
-        last_shapes_.push_back( { nw ? "nw_qpair" : var.hmax ? "sw_qpair4h" : var.cols == 4 ? "sw_qpair4" : "sw_qpair", R, mb,
+        last_shapes_.push_back( { nw ? "nw_qpair" : var.hmax ? "sw_qpair4h" : var.g8 ? "sw_qpair4g8"
+                : var.cols == 4 ? "sw_qpair4" : "sw_qpair", R, mb,
                 (uint32_t) cls.size(), bucket } );
         QPairParams p{};
         int per_sm = 0;

@@ -165,9 +165,9 @@ struct TuningTable {
     std::string source = "built-in";
     // query-pair kernel: cost per (query pair, pass, database column) by
     // [bucket][R / 4 - 4][resident CTAs per SM - 4][variant: 2 columns per
-    // step, 4 columns, 4 columns with the running maximum in fp16x2];
-    // 0 = not measured
-    double qpair[TUNE_BUCKETS][4][2][3] = {};
+    // step, 4 columns, 4 columns with the running maximum in fp16x2, 4 columns
+    // with 8 threads per sequence (R = 24 only)]; 0 = not measured
+    double qpair[TUNE_BUCKETS][4][2][4] = {};
     // single-query kernel: cost per (pass, database column) by
     // [bucket][G = 8, 16, 32][R / 8 - 1]; 0 = not measured
     double fast[TUNE_BUCKETS][3][4] = {};

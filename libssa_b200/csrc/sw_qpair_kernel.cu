@@ -297,9 +297,13 @@ __device__ __forceinline__ uint32_t hmax_bits( uint32_t a, uint32_t b ) {
 // HM: track the running maximum with hmax_bits (one instruction per cell
 // pair, off the ALU pipe) instead of the 3-way integer max (half an ALU
 // instruction per cell pair).
-template <int R, int MB, bool HM>
+// G: threads per database sequence (4, or 8 with R = 12: one group per
+// quarter-warp, whose rows 12k fall into 8 distinct shared-memory bank groups,
+// so the 128-bit profile loads are conflict-free; a pass still holds 96 rows).
+template <int R, int MB, bool HM, int G = QP_G>
 __global__ void __launch_bounds__( QP_THREADS, MB ) sw_qpair4_kernel( QPairParams p ) {
-    constexpr int G = QP_G;
+    static_assert( G == 4 || G == 8, "4 or 8 threads per sequence" );
+    constexpr int GPW = 32 / G;                  // sequences per warp
     constexpr int C = 4;
     constexpr uint32_t GR = (uint32_t) (G * R);
     extern __shared__ __align__( 16 ) uint32_t qsm[];
@@ -329,7 +333,7 @@ __global__ void __launch_bounds__( QP_THREADS, MB ) sw_qpair4_kernel( QPairParam
         const uint32_t * prof = p.prof + p.prof_off[qp];
         const uint32_t slot_a = p.qp_slots[2 * qp], slot_b = p.qp_slots[2 * qp + 1];
 
-        for( uint32_t b0 = seq_begin; b0 < seq_end; b0 += (uint32_t) QP_GPW ) {
+        for( uint32_t b0 = seq_begin; b0 < seq_end; b0 += (uint32_t) GPW ) {
             const uint32_t idx = b0 + (uint32_t) g;
             const bool valid = idx < seq_end;
             const uint32_t id = valid ? p.order[idx] : 0u;
@@ -549,23 +553,30 @@ __global__ void __launch_bounds__( QP_THREADS, MB ) sw_qpair4_kernel( QPairParam
 }
 
 // grid == 0: report the resident CTAs per SM in *blocks_per_sm without launching.
-template <int R, int MB, bool HM>
+template <int R, int MB, bool HM, int G = QP_G>
 static cudaError_t launch_qp4_one( const QPairParams & p, int grid, cudaStream_t st, int * blocks_per_sm ) {
-    const size_t smem = (size_t) (QP_THREADS / 32) * QP_CODES * QP_G * R * sizeof(uint32_t);
-    cudaError_t e = cudaFuncSetAttribute( sw_qpair4_kernel<R, MB, HM>,
+    const size_t smem = (size_t) (QP_THREADS / 32) * QP_CODES * G * R * sizeof(uint32_t);
+    cudaError_t e = cudaFuncSetAttribute( sw_qpair4_kernel<R, MB, HM, G>,
             cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem );
     if( e != cudaSuccess )
         return e;
     if( grid == 0 )
-        return cudaOccupancyMaxActiveBlocksPerMultiprocessor( blocks_per_sm, sw_qpair4_kernel<R, MB, HM>,
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor( blocks_per_sm, sw_qpair4_kernel<R, MB, HM, G>,
                 QP_THREADS, smem );
-    sw_qpair4_kernel<R, MB, HM><<<grid, QP_THREADS, smem, st>>>( p );
+    sw_qpair4_kernel<R, MB, HM, G><<<grid, QP_THREADS, smem, st>>>( p );
     return cudaGetLastError();
 }
 
-// hmax: the running maximum in fp16x2 (4 resident CTAs per SM only)
-cudaError_t launch_sw_qpair4( int R, int mb, bool hmax, const QPairParams & p, int grid, cudaStream_t st,
+// hmax: the running maximum in fp16x2 (4 resident CTAs per SM only);
+// g8: the class of 96 rows per pass (R = 24) as 8 threads of 12 rows
+cudaError_t launch_sw_qpair4( int R, int mb, bool hmax, bool g8, const QPairParams & p, int grid, cudaStream_t st,
         int * blocks_per_sm ) {
+    if( g8 ) {
+        if( R != 24 || hmax )
+            return cudaErrorInvalidValue;
+        return mb == 5 ? launch_qp4_one<12, 5, false, 8>( p, grid, st, blocks_per_sm )
+                       : launch_qp4_one<12, 4, false, 8>( p, grid, st, blocks_per_sm );
+    }
 #define SSA_QP4_CASE( RR ) \
     case RR: \
         return hmax ? launch_qp4_one<RR, 4, true>( p, grid, st, blocks_per_sm ) \

@@ -19,6 +19,7 @@
 //   qpair <bucket> <R> <MB> <ps per query pair, pass and database column>
 //   qpair4 <bucket> <R> <MB> <ps ...>       (the kernel with 4 columns per step)
 //   qpair4h <bucket> <R> <MB> <ps ...>      (4 columns, running maximum in fp16x2)
+//   qpair4g8 <bucket> 24 <MB> <ps ...>      (4 columns, 96-row passes as 8 threads of 12 rows)
 //   fast <bucket> <G> <R> <ps per pass and database column>
 // Buckets: db_bucket() below.  Missing entries fall back to the built-in
 // costs (measured the same way on a B200 before the tuner existed).
@@ -92,8 +93,11 @@ void load( TuningTable & t ) {
             while( !t.device.empty() && (t.device.back() == '\n' || t.device.back() == '\r' || t.device.back() == ' ') )
                 t.device.pop_back();
         }
-        else if( !strcmp( key, "qpair" ) || !strcmp( key, "qpair4" ) || !strcmp( key, "qpair4h" ) ) {
-            const int ci = !strcmp( key, "qpair" ) ? 0 : !strcmp( key, "qpair4" ) ? 1 : 2;
+        else if( !strcmp( key, "qpair" ) || !strcmp( key, "qpair4" ) || !strcmp( key, "qpair4h" ) ||
+                !strcmp( key, "qpair4g8" ) ) {
+            const int ci = !strcmp( key, "qpair" ) ? 0 : !strcmp( key, "qpair4" ) ? 1 : !strcmp( key, "qpair4h" ) ? 2 : 3;
+            if( ci == 3 && strstr( line, " 24 " ) == nullptr )
+                continue;
             int b, R, mb;
             double ps;
             if( sscanf( line, "%*s %d %d %d %lf", &b, &R, &mb, &ps ) == 4 && b >= 0 && b < TUNE_BUCKETS &&

@@ -10,7 +10,8 @@ script times every candidate, per database bucket, on seeded synthetic data:
 * the query-pair Smith-Waterman kernel (batches): rows per thread
   R in {16, 20, 24, 28} x resident CTAs per SM in {4, 5} x columns per step
   in {2, 4} (column-strip width: two or four dependency chains per thread),
-  and the 4-column kernel with its running maximum in fp16x2, on 64 queries of
+  the 4-column kernel with its running maximum in fp16x2, and (R = 24) the
+  4-column kernel with 8 threads of 12 rows per sequence, on 64 queries of
   exactly two passes (2 x 4R rows); cost = entry-pass device time per
   (query pair x pass x database column);
 * the single-query kernel (sw_align): threads per sequence G in {8, 16, 32}
@@ -42,8 +43,8 @@ DEFAULT_OUT = os.path.join(HERE, "tuning", "b200.tune")
 LENGTHS = [(150.0, 20, 600), (350.0, 20, 5000), (1500.0, 100, 20000)]
 COUNTS = [10_000, 200_000]
 QPAIR_R = (16, 20, 24, 28)
-# (resident CTAs per SM, columns per step, running maximum in fp16x2)
-QPAIR_VARIANTS = ((4, 2, 0), (5, 2, 0), (4, 4, 0), (5, 4, 0), (4, 4, 1))
+# (resident CTAs per SM, columns per step, running maximum in fp16x2, 8 threads per sequence)
+QPAIR_VARIANTS = ((4, 2, 0, 0), (5, 2, 0, 0), (4, 4, 0, 0), (5, 4, 0, 0), (4, 4, 1, 0), (4, 4, 0, 1), (5, 4, 0, 1))
 FAST_G = (8, 16, 32)
 FAST_R = (8, 16, 24, 32)
 
@@ -96,19 +97,23 @@ def tune(reps: int = 3, log=print) -> list[str]:
                 qs = [L.init_sequence_fasta(L.READ_FROM_STRING,
                                             W.random_residues(rng, rows, W.AA20).tobytes().decode())
                       for _ in range(64)]
-                for mb, c, hm in QPAIR_VARIANTS:
+                for mb, c, hm, g8 in QPAIR_VARIANTS:
+                    if g8 and R != 24:
+                        continue
                     os.environ["SSA_B200_QP_R"] = str(R)
                     os.environ["SSA_B200_QP_MB"] = str(mb)
                     os.environ["SSA_B200_QP_C"] = str(c)
                     os.environ["SSA_B200_QP_HMAX"] = str(hm)
+                    os.environ["SSA_B200_QP_G8"] = str(g8)
                     try:
                         t = _entry_seconds(L, lambda: L.align_batch(L.SSA_SMITH_WATERMAN, qs, 10,
                                                                     L.BIT_WIDTH_8, L.COMPUTE_SCORE), reps)
                     finally:
-                        for v in ("SSA_B200_QP_R", "SSA_B200_QP_MB", "SSA_B200_QP_C", "SSA_B200_QP_HMAX"):
+                        for v in ("SSA_B200_QP_R", "SSA_B200_QP_MB", "SSA_B200_QP_C", "SSA_B200_QP_HMAX",
+                                  "SSA_B200_QP_G8"):
                             del os.environ[v]
                     ps = t / (32 * 2 * cols) * 1e12
-                    kind = "qpair4h" if hm else "qpair4" if c == 4 else "qpair"
+                    kind = "qpair4g8" if g8 else "qpair4h" if hm else "qpair4" if c == 4 else "qpair"
                     lines.append(f"{kind} {bucket} {R} {mb} {ps:.4f}")
                 for q in qs:
                     L.free_sequence(q)
@@ -149,6 +154,7 @@ def write(lines: list[str], path: str, version: int) -> None:
         f.write("# qpair <bucket> <R> <CTAs per SM> <ps per query pair, pass and database column>\n")
         f.write("# qpair4 <bucket> <R> <CTAs per SM> <ps ...>  (4 columns per step)\n")
         f.write("# qpair4h <bucket> <R> <CTAs per SM> <ps ...>  (4 columns, running maximum in fp16x2)\n")
+        f.write("# qpair4g8 <bucket> 24 <CTAs per SM> <ps ...>  (4 columns, 8 threads of 12 rows per sequence)\n")
         f.write("# fast <bucket> <G> <R> <ps per pass and database column>\n")
         f.write("# bucket = length bucket (mean <250, <1000, longer) + 3 x size bucket (<50,000 sequences, more)\n")
         f.write(f"version {version}\n")

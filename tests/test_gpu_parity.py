@@ -215,28 +215,33 @@ def test_batched_random_against_oracle(built_library, seed):
 
 @pytest.mark.parametrize("shape", [(16, 4, 4, 0), (20, 4, 4, 0), (24, 4, 4, 0), (28, 4, 4, 0), (20, 5, 2, 0),
                                    (24, 5, 2, 0), (16, 5, 4, 0), (20, 5, 4, 0), (16, 4, 4, 1), (20, 4, 4, 1),
-                                   (24, 4, 4, 1), (28, 4, 4, 1)],
-                         ids=lambda s: f"R{s[0]}_ctas{s[1]}_cols{s[2]}" + ("_hmax" if s[3] else ""))
+                                   (24, 4, 4, 1), (28, 4, 4, 1), (24, 4, 4, 8), (24, 5, 4, 8)],
+                         ids=lambda s: f"R{s[0]}_ctas{s[1]}_cols{s[2]}" + ("_hmax" if s[3] == 1 else
+                                                                           "_g8" if s[3] == 8 else ""))
 @pytest.mark.parametrize("seed", range(4))
 def test_batched_kernel_variants_against_oracle(built_library, monkeypatch, shape, seed):
     """Every variant of the query-pair kernel the shape table can select --
     rows per thread, 4 or 5 resident CTAs per SM, 2 or 4 columns per step,
-    the running maximum as integer or fp16x2 max -- pinned, on batches with
+    the running maximum as integer or fp16x2 max, 4 or 8 threads per sequence
+    -- pinned, on batches with
     multi-pass queries, overflowing copies and empty records, against the
     oracle query by query (scores, overflow blocks through the tie order,
     CIGARs)."""
-    R, mb, cols, hm = shape
+    R, mb, cols, extra = shape
+    hm, g8 = extra == 1, extra == 8
     monkeypatch.setenv("SSA_B200_QP_R", str(R))
     monkeypatch.setenv("SSA_B200_QP_MB", str(mb))
     monkeypatch.setenv("SSA_B200_QP_C", str(cols))
-    monkeypatch.setenv("SSA_B200_QP_HMAX", str(hm))
+    monkeypatch.setenv("SSA_B200_QP_HMAX", str(int(hm)))
+    monkeypatch.setenv("SSA_B200_QP_G8", str(int(g8)))
     c = _batch_case(100 + seed)
     product_setup(1, c["matrix"], c["gap"], c["chunk"], c["simd"], records=c["records"])
     batched, _ = product_search("sw", 8, 1, c["hits"], c["queries"], batch=True)
     import libssa_b200 as L
     used = [u for u in L.tuning_report()["last_call"] if u["kernel"].startswith("sw_qpair")]
     assert used and all(u["R"] == R and u["ctas_per_sm"] == mb for u in used), used
-    assert all(u["kernel"] == ("sw_qpair4h" if hm else "sw_qpair4" if cols == 4 else "sw_qpair") for u in used), used
+    assert all(u["kernel"] == ("sw_qpair4h" if hm else "sw_qpair4g8" if g8 else "sw_qpair4" if cols == 4
+                               else "sw_qpair") for u in used), used
     for qi, q in enumerate(c["queries"]):
         exp, _ = oracle_search("sw", 8, 1, c["hits"], 1, c["matrix"], c["gap"], c["chunk"], c["simd"], q,
                                c["records"])

@@ -54,5 +54,8 @@ def test_committed_table_is_the_default(built_library):
         # the fp16x2-maximum variant exists at 4 CTAs per SM only
         qp = {(int(x[1]), int(x[2]), int(x[3])) for x in lines if x[0] == "qpair4h"}
         assert not qp or qp == {(b, R, 4) for b in range(6) for R in (16, 20, 24, 28)}
+        # the 8-threads-per-sequence variant exists for the 96-row class only
+        qp = {(int(x[1]), int(x[2]), int(x[3])) for x in lines if x[0] == "qpair4g8"}
+        assert not qp or qp == {(b, 24, mb) for b in range(6) for mb in (4, 5)}
     else:
         assert r["source"] == "built-in"
