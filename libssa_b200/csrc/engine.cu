@@ -714,13 +714,13 @@ constexpr uint32_t FAST_MAX_ROWS = 8192;    // longer queries run the lane emula
 constexpr uint32_t FAST_MAX_PASS_ROWS = 512; // G x R: 16 KiB profile slice per warp
 
 // Threads per group G, rows per thread R and passes P for a query of Q rows:
-// the smallest estimated issue cost per database column, counting the
-// wavefront fill (G - 1 steps per pass) and a per-step overhead.  (A model
-// that also bounds small databases by the longest sequence's latency picked
-// G = 32 for a 375-row query against 10,000 sequences, which measured slower
-// than this choice, G = 8, R = 24, P = 2.)
-// With a measured shape table for the database's bucket (tuning.cpp) the cost
-// of a shape is passes x its measured cost per pass and column.
+// without a measured table, the smallest estimated issue cost per database
+// column, counting the wavefront fill (G - 1 steps per pass) and a per-step
+// overhead.  With a measured shape table for the database's bucket
+// (tuning.cpp) the cost of a shape is passes x its measured cost per pass and
+// column; on a small database that measurement includes the latency of the
+// longest pairs, so it favours wide groups there (a 375-row query against
+// 10,000 sequences: G = 32, R = 16, one pass).
 static FastShape choose_shape( uint32_t Q, double mean_len, int bucket ) {
     FastShape best{ 0, 0, 0 };
     double best_cost = 1e300;
