@@ -171,7 +171,7 @@ struct FastParams {
     int gap_oe;                   // (int8) (gapO + gapE)
     int gap_e;
     PassSink sink;
-    int4 * scratch;               // per warp and group slot (4 per warp): scratch_cols entries
+    int4 * scratch;               // per warp and group slot (4 per warp, 8 for the 4-column kernel): scratch_cols entries
     uint32_t scratch_cols;
     uint32_t slice_rows;          // largest G x R of the launch: rows of a warp's profile slice
 };
@@ -179,6 +179,9 @@ struct FastParams {
 constexpr int FAST_THREADS = 128;   // threads per CTA of the fast pass
 
 cudaError_t launch_sw_fast( int R, const FastParams & p, int grid, cudaStream_t st, int * blocks_per_sm );
+// the same pass with one 4-column block per step (G = 4, 8, 16 or 32; scratch
+// rows for 8 groups per warp)
+cudaError_t launch_sw_fast4( int R, const FastParams & p, int grid, cudaStream_t st, int * blocks_per_sm );
 cudaError_t launch_build_profile8( const uint8_t * qcodes, const uint64_t * qoff, const uint32_t * qlen,
         const uint32_t * slots, uint32_t n, const uint32_t * rows_of, const int64_t * matrix, int8_t * prof,
         const uint64_t * prof_off, cudaStream_t st );

@@ -450,7 +450,8 @@ public:
     void shutdown() {
         DevBuf * bufs[] = { &d_codes_, &d_off_, &d_len_, &d_order_, &d_pair_res_, &d_pair_off_, &d_pair_cols_,
             &d_pair_ids_, &d_prof8_, &d_prof8_off_, &d_rows_, &d_slots_, &d_bounds_, &d_group_,
-            &d_scratch_fast_[0], &d_scratch_fast_[1], &d_scratch_fast_[2], &d_scratch_fast_[3], &d_qcodes_, &d_qoff_, &d_qlen_, &d_qpad_,
+            &d_scratch_fast_[0], &d_scratch_fast_[1], &d_scratch_fast_[2], &d_scratch_fast_[3], &d_scratch_fast_[4],
+            &d_scratch_fast_[5], &d_scratch_fast_[6], &d_scratch_fast_[7], &d_qcodes_, &d_qoff_, &d_qlen_, &d_qpad_,
             &d_prof_off_, &d_prof_, &d_matrix_, &d_score_, &d_list_a_, &d_list_b_, &d_counts_, &d_scratch_,
             &d_tb_hits_, &d_tb_regions_, &d_tb_last_, &d_tb_last_off_, &d_tb_dirs_, &d_tb_dir_off_, &d_tb_ops_,
             &d_tb_ops_off_, &d_tb_ops_len_, &d_qp_prof_, &d_qp_off_, &d_qp_rows_, &d_qp_slots_, &d_qp_units_,
@@ -526,7 +527,7 @@ private:
     DevBuf d_codes_, d_off_, d_len_, d_order_;
     DevBuf d_pair_res_, d_pair_off_, d_pair_cols_, d_pair_ids_;
     DevBuf d_prof8_, d_prof8_off_, d_rows_, d_slots_;
-    DevBuf d_scratch_fast_[4];
+    DevBuf d_scratch_fast_[8];      // per class of the single-query pass
     DevBuf d_bounds_, d_group_;
     DevBuf d_qp_prof_, d_qp_off_, d_qp_rows_, d_qp_slots_, d_qp_units_, d_qp_lmax_;
     // serving: fixed query slots and their own score rows
@@ -708,44 +709,71 @@ static bool fast_eligible( const SearchRequest & req ) {
 
 struct FastShape {
     int G, R, P;
+    int C;      // columns per step: 1 (sw_fast_kernel) or 4 (sw_fast4_kernel)
 };
 
 constexpr uint32_t FAST_MAX_ROWS = 8192;    // longer queries run the lane emulation
 constexpr uint32_t FAST_MAX_PASS_ROWS = 512; // G x R: 16 KiB profile slice per warp
 
-// Threads per group G, rows per thread R and passes P for a query of Q rows:
-// without a measured table, the smallest estimated issue cost per database
-// column, counting the wavefront fill (G - 1 steps per pass) and a per-step
-// overhead.  With a measured shape table for the database's bucket
-// (tuning.cpp) the cost of a shape is passes x its measured cost per pass and
-// column; on a small database that measurement includes the latency of the
-// longest pairs, so it favours wide groups there (a 375-row query against
-// 10,000 sequences: G = 32, R = 16, one pass).
+// Threads per group G, rows per thread R, passes P and columns per step C for
+// a query of Q rows: without a measured table, the one-column kernel with the
+// smallest estimated issue cost per database column, counting the wavefront
+// fill (G - 1 steps per pass) and a per-step overhead.  With a measured shape
+// table for the database's bucket (tuning.cpp) the cost of a shape is
+// passes x its measured cost per pass and column, over both kernels; on a
+// small database that measurement includes the latency of the longest pairs,
+// so it favours wide groups there.
 static FastShape choose_shape( uint32_t Q, double mean_len, int bucket ) {
-    FastShape best{ 0, 0, 0 };
+    FastShape best{ 0, 0, 0, 1 };
     double best_cost = 1e300;
     const int Gs[] = { 8, 16, 32 };
+    const int G4s[] = { 4, 8, 16, 32 };
     const int Rs[] = { 8, 16, 24, 32 };
     const TuningTable & tt = tuning();
-    bool measured = false;
+    bool measured = false, measured4 = false;
     for( int gi = 0; gi < 3 && tt.has_fast; gi++ )
         for( int ri = 0; ri < 4; ri++ )
             measured |= tt.fast[bucket][gi][ri] > 0;
-    for( int gi = 0; gi < 3; gi++ ) {
-        const int G = Gs[gi];
-        for( int ri = 0; ri < 4; ri++ ) {
+    for( int gi = 0; gi < 4 && tt.has_fast4; gi++ )
+        for( int ri = 0; ri < 4; ri++ )
+            measured4 |= tt.fast4[bucket][gi][ri] > 0;
+    auto fits = []( int G, int R, uint32_t Q, uint32_t * P ) {
+        const uint32_t per = (uint32_t) (G * R);
+        *P = (Q + per - 1) / per;
+        return per <= FAST_MAX_PASS_ROWS && (uint64_t) *P * per <= FAST_MAX_ROWS;
+    };
+    // the model's cost units are not the table's: with only the 4-column
+    // kernel measured, the one-column kernel is not a candidate
+    if( measured || !measured4 ) {
+        for( int gi = 0; gi < 3; gi++ ) {
+            const int G = Gs[gi];
+            for( int ri = 0; ri < 4; ri++ ) {
+                const int R = Rs[ri];
+                uint32_t P;
+                if( !fits( G, R, Q, &P ) )
+                    continue;
+                if( measured && tt.fast[bucket][gi][ri] <= 0 )
+                    continue;
+                const double cost = measured ? (double) P * tt.fast[bucket][gi][ri]
+                                             : (double) P * G * (mean_len + G - 1) * (8.0 * R + 24.0);
+                if( cost < best_cost ) {
+                    best_cost = cost;
+                    best = FastShape{ G, R, (int) P, 1 };
+                }
+            }
+        }
+    }
+    for( int gi = 0; gi < 4 && measured4; gi++ ) {
+        const int G = G4s[gi];
+        for( int ri = 0; ri < 3; ri++ ) {     // R = 8, 16, 24
             const int R = Rs[ri];
-            const uint32_t per = (uint32_t) (G * R);
-            const uint32_t P = (Q + per - 1) / per;
-            if( per > FAST_MAX_PASS_ROWS || (uint64_t) P * per > FAST_MAX_ROWS )
+            uint32_t P;
+            if( !fits( G, R, Q, &P ) || tt.fast4[bucket][gi][ri] <= 0 )
                 continue;
-            if( measured && tt.fast[bucket][gi][ri] <= 0 )
-                continue;
-            const double cost = measured ? (double) P * tt.fast[bucket][gi][ri]
-                                         : (double) P * G * (mean_len + G - 1) * (8.0 * R + 24.0);
+            const double cost = (double) P * tt.fast4[bucket][gi][ri];
             if( cost < best_cost ) {
                 best_cost = cost;
-                best = FastShape{ G, R, (int) P };
+                best = FastShape{ G, R, (int) P, 4 };
             }
         }
     }
@@ -762,27 +790,33 @@ void Engine::run_fast_entry( const SearchRequest & req, uint32_t nq, PairTask * 
     std::vector<FastShape> shape( nq );
     std::vector<uint32_t> rows_of( nq, 0 );
     std::vector<uint32_t> fallback;
-    std::vector<std::vector<uint32_t>> by_r( 4 );   // R = 8, 16, 24, 32
+    // classes: [columns per step 1 or 4][R = 8, 16, 24, 32]
+    std::vector<std::vector<uint32_t>> by_r( 8 );
     const int bucket = db_bucket( db_.mean_len, db_.order_desc.size() );
-    // SSA_B200_FAST_SHAPE=G,R pins the shape (tuning)
-    int pin_g = 0, pin_r = 0;
-    if( const char * pin = getenv( "SSA_B200_FAST_SHAPE" ) )
-        if( sscanf( pin, "%d,%d", &pin_g, &pin_r ) != 2 )
+    // SSA_B200_FAST_SHAPE=G,R[,C] pins the shape and the kernel (tuning, tests)
+    int pin_g = 0, pin_r = 0, pin_c = 1;
+    if( const char * pin = getenv( "SSA_B200_FAST_SHAPE" ) ) {
+        const int n = sscanf( pin, "%d,%d,%d", &pin_g, &pin_r, &pin_c );
+        const bool g_ok = pin_c == 4 ? (pin_g == 4 || pin_g == 8 || pin_g == 16 || pin_g == 32)
+                                     : (pin_g == 8 || pin_g == 16 || pin_g == 32);
+        const int r_max = pin_c == 4 ? 24 : 32;
+        if( n < 2 || (n == 3 && pin_c != 1 && pin_c != 4) || !g_ok || pin_r < 8 || pin_r > r_max || pin_r % 8 )
             pin_g = pin_r = 0;
+    }
     for( uint32_t s = 0; s < nq; s++ ) {
         shape[s] = choose_shape( h_qlen_[s], db_.mean_len, bucket );
         if( pin_g && shape[s].G ) {
             const uint32_t per = (uint32_t) (pin_g * pin_r);
             const uint32_t P = (h_qlen_[s] + per - 1) / per;
             if( per <= FAST_MAX_PASS_ROWS && (uint64_t) P * per <= FAST_MAX_ROWS )
-                shape[s] = FastShape{ pin_g, pin_r, (int) P };
+                shape[s] = FastShape{ pin_g, pin_r, (int) P, pin_c };
         }
         if( shape[s].G == 0 ) {
             fallback.push_back( s );
             continue;
         }
         rows_of[s] = (uint32_t) (shape[s].G * shape[s].R * shape[s].P);
-        by_r[shape[s].R / 8 - 1].push_back( s );
+        by_r[(shape[s].C == 4 ? 4 : 0) + shape[s].R / 8 - 1].push_back( s );
     }
     // profiles: one 32 x rows int8 table per slot
     std::vector<uint64_t> prof_off( nq, 0 );
@@ -859,10 +893,12 @@ void Engine::run_fast_entry( const SearchRequest & req, uint32_t nq, PairTask * 
     CUDA_CHECK( cudaEventRecord( ev_ready_, stream_ ) );
     const uint32_t cols_max = ((db_.max_len + 7u) & ~7u) + 8;
     size_t class_first = 0;
-    for( int ri = 0; ri < 4; ri++ ) {
-        const std::vector<uint32_t> & cls = by_r[ri];
+    for( int ci = 0; ci < 8; ci++ ) {
+        const std::vector<uint32_t> & cls = by_r[ci];
         if( cls.empty() )
             continue;
+        const bool four = ci >= 4;
+        const int ri = ci % 4;                 // classes of equal R share a stream
         const int R = 8 * (ri + 1);
         bool multi = false;
         uint32_t slice_rows = 0;
@@ -875,12 +911,16 @@ void Engine::run_fast_entry( const SearchRequest & req, uint32_t nq, PairTask * 
             for( uint32_t s : cls )
                 by_g[shape[s].G]++;
             for( auto & kv : by_g )
-                last_shapes_.push_back( { "sw_fast", kv.first, R, kv.second, bucket } );
+                last_shapes_.push_back( { four ? "sw_fast4" : "sw_fast", kv.first, R, kv.second, bucket } );
         }
+        auto launch = [&]( const FastParams & fp, int g, int * per ) {
+            return four ? launch_sw_fast4( R, fp, g, class_stream_[ri], per )
+                        : launch_sw_fast( R, fp, g, class_stream_[ri], per );
+        };
         FastParams p{};
         p.slice_rows = slice_rows;
         int per_sm = 0;
-        CUDA_CHECK( launch_sw_fast( R, p, 0, class_stream_[ri], &per_sm ) );
+        CUDA_CHECK( launch( p, 0, &per_sm ) );
         const int grid = sms_ * std::max( 1, per_sm );
         CUDA_CHECK( cudaStreamWaitEvent( class_stream_[ri], ev_ready_, 0 ) );
         unsigned long long * unit_counter = d_counts_.as<unsigned long long>() + 8 + ri;   // bytes 64..95
@@ -907,11 +947,12 @@ void Engine::run_fast_entry( const SearchRequest & req, uint32_t nq, PairTask * 
         p.sink.next_cap = cap;
         p.sink.error_flags = d_counts_.as<unsigned>() + 2;
         if( multi ) {
-            p.scratch = (int4 *) d_scratch_fast_[ri].ensure( (size_t) grid * (FAST_THREADS / 32) * 4 * cols_max *
-                    sizeof(int4) );
+            // a scratch row per group: 4 groups per warp (8 in the 4-column kernel)
+            p.scratch = (int4 *) d_scratch_fast_[ci].ensure( (size_t) grid * (FAST_THREADS / 32) * (four ? 8 : 4) *
+                    cols_max * sizeof(int4) );
             p.scratch_cols = cols_max;
         }
-        CUDA_CHECK( launch_sw_fast( R, p, grid, class_stream_[ri], nullptr ) );
+        CUDA_CHECK( launch( p, grid, nullptr ) );
         launches_++;
         CUDA_CHECK( cudaEventRecord( ev_class_[ri], class_stream_[ri] ) );
         CUDA_CHECK( cudaStreamWaitEvent( stream_, ev_class_[ri], 0 ) );
@@ -2677,7 +2718,7 @@ std::string tuning_report() {
     bool first = true;
     for( const auto & u : Engine::get().last_shapes_ ) {
         char buf[160];
-        const bool qp = strcmp( u.kernel, "sw_fast" ) != 0;
+        const bool qp = strncmp( u.kernel, "sw_fast", 7 ) != 0;
         snprintf( buf, sizeof buf, "%s{\"kernel\": \"%s\", \"%s\": %d, \"%s\": %d, \"%s\": %u, \"bucket\": %d}",
                 first ? "" : ", ", u.kernel, qp ? "R" : "G", u.a, qp ? "ctas_per_sm" : "R", u.b,
                 qp ? "query_pairs" : "queries", u.n, u.bucket );

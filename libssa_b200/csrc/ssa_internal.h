@@ -172,6 +172,9 @@ struct TuningTable {
     // [bucket][G = 8, 16, 32][R / 8 - 1]; 0 = not measured
     double fast[TUNE_BUCKETS][3][4] = {};
     bool has_fast = false;
+    // the same for its 4-column variant: [bucket][G = 4, 8, 16, 32][R / 8 - 1]
+    double fast4[TUNE_BUCKETS][4][4] = {};
+    bool has_fast4 = false;
 };
 
 const TuningTable & tuning();

@@ -305,6 +305,301 @@ cudaError_t launch_sw_fast( int R, const FastParams & p, int grid, cudaStream_t 
     }
 }
 
+// ---- four columns per step ------------------------------------------------
+// The same pass with one 4-column block per step: thread k of a group works
+// on block step - k and interleaves the block's four columns row by row (cell
+// (r, c + j) in row iteration r + j), so a thread carries four independent
+// dependency chains and the recurrence can take its cheaper form
+//     H = max(Hdiag + V, max(E, F, 0)),  E' / F' = max(E / F + gapE, H + gapO + gapE),
+// two ALU instructions for H (3-way max, fused add-max), one IADD shared by
+// both gap updates and two fused add-max: with the PRMT that builds the 16x2
+// profile word and half a 3-way max for the running maximum, 5.5 ALU
+// instructions and one IADD per cell pair (the one-column kernel above needs
+// 7 and 2 to keep its row-to-row chain at one instruction).  Each thread
+// records the first block in which its own running maximum reached 255; the
+// group's minimum over threads and passes is the reference lane's overflow
+// block.  A block's residues are one 8-byte load (4 columns x 2 sequences),
+// read with the streaming cache operator; the boundary row of a multi-pass
+// query (H and F of four columns, 32 bytes per block) goes through the
+// group's scratch row, thread 0 reading it one block ahead.  G (threads per
+// pair) is 4, 8, 16 or 32, so a warp holds up to 8 groups; R is 8, 16 or 24.
+constexpr uint32_t FAST_CROSS_ADD =
+        ((0x8000u - (FAST_BIAS + FAST_THRESHOLD)) << 16) | (0x8000u - (FAST_BIAS + FAST_THRESHOLD));
+
+template <int R>
+__global__ void __launch_bounds__( 128, 4 ) sw_fast4_kernel( FastParams p ) {
+    constexpr int C = 4;
+    extern __shared__ __align__( 16 ) int8_t sprof[];
+    const int lane = threadIdx.x & 31;
+    const uint32_t warp_in_cta = threadIdx.x >> 5;
+    const uint32_t warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int8_t * slice = sprof + (size_t) warp_in_cta * 32u * p.slice_rows;
+    const uint32_t GOE32 = (uint32_t) ((int32_t) p.gap_oe * 65536 + (int32_t) p.gap_oe);
+    const uint32_t GE2 = ((uint32_t) (uint16_t) (int16_t) p.gap_e << 16) | (uint16_t) (int16_t) p.gap_e;
+    uint64_t loaded_key = ~0ull;
+
+    for( ;; ) {
+        unsigned long long u = 0;
+        if( lane == 0 )
+            u = atomicAdd( p.unit_counter, 1ull );
+        u = __shfl_sync( 0xffffffffu, u, 0 );
+        if( u >= p.n_units )
+            break;
+        const uint32_t slot = p.unit_slots[u % p.n_class];
+        const uint32_t chunk = (uint32_t) (u / p.n_class);
+        const uint32_t pair_begin = p.chunk_bounds[chunk], pair_end = p.chunk_bounds[chunk + 1];
+        const int G = (int) p.slot_group[slot];
+        const uint32_t GR = (uint32_t) (G * R);
+        const uint32_t rows = p.slot_rows[slot];
+        const uint32_t passes = rows / GR;
+        const int GPW = 32 / G;
+        const int k = lane % G;
+        const int g = lane / G;
+        const int8_t * prof = p.prof8 + p.prof8_off[slot];
+        int4 * scratch = p.scratch + ((uint64_t) warp_global * 8u + (uint32_t) g) * p.scratch_cols;
+
+        for( uint32_t b0 = pair_begin; b0 < pair_end; b0 += (uint32_t) GPW ) {
+            const uint32_t pair = b0 + (uint32_t) g;
+            const bool valid = pair < pair_end;
+            const uint32_t nb = valid ? p.pair_cols[pair] >> 2 : 0u;      // 4-column blocks
+            const uint32_t max_nb = __reduce_max_sync( 0xffffffffu, nb );
+            const uint8_t * res = p.pair_res + (valid ? p.pair_off[pair] : 0ull);
+
+            uint32_t best = FAST_BIAS2;
+            int cross_lo = INT_MAX, cross_hi = INT_MAX;
+
+            for( uint32_t pass = 0; pass < passes; pass++ ) {
+                const bool last_pass = (pass + 1 == passes);
+                const uint64_t key = ((uint64_t) slot << 16) | pass;
+                if( key != loaded_key ) {
+                    __syncwarp();
+                    const uint32_t per_code = GR / 16u;
+                    const uint4 * src = reinterpret_cast<const uint4 *>( prof + (size_t) pass * GR );
+                    uint4 * dst = reinterpret_cast<uint4 *>( slice );
+                    for( uint32_t i = (uint32_t) lane; i < 32u * per_code; i += 32u ) {
+                        const uint32_t code = i / per_code, w = i % per_code;
+                        dst[i] = src[(size_t) code * (rows / 16u) + w];
+                    }
+                    loaded_key = key;
+                    __syncwarp();
+                }
+                uint32_t H[R], E[R];
+#pragma unroll
+                for( int r = 0; r < R; r++ ) {
+                    H[r] = FAST_BIAS2;
+                    E[r] = FAST_BIAS2;
+                }
+                uint32_t diag = FAST_BIAS2, smax = FAST_BIAS2, seen = 0;
+                uint32_t out_h[C], out_f[C];
+#pragma unroll
+                for( int j = 0; j < C; j++ ) {
+                    out_h[j] = FAST_BIAS2;
+                    out_f[j] = FAST_BIAS2;
+                }
+                // residues of blocks b .. b + 3 (8 bytes each: a0 b0 a1 b1 a2
+                // b2 a3 b3), one block fetched ahead every step; outside the
+                // pair the reads are clamped to its blocks (never used)
+                const uint32_t last_block = nb ? nb - 1u : 0u;
+                auto fetch = [&]( int32_t b ) -> uint2 {
+                    const uint32_t c = min( (uint32_t) max( b, 0 ), last_block );
+                    return __ldcs( reinterpret_cast<const uint2 *>( res + 8u * c ) );
+                };
+                uint2 q0 = fetch( -k ), q1 = fetch( 1 - k ), q2 = fetch( 2 - k ), q3 = fetch( 3 - k );
+                const bool reads_boundary = (k == 0) && pass > 0;
+                int4 bq0 = make_int4( 0, 0, 0, 0 ), bq1 = bq0;
+                if( reads_boundary && nb > 0 ) {
+                    bq0 = scratch[0];
+                    bq1 = scratch[1];
+                }
+                const uint32_t row0 = (uint32_t) (k * R);
+                const uint32_t steps = max_nb + (uint32_t) G - 1u;
+                for( uint32_t s = 0; s < steps; s++ ) {
+                    uint32_t up_h[C], up_f[C];
+#pragma unroll
+                    for( int j = 0; j < C; j++ ) {
+                        up_h[j] = __shfl_up_sync( 0xffffffffu, out_h[j], 1, G );
+                        up_f[j] = __shfl_up_sync( 0xffffffffu, out_f[j], 1, G );
+                    }
+                    const int32_t b = (int32_t) s - k;
+                    const uint2 w = q0;
+                    q0 = q1;
+                    q1 = q2;
+                    q2 = q3;
+                    q3 = fetch( b + 4 );
+                    const int4 bnd0 = bq0, bnd1 = bq1;
+                    if( reads_boundary ) {
+                        const uint32_t nxt = (uint32_t) b + 1u;
+                        if( nxt < nb && 2u * nxt + 1u < p.scratch_cols ) {
+                            bq0 = scratch[2u * nxt];
+                            bq1 = scratch[2u * nxt + 1u];
+                        }
+                    }
+                    if( b < 0 || (uint32_t) b >= nb )
+                        continue;
+                    if( k == 0 ) {
+                        if( pass ) {
+                            up_h[0] = (uint32_t) bnd0.x;
+                            up_f[0] = (uint32_t) bnd0.y;
+                            up_h[1] = (uint32_t) bnd0.z;
+                            up_f[1] = (uint32_t) bnd0.w;
+                            up_h[2] = (uint32_t) bnd1.x;
+                            up_f[2] = (uint32_t) bnd1.y;
+                            up_h[3] = (uint32_t) bnd1.z;
+                            up_f[3] = (uint32_t) bnd1.w;
+                        }
+                        else {
+#pragma unroll
+                            for( int j = 0; j < C; j++ ) {
+                                up_h[j] = FAST_BIAS2;
+                                up_f[j] = FAST_BIAS2;
+                            }
+                        }
+                    }
+                    // profile rows of column j's two residues
+                    const int8_t * pa_base[C];
+                    const int8_t * pb_base[C];
+#pragma unroll
+                    for( int j = 0; j < C; j++ ) {
+                        const uint32_t word = j < 2 ? w.x : w.y;
+                        const uint32_t sh = 16u * (uint32_t) (j & 1);
+                        pa_base[j] = slice + ((word >> sh) & 0xffu) * GR + row0;
+                        pb_base[j] = slice + ((word >> (sh + 8u)) & 0xffu) * GR + row0;
+                    }
+                    uint32_t pa[C], pb[C], f[C];
+                    // hv[j][r]: H of chain j (column c + j) at row r; only the
+                    // last two rows of chains 0..2 stay live
+                    uint32_t hv[C][R];
+#pragma unroll
+                    for( int j = 0; j < C; j++ )
+                        f[j] = up_f[j];
+#pragma unroll
+                    for( int it = 0; it < R + C - 1; it++ ) {
+                        uint32_t hnew[C];
+#pragma unroll
+                        for( int j = 0; j < C; j++ ) {
+                            const int r = it - j;
+                            if( r < 0 || r >= R )
+                                continue;
+                            if( (r & 3) == 0 ) {
+                                pa[j] = *reinterpret_cast<const uint32_t *>( pa_base[j] + r );
+                                pb[j] = *reinterpret_cast<const uint32_t *>( pb_base[j] + r );
+                            }
+                            const uint32_t v = prmt( pa[j], pb[j], sx_sel( r & 3 ) );
+                            uint32_t hd;
+                            if( r == 0 )
+                                hd = (j == 0) ? diag : up_h[j - 1];
+                            else
+                                hd = (j == 0) ? H[r - 1] : hv[j - 1][r - 1];
+                            const uint32_t t = __vimax3_s16x2( E[r], f[j], FAST_BIAS2 );
+                            const uint32_t h = __viaddmax_s16x2( hd, v, t );
+                            const uint32_t hg = h + GOE32;                  // no borrow: h >= bias
+                            f[j] = __viaddmax_s16x2( f[j], GE2, hg );
+                            E[r] = __viaddmax_s16x2( E[r], GE2, hg );
+                            hv[j][r] = h;
+                            hnew[j] = h;
+                        }
+                        const int j0 = it - (R - 1) > 0 ? it - (R - 1) : 0;
+                        const int j1 = it < C - 1 ? it : C - 1;
+#pragma unroll
+                        for( int j = j0; j <= j1; j += 2 ) {
+                            if( j + 1 <= j1 )
+                                smax = __vimax3_s16x2( smax, hnew[j], hnew[j + 1] );
+                            else
+                                smax = __vmaxs2( smax, hnew[j] );
+                        }
+                        // chain 3 leaves column c + 3 in H
+                        if( it - (C - 1) >= 0 && it - (C - 1) < R )
+                            H[it - (C - 1)] = hnew[C - 1];
+                    }
+                    diag = up_h[C - 1];
+#pragma unroll
+                    for( int j = 0; j < C; j++ ) {
+                        out_h[j] = hv[j][R - 1];
+                        out_f[j] = f[j];
+                    }
+                    // first block at which this thread's maximum reached 255
+                    const uint32_t ge = (smax + FAST_CROSS_ADD) & 0x80008000u;
+                    if( ge != seen ) {
+                        if( (ge & 0x8000u) && !(seen & 0x8000u) )
+                            cross_lo = min( cross_lo, b );
+                        if( (ge & 0x80000000u) && !(seen & 0x80000000u) )
+                            cross_hi = min( cross_hi, b );
+                        seen = ge;
+                    }
+                    if( k == G - 1 && !last_pass ) {
+                        if( 2u * (uint32_t) b + 1u < p.scratch_cols ) {
+                            scratch[2u * b] = make_int4( (int) out_h[0], (int) out_f[0], (int) out_h[1],
+                                    (int) out_f[1] );
+                            scratch[2u * b + 1u] = make_int4( (int) out_h[2], (int) out_f[2], (int) out_h[3],
+                                    (int) out_f[3] );
+                        }
+                        else {
+                            atomicOr( p.sink.error_flags, ERR_SCRATCH_OVERFLOW );
+                        }
+                    }
+                }
+                best = __vmaxs2( best, smax );
+                __syncwarp();
+            }
+            for( int o = 1; o < G; o <<= 1 ) {
+                best = __vmaxs2( best, __shfl_xor_sync( 0xffffffffu, best, o, G ) );
+                cross_lo = min( cross_lo, __shfl_xor_sync( 0xffffffffu, cross_lo, o, G ) );
+                cross_hi = min( cross_hi, __shfl_xor_sync( 0xffffffffu, cross_hi, o, G ) );
+            }
+            if( valid && k == 0 ) {
+                const uint2 ids = p.pair_ids[pair];
+                const uint32_t idv[2] = { ids.x, ids.y };
+                const int cross[2] = { cross_lo, cross_hi };
+                const uint32_t sv[2] = { best & 0xffffu, best >> 16 };
+#pragma unroll
+                for( int h = 0; h < 2; h++ ) {
+                    if( idv[h] == 0xffffffffu )
+                        continue;
+                    int32_t * dst = p.sink.score + (uint64_t) slot * p.sink.score_stride + idv[h];
+                    if( cross[h] == INT_MAX ) {
+                        *dst = (int32_t) (sv[h] - FAST_BIAS);
+                    }
+                    else {
+                        *dst = FAST_THRESHOLD;
+                        unsigned q = atomicAdd( p.sink.next_count, 1u );
+                        if( q < p.sink.next_cap )
+                            p.sink.next[q] = PairTask{ slot, idv[h], cross[h] + 1, 0 };
+                        else
+                            atomicOr( p.sink.error_flags, ERR_REQUEUE_OVERFLOW );
+                    }
+                }
+            }
+        }
+    }
+}
+
+template <int R>
+static cudaError_t launch_four( const FastParams & p, int grid, size_t smem, cudaStream_t st, int * blocks_per_sm ) {
+    cudaError_t e = cudaFuncSetAttribute( sw_fast4_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem );
+    if( e != cudaSuccess )
+        return e;
+    if( grid == 0 )
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor( blocks_per_sm, sw_fast4_kernel<R>, FAST_THREADS, smem );
+    sw_fast4_kernel<R><<<grid, FAST_THREADS, smem, st>>>( p );
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sw_fast4( int R, const FastParams & p, int grid, cudaStream_t st, int * blocks_per_sm ) {
+    // one profile slice per warp
+    const size_t smem = (size_t) (FAST_THREADS / 32) * 32u * p.slice_rows;
+    switch( R ) {
+    case 8:
+        return launch_four<8>( p, grid, smem, st, blocks_per_sm );
+    case 16:
+        return launch_four<16>( p, grid, smem, st, blocks_per_sm );
+    case 24:
+        return launch_four<24>( p, grid, smem, st, blocks_per_sm );
+    default:    // R = 32 would spill at 128 registers
+
+        return cudaErrorInvalidValue;
+    }
+}
+
 // prof8[slot][code][row]: the query's 8-bit scores, -128 past the query and for
 // the neutral pad code used after a sequence's last 4-column block.
 __global__ void build_profile8_kernel( const uint8_t * qcodes, const uint64_t * qoff, const uint32_t * qlen,

@@ -5,13 +5,13 @@
 // per vector (src/algo/8/search_8_util.h:25-27, src/algo/8/search_8.c:41-56).
 // The B200 entry kernels have free shape parameters instead -- rows per
 // thread R and resident CTAs per SM of the query-pair kernel, threads per
-// sequence G and rows per thread R of the single-query kernel -- whose best
-// values depend on the query length (padding to whole passes) and on the
-// database (wavefront fill per sequence, occupancy).  libssa_b200/tune.py
-// times every candidate on the device and writes the measured cost of a unit
-// of work per candidate and database bucket into a text file; the engine
-// reads it once and picks, per query, the shape with the smallest
-// passes x cost.
+// sequence G, rows per thread R and columns per step of the single-query
+// kernel -- whose best values depend on the query length (padding to whole
+// passes) and on the database (wavefront fill per sequence, occupancy).
+// libssa_b200/tune.py times every candidate on the device and writes the
+// measured cost of a unit of work per candidate and database bucket into a
+// text file; the engine reads it once and picks, per query, the shape with
+// the smallest passes x cost.
 //
 // File format (one entry per line, '#' starts a comment):
 //   version <n>
@@ -21,6 +21,7 @@
 //   qpair4h <bucket> <R> <MB> <ps ...>      (4 columns, running maximum in fp16x2)
 //   qpair4g8 <bucket> 24 <MB> <ps ...>      (4 columns, 96-row passes as 8 threads of 12 rows)
 //   fast <bucket> <G> <R> <ps per pass and database column>
+//   fast4 <bucket> <G> <R> <ps ...>          (the single-query kernel with 4 columns per step)
 // Buckets: db_bucket() below.  Missing entries fall back to the built-in
 // costs (measured the same way on a B200 before the tuner existed).
 #include "ssa_internal.h"
@@ -118,6 +119,16 @@ void load( TuningTable & t ) {
                 const int gi = G == 8 ? 0 : G == 16 ? 1 : 2;
                 t.fast[b][gi][R / 8 - 1] = ps;
                 t.has_fast = true;
+            }
+        }
+        else if( !strcmp( key, "fast4" ) ) {
+            int b, G, R;
+            double ps;
+            if( sscanf( line, "%*s %d %d %d %lf", &b, &G, &R, &ps ) == 4 && b >= 0 && b < TUNE_BUCKETS &&
+                    (G == 4 || G == 8 || G == 16 || G == 32) && R >= 8 && R <= 24 && R % 8 == 0 && ps > 0 ) {
+                const int gi = G == 4 ? 0 : G == 8 ? 1 : G == 16 ? 2 : 3;
+                t.fast4[b][gi][R / 8 - 1] = ps;
+                t.has_fast4 = true;
             }
         }
     }

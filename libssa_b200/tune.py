@@ -14,9 +14,11 @@ script times every candidate, per database bucket, on seeded synthetic data:
   4-column kernel with 8 threads of 12 rows per sequence, on 64 queries of
   exactly two passes (2 x 4R rows); cost = entry-pass device time per
   (query pair x pass x database column);
-* the single-query kernel (sw_align): threads per sequence G in {8, 16, 32}
-  x rows per thread R in {8, 16, 24, 32}, on one query of two passes
-  (2 x G x R rows); cost = entry-pass device time per (pass x database column).
+* the single-query kernels (sw_align): with one column per step, threads
+  per sequence pair G in {8, 16, 32} x rows per thread R in {8, 16, 24, 32};
+  with one 4-column block per step, G in {4, 8, 16, 32} x R in {8, 16, 24};
+  G x R <= 512, on one query of two passes (2 x G x R rows); cost =
+  entry-pass device time per (pass x database column).
 
 Database buckets (the engine's db_bucket): mean sequence length below 250,
 below 1,000 or longer, times fewer or more than 50,000 sequences; each gets a
@@ -47,6 +49,9 @@ QPAIR_R = (16, 20, 24, 28)
 QPAIR_VARIANTS = ((4, 2, 0, 0), (5, 2, 0, 0), (4, 4, 0, 0), (5, 4, 0, 0), (4, 4, 1, 0), (4, 4, 0, 1), (5, 4, 0, 1))
 FAST_G = (8, 16, 32)
 FAST_R = (8, 16, 24, 32)
+FAST4_G = (4, 8, 16, 32)
+FAST4_R = (8, 16, 24)
+KINDS = ("qpair", "fast")
 
 
 def bucket_db(length_b: int, size_b: int, seed: int) -> tuple[np.ndarray, np.ndarray]:
@@ -78,7 +83,20 @@ def _entry_seconds(L, fn, reps: int) -> float:
     return best
 
 
-def tune(reps: int = 3, log=print) -> list[str]:
+def _fast_candidates():
+    for G in FAST_G:
+        for R in FAST_R:
+            if G * R <= 512:
+                yield "fast", G, R, 1
+    for G in FAST4_G:
+        for R in FAST4_R:
+            if G * R <= 512:
+                yield "fast4", G, R, 4
+
+
+def tune(reps: int = 3, log=print, kinds=KINDS) -> list[str]:
+    """Times the candidates of the kernels in `kinds` ("qpair": the batched
+    query-pair kernel; "fast": the single-query kernels) on every bucket."""
     import libssa_b200 as L
     L.load()
     _setup(L)
@@ -92,7 +110,7 @@ def tune(reps: int = 3, log=print) -> list[str]:
             cols = int(np.sum((np.diff(offsets).astype(np.int64) + 3) // 4 * 4))
             t0 = time.time()
             # query-pair kernel: 32 pairs of queries of exactly two passes
-            for R in QPAIR_R:
+            for R in (QPAIR_R if "qpair" in kinds else ()):
                 rows = 2 * 4 * R
                 qs = [L.init_sequence_fasta(L.READ_FROM_STRING,
                                             W.random_residues(rng, rows, W.AA20).tobytes().decode())
@@ -117,21 +135,18 @@ def tune(reps: int = 3, log=print) -> list[str]:
                     lines.append(f"{kind} {bucket} {R} {mb} {ps:.4f}")
                 for q in qs:
                     L.free_sequence(q)
-            # single-query kernel: one query of exactly two passes
-            for G in FAST_G:
-                for R in FAST_R:
-                    if G * R > 512:
-                        continue
-                    q = L.init_sequence_fasta(L.READ_FROM_STRING,
-                                              W.random_residues(rng, 2 * G * R, W.AA20).tobytes().decode())
-                    os.environ["SSA_B200_FAST_SHAPE"] = f"{G},{R}"
-                    try:
-                        t = _entry_seconds(L, lambda: L.sw_align(q, 10, L.BIT_WIDTH_8, L.COMPUTE_SCORE), reps)
-                    finally:
-                        del os.environ["SSA_B200_FAST_SHAPE"]
-                    L.free_sequence(q)
-                    ps = t / (2 * cols) * 1e12
-                    lines.append(f"fast {bucket} {G} {R} {ps:.4f}")
+            # single-query kernels: one query of exactly two passes
+            for kind, G, R, C in (_fast_candidates() if "fast" in kinds else ()):
+                q = L.init_sequence_fasta(L.READ_FROM_STRING,
+                                          W.random_residues(rng, 2 * G * R, W.AA20).tobytes().decode())
+                os.environ["SSA_B200_FAST_SHAPE"] = f"{G},{R},{C}"
+                try:
+                    t = _entry_seconds(L, lambda: L.sw_align(q, 10, L.BIT_WIDTH_8, L.COMPUTE_SCORE), reps)
+                finally:
+                    del os.environ["SSA_B200_FAST_SHAPE"]
+                L.free_sequence(q)
+                ps = t / (2 * cols) * 1e12
+                lines.append(f"{kind} {bucket} {G} {R} {ps:.4f}")
             log(f"bucket {bucket}: {COUNTS[size_b]} sequences, mean length {LENGTHS[length_b][0]:.0f}, "
                 f"{time.time() - t0:.1f} s")
     return lines
@@ -156,6 +171,7 @@ def write(lines: list[str], path: str, version: int) -> None:
         f.write("# qpair4h <bucket> <R> <CTAs per SM> <ps ...>  (4 columns, running maximum in fp16x2)\n")
         f.write("# qpair4g8 <bucket> 24 <CTAs per SM> <ps ...>  (4 columns, 8 threads of 12 rows per sequence)\n")
         f.write("# fast <bucket> <G> <R> <ps per pass and database column>\n")
+        f.write("# fast4 <bucket> <G> <R> <ps ...>  (4 columns per step)\n")
         f.write("# bucket = length bucket (mean <250, <1000, longer) + 3 x size bucket (<50,000 sequences, more)\n")
         f.write(f"version {version}\n")
         f.write(f"device {device_name()}\n")
@@ -163,14 +179,35 @@ def write(lines: list[str], path: str, version: int) -> None:
             f.write(ln + "\n")
 
 
+def kept_entries(path: str, kinds) -> list[str]:
+    """The entries of an existing table that a run measuring only `kinds`
+    keeps: every cost line of the other kernels ("qpair*" lines belong to
+    "qpair", "fast*" lines to "fast")."""
+    if not os.path.exists(path):
+        return []
+    kept = []
+    with open(path) as f:
+        for ln in f:
+            ln = ln.split("#", 1)[0].strip()
+            if not ln or ln.split()[0] in ("version", "device"):
+                continue
+            if not ln.split()[0].startswith(tuple(kinds)):
+                kept.append(ln)
+    return kept
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=DEFAULT_OUT)
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--version", type=int, default=int(time.strftime("%Y%m%d")))
+    ap.add_argument("--kernels", default="all", choices=["all", *KINDS],
+                    help="measure only these kernels and keep the other entries of the existing table")
     args = ap.parse_args()
+    kinds = KINDS if args.kernels == "all" else (args.kernels,)
+    kept = kept_entries(args.out, kinds) if args.kernels != "all" else []
     os.environ["SSA_B200_TUNING"] = "builtin"     # measure with nothing pinned by an older table
-    lines = tune(args.reps)
+    lines = kept + tune(args.reps, kinds=kinds)
     write(lines, args.out, args.version)
     print(f"wrote {args.out} ({len(lines)} entries)")
 

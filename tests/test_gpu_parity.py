@@ -248,6 +248,35 @@ def test_batched_kernel_variants_against_oracle(built_library, monkeypatch, shap
         assert batched[qi] == exp, (shape, seed, qi, len(q))
 
 
+FAST_SHAPES = [(G, R, 4) for G in (4, 8, 16, 32) for R in (8, 16, 24) if G * R <= 512] + \
+              [(8, 32, 1), (16, 16, 1), (32, 8, 1), (16, 32, 1)]
+
+
+@pytest.mark.parametrize("shape", FAST_SHAPES, ids=lambda s: f"G{s[0]}_R{s[1]}_cols{s[2]}")
+@pytest.mark.parametrize("seed", range(2))
+def test_single_query_kernel_variants_against_oracle(built_library, monkeypatch, shape, seed):
+    """Every shape of the single-query (sw_align) entry kernels the shape table
+    can select -- threads per sequence pair G, rows per thread R, one or four
+    columns per step -- pinned, on queries of one to several passes against
+    databases with overflowing copies and empty records, against the oracle
+    (scores, overflow blocks through the tie order and the counters, CIGARs)."""
+    G, R, cols = shape
+    monkeypatch.setenv("SSA_B200_FAST_SHAPE", f"{G},{R},{cols}")
+    c = _batch_case(300 + seed)
+    qs = c["queries"][:3]
+    product_setup(1, c["matrix"], c["gap"], c["chunk"], c["simd"], records=c["records"])
+    import libssa_b200 as L
+    for q in qs:
+        res, ovf = product_search("sw", 8, 1, c["hits"], [q])
+        used = [u for u in L.tuning_report()["last_call"] if u["kernel"].startswith("sw_fast")]
+        assert used and all(u["kernel"] == ("sw_fast4" if cols == 4 else "sw_fast") and u["G"] == G and
+                            u["R"] == R for u in used), used
+        exp, eovf = oracle_search("sw", 8, 1, c["hits"], 1, c["matrix"], c["gap"], c["chunk"], c["simd"], q,
+                                  c["records"])
+        assert res[0] == exp, (shape, seed, len(q))
+        assert tuple(ovf[0]) == tuple(eovf), (shape, seed, len(q))
+
+
 def _nw_batch_case(seed):
     rng = np.random.default_rng(2000 + seed)
     nuc = seed % 2 == 0

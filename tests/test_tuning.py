@@ -57,5 +57,22 @@ def test_committed_table_is_the_default(built_library):
         # the 8-threads-per-sequence variant exists for the 96-row class only
         qp = {(int(x[1]), int(x[2]), int(x[3])) for x in lines if x[0] == "qpair4g8"}
         assert not qp or qp == {(b, 24, mb) for b in range(6) for mb in (4, 5)}
+        # every bucket has a cost for every shape of both single-query kernels
+        fast = {(int(x[1]), int(x[2]), int(x[3])) for x in lines if x[0] == "fast"}
+        assert fast == {(b, G, R) for b in range(6) for G in (8, 16, 32) for R in (8, 16, 24, 32) if G * R <= 512}
+        fast4 = {(int(x[1]), int(x[2]), int(x[3])) for x in lines if x[0] == "fast4"}
+        assert fast4 == {(b, G, R) for b in range(6) for G in (4, 8, 16, 32) for R in (8, 16, 24) if G * R <= 512}
     else:
         assert r["source"] == "built-in"
+
+
+def test_partial_run_keeps_the_other_kernels(tmp_path):
+    """python -m libssa_b200.tune --kernels fast re-measures the single-query
+    kernels only; the query-pair entries of the existing table are kept."""
+    from libssa_b200.tune import kept_entries
+    path = tmp_path / "t.tune"
+    path.write_text("# c\nversion 3\ndevice X\nqpair 0 16 4 33.5\nqpair4h 1 20 4 26.7  # note\n"
+                    "fast 0 8 8 122.2\nfast4 2 4 16 80.0\n")
+    assert kept_entries(str(path), ("fast",)) == ["qpair 0 16 4 33.5", "qpair4h 1 20 4 26.7"]
+    assert kept_entries(str(path), ("qpair",)) == ["fast 0 8 8 122.2", "fast4 2 4 16 80.0"]
+    assert kept_entries(str(tmp_path / "absent.tune"), ("fast",)) == []
