@@ -921,6 +921,9 @@ void Engine::run_fast_entry( const SearchRequest & req, uint32_t nq, PairTask * 
         p.slice_rows = slice_rows;
         int per_sm = 0;
         CUDA_CHECK( launch( p, 0, &per_sm ) );
+        // SSA_B200_FAST_CTAS=n caps the resident CTAs per SM (tuning)
+        if( const char * cap_env = getenv( "SSA_B200_FAST_CTAS" ) )
+            per_sm = std::min( per_sm, std::max( 1, atoi( cap_env ) ) );
         const int grid = sms_ * std::max( 1, per_sm );
         CUDA_CHECK( cudaStreamWaitEvent( class_stream_[ri], ev_ready_, 0 ) );
         unsigned long long * unit_counter = d_counts_.as<unsigned long long>() + 8 + ri;   // bytes 64..95

@@ -836,46 +836,88 @@ __global__ void __launch_bounds__( 256 ) tb_fwddir_kernel( TbParams p ) {
 }
 
 // ---------------------------------------------------------------------------
-// 4. Walk (reference: src/algo/cigar.c:300-334): one thread per hit writes the
+// 4. Walk (reference: src/algo/cigar.c:300-334): one warp per hit writes the
 //    moves in traceback order (end to begin); the host run-length encodes.
+//    Each step reads the direction word of the current cell, which the
+//    previous step chose, so a walk that reads HBM or L2 word by word waits a
+//    memory round trip per move.  In 32 moves the path stays within 32 rows
+//    and 32 columns of its current cell (every move leaves the row or the
+//    column or both by one), so the warp loads that window (32 columns, at
+//    most 5 words of 8 rows each) into shared memory with one load round,
+//    lane 0 walks up to 32 moves from it, and the warp loads the next window.
 // ---------------------------------------------------------------------------
-__global__ void tb_walk_kernel( TbParams p ) {
-    const uint32_t h = blockIdx.x * blockDim.x + threadIdx.x;
+constexpr int TB_WALK_WARPS = 4;                 // hits per CTA
+constexpr int TB_WALK_WORDS = 32 / TB_R + 1;     // direction words a 32-row window spans
+
+__global__ void __launch_bounds__( 32 * TB_WALK_WARPS ) tb_walk_kernel( TbParams p ) {
+    __shared__ uint16_t win[TB_WALK_WARPS][32][TB_WALK_WORDS];
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    const uint32_t h = blockIdx.x * TB_WALK_WARPS + (uint32_t) wib;
     if( h >= p.n_hits )
-        return;
+        return;                                  // the whole warp
     const TbRegion rg = p.regions[h];
     if( rg.status != 0 ) {
-        p.ops_len[h] = 0;
+        if( lane == 0 )
+            p.ops_len[h] = 0;
         return;
     }
     const uint32_t words = (uint32_t) rg.dir_words;
     const uint16_t * dir = p.dirs + p.dir_off[h];
     char * out = p.ops + p.ops_off[h];
     const uint64_t cap = p.ops_off[h + 1] - p.ops_off[h];
+    const int64_t a_begin = rg.a_begin, b_begin = rg.b_begin;
+    const int64_t j_lo = max( b_begin, (int64_t) rg.dir_col0 );   // columns held in the layout
     int64_t i = rg.a_end, j = rg.b_end;
     uint64_t n = 0;
-    while( i >= rg.a_begin && j >= rg.b_begin && i >= 0 && j >= 0 ) {
-        const uint32_t word = dir[(uint64_t) (j - rg.dir_col0) * words + (uint64_t) (i / TB_R)];
-        const uint32_t op = (word >> (2 * (i % TB_R))) & 3u;
-        char ch;
-        if( op == 2u ) {
-            j--;
-            ch = 'I';
+    while( i >= a_begin && j >= b_begin && i >= 0 && j >= 0 ) {
+        // the window: columns j - 31 .. j, words of rows max(i - 31, 0) .. i
+        const int64_t w0 = max( i - 31, (int64_t) 0 ) / TB_R;
+        const int64_t jc = j - lane;
+#pragma unroll
+        for( int k = 0; k < TB_WALK_WORDS; k++ ) {
+            const int64_t w = w0 + k;
+            uint16_t v = 0;
+            if( jc >= j_lo && w <= i / TB_R && w < (int64_t) words )
+                v = dir[(uint64_t) (jc - rg.dir_col0) * words + (uint64_t) w];
+            win[wib][lane][k] = v;
         }
-        else if( op == 1u ) {
-            i--;
-            ch = 'D';
+        __syncwarp();
+        if( lane == 0 ) {
+            const int64_t j0 = j;
+            for( int m = 0; m < 32 && i >= a_begin && j >= b_begin && i >= 0 && j >= 0; m++ ) {
+                const uint32_t word = win[wib][j0 - j][i / TB_R - w0];
+                const uint32_t op = (word >> (2 * (i % TB_R))) & 3u;
+                char ch;
+                if( op == 2u ) {
+                    j--;
+                    ch = 'I';
+                }
+                else if( op == 1u ) {
+                    i--;
+                    ch = 'D';
+                }
+                else {
+                    i--;
+                    j--;
+                    ch = 'M';
+                }
+                if( n < cap )
+                    out[n] = ch;
+                n++;
+            }
         }
-        else {
-            i--;
-            j--;
-            ch = 'M';
-        }
-        if( n < cap )
-            out[n] = ch;
-        n++;
+        i = __shfl_sync( 0xffffffffu, i, 0 );
+        j = __shfl_sync( 0xffffffffu, j, 0 );
+        n = __shfl_sync( 0xffffffffu, n, 0 );
+        __syncwarp();
     }
-    p.ops_len[h] = (uint32_t) n;
+    if( lane == 0 )
+        p.ops_len[h] = (uint32_t) n;
+}
+
+static void launch_walk( const TbParams & p, cudaStream_t st ) {
+    tb_walk_kernel<<<(p.n_hits + TB_WALK_WARPS - 1) / TB_WALK_WARPS, 32 * TB_WALK_WARPS, 0, st>>>( p );
 }
 
 // Region phase (Smith-Waterman hits only): forward and reverse passes.  They
@@ -935,7 +977,7 @@ cudaError_t launch_tb_fused( const TbParams & p, int group, int grid, cudaStream
                 cudaEventRecord( ev[1], st );
             tb_reverse_kernel<1><<<grid, 256, 0, st>>>( p );
         }
-        tb_walk_kernel<<<(p.n_hits + 127) / 128, 128, 0, st>>>( p );
+        launch_walk( p, st );
     }
     else if( ev ) {
         cudaEventRecord( ev[1], st );
@@ -960,7 +1002,7 @@ cudaError_t launch_tb_paths( const TbParams & p, int group, int grid, cudaStream
             tb_directions_kernel<1><<<grid, 256, 0, st>>>( p );
         if( ev )
             cudaEventRecord( ev[1], st );
-        tb_walk_kernel<<<(p.n_hits + 127) / 128, 128, 0, st>>>( p );
+        launch_walk( p, st );
     }
     else if( ev ) {
         cudaEventRecord( ev[1], st );
