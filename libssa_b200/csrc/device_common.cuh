@@ -232,6 +232,8 @@ cudaError_t launch_sw_qpair( int R, int mb, const QPairParams & p, int grid, cud
 cudaError_t launch_sw_qpair4( int R, int mb, bool hmax, bool g8, const QPairParams & p, int grid, cudaStream_t st,
         int * blocks_per_sm );
 cudaError_t launch_nw_qpair( int R, const QPairParams & p, int grid, cudaStream_t st, int * blocks_per_sm );
+// the same pass with one 4-column block per step (four dependency chains per thread)
+cudaError_t launch_nw_qpair4( int R, const QPairParams & p, int grid, cudaStream_t st, int * blocks_per_sm );
 // width 8: (int8) scores, -128 past a query (Smith-Waterman 8-bit entry);
 // width 16: (int16) scores, 0 past a query (Needleman-Wunsch 16-bit entry)
 cudaError_t launch_build_profile_qp( const uint8_t * qcodes, const uint64_t * qoff, const uint32_t * qlen,

@@ -1209,19 +1209,23 @@ void Engine::run_qpair_entry( const SearchRequest & req, uint32_t nq, PairTask *
         if( cls.empty() )
             continue;
         const int R = 4 * (ri + 4);
-        const QpVariant var = nw ? QpVariant{ 4, 2, false, false, 0 } : qpair_variant( bucket, R, pinned_mb, pinned_c,
-                pinned_h, pinned_g8 );
+        // Needleman-Wunsch: 4 columns per step unless SSA_B200_QP_C=2 pins the
+        // 2-column kernel (4 resident CTAs per SM either way)
+        const QpVariant var = nw ? QpVariant{ 4, pinned_c == 2 ? 2 : 4, false, false, 0 }
+                                 : qpair_variant( bucket, R, pinned_mb, pinned_c, pinned_h, pinned_g8 );
         const int mb = var.mb;
         auto launch = [&]( const QPairParams & pp, int grid, int * per ) {
             if( nw )
-                return launch_nw_qpair( R, pp, grid, class_stream_[ri], per );
+                return var.cols == 4 ? launch_nw_qpair4( R, pp, grid, class_stream_[ri], per )
+                                     : launch_nw_qpair( R, pp, grid, class_stream_[ri], per );
             return var.cols == 4 ? launch_sw_qpair4( R, mb, var.hmax, var.g8, pp, grid, class_stream_[ri], per )
                                  : launch_sw_qpair( R, mb, pp, grid, class_stream_[ri], per );
         };
         bool multi = false;
         for( uint32_t i : cls )
             multi |= qp_rows[i] > (uint32_t) (QP_G * R);
-        last_shapes_.push_back( { nw ? "nw_qpair" : var.hmax ? "sw_qpair4h" : var.g8 ? "sw_qpair4g8"
+        last_shapes_.push_back( { nw ? (var.cols == 4 ? "nw_qpair4" : "nw_qpair") : var.hmax ? "sw_qpair4h"
+                : var.g8 ? "sw_qpair4g8"
                 : var.cols == 4 ? "sw_qpair4" : "sw_qpair", R, mb,
                 (uint32_t) cls.size(), bucket } );
         QPairParams p{};

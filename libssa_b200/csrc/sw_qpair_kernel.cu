@@ -913,6 +913,304 @@ cudaError_t launch_nw_qpair( int R, const QPairParams & p, int grid, cudaStream_
     }
 }
 
+// ---------------------------------------------------------------------------
+// Needleman-Wunsch, 16-bit entry, one 4-column block per step.  Arithmetic,
+// boundaries, exact range and redo list are those of nw_qpair_kernel; the
+// block layout is that of sw_qpair4_kernel: chain j of a thread computes
+// column 4b + j, the four chains run skewed by one row (iteration it holds
+// cell (it - j, 4b + j) of every chain), a 4-byte load brings a block's
+// residues, and a pass boundary carries H and F of the four columns in two
+// int4.  A query's score is H at its last row in the sequence's last column
+// L - 1, i.e. block (L - 1) / 4, chain (L - 1) % 4.
+// ---------------------------------------------------------------------------
+
+// One block of R rows and four columns.  up_h[j]: H of the row above this
+// thread's first row in column 4b + j; f[j]: F entering the first row (on
+// return: F leaving the last row); out_h[j]: H of the last row.  CAPTURE:
+// record chain jl's H at rows ra and rb (a query's last row, relative to
+// the thread's first row) in cap_a / cap_b.
+template <int R, bool CAPTURE>
+__device__ __forceinline__ void nw4_block( uint32_t (&H)[R], uint32_t (&E)[R], const uint32_t * const (&pc)[4],
+        uint32_t diag, const uint32_t (&up_h)[4], uint32_t (&f)[4], uint32_t (&out_h)[4], uint32_t GOE32,
+        uint32_t GE2, int jl, int ra, int rb, uint32_t & cap_a, uint32_t & cap_b ) {
+    constexpr int C = 4;
+    uint4 x[C];
+    // hv[j][r]: H of chain j at row r; only the last two rows of chains 0..2
+    // stay live
+    uint32_t hv[C][R];
+#pragma unroll
+    for( int it = 0; it < R + C - 1; it++ ) {
+#pragma unroll
+        for( int j = 0; j < C; j++ ) {
+            const int r = it - j;
+            if( r < 0 || r >= R )
+                continue;
+            if( (r & 3) == 0 )
+                x[j] = *reinterpret_cast<const uint4 *>( pc[j] + r );
+            const uint32_t v = (r & 3) == 0 ? x[j].x : (r & 3) == 1 ? x[j].y : (r & 3) == 2 ? x[j].z : x[j].w;
+            uint32_t hd;
+            if( r == 0 )
+                hd = (j == 0) ? diag : up_h[j - 1];
+            else
+                hd = (j == 0) ? H[r - 1] : hv[j - 1][r - 1];
+            const uint32_t h = __viaddmax_u16x2( hd, v, __vmaxu2( E[r], f[j] ) );
+            const uint32_t hg = h + GOE32;
+            f[j] = __viaddmax_u16x2( f[j], GE2, hg );
+            E[r] = __viaddmax_u16x2( E[r], GE2, hg );
+            hv[j][r] = h;
+            if constexpr( CAPTURE ) {
+                if( j == jl && r == ra )
+                    cap_a = h;
+                if( j == jl && r == rb )
+                    cap_b = h;
+            }
+            // chain 3 leaves column 4b + 3 in H (chain 0 of this block has
+            // read H[r] at iteration r + 1 < r + 3)
+            if( j == C - 1 )
+                H[r] = h;
+        }
+    }
+#pragma unroll
+    for( int j = 0; j < C; j++ )
+        out_h[j] = hv[j][R - 1];
+}
+
+template <int R>
+__global__ void __launch_bounds__( QP_THREADS, 4 ) nw_qpair4_kernel( QPairParams p ) {
+    constexpr int G = QP_G;
+    constexpr int C = 4;
+    constexpr uint32_t GR = (uint32_t) (G * R);
+    extern __shared__ __align__( 16 ) uint32_t qsm[];
+    const int lane = threadIdx.x & 31;
+    const uint32_t warp_in_cta = threadIdx.x >> 5;
+    const uint32_t warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    uint32_t * slice = qsm + warp_in_cta * (QP_CODES * GR);
+    const int k = lane & (G - 1);
+    const int g = lane / G;
+    const int gO = p.gap_open, gE = p.gap_e;
+    const uint32_t GOE32 = (uint32_t) ((int32_t) p.gap_oe * 65536 + (int32_t) p.gap_oe);
+    const uint32_t GE2 = ((uint32_t) (uint16_t) (int16_t) gE << 16) | (uint16_t) (int16_t) gE;
+    int4 * scratch = p.scratch + ((uint64_t) warp_global * QP_GPW + (uint32_t) g) * p.scratch_cols;
+    uint64_t loaded_key = ~0ull;
+    auto left_h = [&]( int32_t i ) { return gO + (i + 1) * gE; };           // H(i, -1)
+    auto left_e = [&]( int32_t i ) { return 2 * gO + (i + 2) * gE; };       // E entering column 0
+    auto top_h = [&]( int32_t j ) { return j < 0 ? 0 : gO + (j + 1) * gE; };   // H(-1, j)
+    auto top_f = [&]( int32_t c ) { return 2 * gO + (c + 2) * gE; };        // F entering row 0
+
+    for( ;; ) {
+        unsigned long long u = 0;
+        if( lane == 0 )
+            u = atomicAdd( p.unit_counter, 1ull );
+        u = __shfl_sync( 0xffffffffu, u, 0 );
+        if( u >= p.n_units )
+            break;
+        const uint32_t qp = p.unit_pairs[u / p.n_chunks];
+        const uint32_t chunk = (uint32_t) (u % p.n_chunks);
+        const uint32_t seq_begin = p.chunk_bounds[chunk], seq_end = p.chunk_bounds[chunk + 1];
+        const uint32_t rows = p.qp_rows[qp];
+        const uint32_t passes = rows / GR;
+        const uint32_t * prof = p.prof + p.prof_off[qp];
+        const uint32_t slot_a = p.qp_slots[2 * qp], slot_b = p.qp_slots[2 * qp + 1];
+        const int32_t qa_last = (int32_t) p.qlen[slot_a] - 1;
+        const int32_t qb_last = (slot_b == 0xffffffffu) ? -1 : (int32_t) p.qlen[slot_b] - 1;
+        const uint32_t lmax = p.qp_lmax[qp];
+
+        for( uint32_t b0 = seq_begin; b0 < seq_end; b0 += (uint32_t) QP_GPW ) {
+            const uint32_t idx = b0 + (uint32_t) g;
+            const bool valid = idx < seq_end;
+            const uint32_t id = valid ? p.order[idx] : 0u;
+            const uint32_t L = valid ? p.db.lens[id] : 0u;
+            const bool exact = valid && L <= lmax;
+            if( valid && !exact && k == 0 ) {
+                // beyond the guarded range: the lane emulation scores it
+                const uint32_t slots[2] = { slot_a, slot_b };
+                for( int h = 0; h < 2; h++ ) {
+                    if( slots[h] == 0xffffffffu )
+                        continue;
+                    const unsigned q = atomicAdd( p.redo_count, 1u );
+                    if( q < p.redo_cap )
+                        p.redo[q] = PairTask{ slots[h], id, 0, 0 };
+                    else
+                        atomicOr( p.sink.error_flags, ERR_REQUEUE_OVERFLOW );
+                }
+            }
+            const uint32_t nb = exact ? (L + 3u) >> 2 : 0u;         // 4-column blocks
+            const uint32_t max_nb = __reduce_max_sync( 0xffffffffu, nb );
+            if( max_nb == 0 )
+                continue;
+            const uint8_t * res = p.db.codes + (valid ? p.db.offsets[id] : 0ull);
+            const int32_t last_col = (int32_t) L - 1;
+            const int32_t cap_blk = last_col >> 2;
+            const int jl = last_col & 3;
+            uint32_t cap_a = 0, cap_b = 0;
+
+            for( uint32_t pass = 0; pass < passes; pass++ ) {
+                const bool last_pass = (pass + 1 == passes);
+                const uint64_t key = ((uint64_t) qp << 24) | pass;
+                if( key != loaded_key ) {
+                    __syncwarp();
+                    constexpr uint32_t per_code = GR / 4u;
+                    const uint4 * src = reinterpret_cast<const uint4 *>( prof + (size_t) pass * GR );
+                    uint4 * dst = reinterpret_cast<uint4 *>( slice );
+                    for( uint32_t i = (uint32_t) lane; i < QP_CODES * per_code; i += 32u ) {
+                        const uint32_t code = i / per_code, w = i % per_code;
+                        dst[i] = src[(size_t) code * (rows / 4u) + w];
+                    }
+                    loaded_key = key;
+                    __syncwarp();
+                }
+                const int32_t row0 = (int32_t) (pass * GR) + k * R;
+                const int ra = qa_last - row0, rb = qb_last - row0;
+                // does this thread hold a query's last row in this pass?
+                const bool holds_last = (ra >= 0 && ra < R) || (rb >= 0 && rb < R);
+                uint32_t H[R], E[R];
+#pragma unroll
+                for( int r = 0; r < R; r++ ) {
+                    H[r] = nw_pack( left_h( row0 + r ) );
+                    E[r] = nw_pack( left_e( row0 + r ) );
+                }
+                uint32_t diag = nw_pack( row0 == 0 ? 0 : left_h( row0 - 1 ) );
+                uint32_t out_h[C], out_f[C];
+#pragma unroll
+                for( int j = 0; j < C; j++ ) {
+                    out_h[j] = 0;
+                    out_f[j] = 0;
+                }
+                // residues of blocks b .. b + 3, one block fetched ahead every
+                // step; past the last block the reads stay inside the padded
+                // record or the next one (never used)
+                const uint32_t fetch_limit = nb + 3u;
+                auto fetch = [&]( int32_t b ) -> uint32_t {
+                    const uint32_t c = min( (uint32_t) max( b, 0 ), fetch_limit );
+                    return __ldcs( reinterpret_cast<const unsigned int *>( res + 4u * c ) );
+                };
+                uint32_t q0 = fetch( -k ), q1 = fetch( 1 - k ), q2 = fetch( 2 - k ), q3 = fetch( 3 - k );
+                // thread 0: the previous pass's bottom row, one block ahead
+                const bool reads_boundary = (k == 0) && pass > 0;
+                int4 bq0 = make_int4( 0, 0, 0, 0 ), bq1 = bq0;
+                if( reads_boundary && nb > 0 ) {
+                    bq0 = scratch[0];
+                    bq1 = scratch[1];
+                }
+                const uint32_t steps = max_nb + (uint32_t) G - 1u;
+                for( uint32_t s = 0; s < steps; s++ ) {
+                    uint32_t up_h[C], up_f[C];
+#pragma unroll
+                    for( int j = 0; j < C; j++ ) {
+                        up_h[j] = __shfl_up_sync( 0xffffffffu, out_h[j], 1, G );
+                        up_f[j] = __shfl_up_sync( 0xffffffffu, out_f[j], 1, G );
+                    }
+                    const int32_t b = (int32_t) s - k;
+                    const uint32_t w = q0;
+                    q0 = q1;
+                    q1 = q2;
+                    q2 = q3;
+                    q3 = fetch( b + 4 );
+                    const int4 bnd0 = bq0, bnd1 = bq1;
+                    if( reads_boundary ) {
+                        const uint32_t nxt = (uint32_t) b + 1u;
+                        if( nxt < nb && 2u * nxt + 1u < p.scratch_cols ) {
+                            bq0 = scratch[2u * nxt];
+                            bq1 = scratch[2u * nxt + 1u];
+                        }
+                    }
+                    if( b < 0 || (uint32_t) b >= nb )
+                        continue;
+                    if( k == 0 ) {
+                        if( pass ) {
+                            up_h[0] = (uint32_t) bnd0.x;
+                            up_f[0] = (uint32_t) bnd0.y;
+                            up_h[1] = (uint32_t) bnd0.z;
+                            up_f[1] = (uint32_t) bnd0.w;
+                            up_h[2] = (uint32_t) bnd1.x;
+                            up_f[2] = (uint32_t) bnd1.y;
+                            up_h[3] = (uint32_t) bnd1.z;
+                            up_f[3] = (uint32_t) bnd1.w;
+                        }
+                        else {
+                            const int32_t c = 4 * b;
+#pragma unroll
+                            for( int j = 0; j < C; j++ ) {
+                                up_h[j] = nw_pack( top_h( c + j ) );
+                                up_f[j] = nw_pack( top_f( c + j ) );
+                            }
+                        }
+                    }
+                    const uint32_t * pc[C];
+#pragma unroll
+                    for( int j = 0; j < C; j++ )
+                        pc[j] = slice + ((w >> (8 * j)) & 0xffu) * GR + (uint32_t) (k * R);
+                    uint32_t f[C];
+#pragma unroll
+                    for( int j = 0; j < C; j++ )
+                        f[j] = up_f[j];
+                    if( holds_last && b == cap_blk )
+                        nw4_block<R, true>( H, E, pc, diag, up_h, f, out_h, GOE32, GE2, jl, ra, rb, cap_a, cap_b );
+                    else
+                        nw4_block<R, false>( H, E, pc, diag, up_h, f, out_h, GOE32, GE2, jl, ra, rb, cap_a, cap_b );
+                    diag = up_h[C - 1];
+#pragma unroll
+                    for( int j = 0; j < C; j++ )
+                        out_f[j] = f[j];
+                    if( k == G - 1 && !last_pass ) {
+                        if( 2u * (uint32_t) b + 1u < p.scratch_cols ) {
+                            scratch[2u * b] = make_int4( (int) out_h[0], (int) out_f[0], (int) out_h[1],
+                                    (int) out_f[1] );
+                            scratch[2u * b + 1u] = make_int4( (int) out_h[2], (int) out_f[2], (int) out_h[3],
+                                    (int) out_f[3] );
+                        }
+                        else {
+                            atomicOr( p.sink.error_flags, ERR_SCRATCH_OVERFLOW );
+                        }
+                    }
+                }
+                __syncwarp();
+            }
+            // the threads holding the last rows report (values are > 0 with the bias)
+#pragma unroll
+            for( int o = 1; o < G; o <<= 1 ) {
+                cap_a = max( cap_a, __shfl_xor_sync( 0xffffffffu, cap_a, o, G ) );
+                cap_b = max( cap_b, __shfl_xor_sync( 0xffffffffu, cap_b, o, G ) );
+            }
+            if( exact && k == 0 ) {
+                p.sink.score[(uint64_t) slot_a * p.sink.score_stride + id] =
+                        (int32_t) (cap_a & 0xffffu) - (int32_t) NWQ_BIAS;
+                if( slot_b != 0xffffffffu )
+                    p.sink.score[(uint64_t) slot_b * p.sink.score_stride + id] =
+                            (int32_t) (cap_b >> 16) - (int32_t) NWQ_BIAS;
+            }
+        }
+    }
+}
+
+template <int R>
+static cudaError_t launch_nw4_one( const QPairParams & p, int grid, cudaStream_t st, int * blocks_per_sm ) {
+    const size_t smem = (size_t) (QP_THREADS / 32) * QP_CODES * QP_G * R * sizeof(uint32_t);
+    cudaError_t e = cudaFuncSetAttribute( nw_qpair4_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            (int) smem );
+    if( e != cudaSuccess )
+        return e;
+    if( grid == 0 )
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor( blocks_per_sm, nw_qpair4_kernel<R>, QP_THREADS, smem );
+    nw_qpair4_kernel<R><<<grid, QP_THREADS, smem, st>>>( p );
+    return cudaGetLastError();
+}
+
+cudaError_t launch_nw_qpair4( int R, const QPairParams & p, int grid, cudaStream_t st, int * blocks_per_sm ) {
+    switch( R ) {
+    case 16:
+        return launch_nw4_one<16>( p, grid, st, blocks_per_sm );
+    case 20:
+        return launch_nw4_one<20>( p, grid, st, blocks_per_sm );
+    case 24:
+        return launch_nw4_one<24>( p, grid, st, blocks_per_sm );
+    case 28:
+        return launch_nw4_one<28>( p, grid, st, blocks_per_sm );
+    default:
+        return cudaErrorInvalidValue;
+    }
+}
+
 // prof[qp][code][row] = (A's score, B's score) as a 16x2 word at the entry
 // width; rows past a query, and the absent query of an odd batch, score -128
 // (8-bit Smith-Waterman: never raises a maximum) or 0 (16-bit

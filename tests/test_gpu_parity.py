@@ -319,14 +319,21 @@ def test_nw16_redo_list_grows(built_library, monkeypatch, seed):
         assert batched[qi] == exp, (seed, qi, len(q))
 
 
+@pytest.mark.parametrize("cols", [4, 2], ids=lambda c: f"cols{c}")
 @pytest.mark.parametrize("seed", range(8))
-def test_nw16_batched_against_oracle(built_library, seed):
+def test_nw16_batched_against_oracle(built_library, monkeypatch, seed, cols):
     """Needleman-Wunsch at the 16-bit entry through the query-pair kernel
-    (single queries and batches), including sequences beyond its exact range
-    that go to the lane emulation, against the oracle query by query."""
+    (single queries and batches; one 4-column block per step, the default, or
+    two columns per step, pinned), including multi-pass queries and sequences
+    beyond its exact range that go to the lane emulation, against the oracle
+    query by query."""
+    monkeypatch.setenv("SSA_B200_QP_C", str(cols))
     c = _nw_batch_case(seed)
     product_setup(c["symtype"], c["matrix"], c["gap"], c["chunk"], c["simd"], records=c["records"])
     batched, _ = product_search("nw", 16, 1, c["hits"], c["queries"], batch=True)
+    import libssa_b200 as L
+    used = [u for u in L.tuning_report()["last_call"] if u["kernel"].startswith("nw_qpair")]
+    assert used and all(u["kernel"] == ("nw_qpair4" if cols == 4 else "nw_qpair") for u in used), used
     single, ovf = product_search("nw", 16, 1, c["hits"], c["queries"][:1])
     for qi, q in enumerate(c["queries"]):
         exp, eovf = oracle_search("nw", 16, 1, c["hits"], c["symtype"], c["matrix"], c["gap"], c["chunk"], c["simd"],
