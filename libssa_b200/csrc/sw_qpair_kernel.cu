@@ -975,6 +975,38 @@ __device__ __forceinline__ void nw4_block( uint32_t (&H)[R], uint32_t (&E)[R], c
         out_h[j] = hv[j][R - 1];
 }
 
+// Pass-boundary staging of nw_qpair4_kernel: thread 0 of a group copies the
+// boundary row of block b + NW4_AHEAD into a ring of NW4_SLOTS shared-memory
+// slots (two int4 each) with cp.async while it computes block b, instead of
+// holding the prefetched row in registers.  One commit group per block (empty
+// past the last block), so waiting until at most NW4_AHEAD - 1 groups are in
+// flight leaves block b's copy complete.  The slot written at step b is the
+// one read at step b - 1, whose values that step has already consumed.
+constexpr int NW4_AHEAD = 2;
+constexpr int NW4_SLOTS = NW4_AHEAD + 1;
+
+__device__ __forceinline__ void cp_async16( void * smem, const void * gmem ) {
+    const uint32_t s = (uint32_t) __cvta_generic_to_shared( smem );
+    asm volatile( "cp.async.cg.shared.global [%0], [%1], 16;" ::"r"( s ), "l"( gmem ) : "memory" );
+}
+
+__device__ __forceinline__ void cp_async_commit() {
+    asm volatile( "cp.async.commit_group;" ::: "memory" );
+}
+
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile( "cp.async.wait_group %0;" ::"n"( N ) : "memory" );
+}
+
+// shared memory of nw_qpair4_kernel: the warps' profile slices, then the
+// groups' boundary rings
+template <int R>
+constexpr size_t nw4_smem_bytes() {
+    return (size_t) (QP_THREADS / 32) * QP_CODES * QP_G * R * sizeof(uint32_t) +
+            (size_t) (QP_THREADS / QP_G) * NW4_SLOTS * 2 * sizeof(int4);
+}
+
 template <int R>
 __global__ void __launch_bounds__( QP_THREADS, 4 ) nw_qpair4_kernel( QPairParams p ) {
     constexpr int G = QP_G;
@@ -991,6 +1023,9 @@ __global__ void __launch_bounds__( QP_THREADS, 4 ) nw_qpair4_kernel( QPairParams
     const uint32_t GOE32 = (uint32_t) ((int32_t) p.gap_oe * 65536 + (int32_t) p.gap_oe);
     const uint32_t GE2 = ((uint32_t) (uint16_t) (int16_t) gE << 16) | (uint16_t) (int16_t) gE;
     int4 * scratch = p.scratch + ((uint64_t) warp_global * QP_GPW + (uint32_t) g) * p.scratch_cols;
+    // this group's boundary ring, after all warps' profile slices
+    int4 * ring = reinterpret_cast<int4 *>( qsm + (QP_THREADS / 32) * (QP_CODES * GR) ) +
+            (size_t) (threadIdx.x / G) * (NW4_SLOTS * 2);
     uint64_t loaded_key = ~0ull;
     auto left_h = [&]( int32_t i ) { return gO + (i + 1) * gE; };           // H(i, -1)
     auto left_e = [&]( int32_t i ) { return 2 * gO + (i + 2) * gE; };       // E entering column 0
@@ -1076,21 +1111,28 @@ __global__ void __launch_bounds__( QP_THREADS, 4 ) nw_qpair4_kernel( QPairParams
                     out_h[j] = 0;
                     out_f[j] = 0;
                 }
-                // residues of blocks b .. b + 3, one block fetched ahead every
-                // step; past the last block the reads stay inside the padded
-                // record or the next one (never used)
+                // residues of blocks b and b + 1, one block fetched two steps
+                // ahead (a step takes thousands of cycles); past the last block
+                // the reads stay inside the padded record or the next one
+                // (never used)
                 const uint32_t fetch_limit = nb + 3u;
                 auto fetch = [&]( int32_t b ) -> uint32_t {
                     const uint32_t c = min( (uint32_t) max( b, 0 ), fetch_limit );
                     return __ldcs( reinterpret_cast<const unsigned int *>( res + 4u * c ) );
                 };
-                uint32_t q0 = fetch( -k ), q1 = fetch( 1 - k ), q2 = fetch( 2 - k ), q3 = fetch( 3 - k );
-                // thread 0: the previous pass's bottom row, one block ahead
+                uint32_t q0 = fetch( -k ), q1 = fetch( 1 - k );
+                // thread 0: the previous pass's bottom row, NW4_AHEAD blocks
+                // ahead through the ring
                 const bool reads_boundary = (k == 0) && pass > 0;
-                int4 bq0 = make_int4( 0, 0, 0, 0 ), bq1 = bq0;
-                if( reads_boundary && nb > 0 ) {
-                    bq0 = scratch[0];
-                    bq1 = scratch[1];
+                if( reads_boundary ) {
+#pragma unroll
+                    for( int x = 0; x < NW4_AHEAD; x++ ) {
+                        if( (uint32_t) x < nb && 2u * (uint32_t) x + 1u < p.scratch_cols ) {
+                            cp_async16( ring + 2 * x, scratch + 2 * x );
+                            cp_async16( ring + 2 * x + 1, scratch + 2 * x + 1 );
+                        }
+                        cp_async_commit();
+                    }
                 }
                 const uint32_t steps = max_nb + (uint32_t) G - 1u;
                 for( uint32_t s = 0; s < steps; s++ ) {
@@ -1103,21 +1145,23 @@ __global__ void __launch_bounds__( QP_THREADS, 4 ) nw_qpair4_kernel( QPairParams
                     const int32_t b = (int32_t) s - k;
                     const uint32_t w = q0;
                     q0 = q1;
-                    q1 = q2;
-                    q2 = q3;
-                    q3 = fetch( b + 4 );
-                    const int4 bnd0 = bq0, bnd1 = bq1;
-                    if( reads_boundary ) {
-                        const uint32_t nxt = (uint32_t) b + 1u;
-                        if( nxt < nb && 2u * nxt + 1u < p.scratch_cols ) {
-                            bq0 = scratch[2u * nxt];
-                            bq1 = scratch[2u * nxt + 1u];
-                        }
-                    }
+                    q1 = fetch( b + 2 );
                     if( b < 0 || (uint32_t) b >= nb )
                         continue;
                     if( k == 0 ) {
                         if( pass ) {
+                            // block b's copy is complete once at most
+                            // NW4_AHEAD - 1 later groups are in flight
+                            cp_async_wait<NW4_AHEAD - 1>();
+                            const uint32_t slot = (uint32_t) b % (uint32_t) NW4_SLOTS;
+                            const int4 bnd0 = ring[2 * slot], bnd1 = ring[2 * slot + 1];
+                            const uint32_t nxt = (uint32_t) b + (uint32_t) NW4_AHEAD;
+                            if( nxt < nb && 2u * nxt + 1u < p.scratch_cols ) {
+                                const uint32_t ns = nxt % (uint32_t) NW4_SLOTS;
+                                cp_async16( ring + 2 * ns, scratch + 2u * nxt );
+                                cp_async16( ring + 2 * ns + 1, scratch + 2u * nxt + 1u );
+                            }
+                            cp_async_commit();
                             up_h[0] = (uint32_t) bnd0.x;
                             up_f[0] = (uint32_t) bnd0.y;
                             up_h[1] = (uint32_t) bnd0.z;
@@ -1164,6 +1208,10 @@ __global__ void __launch_bounds__( QP_THREADS, 4 ) nw_qpair4_kernel( QPairParams
                         }
                     }
                 }
+                // every copy issued was for a block this pass computed and
+                // waited for; drain the (empty) groups before the ring's reuse
+                if( reads_boundary )
+                    cp_async_wait<0>();
                 __syncwarp();
             }
             // the threads holding the last rows report (values are > 0 with the bias)
@@ -1185,7 +1233,7 @@ __global__ void __launch_bounds__( QP_THREADS, 4 ) nw_qpair4_kernel( QPairParams
 
 template <int R>
 static cudaError_t launch_nw4_one( const QPairParams & p, int grid, cudaStream_t st, int * blocks_per_sm ) {
-    const size_t smem = (size_t) (QP_THREADS / 32) * QP_CODES * QP_G * R * sizeof(uint32_t);
+    const size_t smem = nw4_smem_bytes<R>();
     cudaError_t e = cudaFuncSetAttribute( nw_qpair4_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
             (int) smem );
     if( e != cudaSuccess )
